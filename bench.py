@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark: cell-updates/s of the finite-volume step on one B200 per rank.
+
+Workload (N=1): 3D Euler on a hierarchical Cartesian tree, base 64^3 on the
+unit cube refined +2 levels inside the sphere r = 0.25 at the centre
+(1,448,336 leaf cells), seeded perturbed 3D Riemann problem, zero-gradient
+outflow on all faces, AUSM flux, RK2 -- see hom3_b200/workloads.py.  One
+"step" is one full time step of the solver (Solver::solve: boundary
+conditions, dt, both RK stages) over all leaf cells.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+    python bench.py --impl reference ...   # CPU restatement of hom3, all host threads
+
+N > 1 runs independent replicas of the workload, one per GPU (the single grid
+is not domain-decomposed): weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 1024 * 1024
+FALLBACK_HBM_GBS = 6650.0
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        busy = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(busy), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def allreduce_max(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_workload(args):
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200 import workloads as W
+
+    spec = W.riemann3d_spec(args.base_level, args.extra_levels)
+    t = hb.build_tables(spec, spec.cube_boundaries())
+    fg = t["first_ghost"]
+    modes = W.fourier_modes()
+    q = np.zeros((5, t["ncells"]))
+    q[:, :fg] = hb.cell_average(W.riemann3d_ic(modes), t["x_center"][:, :fg], t["length"][:fg], 3)
+    prec = F.MIXED if args.precision == "mixed" else F.FP64
+    s = hb.Solver(3, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, prec, cfl=args.cfl, time_end=1e30)
+    s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg, W.riemann3d_conditions(),
+               t["subface_cells"])
+    return s, t, q, modes
+
+
+def cpu_oracle_run(args, steps_budget_s=15.0, max_steps=None):
+    """The CPU restatement of hom3 (oracle/) on the same workload, OpenMP over
+    all host threads; returns (cell-updates/s, cells, steps, threads, seconds)."""
+    from oracle import h3o
+    from hom3_b200 import workloads as W
+
+    threads = os.cpu_count() or 1
+    h3o.set_num_threads(threads)
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=args.base_level)
+    w.refine_sphere([0.5, 0.5, 0.5], 0.25, args.base_level + args.extra_levels)
+    bcs = [h3o.bc(h3o.BC_EULER_NEUMANN, g) for g in w.cube_boundaries()]
+    s = w.add_solver(h3o.EULER, h3o.AUSM, h3o.RK2, bcs=bcs, ic_kind=h3o.IC_RIEMANN3D_PERTURBED,
+                     ic=W.riemann3d_oracle_ic(W.fourier_modes()), time_end=1e30, cfl=args.cfl)
+    s.initialize()
+    s.solve(1)  # warm-up step
+    t0 = time.perf_counter()
+    s.solve(1)
+    one = time.perf_counter() - t0
+    n = max(1, min(int(steps_budget_s / max(one, 1e-6)), 50))
+    if max_steps is not None:
+        n = max(1, min(n, max_steps))
+    t0 = time.perf_counter()
+    s.solve(n)
+    el = time.perf_counter() - t0
+    return s.first_ghost * n / el, s.first_ghost, n, threads, el
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    w_cfg = workload_config(args, None)
+    ups, cells, n, threads, el = cpu_oracle_run(args, steps_budget_s=20.0, max_steps=max(args.steps, 1))
+    line = {
+        "impl": "reference", "metric": "cell-updates/s", "value": ups, "unit": "cell-updates/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": w_cfg,
+        "cpu_baseline": {"value": ups, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"{n} full RK2 steps of the same {cells}-cell grid (after 2 warm-up steps); "
+                                   "hom3 itself is uncompilable here (Eigen/Boost/MPI absent), so the "
+                                   "reference is the oracle's C++ restatement of hom3, OpenMP"},
+        "e2e": {"value": ups, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, t):
+    cfg = {"workload": "3D Euler hierarchical tree: 64^3 base on [0,1]^3 +2 levels in sphere r=0.25, "
+                       "perturbed 3D Riemann (16 Fourier modes, seed 0), outflow BCs, AUSM, RK2"
+                       if (args.base_level, args.extra_levels) == (6, 2) else
+                       f"3D Euler hierarchical tree: base level {args.base_level} +{args.extra_levels} levels",
+           "time_integration": "rk2", "flux": "ausm", "precision": args.precision, "cfl": args.cfl,
+           "parallelism": f"replicas x{args.gpus}"}
+    if t is not None:
+        fg = t["first_ghost"]
+        cfg["leaf_cells"] = int(fg)
+        cfg["ghost_cells"] = int(t["ncells"] - fg)
+        cfg["subface_groups"] = int(0 if t["subface_cells"] is None else t["subface_cells"].shape[1])
+    return cfg
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--base-level", type=int, default=6)
+    ap.add_argument("--extra-levels", type=int, default=2)
+    ap.add_argument("--cfl", type=float, default=0.4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    s, t, q0, _ = build_workload(args)
+    fg, n = t["first_ghost"], t["ncells"]
+    stream = torch.cuda.ExternalStream(s.stream())
+    state_bytes = 5 * n * 8
+    # ---- device-resident timing ('value') ----
+    s.set_state(q0, 0)
+    s.reset_time()
+    s.solve(args.warmup)
+    torch.cuda.synchronize()
+    barrier(ws)
+    l0 = s.launches()
+    s.profile(True)
+    with ClockSampler(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        barrier(ws)
+        ev0.record(stream)
+        s.solve(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+    s.profile(False)
+    launches = s.launches() - l0
+    kern = s.profile_read()
+    barrier(ws)
+    ms_max = allreduce_max(ms, ws)
+    status = s.status()
+    value = fg * args.steps * ws / (ms_max * 1e-3)
+    # ---- end-to-end through the C ABI with host buffers ('e2e') ----
+    pinned = torch.empty((5, n), dtype=torch.float64, pin_memory=True).numpy()
+    pinned[:] = q0
+    out = torch.empty((5, n), dtype=torch.float64, pin_memory=True).numpy()
+    torch.cuda.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    s.set_state(pinned, 0)          # H2D of the initial state
+    s.reset_time()
+    for _ in range(args.steps):     # hom3's run loop: solve, then read dt (utilities.hpp:103-110)
+        s.solve(1)
+        dt = s.dt()
+        if not (1e-300 <= dt <= 1e300):
+            raise RuntimeError("solution diverged")
+    s.state(0, out=out)             # D2H of the final state
+    e2e_s = time.perf_counter() - t0
+    e2e_s = allreduce_max(e2e_s, ws)
+    e2e = fg * args.steps * ws / e2e_s
+    # ---- roofline of the dominant kernel (second RK stage) ----
+    peak, peak_kind = peaks()
+    st2_ms, st2_n = kern.get("stage2", (0.0, 0))
+    st1_ms, st1_n = kern.get("stage1", (0.0, 0))
+    bytes_st2 = fg * (3 * 5 * 8 + 6 * 4 + 1)      # read lhs, rhs; write lhs; int32 neighbours; level byte
+    bytes_st1 = fg * (2 * 5 * 8 + 6 * 4 + 1)
+    st2_avg = st2_ms / max(st2_n, 1)
+    achieved = bytes_st2 / (st2_avg * 1e-3) / 1e9 if st2_n else None
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "stage2_traffic.json")
+    if os.path.exists(tp):
+        try:
+            d = json.load(open(tp))
+            traffic = d["dram_bytes_per_leaf_cell"] * fg
+        except Exception:
+            traffic = None
+    step_bytes = bytes_st1 + bytes_st2
+    line = {
+        "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-state",
+        "data": "synthetic", "config": workload_config(args, t),
+        "roofline": {"bound": "hbm", "kernel": "k_stage (second RK stage)", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "peak_source": peak_kind, "algorithmic_bytes_per_launch": bytes_st2,
+                     "avg_launch_ms": st2_avg,
+                     "step_frac": (step_bytes * args.steps / ((st1_ms + st2_ms) * 1e-3) / 1e9 / peak)
+                     if st1_n and st2_n else None},
+        "kernels_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in kern.items()},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "e2e": {"value": e2e, "unit": "cell-updates/s",
+                "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": 8 + state_bytes / args.steps,
+                "what": "C-ABI run loop with host buffers: h3c_set_state (pinned host) + K x (h3c_solve(1) + "
+                        "h3c_dt read-back) + h3c_get_state"},
+        "working_set_mb": round((2 * state_bytes + 6 * 4 * n + n) / 2 ** 20, 1),
+        "l2": "no flush: the working set (both states + tables) exceeds the 126 MB L2",
+        "device_status": status,
+    }
+    if ws == 1 and rank == 0 and not args.no_cpu_baseline:
+        ups, cells, nst, threads, el = cpu_oracle_run(args)
+        line["cpu_baseline"] = {"value": ups, "unit": "cell-updates/s", "cores": threads, "kind": "port",
+                                "sample": f"{nst} RK2 steps of the same {cells}-cell workload, {el:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,719 @@
+// fv_kernels.cuh -- sm_100a kernels of the finite-volume step.
+//
+// One thread per cell.  Cells are stored in Morton order (interior cells
+// [0, n_int), ghosts after them), state as SoA FP64 columns q[v * ld + c].
+// The arithmetic follows hom3's physics plugins operation by operation
+// (citations per function, paths relative to hom3's src/), so the FP64 path
+// reproduces hom3's per-step results to rounding (FMA contraction is the only
+// difference).  R is the arithmetic type of the face flux: double for the
+// drop-in path, float for the mixed path (state, residual accumulation, update
+// and dt stay FP64).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace h3c {
+
+constexpr int kBlock = 256;
+constexpr int kMaxLevels = 32;
+constexpr int kMaxBcs = 64;
+
+enum Physics { EULER = 0, CNS = 1, HEAT = 2 };
+enum Flux { AUSM = 0, LLF = 1 };
+enum BcKind {
+  BC_EULER_NEUMANN = 0, BC_EULER_DIRICHLET = 1, BC_EULER_VORTEX = 2, BC_CNS_INFLOW = 3,
+  BC_CNS_OUTFLOW = 4, BC_CNS_ADIABATIC_NOSLIP = 5, BC_CNS_ADIABATIC_SLIP = 6,
+  BC_CNS_ISOTHERMAL_NOSLIP = 7, BC_HEAT_DIRICHLET = 8, BC_HEAT_NEUMANN = 9,
+  BC_CPL_EULER_EULER = 10, BC_CPL_CNS_HEAT = 11, BC_CPL_HEAT_CNS = 12, BC_CPL_HEAT_HEAT = 13,
+  BC_PERIODIC = 14
+};
+
+// Device-resident step scalars (solver.hpp:406-416) and reduction slots.
+struct Scalars {
+  double dt, time, tEnd, forced_dt;
+  long long step, forced_step;
+  long long dtmin_ord;  // min of cell dt for the next set_dt (ordered bits)
+  long long mindt_ord;  // min of cell dt for h3c_min_dt
+  int status;           // bit0: dt outside [1e-300, 1e300] or non-finite
+  int pad;
+};
+
+// Physical constants of one solver (euler/quantities.hpp, cns/quantities.hpp)
+struct PhysConst {
+  double gamma, gm1, cfl, cflv, Re0, Pr0, sOverTref, sOverTrefP1;
+};
+
+struct BcParam {
+  int kind;
+  int wall;          // tangential velocity slopes flip sign (cns walls)
+  double v[8];
+  double partner_gamma;
+  int partner_physics;
+  int partner_nd;
+};
+
+// The partner state a coupling / periodic condition reads at launch time.
+struct PartnerView {
+  const double* q;  // partner lhs (coupling); unused for periodic (own target state)
+  long long ld;
+};
+
+struct Geometry {
+  const int* __restrict__ nbr;            // [2nd][ld] (>=0 cell, -1 none, <=-2 sub-face group)
+  const unsigned char* __restrict__ lvl;  // [ld] index into len[]
+  const int* __restrict__ sub;            // [2^(nd-1)][nsub]
+  long long nsub;
+  long long n_int, n_tot, ld;
+  double len[kMaxLevels];
+};
+
+struct GhostTables {
+  const int* __restrict__ bndry;          // [ng] boundary cell of each ghost
+  const unsigned char* __restrict__ pos;  // [ng] position of the ghost w.r.t. its boundary cell
+  const unsigned char* __restrict__ bc_apply;  // [ng] bc applied by apply_bcs (255: none)
+  const unsigned char* __restrict__ bc_own;    // [ng] the ghost's own bc index
+  const double* __restrict__ dx;          // [ng] |x_b - x_g| (cell_dx, solver.hpp:590-592)
+  const int* __restrict__ partner;        // [ng] partner cell (internal numbering) or -1
+  const double* __restrict__ xc;          // [nd][ld] cell centres (vortex bc)
+  long long ng;
+  const BcParam* bcs;                     // [n_bcs] device array
+};
+
+// ---------------------------------------------------------------------------
+// ordered-bits min for doubles (NaN never wins, as std::min(dt, NaN) in hom3)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ long long dbl_to_ord(double x) {
+  long long i = __double_as_longlong(x);
+  return i >= 0 ? i : (i ^ 0x7fffffffffffffffLL);
+}
+__host__ __device__ inline double ord_to_dbl(long long o) {
+  long long i = o >= 0 ? o : (o ^ 0x7fffffffffffffffLL);
+#ifdef __CUDA_ARCH__
+  return __longlong_as_double(i);
+#else
+  double d;
+  memcpy(&d, &i, 8);
+  return d;
+#endif
+}
+constexpr long long kOrdMax = 0x7fefffffffffffffLL;  // bits of DBL_MAX
+
+__device__ __forceinline__ void block_min_atomic(long long v, long long* dst) {
+  __shared__ long long red[kBlock / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    long long w = __shfl_down_sync(0xffffffffu, v, o);
+    v = w < v ? w : v;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? red[lane] : kOrdMax;
+    for (int o = 16; o > 0; o >>= 1) {
+      long long w = __shfl_down_sync(0xffffffffu, v, o);
+      v = w < v ? w : v;
+    }
+    if (lane == 0 && v < kOrdMax) atomicMin(dst, v);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// primitive variables: euler/physics.hpp:83-125
+// ---------------------------------------------------------------------------
+template <class R, int ND> struct Prim {
+  R q[ND + 2];
+  R u[ND];
+  R p, a;
+};
+
+template <class R, int ND>
+__device__ __forceinline__ void make_prim(Prim<R, ND>& P, R gamma, R gm1) {
+  const R rho = P.q[ND];
+  R um2 = R(0);
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    P.u[d] = P.q[d] / rho;
+    um2 = d == 0 ? P.u[d] * P.u[d] : um2 + P.u[d] * P.u[d];
+  }
+  P.p = gm1 * (P.q[ND + 1] - R(0.5) * rho * um2);
+  P.a = sqrt(gamma * P.p / rho);
+}
+
+template <class R, int ND>
+__device__ __forceinline__ void load_prim(Prim<R, ND>& P, const double* __restrict__ q, long long ld,
+                                          int c, R gamma, R gm1) {
+#pragma unroll
+  for (int v = 0; v < ND + 2; ++v) P.q[v] = (R)__ldg(q + v * ld + c);
+  make_prim<R, ND>(P, gamma, gm1);
+}
+
+// m_int_, p_int_: euler/physics.hpp:297-310
+template <class R> __device__ __forceinline__ R m_int(R s, R M) {
+  return fabs(M) > R(1) ? R(0.5) * (M + s * fabs(M)) : (s * R(0.25)) * ((M + s) * (M + s));
+}
+template <class R> __device__ __forceinline__ R p_int(R s, R M) {
+  return fabs(M) > R(1) ? R(0.5) * (M + s * fabs(M)) / M : (R(0.25) * ((M + s) * (M + s))) * (R(2) - s * M);
+}
+
+// AUSM (Liou-Steffen): euler/physics.hpp:276-293, theta_ :315-325
+template <class R, int ND>
+__device__ __forceinline__ void ausm(const Prim<R, ND>& L, const Prim<R, ND>& Rt, int d, R* f) {
+  const R ML = L.u[d] / L.a;
+  const R MR = Rt.u[d] / Rt.a;
+  const R mi = m_int<R>(R(1), ML) + m_int<R>(R(-1), MR);
+  const R pi = p_int<R>(R(1), ML) * L.p + p_int<R>(R(-1), MR) * Rt.p;
+  const bool left = mi >= R(0);
+  const R a = left ? L.a : Rt.a;
+#pragma unroll
+  for (int v = 0; v < ND + 1; ++v) f[v] = ((left ? L.q[v] : Rt.q[v]) * a) * mi;
+  f[ND + 1] = (((left ? L.q[ND + 1] + L.p : Rt.q[ND + 1] + Rt.p)) * a) * mi;
+#pragma unroll
+  for (int v = 0; v < ND; ++v)
+    if (v == d) f[v] = f[v] + pi;
+}
+
+// Euler flux: euler/physics.hpp:98-113; LLF: :262-267
+template <class R, int ND>
+__device__ __forceinline__ void llf(const Prim<R, ND>& L, const Prim<R, ND>& Rt, int d, R dx_dt, R* f) {
+  R fl[ND + 2], fr[ND + 2];
+  fl[ND] = L.q[d];
+  fr[ND] = Rt.q[d];
+#pragma unroll
+  for (int i = 0; i < ND; ++i) {
+    fl[i] = L.q[i] * L.u[d];
+    fr[i] = Rt.q[i] * Rt.u[d];
+  }
+#pragma unroll
+  for (int i = 0; i < ND; ++i)
+    if (i == d) { fl[i] = fl[i] + L.p; fr[i] = fr[i] + Rt.p; }
+  fl[ND + 1] = L.u[d] * (L.q[ND + 1] + L.p);
+  fr[ND + 1] = Rt.u[d] * (Rt.q[ND + 1] + Rt.p);
+#pragma unroll
+  for (int v = 0; v < ND + 2; ++v) f[v] = R(0.5) * ((fl[v] + fr[v]) + dx_dt * (L.q[v] - Rt.q[v]));
+}
+
+// Sutherland's law: cns/quantities.hpp:467-469
+template <class R> __device__ __forceinline__ R sutherland(R T, R sOverTref, R sOverTrefP1) {
+  return (T * sqrt(T)) * sOverTrefP1 / (T + sOverTref);
+}
+
+// Three-point viscous flux: cns/physics.hpp:305-338 with the surface helpers
+// :221-293 and surface_slope (solver.hpp:656-678).  sl/sr: cell slopes
+// [sd][v] of the left / right cell.
+template <class R, int ND>
+__device__ __forceinline__ void viscous(const Prim<R, ND>& L, const Prim<R, ND>& Rt, const R* sl,
+                                        const R* sr, int d, R len_r, const PhysConst& pc, R* f) {
+  constexpr int NV = ND + 2;
+  const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+  const R rho_s = R(0.5) * (L.q[ND] + Rt.q[ND]);
+  R rho_u_s[ND], u_s[ND];
+  R umag2 = R(0);
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    rho_u_s[k] = R(0.5) * (L.q[k] + Rt.q[k]);
+    u_s[k] = rho_u_s[k] / rho_s;
+    umag2 = k == 0 ? u_s[k] * u_s[k] : umag2 + u_s[k] * u_s[k];
+  }
+  const R rho_E_s = R(0.5) * (L.q[ND + 1] + Rt.q[ND + 1]);
+  const R p_s = gm1 * (rho_E_s - R(0.5) * rho_s * umag2);
+  auto gs = [&](int v, int sd) -> R {
+    return sd == d ? (Rt.q[v] - L.q[v]) / len_r : R(0.5) * (sr[sd * NV + v] + sl[sd * NV + v]);
+  };
+  const R rs2 = rho_s * rho_s;
+  R gu[ND][ND];  // gu[c][sd] = d u_c / d x_sd at the surface
+#pragma unroll
+  for (int c = 0; c < ND; ++c)
+#pragma unroll
+    for (int sd = 0; sd < ND; ++sd) gu[c][sd] = (gs(c, sd) * rho_s - gs(ND, sd) * rho_u_s[c]) / rs2;
+  const R p_avg = R(0.5) * (L.p + Rt.p);
+  const R mu_s = sutherland<R>(gamma * p_avg / rho_s, (R)pc.sOverTref, (R)pc.sOverTrefP1);
+  R grad_rho_umag2 = gs(ND, d) * umag2;
+#pragma unroll
+  for (int k = 0; k < ND; ++k) grad_rho_umag2 = grad_rho_umag2 + rho_s * R(2) * u_s[k] * gu[k][d];
+  const R gradP = gm1 * (gs(ND + 1, d) - R(0.5) * grad_rho_umag2);
+  const R gradRho = gs(ND, d);
+  const R qf = -mu_s * gamma / (gm1 * (R)pc.Pr0 * rho_s) * (gradP - p_s / rho_s * gradRho);
+  // nabla_u(i, j) = gu[j][i]; trace = sum gu[i][i]
+  R tr = gu[0][0];
+#pragma unroll
+  for (int i = 1; i < ND; ++i) tr = tr + gu[i][i];
+  const R div_u = tr * R(2) / R(3);
+  const R invRe = R(1) / (R)pc.Re0;
+  R Eacc = R(0);
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    // nabla_u(k, d) + nabla_u(d, k) = gu[d][k] + gu[k][d]
+    R t = gu[d][k] + gu[k][d];
+    if (k == d) t = t - div_u;
+    const R tkd = -mu_s * t;
+    f[k] = invRe * tkd;
+    Eacc = k == 0 ? u_s[k] * tkd : Eacc + u_s[k] * tkd;
+  }
+  f[ND] = R(0);
+  f[ND + 1] = invRe * (Eacc + qf);
+}
+
+// ---------------------------------------------------------------------------
+// per-cell time step: euler/physics.hpp:182-196, cns/physics.hpp:167-187,
+// heat/physics.hpp:82-85
+// ---------------------------------------------------------------------------
+template <int ND, int PHYS>
+__device__ __forceinline__ double cell_dt(const double* q, double h, const PhysConst& pc) {
+  if (PHYS == HEAT) return pc.cfl * 0.5 * (h * h);
+  Prim<double, ND> P;
+#pragma unroll
+  for (int v = 0; v < ND + 2; ++v) P.q[v] = q[v];
+  make_prim<double, ND>(P, pc.gamma, pc.gm1);
+  double S = -1.7976931348623157e308;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const double cand = fabs(P.u[d]) + P.a;
+    S = (S < cand) ? cand : S;
+  }
+  const double dt_inv = pc.cfl * h / S;
+  if (PHYS != CNS) return dt_inv;
+  const double T = pc.gamma * P.p / P.q[ND];
+  const double S_coeff = sutherland<double>(T, pc.sOverTref, pc.sOverTrefP1) / (P.q[ND] * h);
+  const double a1 = S_coeff / pc.Re0, a2 = S_coeff / (pc.Re0 * pc.Pr0 * pc.gm1);
+  const double S_visc = (a1 < a2) ? a2 : a1;
+  const double dt_v = pc.cflv * h / (2 * S_visc);
+  return (dt_v < dt_inv) ? dt_v : dt_inv;
+}
+
+template <int ND, int PHYS>
+__global__ void __launch_bounds__(kBlock) k_cfl(const double* __restrict__ q, Geometry g, PhysConst pc,
+                                                long long* dst) {
+  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long o = kOrdMax;
+  if (c < g.n_int) {
+    double qc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qc[v] = __ldg(q + v * g.ld + c);
+    const double dt = cell_dt<ND, PHYS>(qc, g.len[g.lvl[c]], pc);
+    if (!isnan(dt)) o = dbl_to_ord(dt);
+  }
+  block_min_atomic(o, dst);
+}
+
+// set_dt: solver.hpp:541-551 (dtmin_ord holds compute_dt of the current lhs)
+__global__ void k_set_dt(Scalars* s, int reset_after) {
+  double dt;
+  if (s->time + s->dt < s->tEnd) {
+    dt = (s->step == s->forced_step) ? s->forced_dt : ord_to_dbl(s->dtmin_ord);
+  } else {
+    dt = s->tEnd - s->time;
+  }
+  s->dt = dt;
+  if (!(dt >= 1e-300 && dt <= 1e300)) s->status |= 1;  // utilities.hpp:74-76
+  if (reset_after) s->dtmin_ord = kOrdMax;
+}
+// advance: solver.hpp:502-505
+__global__ void k_advance(Scalars* s) {
+  s->time += s->dt;
+  s->step += 1;
+}
+__global__ void k_reset_slot(long long* slot) { *slot = kOrdMax; }
+
+// ---------------------------------------------------------------------------
+// isentropic vortex: euler/initial_conditions.hpp:343-368 (2D, hom3's fixed
+// parameters: beta 5, gamma 1.4, centre (-5,-5), u = v = 1)
+// ---------------------------------------------------------------------------
+__device__ inline void isentropic_vortex(double x0, double x1, double t, double* out) {
+  const double PI = 3.141592653589793238462643383279502884;
+  const double beta = 5, gamma = 1.4, c0 = -5.0, c1 = -5.0, uu = 1, vv = 1;
+  const double x_t = x0 - uu * t, y_t = x1 - vv * t;
+  const double r = sqrt((x_t - c0) * (x_t - c0) + (y_t - c1) * (y_t - c1));
+  const double eT1mr2 = exp(1 - r * r);
+  const double eT21mr2 = exp(2 * (1 - r * r));
+  const double pu = uu - beta * eT1mr2 * (y_t - c1) / (2 * PI);
+  const double pv = vv + beta * eT1mr2 * (x_t - c0) / (2 * PI);
+  const double rho = pow((1 - ((gamma - 1) * (beta * beta) * eT21mr2) / (16 * gamma * (PI * PI))), 1 / (gamma - 1));
+  const double p = pow(rho, gamma);
+  out[0] = rho * pu;
+  out[1] = rho * pv;
+  out[2] = rho;
+  out[3] = p / (1.4 - 1.0) + 0.5 * rho * (pu * pu + pv * pv);
+}
+
+// ---------------------------------------------------------------------------
+// boundary conditions: one thread per ghost.  apply_bcs (solver.hpp:561-586)
+// with the conditions of euler/, cns/, heat/ boundary_conditions.hpp and the
+// coupling conditions; bc_apply[] carries hom3's segment assignment.
+// ---------------------------------------------------------------------------
+// Temperature of a partner cell from the partner's lhs: euler/physics.hpp:144-145
+// (gamma p / rho) for Euler/CNS, heat/physics.hpp:51-58 (T itself) for heat.
+__device__ __forceinline__ double partner_T(const BcParam& B, const PartnerView& pv, int o) {
+  if (B.partner_physics == HEAT) return pv.q[o];
+  const int pnd = B.partner_nd;
+  const double* pq = pv.q;
+  const long long pld = pv.ld;
+  const double rho = pq[pnd * pld + o];
+  double um2 = 0;
+  for (int d = 0; d < pnd; ++d) {
+    const double u = pq[d * pld + o] / rho;
+    um2 = d == 0 ? u * u : um2 + u * u;
+  }
+  const double p = (B.partner_gamma - 1.) * (pq[(pnd + 1) * pld + o] - 0.5 * rho * um2);
+  return B.partner_gamma * p / rho;
+}
+
+// q: the state the condition is applied to (lhs or rhs); qlhs: the solver's
+// lhs, which the coupling conditions read temperatures from in both cases.
+template <int ND, int PHYS>
+__global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const double* __restrict__ qlhs,
+                                               Geometry g, GhostTables gt, PhysConst pc,
+                                               const Scalars* __restrict__ sc, PartnerView pv) {
+  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= gt.ng) return;
+  const int b = gt.bc_apply[i];
+  if (b == 255) return;
+  const BcParam& B = gt.bcs[b];
+  const long long gcell = g.n_int + i;
+  const int bc = gt.bndry[i];
+  const long long ld = g.ld;
+  double qb[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) qb[v] = q[v * ld + bc];
+  double out[NV];
+  switch (B.kind) {
+    case BC_EULER_NEUMANN:  // euler/boundary_conditions.hpp:253-264
+    case BC_HEAT_NEUMANN:   // heat/boundary_conditions.hpp:186-194
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[v] = qb[v] - gt.dx[i] * B.v[v];
+      break;
+    case BC_EULER_DIRICHLET:  // euler/boundary_conditions.hpp:279-288
+    case BC_HEAT_DIRICHLET:   // heat/boundary_conditions.hpp:161-168
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[v] = 2.0 * B.v[v] - qb[v];
+      break;
+    case BC_EULER_VORTEX: {  // euler/boundary_conditions.hpp:304-316
+      double vg[4] = {0, 0, 0, 0}, vb[4] = {0, 0, 0, 0};
+      if (ND == 2) {
+        const double t = sc->time;
+        isentropic_vortex(gt.xc[gcell], gt.xc[ld + gcell], t, vg);
+        isentropic_vortex(gt.xc[bc], gt.xc[ld + bc], t, vb);
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        out[v] = vg[v & 3];
+        q[v * ld + bc] = vb[v & 3];  // also overwrites the boundary cell
+      }
+      break;
+    }
+    case BC_CPL_EULER_EULER: {  // euler/coupling_conditions.hpp:452-460
+      const int o = gt.partner[i];
+      if (o < 0 || pv.q == nullptr) return;  // host refuses to launch without partner tables
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[v] = pv.q[v * pv.ld + o];
+      break;
+    }
+    case BC_PERIODIC: {  // EXTENSION (not in hom3): copy of the paired cell
+      const int o = gt.partner[i];
+      if (o < 0) return;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[v] = q[v * ld + o];
+      break;
+    }
+    case BC_CPL_HEAT_CNS:     // heat/coupling_conditions.hpp:233-246
+    case BC_CPL_HEAT_HEAT: {  // :256-269
+      if (gt.partner[i] < 0 || pv.q == nullptr) return;
+      const double Tother = partner_T(B, pv, gt.partner[i]);
+      const double Tthis = qlhs[bc];
+      const double Ts = B.kind == BC_CPL_HEAT_CNS ? 0.5 * (Tother + Tthis) : 0.5 * (Tthis + Tother);
+      out[0] = 2.0 * Ts - qb[0];
+      break;
+    }
+    default: {
+      if (PHYS == HEAT) { out[0] = qb[0]; break; }
+      const double gamma = pc.gamma;
+      // pv of the boundary cell: euler/quantities.hpp:173-186
+      double bp[ND + 2], gp[ND + 2];
+      bp[ND] = qb[ND];
+      double vm2 = 0;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        bp[d] = qb[d] / qb[ND];
+        vm2 = d == 0 ? bp[d] * bp[d] : vm2 + bp[d] * bp[d];
+      }
+      bp[ND + 1] = (gamma - 1.0) * (qb[ND + 1] - 0.5 * qb[ND] * vm2);
+#pragma unroll
+      for (int v = 0; v < ND + 2; ++v) gp[v] = bp[v];
+      if (B.kind == BC_CNS_INFLOW) {  // cns/boundary_conditions.hpp:37-61
+#pragma unroll
+        for (int d = 0; d < ND; ++d) gp[d] = 2.0 * B.v[d] - bp[d];
+        gp[ND] = 2.0 * B.v[ND] - bp[ND];
+      } else if (B.kind == BC_CNS_OUTFLOW) {  // :81-101
+        gp[ND + 1] = 2.0 * B.v[ND + 1] - bp[ND + 1];
+      } else if (B.kind == BC_CNS_ADIABATIC_NOSLIP) {  // :124-141
+#pragma unroll
+        for (int d = 0; d < ND; ++d) gp[d] = 0.0 - bp[d];
+      } else if (B.kind == BC_CNS_ADIABATIC_SLIP) {  // :164-190
+        const int ndir = gt.pos[i] >> 1;  // floor(boundary position w.r.t. the ghost / 2)
+#pragma unroll
+        for (int d = 0; d < ND; ++d)
+          if (d == ndir) gp[d] = 0.0 - bp[d];
+      } else if (B.kind == BC_CNS_ISOTHERMAL_NOSLIP || B.kind == BC_CPL_CNS_HEAT) {  // :209-228
+        double Ts = B.v[0];
+        if (B.kind == BC_CPL_CNS_HEAT) {  // cns/coupling_conditions.hpp:278-292
+          if (gt.partner[i] < 0 || pv.q == nullptr) return;
+          double ql[ND + 2];
+#pragma unroll
+          for (int v = 0; v < ND + 2; ++v) ql[v] = qlhs[v * ld + bc];
+          double um2 = 0;
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            const double u = ql[d] / ql[ND];
+            um2 = d == 0 ? u * u : um2 + u * u;
+          }
+          const double pf = pc.gm1 * (ql[ND + 1] - 0.5 * ql[ND] * um2);
+          const double Tf = gamma * pf / ql[ND];
+          Ts = 0.5 * (Tf + partner_T(B, pv, gt.partner[i]));
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d) gp[d] = 0.0 - bp[d];
+        const double rho_srfc = bp[ND + 1] * gamma / Ts;
+        gp[ND] = 2.0 * rho_srfc - bp[ND];
+      }
+      // cv: euler/quantities.hpp:153-166
+      out[ND] = gp[ND];
+      double gm2 = 0;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        out[d] = gp[ND] * gp[d];
+        gm2 = d == 0 ? gp[d] * gp[d] : gm2 + gp[d] * gp[d];
+      }
+      out[ND + 1] = gp[ND + 1] / (gamma - 1.0) + 0.5 * gp[ND] * gm2;
+      break;
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) q[v * ld + gcell] = out[v];
+}
+
+// ---------------------------------------------------------------------------
+// cell slopes for the viscous flux: slope (solver.hpp:596-623) of every cell,
+// ghosts included, stored as sl[(sd * NV + v) * ld + c].  Interior cells
+// have both neighbours; a ghost takes its boundary cell's central slope, with
+// the wall conditions' sign flip of tangential velocity slopes
+// (boundary_condition.hpp:63-67, cns/boundary_conditions.hpp:143-147,230-234).
+// ---------------------------------------------------------------------------
+template <int ND>
+__global__ void __launch_bounds__(kBlock) k_slopes(const double* __restrict__ q, Geometry g, GhostTables gt,
+                                                   double* __restrict__ sl) {
+  constexpr int NV = ND + 2;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n_tot) return;
+  const long long ld = g.ld;
+  long long b = c;
+  int dg = -1;
+  bool wall = false;
+  if (c >= g.n_int) {
+    const long long i = c - g.n_int;
+    const BcParam& B = gt.bcs[gt.bc_own[i]];
+    b = B.kind == BC_PERIODIC ? gt.partner[i] : gt.bndry[i];
+    if (b < 0) return;
+    dg = gt.pos[i] >> 1;
+    wall = B.wall != 0;
+  }
+  const double h2 = 2. * g.len[g.lvl[b]];
+#pragma unroll
+  for (int sd = 0; sd < ND; ++sd) {
+    const int m = g.nbr[(2 * sd) * ld + b];
+    const int p = g.nbr[(2 * sd + 1) * ld + b];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double s = (__ldg(q + v * ld + p) - __ldg(q + v * ld + m)) / h2;
+      if (wall && v < ND && sd != dg) s = -s;
+      sl[(sd * NV + v) * ld + c] = s;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stage kernel: num_flux (solver.hpp:440-460) + the explicit update of evolve
+// (solver.hpp:470-494).
+//   MODE 0:  out = qin + dt/dx * R(qin)                 (FE, RK2 stage 1)
+//   MODE 2:  out = 0.5 * ((out + qin) + dt/dx * R(qin))  (RK2 stage 2, in place on lhs)
+// FUSE: also reduce the next step's cell dt of `out` into *dtmin (the
+// compute_dt of the next set_dt; valid when no condition rewrites interior cells).
+// HANG: the grid has coarse/fine faces (EXTENSION, not in hom3).
+// ---------------------------------------------------------------------------
+template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG, bool FUSE>
+__global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin, double* out,
+                                                  const double* __restrict__ sl, Geometry g, PhysConst pc,
+                                                  const Scalars* __restrict__ sc, long long* dtmin) {
+  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = c < g.n_int;
+  long long ord = kOrdMax;
+  if (live) {
+    const long long ld = g.ld;
+    const double dt = sc->dt;
+    const double dx = g.len[g.lvl[c]];
+    double qc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+
+    if (PHYS == HEAT) {
+      // three_point: heat/physics.hpp:113-119, (1/dx)(T_l - T_r)
+      const double idx = 1 / dx;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        const int m = g.nbr[(2 * d) * ld + c], p = g.nbr[(2 * d + 1) * ld + c];
+        double fm, fp;
+        if (!HANG || m >= 0) {
+          fm = idx * (__ldg(qin + m) - qc[0]);
+        } else {
+          const long long k = -m - 2;
+          double ws = 0;
+#pragma unroll
+          for (int j = 0; j < (1 << (ND - 1)); ++j) {
+            const double f = idx * (__ldg(qin + g.sub[j * g.nsub + k]) - qc[0]);
+            ws = j == 0 ? f : ws + f;
+          }
+          fm = (ND == 2 ? 0.5 : 0.25) * ws;
+        }
+        if (!HANG || p >= 0) {
+          fp = idx * (qc[0] - __ldg(qin + p));
+        } else {
+          const long long k = -p - 2;
+          double ws = 0;
+#pragma unroll
+          for (int j = 0; j < (1 << (ND - 1)); ++j) {
+            const double f = idx * (qc[0] - __ldg(qin + g.sub[j * g.nsub + k]));
+            ws = j == 0 ? f : ws + f;
+          }
+          fp = (ND == 2 ? 0.5 : 0.25) * ws;
+        }
+        acc[0] = acc[0] + (fm - fp);
+      }
+    } else {
+      const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+      Prim<R, ND> Pc;
+#pragma unroll
+      for (int v = 0; v < ND + 2; ++v) Pc.q[v] = (R)qc[v];
+      make_prim<R, ND>(Pc, gamma, gm1);
+      const R dx_dt = (R)(dx / dt);
+      R slc[PHYS == CNS ? ND * (ND + 2) : 1];
+      if (PHYS == CNS) {
+#pragma unroll
+        for (int k = 0; k < ND * (ND + 2); ++k) slc[k] = (R)__ldg(sl + k * ld + c);
+      }
+      // flux of the face (l = a, r = b) with a or b the centre cell
+      auto face = [&](const Prim<R, ND>& L, const Prim<R, ND>& Rt, const R* sL, const R* sR, R len_r, int d,
+                      R* f) {
+        if (FLUX == LLF) llf<R, ND>(L, Rt, d, dx_dt, f);
+        else ausm<R, ND>(L, Rt, d, f);
+        if (PHYS == CNS) {
+          R fv[ND + 2];
+          viscous<R, ND>(L, Rt, sL, sR, d, len_r, pc, fv);
+#pragma unroll
+          for (int v = 0; v < ND + 2; ++v) f[v] = f[v] + fv[v];
+        }
+      };
+      auto load_nb = [&](int n, Prim<R, ND>& P, R* sn) {
+        load_prim<R, ND>(P, qin, ld, n, gamma, gm1);
+        if (PHYS == CNS) {
+#pragma unroll
+          for (int k = 0; k < ND * (ND + 2); ++k) sn[k] = (R)__ldg(sl + k * ld + n);
+        }
+      };
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        const int m = g.nbr[(2 * d) * ld + c], p = g.nbr[(2 * d + 1) * ld + c];
+        double fm[NV], fp[NV];
+        {
+          if (!HANG || m >= 0) {
+            Prim<R, ND> Pn;
+            R sn[PHYS == CNS ? ND * (ND + 2) : 1];
+            load_nb(m, Pn, sn);
+            R f[ND + 2];
+            face(Pn, Pc, sn, slc, (R)dx, d, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
+          } else {
+            const long long k = -m - 2;
+#pragma unroll
+            for (int j = 0; j < (1 << (ND - 1)); ++j) {
+              const int n = g.sub[j * g.nsub + k];
+              Prim<R, ND> Pn;
+              R sn[PHYS == CNS ? ND * (ND + 2) : 1];
+              load_nb(n, Pn, sn);
+              R f[ND + 2];
+              face(Pn, Pc, sn, slc, (R)dx, d, f);
+#pragma unroll
+              for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
+            }
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fm[v] = (ND == 2 ? 0.5 : 0.25) * fm[v];
+          }
+        }
+        {
+          if (!HANG || p >= 0) {
+            Prim<R, ND> Pn;
+            R sn[PHYS == CNS ? ND * (ND + 2) : 1];
+            load_nb(p, Pn, sn);
+            R f[ND + 2];
+            face(Pc, Pn, slc, sn, (R)g.len[g.lvl[p]], d, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
+          } else {
+            const long long k = -p - 2;
+#pragma unroll
+            for (int j = 0; j < (1 << (ND - 1)); ++j) {
+              const int n = g.sub[j * g.nsub + k];
+              Prim<R, ND> Pn;
+              R sn[PHYS == CNS ? ND * (ND + 2) : 1];
+              load_nb(n, Pn, sn);
+              R f[ND + 2];
+              face(Pc, Pn, slc, sn, (R)g.len[g.lvl[n]], d, f);
+#pragma unroll
+              for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
+            }
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fp[v] = (ND == 2 ? 0.5 : 0.25) * fp[v];
+          }
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - fp[v]);
+      }
+    }
+    const double k = dt / dx;
+    double o[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if (MODE == 0) o[v] = qc[v] + k * acc[v];
+      else o[v] = 0.5 * ((out[v * ld + c] + qc[v]) + k * acc[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
+    if (FUSE) {
+      const double cd = cell_dt<ND, PHYS>(o, dx, pc);
+      if (!isnan(cd)) ord = dbl_to_ord(cd);
+    }
+  }
+  if (FUSE) block_min_atomic(ord, dtmin);
+}
+
+// gather / scatter between the caller's numbering and the internal one
+__global__ void k_gather(const double* __restrict__ src, long long src_ld, double* __restrict__ dst,
+                         long long dst_ld, const long long* __restrict__ dev_to_caller, long long n, int nv) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const long long s = dev_to_caller[c];
+  for (int v = 0; v < nv; ++v) dst[v * dst_ld + c] = src[v * src_ld + s];
+}
+__global__ void k_scatter(const double* __restrict__ src, long long src_ld, double* __restrict__ dst,
+                          long long dst_ld, const long long* __restrict__ dev_to_caller, long long n, int nv) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const long long s = dev_to_caller[c];
+  for (int v = 0; v < nv; ++v) dst[v * dst_ld + s] = src[v * src_ld + c];
+}
+
+}  // namespace h3c

@@ -1,0 +1,884 @@
+// h3c_solver.cu -- host side of the C ABI declared in include/h3c.h.
+//
+// Takes hom3's cell container (caller numbering), renumbers interior cells
+// along a Morton curve, uploads int32 SoA neighbour tables and per-ghost
+// boundary tables, and drives the step kernels of fv_kernels.cuh on the
+// solver's stream.  The step scalars (dt, time, step, forced dt) live on the
+// device so a run of steps never waits for the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/h3c.h"
+#include "fv_kernels.cuh"
+
+using namespace h3c;
+
+namespace {
+std::string g_last_error;  // errors not tied to a solver (NULL handle)
+
+constexpr long long kForcedNone = std::numeric_limits<long long>::max();
+}  // namespace
+
+struct h3c_solver_s {
+  h3c_desc desc{};
+  int nd = 2, nv = 4;
+  PhysConst pc{};
+  double Re0 = 1, Pr0 = 1;
+  cudaStream_t stream = nullptr;
+  bool own_stream = true;
+  // grid
+  bool has_grid = false;
+  long long n_int = 0, n_tot = 0, ng = 0, ld = 0, nsub = 0;
+  int* d_nbr = nullptr;
+  unsigned char* d_lvl = nullptr;
+  int* d_sub = nullptr;
+  double lens[kMaxLevels] = {0};
+  int nlev = 0;
+  int* d_gbndry = nullptr;
+  unsigned char *d_gpos = nullptr, *d_gapply = nullptr, *d_gown = nullptr;
+  double* d_gdx = nullptr;
+  int* d_gpartner = nullptr;
+  double* d_xc = nullptr;
+  int n_bcs = 0;
+  std::vector<h3c_bc> bcs;
+  std::vector<BcParam> h_bcs;
+  BcParam* d_bcs = nullptr;
+  h3c_solver partner = nullptr;
+  // state
+  double* d_q[2] = {nullptr, nullptr};
+  double* d_slopes = nullptr;
+  double* d_stage = nullptr;  // host<->device staging in caller numbering
+  long long stage_cap = 0;
+  long long* d_dev2caller = nullptr;
+  std::vector<long long> dev2caller, caller2dev;
+  Scalars* d_sc = nullptr;
+  bool unfused_dt = false;  // a condition rewrites interior cells (vortex)
+  bool needs_partner = false, needs_periodic = false;  // coupling / periodic conditions present
+  bool partner_set = false, periodic_set = false;
+  std::string err;
+  // launch accounting and optional per-kernel CUDA-event timing (h3c_profile)
+  long long launches = 0;
+  bool prof = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> prof_rec;
+
+  int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    err = buf;
+    return code;
+  }
+  int cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return H3C_OK;
+    return fail(e == cudaErrorMemoryAllocation ? H3C_E_NOMEM : H3C_E_CUDA, "%s: %s", what,
+                cudaGetErrorString(e));
+  }
+};
+
+#define H3C_CUDA(s, call)                          \
+  do {                                             \
+    int rc__ = (s)->cuda((call), #call);           \
+    if (rc__ != H3C_OK) return rc__;               \
+  } while (0)
+
+namespace {
+
+template <class T> void dfree(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void free_grid(h3c_solver s) {
+  dfree(s->d_nbr); dfree(s->d_lvl); dfree(s->d_sub); dfree(s->d_gbndry); dfree(s->d_gpos);
+  dfree(s->d_gapply); dfree(s->d_gown); dfree(s->d_gdx); dfree(s->d_gpartner); dfree(s->d_xc);
+  dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_slopes); dfree(s->d_stage);
+  dfree(s->d_dev2caller);
+  s->has_grid = false;
+}
+
+Geometry geometry(const h3c_solver s) {
+  Geometry g;
+  g.nbr = s->d_nbr;
+  g.lvl = s->d_lvl;
+  g.sub = s->d_sub;
+  g.nsub = s->nsub;
+  g.n_int = s->n_int;
+  g.n_tot = s->n_tot;
+  g.ld = s->ld;
+  for (int i = 0; i < kMaxLevels; ++i) g.len[i] = s->lens[i];
+  return g;
+}
+
+GhostTables ghosts(const h3c_solver s) {
+  GhostTables t;
+  t.bndry = s->d_gbndry;
+  t.pos = s->d_gpos;
+  t.bc_apply = s->d_gapply;
+  t.bc_own = s->d_gown;
+  t.dx = s->d_gdx;
+  t.partner = s->d_gpartner;
+  t.xc = s->d_xc;
+  t.ng = s->ng;
+  t.bcs = s->d_bcs;
+  return t;
+}
+
+unsigned blocks(long long n) { return (unsigned)std::max<long long>(1, (n + kBlock - 1) / kBlock); }
+
+// kernel kinds reported by h3c_profile_read
+enum { K_BC = 0, K_CFL = 1, K_SCALAR = 2, K_STAGE1 = 3, K_STAGE2 = 4, K_SLOPES = 5, K_COPY = 6, K_NKINDS = 8 };
+
+cudaEvent_t take_event(h3c_solver s) {
+  cudaEvent_t e;
+  if (!s->ev_pool.empty()) {
+    e = s->ev_pool.back();
+    s->ev_pool.pop_back();
+  } else {
+    cudaEventCreate(&e);
+  }
+  return e;
+}
+
+// Counts one kernel launch of `kind` and, when profiling, brackets it with
+// events on the solver's stream.
+struct Launch {
+  h3c_solver s;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  Launch(h3c_solver s_, int k) : s(s_), kind(k) {
+    s->launches++;
+    if (s->prof) {
+      a = take_event(s);
+      b = take_event(s);
+      cudaEventRecord(a, s->stream);
+    }
+  }
+  ~Launch() {
+    if (s->prof) {
+      cudaEventRecord(b, s->stream);
+      s->prof_rec.push_back({kind, {a, b}});
+    }
+  }
+};
+
+// ---- kernel dispatch -------------------------------------------------------
+template <int ND, int PHYS>
+void launch_bc_t(h3c_solver s, int which) {
+  PartnerView pv{nullptr, 0};
+  if (s->partner) pv = PartnerView{s->partner->d_q[0], s->partner->ld};
+  Launch L(s, K_BC);
+  k_bc<ND, PHYS><<<blocks(s->ng), kBlock, 0, s->stream>>>(s->d_q[which], s->d_q[0], geometry(s), ghosts(s),
+                                                          s->pc, s->d_sc, pv);
+}
+void launch_bc(h3c_solver s, int which) {
+  if (s->ng == 0) return;
+  if (s->nd == 2) {
+    if (s->desc.physics == H3C_EULER) launch_bc_t<2, EULER>(s, which);
+    else if (s->desc.physics == H3C_CNS) launch_bc_t<2, CNS>(s, which);
+    else launch_bc_t<2, HEAT>(s, which);
+  } else {
+    if (s->desc.physics == H3C_EULER) launch_bc_t<3, EULER>(s, which);
+    else if (s->desc.physics == H3C_CNS) launch_bc_t<3, CNS>(s, which);
+    else launch_bc_t<3, HEAT>(s, which);
+  }
+}
+
+template <int ND, int PHYS>
+void launch_cfl_t(h3c_solver s, long long* slot) {
+  Launch L(s, K_CFL);
+  k_cfl<ND, PHYS><<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_q[0], geometry(s), s->pc, slot);
+}
+void launch_cfl(h3c_solver s, long long* slot) {
+  {
+    Launch L(s, K_SCALAR);
+    k_reset_slot<<<1, 1, 0, s->stream>>>(slot);
+  }
+  if (s->nd == 2) {
+    if (s->desc.physics == H3C_EULER) launch_cfl_t<2, EULER>(s, slot);
+    else if (s->desc.physics == H3C_CNS) launch_cfl_t<2, CNS>(s, slot);
+    else launch_cfl_t<2, HEAT>(s, slot);
+  } else {
+    if (s->desc.physics == H3C_EULER) launch_cfl_t<3, EULER>(s, slot);
+    else if (s->desc.physics == H3C_CNS) launch_cfl_t<3, CNS>(s, slot);
+    else launch_cfl_t<3, HEAT>(s, slot);
+  }
+}
+
+void launch_slopes(h3c_solver s, int which) {
+  Launch L(s, K_SLOPES);
+  if (s->nd == 2)
+    k_slopes<2><<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_q[which], geometry(s), ghosts(s), s->d_slopes);
+  else
+    k_slopes<3><<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_q[which], geometry(s), ghosts(s), s->d_slopes);
+}
+
+template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG, bool FUSE>
+void stage_t(h3c_solver s, const double* qin, double* out) {
+  Launch L(s, MODE == 0 ? K_STAGE1 : K_STAGE2);
+  k_stage<ND, PHYS, FLUX, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
+      qin, out, s->d_slopes, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+}
+template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG>
+void stage_f(h3c_solver s, const double* qin, double* out, bool fuse) {
+  if (fuse) stage_t<ND, PHYS, FLUX, R, MODE, HANG, true>(s, qin, out);
+  else stage_t<ND, PHYS, FLUX, R, MODE, HANG, false>(s, qin, out);
+}
+template <int ND, int PHYS, int FLUX, class R, int MODE>
+void stage_h(h3c_solver s, const double* qin, double* out, bool fuse) {
+  if (PHYS != CNS && s->nsub > 0) stage_f<ND, PHYS, FLUX, R, MODE, PHYS != CNS>(s, qin, out, fuse);
+  else stage_f<ND, PHYS, FLUX, R, MODE, false>(s, qin, out, fuse);
+}
+template <int ND, int PHYS, int FLUX, class R>
+void stage_m(h3c_solver s, int mode, const double* qin, double* out, bool fuse) {
+  if (mode == 0) stage_h<ND, PHYS, FLUX, R, 0>(s, qin, out, fuse);
+  else stage_h<ND, PHYS, FLUX, R, 2>(s, qin, out, fuse);
+}
+template <int ND>
+void stage_nd(h3c_solver s, int mode, const double* qin, double* out, bool fuse) {
+  const bool mixed = s->desc.precision == H3C_MIXED;
+  switch (s->desc.physics) {
+    case H3C_EULER:
+      if (s->desc.flux == H3C_FLUX_LLF) {
+        if (mixed) stage_m<ND, EULER, LLF, float>(s, mode, qin, out, fuse);
+        else stage_m<ND, EULER, LLF, double>(s, mode, qin, out, fuse);
+      } else {
+        if (mixed) stage_m<ND, EULER, AUSM, float>(s, mode, qin, out, fuse);
+        else stage_m<ND, EULER, AUSM, double>(s, mode, qin, out, fuse);
+      }
+      break;
+    case H3C_CNS:
+      if (mixed) stage_m<ND, CNS, AUSM, float>(s, mode, qin, out, fuse);
+      else stage_m<ND, CNS, AUSM, double>(s, mode, qin, out, fuse);
+      break;
+    default:
+      stage_m<ND, HEAT, AUSM, double>(s, mode, qin, out, fuse);
+  }
+}
+void launch_stage(h3c_solver s, int mode, const double* qin, double* out, bool fuse) {
+  if (s->nd == 2) stage_nd<2>(s, mode, qin, out, fuse);
+  else stage_nd<3>(s, mode, qin, out, fuse);
+}
+
+__global__ void k_init_time(Scalars* sc, double tEnd) {
+  sc->dt = 0;
+  sc->time = 0;
+  sc->tEnd = tEnd;
+  sc->forced_dt = 0;
+  sc->step = 0;
+  sc->forced_step = 0x7fffffffffffffffLL;
+  sc->dtmin_ord = kOrdMax;
+  sc->mindt_ord = kOrdMax;
+  sc->status = 0;
+}
+__global__ void k_force_dt(Scalars* sc, double dt) {
+  sc->forced_step = sc->step;
+  sc->forced_dt = dt;
+}
+// coupling::apply(Tr0, cns, heat): coupling.hpp:172-183
+__global__ void k_couple_cht(Scalars* cns, Scalars* heat, double scaling) {
+  const double min_dt_cns = ord_to_dbl(cns->mindt_ord);
+  const double min_dt_heat = ord_to_dbl(heat->mindt_ord) / scaling;
+  const double dt = (min_dt_heat < min_dt_cns) ? min_dt_heat : min_dt_cns;  // std::min
+  cns->forced_step = cns->step;
+  cns->forced_dt = dt;
+  heat->forced_step = heat->step;
+  heat->forced_dt = dt * scaling;
+}
+// coupling::apply(s1, s2): coupling.hpp:186-193
+__global__ void k_couple_equal(Scalars* a, Scalars* b) {
+  const double da = ord_to_dbl(a->mindt_ord), db = ord_to_dbl(b->mindt_ord);
+  const double dt = (db < da) ? db : da;
+  a->forced_step = a->step;
+  a->forced_dt = dt;
+  b->forced_step = b->step;
+  b->forced_dt = dt;
+}
+
+// Morton key of an interior cell's lower corner in units of the finest cell
+// (x in the lowest bit: hom3's child positions, grid/grid.hpp:41-59).
+uint64_t morton(const long long* ix, int nd) {
+  uint64_t k = 0;
+  const int bits = nd == 2 ? 31 : 21;
+  for (int b = 0; b < bits; ++b)
+    for (int d = 0; d < nd; ++d) k |= (uint64_t)((ix[d] >> b) & 1) << (b * nd + d);
+  return k;
+}
+
+int valid_cell(long long v, long long n) { return v >= 0 && v < n; }
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+int h3c_last_error(h3c_solver s, char* buf, size_t n) {
+  const std::string& e = s ? s->err : g_last_error;
+  if (buf && n) {
+    std::strncpy(buf, e.c_str(), n - 1);
+    buf[n - 1] = 0;
+  }
+  return (int)e.size();
+}
+
+int h3c_create(const h3c_desc* d, h3c_solver* out) {
+  if (!d || !out) { g_last_error = "h3c_create: null argument"; return H3C_E_INVALID; }
+  if (d->nd != 2 && d->nd != 3) { g_last_error = "h3c_create: nd must be 2 or 3"; return H3C_E_INVALID; }
+  if (d->physics < 0 || d->physics > 2 || d->flux < 0 || d->flux > 1 || d->time_integration < 0 ||
+      d->time_integration > 1 || d->precision < 0 || d->precision > 1) {
+    g_last_error = "h3c_create: unknown physics / flux / time integration / precision";
+    return H3C_E_INVALID;
+  }
+  if (d->physics == H3C_CNS && d->flux != H3C_FLUX_AUSM) {
+    g_last_error = "h3c_create: CNS supports the standard flux (AUSM + three-point) only";
+    return H3C_E_INVALID;
+  }
+  auto s = std::make_unique<h3c_solver_s>();
+  s->desc = *d;
+  s->nd = d->nd;
+  s->nv = d->physics == H3C_HEAT ? 1 : d->nd + 2;
+  // quantities: euler/quantities.hpp:131-145, cns/quantities.hpp:377-384
+  const double gamma = d->gamma, gm1 = gamma - 1.;
+  const double T_inf = 1.0 / (1 + 0.5 * gm1 * (d->Minfty * d->Minfty));
+  const double rho_inf = std::pow(T_inf, 1. / gm1);
+  const double u_inf = d->Minfty * std::sqrt(T_inf);
+  const double sOverTref = d->T0 > 0 ? d->Sutherland0 / d->T0 : 0.0;
+  const double sOverTrefP1 = sOverTref + 1.0;
+  const double mu_inf = std::pow(T_inf, 1.5) * sOverTrefP1 / (T_inf + sOverTref);
+  s->Re0 = d->physics == H3C_CNS ? d->ReInfty * mu_inf / (rho_inf * u_inf) : 1.0;
+  s->Pr0 = d->Pr0;
+  s->pc = PhysConst{gamma, gm1, d->cfl, d->cfl_viscous, s->Re0, d->Pr0, sOverTref, sOverTrefP1};
+  cudaError_t e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    g_last_error = std::string("h3c_create: cudaStreamCreate: ") + cudaGetErrorString(e);
+    return H3C_E_CUDA;
+  }
+  e = cudaMalloc(&s->d_sc, sizeof(Scalars));
+  if (e != cudaSuccess) {
+    cudaStreamDestroy(s->stream);
+    g_last_error = std::string("h3c_create: cudaMalloc: ") + cudaGetErrorString(e);
+    return H3C_E_NOMEM;
+  }
+  k_init_time<<<1, 1, 0, s->stream>>>(s->d_sc, d->time_end);
+  *out = s.release();
+  return H3C_OK;
+}
+
+int h3c_destroy(h3c_solver s) {
+  if (!s) return H3C_OK;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  free_grid(s);
+  dfree(s->d_sc);
+  for (auto& r : s->prof_rec) { cudaEventDestroy(r.second.first); cudaEventDestroy(r.second.second); }
+  for (auto e : s->ev_pool) cudaEventDestroy(e);
+  if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
+  delete s;
+  return H3C_OK;
+}
+
+int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
+  if (!s || !gr) return H3C_E_INVALID;
+  const int nd = s->nd, np = 2 * nd;
+  const long long n = gr->n_cells, fg = gr->first_ghost, ld = gr->ld;
+  if (n <= 0 || fg <= 0 || fg > n || ld < n || !gr->neighbors || !gr->x_center || !gr->length || !gr->bc_idx)
+    return s->fail(H3C_E_INVALID, "h3c_set_grid: bad sizes or null tables");
+  if (n >= (1LL << 31)) return s->fail(H3C_E_INVALID, "h3c_set_grid: more than 2^31 cells");
+  if (gr->n_bcs < 0 || gr->n_bcs > kMaxBcs || (gr->n_bcs > 0 && !gr->bcs))
+    return s->fail(H3C_E_INVALID, "h3c_set_grid: n_bcs must be in [0, %d]", kMaxBcs);
+  const long long nsub = gr->subface_cells ? gr->n_subfaces : 0;
+  if (nsub > 0 && s->desc.physics == H3C_CNS)
+    return s->fail(H3C_E_INVALID, "h3c_set_grid: coarse/fine faces are not supported for CNS");
+  const int nsubc = 1 << (nd - 1);
+  auto nb = [&](int p, long long c) { return gr->neighbors[p * ld + c]; };
+  auto is_group = [&](long long v) { return nsub > 0 && v <= -2 && (-v - 2) < nsub; };
+  // ---- validation --------------------------------------------------------
+  for (long long c = 0; c < fg; ++c) {
+    for (int p = 0; p < np; ++p) {
+      const long long v = nb(p, c);
+      if (!valid_cell(v, n) && !is_group(v))
+        return s->fail(H3C_E_INVALID, "h3c_set_grid: internal cell %lld has no neighbour at position %d", c, p);
+    }
+    if (!(gr->length[c] > 0)) return s->fail(H3C_E_INVALID, "h3c_set_grid: cell %lld has length <= 0", c);
+  }
+  std::vector<int> gb(n - fg), gbp(n - fg);
+  for (long long g = fg; g < n; ++g) {
+    int cnt = 0, first = -1;
+    for (int p = 0; p < np; ++p)
+      if (valid_cell(nb(p, g), n)) { ++cnt; if (first < 0) first = p; }
+    if (cnt != 1)
+      return s->fail(H3C_E_INVALID, "h3c_set_grid: ghost %lld has %d neighbours (expected 1)", g, cnt);
+    const long long b = nb(first, g);
+    if (b >= fg) return s->fail(H3C_E_INVALID, "h3c_set_grid: ghost %lld is linked to ghost %lld", g, b);
+    gb[g - fg] = (int)b;
+    gbp[g - fg] = first;
+    const int bc = gr->bc_idx[g];
+    if (bc < 0 || bc >= gr->n_bcs)
+      return s->fail(H3C_E_INVALID, "h3c_set_grid: ghost %lld has bc index %d (n_bcs %d)", g, bc, gr->n_bcs);
+  }
+  for (long long k = 0; k < nsub; ++k)
+    for (int j = 0; j < nsubc; ++j) {
+      const long long v = gr->subface_cells[j * nsub + k];
+      if (!valid_cell(v, n)) return s->fail(H3C_E_INVALID, "h3c_set_grid: sub-face %lld has an invalid cell", k);
+    }
+  // ---- length levels -------------------------------------------------------
+  std::vector<double> lens;
+  for (long long c = 0; c < n; ++c) {
+    const double l = gr->length[c];
+    if (std::find(lens.begin(), lens.end(), l) == lens.end()) {
+      if ((int)lens.size() == kMaxLevels)
+        return s->fail(H3C_E_INVALID, "h3c_set_grid: more than %d distinct cell lengths", kMaxLevels);
+      lens.push_back(l);
+    }
+  }
+  std::sort(lens.begin(), lens.end(), std::greater<double>());
+  // ---- Morton order of interior cells ---------------------------------------
+  double xmin[3] = {1e300, 1e300, 1e300};
+  double hmin = lens.back();
+  for (long long c = 0; c < fg; ++c)
+    for (int d = 0; d < nd; ++d) xmin[d] = std::min(xmin[d], gr->x_center[d * ld + c] - 0.5 * gr->length[c]);
+  std::vector<std::pair<uint64_t, long long>> keys(fg);
+  for (long long c = 0; c < fg; ++c) {
+    long long ix[3] = {0, 0, 0};
+    for (int d = 0; d < nd; ++d)
+      ix[d] = std::llround((gr->x_center[d * ld + c] - 0.5 * gr->length[c] - xmin[d]) / hmin);
+    keys[c] = {morton(ix, nd), c};
+  }
+  std::stable_sort(keys.begin(), keys.end(),
+                   [](const std::pair<uint64_t, long long>& a, const std::pair<uint64_t, long long>& b) {
+                     return a.first < b.first;
+                   });
+  std::vector<long long> dev2caller(n), caller2dev(n);
+  for (long long i = 0; i < fg; ++i) dev2caller[i] = keys[i].second;
+  for (long long g = fg; g < n; ++g) dev2caller[g] = g;  // ghosts keep the caller's (bc-sorted) order
+  for (long long i = 0; i < n; ++i) caller2dev[dev2caller[i]] = i;
+  // ---- hom3's bc segment discovery (solver.hpp:561-586) -----------------------
+  std::vector<unsigned char> apply(n - fg, 255), own(n - fg);
+  {
+    auto valid_bc = [&](long long c) { return gr->bc_idx[c] >= 0 && gr->bc_idx[c] < gr->n_bcs; };
+    long long first = 0;
+    while (first < n && !valid_bc(first)) ++first;
+    if (first < n) {
+      int bcIdx = gr->bc_idx[first];
+      long long last = 0;
+      while (last < n && gr->bc_idx[last] != bcIdx) ++last;
+      for (int k = 0; k < gr->n_bcs; ++k) {
+        ++bcIdx;
+        const long long f0 = last;
+        last = f0;
+        while (last < n && gr->bc_idx[last] != bcIdx) ++last;
+        for (long long c = std::max(f0, fg); c < last; ++c) apply[c - fg] = (unsigned char)k;
+      }
+    }
+    for (long long g = fg; g < n; ++g) own[g - fg] = (unsigned char)gr->bc_idx[g];
+  }
+  // ---- device tables ---------------------------------------------------------
+  free_grid(s);
+  s->n_int = fg;
+  s->n_tot = n;
+  s->ng = n - fg;
+  s->ld = (n + 31) / 32 * 32;
+  s->nsub = nsub;
+  s->nlev = (int)lens.size();
+  for (int i = 0; i < kMaxLevels; ++i) s->lens[i] = i < s->nlev ? lens[i] : 0.0;
+  const long long L = s->ld;
+  std::vector<int> h_nbr(np * L, -1);
+  std::vector<unsigned char> h_lvl(L, 0);
+  std::vector<double> h_xc(nd * L, 0.0);
+  for (long long i = 0; i < n; ++i) {
+    const long long c = dev2caller[i];
+    h_lvl[i] = (unsigned char)(std::find(lens.begin(), lens.end(), gr->length[c]) - lens.begin());
+    for (int d = 0; d < nd; ++d) h_xc[d * L + i] = gr->x_center[d * ld + c];
+    for (int p = 0; p < np; ++p) {
+      const long long v = nb(p, c);
+      if (valid_cell(v, n)) h_nbr[p * L + i] = (int)caller2dev[v];
+      else if (i < fg && is_group(v)) h_nbr[p * L + i] = (int)v;
+    }
+  }
+  std::vector<int> h_sub(nsubc * std::max<long long>(nsub, 1), 0);
+  for (long long k = 0; k < nsub; ++k)
+    for (int j = 0; j < nsubc; ++j) h_sub[j * nsub + k] = (int)caller2dev[gr->subface_cells[j * nsub + k]];
+  std::vector<int> h_gb(s->ng);
+  std::vector<unsigned char> h_gpos(s->ng);
+  std::vector<double> h_gdx(s->ng);
+  for (long long i = 0; i < s->ng; ++i) {
+    const long long g = fg + i;
+    const long long b = gb[i];
+    h_gb[i] = (int)caller2dev[b];
+    h_gpos[i] = (unsigned char)(gbp[i] ^ 1);  // ghost position w.r.t. its boundary cell
+    double s2 = 0;
+    for (int d = 0; d < nd; ++d) {
+      const double dd = gr->x_center[d * ld + b] - gr->x_center[d * ld + g];
+      s2 += dd * dd;
+    }
+    h_gdx[i] = std::sqrt(s2);
+  }
+  s->needs_partner = s->needs_periodic = false;
+  s->bcs.assign(gr->bcs, gr->bcs + gr->n_bcs);
+  s->n_bcs = gr->n_bcs;
+  s->h_bcs.assign(std::max(1, gr->n_bcs), BcParam{});
+  s->unfused_dt = false;
+  for (int k = 0; k < gr->n_bcs; ++k) {
+    BcParam& B = s->h_bcs[k];
+    B.kind = gr->bcs[k].kind;
+    if (B.kind < 0 || B.kind > H3C_BC_PERIODIC) return s->fail(H3C_E_INVALID, "h3c_set_grid: bc %d kind %d", k, B.kind);
+    B.wall = (B.kind == H3C_BC_CNS_ADIABATIC_NOSLIP || B.kind == H3C_BC_CNS_ISOTHERMAL_NOSLIP ||
+              B.kind == H3C_BC_CPL_CNS_HEAT);
+    for (int j = 0; j < 8; ++j) B.v[j] = gr->bcs[k].v[j];
+    if (B.kind == H3C_BC_EULER_VORTEX) {
+      if (nd != 2 || s->desc.physics == H3C_HEAT)
+        return s->fail(H3C_E_INVALID, "h3c_set_grid: the isentropic vortex condition is 2D Euler/CNS only "
+                                      "(euler/initial_conditions.hpp:370-375)");
+      s->unfused_dt = true;
+    }
+    if (B.kind >= H3C_BC_CPL_EULER_EULER && B.kind <= H3C_BC_CPL_HEAT_HEAT) s->needs_partner = true;
+    if (B.kind == H3C_BC_PERIODIC) s->needs_periodic = true;
+  }
+  s->dev2caller = dev2caller;
+  s->caller2dev = caller2dev;
+  s->partner = nullptr;
+  s->partner_set = s->periodic_set = false;
+  // allocations
+  H3C_CUDA(s, cudaMalloc(&s->d_nbr, sizeof(int) * np * L));
+  H3C_CUDA(s, cudaMalloc(&s->d_lvl, L));
+  H3C_CUDA(s, cudaMalloc(&s->d_sub, sizeof(int) * h_sub.size()));
+  H3C_CUDA(s, cudaMalloc(&s->d_xc, sizeof(double) * nd * L));
+  const long long ngm = std::max<long long>(1, s->ng);
+  H3C_CUDA(s, cudaMalloc(&s->d_gbndry, sizeof(int) * ngm));
+  H3C_CUDA(s, cudaMalloc(&s->d_gpos, ngm));
+  H3C_CUDA(s, cudaMalloc(&s->d_gapply, ngm));
+  H3C_CUDA(s, cudaMalloc(&s->d_gown, ngm));
+  H3C_CUDA(s, cudaMalloc(&s->d_gdx, sizeof(double) * ngm));
+  H3C_CUDA(s, cudaMalloc(&s->d_gpartner, sizeof(int) * ngm));
+  H3C_CUDA(s, cudaMalloc(&s->d_bcs, sizeof(BcParam) * s->h_bcs.size()));
+  H3C_CUDA(s, cudaMalloc(&s->d_q[0], sizeof(double) * s->nv * L));
+  H3C_CUDA(s, cudaMalloc(&s->d_q[1], sizeof(double) * s->nv * L));
+  if (s->desc.physics == H3C_CNS) H3C_CUDA(s, cudaMalloc(&s->d_slopes, sizeof(double) * nd * s->nv * L));
+  H3C_CUDA(s, cudaMalloc(&s->d_dev2caller, sizeof(long long) * n));
+  // uploads (synchronous: tables are set once)
+  H3C_CUDA(s, cudaMemcpy(s->d_nbr, h_nbr.data(), sizeof(int) * np * L, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_lvl, h_lvl.data(), L, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_sub, h_sub.data(), sizeof(int) * h_sub.size(), cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_xc, h_xc.data(), sizeof(double) * nd * L, cudaMemcpyHostToDevice));
+  if (s->ng > 0) {
+    H3C_CUDA(s, cudaMemcpy(s->d_gbndry, h_gb.data(), sizeof(int) * s->ng, cudaMemcpyHostToDevice));
+    H3C_CUDA(s, cudaMemcpy(s->d_gpos, h_gpos.data(), s->ng, cudaMemcpyHostToDevice));
+    H3C_CUDA(s, cudaMemcpy(s->d_gapply, apply.data(), s->ng, cudaMemcpyHostToDevice));
+    H3C_CUDA(s, cudaMemcpy(s->d_gown, own.data(), s->ng, cudaMemcpyHostToDevice));
+    H3C_CUDA(s, cudaMemcpy(s->d_gdx, h_gdx.data(), sizeof(double) * s->ng, cudaMemcpyHostToDevice));
+  }
+  H3C_CUDA(s, cudaMemset(s->d_gpartner, 0xff, sizeof(int) * ngm));
+  H3C_CUDA(s, cudaMemcpy(s->d_bcs, s->h_bcs.data(), sizeof(BcParam) * s->h_bcs.size(), cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_dev2caller, dev2caller.data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemset(s->d_q[0], 0, sizeof(double) * s->nv * L));
+  H3C_CUDA(s, cudaMemset(s->d_q[1], 0, sizeof(double) * s->nv * L));
+  s->has_grid = true;
+  return H3C_OK;
+}
+
+// Coupling and periodic conditions read partner cells: refuse to launch them
+// before the partner tables exist.
+static int ready(h3c_solver s, const char* what) {
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "%s: no grid", what);
+  if (s->needs_partner && !s->partner_set)
+    return s->fail(H3C_E_STATE, "%s: coupling conditions without h3c_set_partner", what);
+  if (s->needs_periodic && !s->periodic_set)
+    return s->fail(H3C_E_STATE, "%s: periodic conditions without h3c_set_periodic", what);
+  return H3C_OK;
+}
+
+static int ensure_stage(h3c_solver s, long long ld) {
+  const long long need = (long long)s->nv * ld;
+  if (need > s->stage_cap) {
+    dfree(s->d_stage);
+    H3C_CUDA(s, cudaMalloc(&s->d_stage, sizeof(double) * need));
+    s->stage_cap = need;
+  }
+  return H3C_OK;
+}
+
+int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld) {
+  if (!s || !q || (which != 0 && which != 1)) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_set_state: no grid");
+  if (ld < s->n_tot) return s->fail(H3C_E_INVALID, "h3c_set_state: ld < n_cells");
+  int rc = ensure_stage(s, s->n_tot);
+  if (rc) return rc;
+  for (int v = 0; v < s->nv; ++v)
+    H3C_CUDA(s, cudaMemcpyAsync(s->d_stage + v * s->n_tot, q + v * ld, sizeof(double) * s->n_tot,
+                                cudaMemcpyHostToDevice, s->stream));
+  k_gather<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_stage, s->n_tot, s->d_q[which], s->ld,
+                                                       s->d_dev2caller, s->n_tot, s->nv);
+  if (which == 0) launch_cfl(s, &s->d_sc->dtmin_ord);
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  return s->cuda(cudaGetLastError(), "h3c_set_state");
+}
+
+int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld) {
+  if (!s || !q || (which != 0 && which != 1)) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_get_state: no grid");
+  if (ld < s->n_tot) return s->fail(H3C_E_INVALID, "h3c_get_state: ld < n_cells");
+  int rc = ensure_stage(s, s->n_tot);
+  if (rc) return rc;
+  k_scatter<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_q[which], s->ld, s->d_stage, s->n_tot,
+                                                        s->d_dev2caller, s->n_tot, s->nv);
+  for (int v = 0; v < s->nv; ++v)
+    H3C_CUDA(s, cudaMemcpyAsync(q + v * ld, s->d_stage + v * s->n_tot, sizeof(double) * s->n_tot,
+                                cudaMemcpyDeviceToHost, s->stream));
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  return s->cuda(cudaGetLastError(), "h3c_get_state");
+}
+
+int h3c_state_device(h3c_solver s, int which, double** ptr, int64_t* ld) {
+  if (!s || !ptr || !ld || (which != 0 && which != 1)) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_state_device: no grid");
+  *ptr = s->d_q[which];
+  *ld = s->ld;
+  return H3C_OK;
+}
+
+int h3c_device_order(h3c_solver s, int64_t* perm) {
+  if (!s || !perm) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_device_order: no grid");
+  for (long long c = 0; c < s->n_tot; ++c) perm[c] = s->caller2dev[c];
+  return H3C_OK;
+}
+
+int h3c_get_stream(h3c_solver s, void** stream) {
+  if (!s || !stream) return H3C_E_INVALID;
+  *stream = (void*)s->stream;
+  return H3C_OK;
+}
+
+int h3c_sizes(h3c_solver s, int64_t* n_cells, int64_t* first_ghost, int* nv) {
+  if (!s) return H3C_E_INVALID;
+  if (n_cells) *n_cells = s->n_tot;
+  if (first_ghost) *first_ghost = s->n_int;
+  if (nv) *nv = s->nv;
+  return H3C_OK;
+}
+
+int h3c_reset_time(h3c_solver s) {
+  if (!s) return H3C_E_INVALID;
+  if (s->ng < 0) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_reset_time: no grid");
+  k_init_time<<<1, 1, 0, s->stream>>>(s->d_sc, s->desc.time_end);
+  launch_cfl(s, &s->d_sc->dtmin_ord);
+  k_set_dt<<<1, 1, 0, s->stream>>>(s->d_sc, 0);
+  return s->cuda(cudaGetLastError(), "h3c_reset_time");
+}
+
+int h3c_apply_bcs(h3c_solver s, int which) {
+  if (!s || (which != 0 && which != 1)) return H3C_E_INVALID;
+  if (int rc = ready(s, "h3c_apply_bcs")) return rc;
+  launch_bc(s, which);
+  return s->cuda(cudaGetLastError(), "h3c_apply_bcs");
+}
+
+// Solver::solve (solver.hpp:140-145): apply_bcs(lhs), set_dt, evolve, advance.
+int h3c_solve(h3c_solver s, int64_t nsteps) {
+  if (!s || nsteps < 0) return H3C_E_INVALID;
+  if (int rc = ready(s, "h3c_solve")) return rc;
+  const bool cns = s->desc.physics == H3C_CNS;
+  const bool fuse = !s->unfused_dt;
+  for (int64_t it = 0; it < nsteps; ++it) {
+    launch_bc(s, 0);
+    if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
+    {
+      Launch L(s, K_SCALAR);
+      k_set_dt<<<1, 1, 0, s->stream>>>(s->d_sc, 1);
+    }
+    if (cns) launch_slopes(s, 0);
+    if (s->desc.time_integration == H3C_EULER_FORWARD) {
+      // evolve(euler_forward): solver.hpp:470-479 (rhs = lhs + R; lhs = rhs as a buffer swap)
+      launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
+      std::swap(s->d_q[0], s->d_q[1]);
+    } else {
+      // evolve(runge_kutta_2): solver.hpp:483-494
+      launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
+      launch_bc(s, 1);
+      if (cns) launch_slopes(s, 1);
+      launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
+    }
+    {
+      Launch L(s, K_SCALAR);
+      k_advance<<<1, 1, 0, s->stream>>>(s->d_sc);
+    }
+  }
+  return s->cuda(cudaGetLastError(), "h3c_solve");
+}
+
+static int read_scalars(h3c_solver s, Scalars* out) {
+  H3C_CUDA(s, cudaMemcpyAsync(out, s->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  return H3C_OK;
+}
+
+int h3c_min_dt(h3c_solver s, double* dt) {
+  if (!s || !dt) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_min_dt: no grid");
+  launch_cfl(s, &s->d_sc->mindt_ord);
+  Scalars sc;
+  int rc = read_scalars(s, &sc);
+  if (rc) return rc;
+  *dt = ord_to_dbl(sc.mindt_ord);
+  return H3C_OK;
+}
+
+int h3c_dt(h3c_solver s, double* dt) {
+  if (!s || !dt) return H3C_E_INVALID;
+  Scalars sc;
+  int rc = read_scalars(s, &sc);
+  if (rc) return rc;
+  *dt = sc.dt;
+  return H3C_OK;
+}
+int h3c_time(h3c_solver s, double* t) {
+  if (!s || !t) return H3C_E_INVALID;
+  Scalars sc;
+  int rc = read_scalars(s, &sc);
+  if (rc) return rc;
+  *t = sc.time;
+  return H3C_OK;
+}
+int h3c_step(h3c_solver s, int64_t* step) {
+  if (!s || !step) return H3C_E_INVALID;
+  Scalars sc;
+  int rc = read_scalars(s, &sc);
+  if (rc) return rc;
+  *step = sc.step;
+  return H3C_OK;
+}
+int h3c_force_dt(h3c_solver s, double dt) {
+  if (!s) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_force_dt: no grid");
+  k_force_dt<<<1, 1, 0, s->stream>>>(s->d_sc, dt);
+  return s->cuda(cudaGetLastError(), "h3c_force_dt");
+}
+int h3c_status(h3c_solver s, int* flags) {
+  if (!s || !flags) return H3C_E_INVALID;
+  Scalars sc;
+  int rc = read_scalars(s, &sc);
+  if (rc) return rc;
+  *flags = sc.status;
+  int zero = 0;
+  H3C_CUDA(s, cudaMemcpy(&s->d_sc->status, &zero, sizeof(int), cudaMemcpyHostToDevice));
+  return H3C_OK;
+}
+
+int h3c_set_partner(h3c_solver s, h3c_solver partner, const int64_t* partner_cells) {
+  if (!s || !partner || !partner_cells) return H3C_E_INVALID;
+  if (!s->has_grid || !partner->has_grid) return s->fail(H3C_E_STATE, "h3c_set_partner: no grid");
+  if (s->nd != partner->nd) return s->fail(H3C_E_INVALID, "h3c_set_partner: dimension mismatch");
+  std::vector<int> h(std::max<long long>(1, s->ng), -1);
+  for (long long i = 0; i < s->ng; ++i) {
+    const long long o = partner_cells[i];
+    if (o >= 0 && o < partner->n_tot) h[i] = (int)partner->caller2dev[o];
+  }
+  // every ghost of a coupling condition needs a partner cell
+  std::vector<unsigned char> own(s->ng);
+  if (s->ng) H3C_CUDA(s, cudaMemcpy(own.data(), s->d_gown, s->ng, cudaMemcpyDeviceToHost));
+  for (long long i = 0; i < s->ng; ++i) {
+    const int kind = s->h_bcs[own[i]].kind;
+    const bool cpl = kind == H3C_BC_CPL_EULER_EULER || kind == H3C_BC_CPL_CNS_HEAT ||
+                     kind == H3C_BC_CPL_HEAT_CNS || kind == H3C_BC_CPL_HEAT_HEAT;
+    if (cpl && h[i] < 0) return s->fail(H3C_E_INVALID, "h3c_set_partner: coupled ghost %lld has no partner", i);
+  }
+  for (int k = 0; k < s->n_bcs; ++k) {
+    s->h_bcs[k].partner_gamma = partner->desc.gamma;
+    s->h_bcs[k].partner_physics = partner->desc.physics;
+    s->h_bcs[k].partner_nd = partner->nd;
+  }
+  H3C_CUDA(s, cudaMemcpy(s->d_bcs, s->h_bcs.data(), sizeof(BcParam) * s->h_bcs.size(), cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_gpartner, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+  s->partner = partner;
+  s->partner_set = true;
+  // coupled solvers run on one stream, so each sees the other's finished steps
+  if (s->stream != partner->stream) {
+    H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    s->stream = partner->stream;
+    s->own_stream = false;
+    // the partner keeps ownership of its stream; it must outlive this solver's use of it
+  }
+  return H3C_OK;
+}
+
+int h3c_set_periodic(h3c_solver s, const int64_t* partner_cells) {
+  if (!s || !partner_cells) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_set_periodic: no grid");
+  std::vector<int> h(std::max<long long>(1, s->ng), -1);
+  std::vector<unsigned char> own(s->ng);
+  if (s->ng) H3C_CUDA(s, cudaMemcpy(own.data(), s->d_gown, s->ng, cudaMemcpyDeviceToHost));
+  for (long long i = 0; i < s->ng; ++i) {
+    const long long o = partner_cells[i];
+    if (o >= 0 && o < s->n_int) h[i] = (int)s->caller2dev[o];
+    if (s->h_bcs[own[i]].kind == H3C_BC_PERIODIC && h[i] < 0)
+      return s->fail(H3C_E_INVALID, "h3c_set_periodic: periodic ghost %lld has no interior partner", i);
+  }
+  H3C_CUDA(s, cudaMemcpy(s->d_gpartner, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+  s->periodic_set = true;
+  return H3C_OK;
+}
+
+int h3c_couple_cht(h3c_solver cns, h3c_solver heat, double Tr0) {
+  if (!cns || !heat) return H3C_E_INVALID;
+  if (!cns->has_grid || !heat->has_grid) return cns->fail(H3C_E_STATE, "h3c_couple_cht: no grid");
+  if (cns->desc.physics != H3C_CNS || heat->desc.physics != H3C_HEAT)
+    return cns->fail(H3C_E_INVALID, "h3c_couple_cht: expects (cns, heat)");
+  if (cns->stream != heat->stream) return cns->fail(H3C_E_STATE, "h3c_couple_cht: solvers are not coupled");
+  const double scaling = Tr0 * cns->Pr0 * cns->Re0;
+  launch_cfl(cns, &cns->d_sc->mindt_ord);
+  launch_cfl(heat, &heat->d_sc->mindt_ord);
+  k_couple_cht<<<1, 1, 0, cns->stream>>>(cns->d_sc, heat->d_sc, scaling);
+  return cns->cuda(cudaGetLastError(), "h3c_couple_cht");
+}
+
+int h3c_couple_equal(h3c_solver a, h3c_solver b) {
+  if (!a || !b) return H3C_E_INVALID;
+  if (!a->has_grid || !b->has_grid) return a->fail(H3C_E_STATE, "h3c_couple_equal: no grid");
+  if (a->stream != b->stream) return a->fail(H3C_E_STATE, "h3c_couple_equal: solvers are not coupled");
+  launch_cfl(a, &a->d_sc->mindt_ord);
+  launch_cfl(b, &b->d_sc->mindt_ord);
+  k_couple_equal<<<1, 1, 0, a->stream>>>(a->d_sc, b->d_sc);
+  return a->cuda(cudaGetLastError(), "h3c_couple_equal");
+}
+
+int h3c_launches(h3c_solver s, int64_t* n) {
+  if (!s || !n) return H3C_E_INVALID;
+  *n = s->launches;
+  return H3C_OK;
+}
+
+int h3c_profile(h3c_solver s, int enable) {
+  if (!s) return H3C_E_INVALID;
+  s->prof = enable != 0;
+  return H3C_OK;
+}
+
+int h3c_profile_read(h3c_solver s, double* ms, int64_t* count, int nkinds) {
+  if (!s || !ms || !count || nkinds <= 0) return H3C_E_INVALID;
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  for (int k = 0; k < nkinds; ++k) { ms[k] = 0; count[k] = 0; }
+  for (auto& r : s->prof_rec) {
+    float t = 0;
+    H3C_CUDA(s, cudaEventElapsedTime(&t, r.second.first, r.second.second));
+    if (r.first < nkinds) { ms[r.first] += t; count[r.first] += 1; }
+    s->ev_pool.push_back(r.second.first);
+    s->ev_pool.push_back(r.second.second);
+  }
+  s->prof_rec.clear();
+  return H3C_OK;
+}
+
+}  // extern "C"

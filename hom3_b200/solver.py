@@ -1,0 +1,437 @@
+"""Python mirror of hom3's Solver interface, running on the C ABI (include/h3c.h).
+
+hom3's drivers use (src/solver/fv/solver.hpp:88-221, utilities.hpp:98-113):
+    Solver(solverIdx, properties); set_initial_condition(f); append_bc(bc);
+    initialize(); solve(); dt(); dt(value); min_dt(); time(); step(); Q<tag>()
+`FvSolver` below offers the same calls; its grid comes from the library's
+own builder (h3c_grid_build).  `Solver` is the thin layer over the ABI used
+when the caller already has hom3's cell tables (the drop-in path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+from typing import Callable, Optional, Sequence
+
+import numpy as np
+
+from . import _ffi as F
+from ._ffi import check, lib
+
+LHS, RHS = 0, 1
+INV64 = np.iinfo(np.int64).max
+INV32 = np.iinfo(np.int32).max
+
+_DEFAULTS = dict(time_end=1.0, cfl=0.2, cfl_viscous=0.4, gamma=1.4, Rspecific=287.058, T0=273.15, rho0=1.225,
+                 Minfty=0.1, ReInfty=100.0, Pr0=0.72, Sutherland0=110.4, diffusivity=1.0, T_ref=273.15)
+# hom3 property names -> desc fields
+_PROP_KEYS = {"timeEnd": "time_end", "CFL": "cfl", "CFL_viscous": "cfl_viscous", "gamma": "gamma",
+              "Rspecific": "Rspecific", "T0": "T0", "rho0": "rho0", "Minfty": "Minfty", "ReInfty": "ReInfty",
+              "Pr0": "Pr0", "Sutherland0": "Sutherland0", "diffusivity": "diffusivity", "T_ref": "T_ref"}
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _lp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+# ---------------------------------------------------------------------------
+# geometry (geometry/implicit.hpp:39-205) and conditions
+# ---------------------------------------------------------------------------
+def _sdf(kind, p, inverted=False) -> F.Sdf:
+    s = F.Sdf()
+    s.kind = kind
+    s.inverted = int(bool(inverted))
+    for i, v in enumerate(p):
+        s.p[i] = float(v)
+    return s
+
+
+def _pad3(v):
+    v = list(v)
+    return v + [0.0] * (3 - len(v))
+
+
+def edge(point, normal) -> F.Sdf:
+    return _sdf(F.SDF_EDGE, _pad3(point) + _pad3(normal))
+
+
+def square(center, lengths, inverted=False) -> F.Sdf:
+    return _sdf(F.SDF_SQUARE, _pad3(center) + _pad3(lengths), inverted)
+
+
+def sphere(center, radius, inverted=False) -> F.Sdf:
+    return _sdf(F.SDF_SPHERE, _pad3(center) + [radius], inverted)
+
+
+def make_cube(x_center, dims, cell_length, tol=0.6):
+    """geometry/implicit.hpp:182-205: cube, cube grown by one cell, inverted cube shrunk by tol cells."""
+    return (square(x_center, dims), square(x_center, [d + cell_length for d in dims]),
+            square(x_center, [d - tol * cell_length for d in dims], inverted=True))
+
+
+@dataclass
+class Condition:
+    kind: int
+    values: Sequence[float] = ()
+
+    def to_c(self) -> F.Bc:
+        b = F.Bc()
+        b.kind = self.kind
+        for i, v in enumerate(self.values):
+            b.v[i] = float(v)
+        return b
+
+
+def euler_neumann(flux=()):
+    return Condition(F.BC_EULER_NEUMANN, flux)
+
+
+def euler_dirichlet(state):
+    return Condition(F.BC_EULER_DIRICHLET, state)
+
+
+def euler_vortex():
+    return Condition(F.BC_EULER_VORTEX)
+
+
+def cns_inflow(pv):
+    return Condition(F.BC_CNS_INFLOW, pv)
+
+
+def cns_outflow(pv):
+    return Condition(F.BC_CNS_OUTFLOW, pv)
+
+
+def cns_adiabatic_noslip():
+    return Condition(F.BC_CNS_ADIABATIC_NOSLIP)
+
+
+def cns_adiabatic_slip():
+    return Condition(F.BC_CNS_ADIABATIC_SLIP)
+
+
+def cns_isothermal_noslip(T):
+    return Condition(F.BC_CNS_ISOTHERMAL_NOSLIP, [T])
+
+
+def heat_dirichlet(T):
+    return Condition(F.BC_HEAT_DIRICHLET, [T])
+
+
+def heat_neumann(q):
+    return Condition(F.BC_HEAT_NEUMANN, [q])
+
+
+# ---------------------------------------------------------------------------
+# thin solver over the ABI
+# ---------------------------------------------------------------------------
+class Solver:
+    """One h3c solver: tables in the caller's numbering, state columns [nv, n_cells]."""
+
+    def __init__(self, nd=2, physics=F.EULER, flux=F.FLUX_AUSM, time_integration=F.EULER_FORWARD,
+                 precision=F.FP64, **props):
+        d = F.Desc()
+        d.nd, d.physics, d.flux, d.time_integration, d.precision = nd, physics, flux, time_integration, precision
+        vals = dict(_DEFAULTS)
+        for k, v in props.items():
+            vals[_PROP_KEYS.get(k, k)] = v
+        for k, v in vals.items():
+            setattr(d, k, float(v))
+        self.desc = d
+        self.nd, self.physics = nd, physics
+        self.nv = 1 if physics == F.HEAT else nd + 2
+        h = C.c_void_p()
+        check(lib().h3c_create(C.byref(d), C.byref(h)))
+        self.h = h
+        self.n_cells = 0
+        self.first_ghost = 0
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().h3c_destroy(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        return check(rc, self.h)
+
+    def set_grid(self, neighbors, x_center, length, bc_idx, first_ghost, conditions: Sequence[Condition],
+                 subface_cells=None):
+        nb = np.ascontiguousarray(neighbors, np.int64)
+        xc = np.ascontiguousarray(x_center, np.float64)
+        ln = np.ascontiguousarray(length, np.float64)
+        bc = np.ascontiguousarray(bc_idx, np.int32)
+        n = ln.shape[0]
+        g = F.Grid()
+        g.n_cells, g.first_ghost, g.ld = n, int(first_ghost), n
+        g.neighbors, g.x_center, g.length = _lp(nb), _dp(xc), _dp(ln)
+        g.bc_idx = bc.ctypes.data_as(C.POINTER(C.c_int32))
+        arr = (F.Bc * max(1, len(conditions)))()
+        for i, c in enumerate(conditions):
+            arr[i] = c.to_c()
+        g.n_bcs, g.bcs = len(conditions), arr
+        if subface_cells is not None and len(subface_cells) and np.asarray(subface_cells).size:
+            sub = np.ascontiguousarray(subface_cells, np.int64)
+            g.n_subfaces = sub.shape[1]
+            g.subface_cells = _lp(sub)
+        self._check(lib().h3c_set_grid(self.h, C.byref(g)))
+        self.n_cells, self.first_ghost = n, int(first_ghost)
+
+    def set_state(self, q, which=LHS):
+        q = np.ascontiguousarray(q, np.float64)
+        assert q.shape == (self.nv, self.n_cells), q.shape
+        self._check(lib().h3c_set_state(self.h, which, _dp(q), self.n_cells))
+
+    def state(self, which=LHS, out=None) -> np.ndarray:
+        if out is None:
+            out = np.empty((self.nv, self.n_cells), np.float64)
+        assert out.shape == (self.nv, self.n_cells) and out.dtype == np.float64 and out.flags.c_contiguous
+        self._check(lib().h3c_get_state(self.h, which, _dp(out), self.n_cells))
+        return out
+
+    Q = state
+
+    def reset_time(self):
+        self._check(lib().h3c_reset_time(self.h))
+
+    def solve(self, nsteps=1):
+        self._check(lib().h3c_solve(self.h, nsteps))
+
+    def apply_bcs(self, which=LHS):
+        self._check(lib().h3c_apply_bcs(self.h, which))
+
+    def _get(self, fn, ctype=C.c_double):
+        v = ctype()
+        self._check(fn(self.h, C.byref(v)))
+        return v.value
+
+    def dt(self, value: Optional[float] = None):
+        """dt() reads, dt(value) forces the next step's dt (solver.hpp:112-115)."""
+        if value is not None:
+            self._check(lib().h3c_force_dt(self.h, float(value)))
+            return None
+        return self._get(lib().h3c_dt)
+
+    def force_dt(self, value):
+        self._check(lib().h3c_force_dt(self.h, float(value)))
+
+    def min_dt(self):
+        return self._get(lib().h3c_min_dt)
+
+    def time(self):
+        return self._get(lib().h3c_time)
+
+    def step(self):
+        return self._get(lib().h3c_step, C.c_int64)
+
+    def status(self):
+        return self._get(lib().h3c_status, C.c_int)
+
+    def stream(self):
+        v = C.c_void_p()
+        self._check(lib().h3c_get_stream(self.h, C.byref(v)))
+        return v.value
+
+    def device_state(self, which=LHS):
+        ptr = C.POINTER(C.c_double)()
+        ld = C.c_int64()
+        self._check(lib().h3c_state_device(self.h, which, C.byref(ptr), C.byref(ld)))
+        return C.cast(ptr, C.c_void_p).value, ld.value
+
+    def device_order(self):
+        out = np.empty(self.n_cells, np.int64)
+        self._check(lib().h3c_device_order(self.h, _lp(out)))
+        return out
+
+    def launches(self):
+        return self._get(lib().h3c_launches, C.c_int64)
+
+    def profile(self, enable=True):
+        self._check(lib().h3c_profile(self.h, int(enable)))
+
+    def profile_read(self) -> dict:
+        n = len(F.KERNEL_KINDS)
+        ms = np.zeros(n)
+        cnt = np.zeros(n, np.int64)
+        self._check(lib().h3c_profile_read(self.h, _dp(ms), _lp(cnt), n))
+        return {k: (float(ms[i]), int(cnt[i])) for i, k in enumerate(F.KERNEL_KINDS) if cnt[i]}
+
+    def set_partner(self, other: "Solver", partner_cells):
+        pc = np.ascontiguousarray(partner_cells, np.int64)
+        self._check(lib().h3c_set_partner(self.h, other.h, _lp(pc)))
+
+    def set_periodic(self, partner_cells):
+        pc = np.ascontiguousarray(partner_cells, np.int64)
+        self._check(lib().h3c_set_periodic(self.h, _lp(pc)))
+
+
+def couple_cht(Tr0, cns: Solver, heat: Solver):
+    """coupling::apply(Tr0, cns, heat) -- coupling.hpp:167-183."""
+    check(lib().h3c_couple_cht(cns.h, heat.h, float(Tr0)), cns.h)
+
+
+def couple_equal(a: Solver, b: Solver):
+    """coupling::apply(s1, s2) -- coupling.hpp:186-193."""
+    check(lib().h3c_couple_equal(a.h, b.h), a.h)
+
+
+# ---------------------------------------------------------------------------
+# grids from the library's builder
+# ---------------------------------------------------------------------------
+@dataclass
+class GridSpec:
+    """hom3 grid properties: root cell and MinLevel level (grid/helpers.hpp:163-179).
+    refine: EXTENSION (not in hom3) -- [(center, radius, level), ...] spheres."""
+    nd: int
+    xmin: Sequence[float]
+    xmax: Sequence[float]
+    level: int
+    refine: Sequence = ()
+
+    def desc(self, domain=None, domain_kind=0, bc_geoms=()) -> F.GridDesc:
+        d = F.GridDesc()
+        d.nd = self.nd
+        for i in range(self.nd):
+            d.xmin[i], d.xmax[i] = self.xmin[i], self.xmax[i]
+        d.min_level = self.level
+        d.n_refine = len(self.refine)
+        for k, (c, r, lvl) in enumerate(self.refine):
+            for i, v in enumerate(c):
+                d.refine_center[k][i] = v
+            d.refine_radius[k] = r
+            d.refine_level[k] = lvl
+        d.domain_kind = domain_kind
+        if domain is not None:
+            d.domain = domain
+        d.n_bcs = len(bc_geoms)
+        for i, g in enumerate(bc_geoms):
+            d.bc_geom[i] = g
+        return d
+
+    def cube_boundaries(self):
+        arr = (F.Sdf * 6)()
+        n = lib().h3c_cube_boundaries(C.byref(self.desc()), arr)
+        if n < 0:
+            check(n)
+        return [arr[i] for i in range(n)]
+
+    @property
+    def root_length(self):
+        return max(self.xmax[i] - self.xmin[i] for i in range(self.nd))
+
+    def cell_length_at_level(self, level):
+        return self.root_length / 2.0 ** level
+
+
+def build_tables(spec: GridSpec, bc_geoms, domain=None, domain_kind=0) -> dict:
+    """Run the library's grid builder and copy its tables out as numpy arrays."""
+    h = C.c_void_p()
+    check(lib().h3c_grid_build(C.byref(spec.desc(domain, domain_kind, bc_geoms)), C.byref(h)))
+    try:
+        v = F.Grid()
+        check(lib().h3c_grid_view(h, C.byref(v)))
+        n, nd = v.n_cells, spec.nd
+        nb = np.ctypeslib.as_array(v.neighbors, shape=(2 * nd * n,)).reshape(2 * nd, n).copy()
+        xc = np.ctypeslib.as_array(v.x_center, shape=(nd * n,)).reshape(nd, n).copy()
+        ln = np.ctypeslib.as_array(v.length, shape=(n,)).copy()
+        bc = np.ctypeslib.as_array(v.bc_idx, shape=(n,)).copy()
+        sub = None
+        if v.n_subfaces > 0:
+            k = 1 << (nd - 1)
+            sub = np.ctypeslib.as_array(v.subface_cells, shape=(k * v.n_subfaces,)).reshape(k, v.n_subfaces).copy()
+        return dict(neighbors=nb, x_center=xc, length=ln, bc_idx=bc, first_ghost=v.first_ghost, ncells=n,
+                    subface_cells=sub)
+    finally:
+        lib().h3c_grid_free(h)
+
+
+def cell_average(f: Callable, x_center: np.ndarray, length: np.ndarray, nd: int) -> np.ndarray:
+    """quadrature::integrate / volume (quadrature.hpp:43-74, solver.hpp:980-992):
+    mean of f over the 2^nd Gauss points (+-1/sqrt(3)), vectorised over cells."""
+    gp = 1 / math.sqrt(3)
+    acc = None
+    for k in range(1 << nd):
+        rel = np.array([(1.0 if (k >> d) & 1 else -1.0) * gp for d in range(nd)])[:, None]
+        x = x_center + (0.5 * length)[None, :] * rel
+        v = np.asarray(f(x), np.float64)
+        acc = v if acc is None else acc + v
+    vol = length.copy()
+    for _ in range(1, nd):
+        vol = length * vol
+    return acc * vol / float(1 << nd) / vol
+
+
+def periodic_partners(tables: dict, spec: GridSpec) -> np.ndarray:
+    """EXTENSION (not in hom3): for each ghost of a full-box uniform grid, the
+    interior cell on the opposite face (wrap-around)."""
+    nd, fg, n = spec.nd, tables["first_ghost"], tables["ncells"]
+    xc, ln = tables["x_center"], tables["length"]
+    lo = np.array([spec.xmin[i] for i in range(nd)])
+    L = spec.root_length
+    h = ln[:fg].min()
+    idx = np.floor((xc[:, :fg] - lo[:, None]) / h).astype(np.int64)
+    m = int(round(L / h))
+    key = {tuple(idx[:, i]): i for i in range(fg)}
+    out = np.full(n - fg, -1, np.int64)
+    gi = np.floor((xc[:, fg:] - lo[:, None]) / h).astype(np.int64) % m
+    for j in range(n - fg):
+        out[j] = key.get(tuple(gi[:, j]), -1)
+    return out
+
+
+def partner_cells(tables_self: dict, tables_other: dict) -> np.ndarray:
+    """Coupling partners (coupling.hpp:24-39): the other solver's cell whose
+    centre is the ghost's position (both grids from the same root and level)."""
+    fg, n = tables_self["first_ghost"], tables_self["ncells"]
+    xo = tables_other["x_center"][:, : tables_other["first_ghost"]]
+    key = {tuple(np.round(xo[:, i], 12)): i for i in range(xo.shape[1])}
+    xs = tables_self["x_center"][:, fg:]
+    out = np.full(n - fg, -1, np.int64)
+    for j in range(n - fg):
+        out[j] = key.get(tuple(np.round(xs[:, j], 12)), -1)
+    return out
+
+
+class FvSolver(Solver):
+    """hom3-style solver: properties, initial condition, boundary conditions,
+    initialize(), solve() (solver.hpp:88-145)."""
+
+    def __init__(self, grid: GridSpec, properties: dict, physics=F.EULER, flux=F.FLUX_AUSM,
+                 time_integration=F.EULER_FORWARD, precision=F.FP64):
+        props = {k: v for k, v in properties.items() if k not in ("initialDomain", "initialCondition")}
+        super().__init__(grid.nd, physics, flux, time_integration, precision, **props)
+        self.grid = grid
+        self.initial_domain = properties.get("initialDomain", (None, 0))
+        self.initial_condition = properties.get("initialCondition")
+        self.bcs: list = []
+        self.tables: Optional[dict] = None
+
+    def set_initial_condition(self, f: Callable):
+        self.initial_condition = f
+
+    def append_bc(self, geometry: F.Sdf, condition: Condition):
+        self.bcs.append((geometry, condition))
+
+    def append_bcs(self, pairs):
+        for g, c in pairs:
+            self.append_bc(g, c)
+
+    def initialize(self):
+        dom, kind = self.initial_domain
+        t = build_tables(self.grid, [g for g, _ in self.bcs], dom, kind)
+        self.tables = t
+        self.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
+                      [c for _, c in self.bcs], t["subface_cells"])
+        q = np.zeros((self.nv, t["ncells"]))
+        fg = t["first_ghost"]
+        if self.initial_condition is not None:
+            q[:, :fg] = cell_average(self.initial_condition, t["x_center"][:, :fg], t["length"][:fg], self.nd)
+        self.set_state(q, LHS)
+        self.reset_time()

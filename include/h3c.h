@@ -1,0 +1,252 @@
+/* h3c.h -- C ABI of hom3_b200, the B200 (sm_100a) finite-volume hot path that
+ * drops in for hom3's Solver::solve().
+ *
+ * hom3 (gnzlbg/hom3) is a header-only C++ library whose plugin interface is
+ * compile-time (CRTP physics plugins, type-erased boundary conditions).  The
+ * entry points below are what a hom3 maintainer binds from C++ to move the
+ * step onto the GPU: the solver keeps building its grid and ghost cells on the
+ * host (Solver::initialize, src/solver/fv/solver.hpp:133-138) and hands the
+ * resulting cell tables to h3c_set_grid; Solver::solve() (solver.hpp:140-145)
+ * becomes h3c_solve.  Every entry point names the hom3 interface it replaces.
+ *
+ * Conventions
+ *  - Every function returns 0 on success or a negative H3C_E* code; the
+ *    message is available from h3c_last_error().  Nothing here exits.
+ *  - Cell numbering at this boundary is the caller's (hom3's container order:
+ *    internal cells [0, first_ghost), ghost cells [first_ghost, n_cells)
+ *    sorted by bc id, container.hpp:58-66, solver.hpp:811-834).  Internally
+ *    cells are renumbered along a Morton space-filling curve.
+ *  - State arrays are column-major (n x nv with leading dimension ld), the
+ *    layout of hom3's lhs/rhs Eigen columns (container.hpp:59-60).
+ *  - A solver owns all of its device memory and runs on its own CUDA stream;
+ *    coupled solvers share one stream (h3c_set_partner).  One handle must not
+ *    be used from two host threads at once.
+ */
+#ifndef H3C_H_
+#define H3C_H_
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define H3C_ABI_VERSION 1
+
+/* error codes */
+#define H3C_OK 0
+#define H3C_E_INVALID (-1)   /* invalid argument or inconsistent tables */
+#define H3C_E_CUDA (-2)      /* CUDA runtime error */
+#define H3C_E_NONFINITE (-3) /* dt or state became non-finite / non-positive */
+#define H3C_E_STATE (-4)     /* call made in the wrong state (e.g. no grid yet) */
+#define H3C_E_TIMEOUT (-5)   /* a bounded device wait ran out */
+#define H3C_E_NOMEM (-6)     /* device allocation failed */
+
+/* physics: euler/physics.hpp:25, cns/physics.hpp:27, heat/physics.hpp:21 */
+#define H3C_EULER 0
+#define H3C_CNS 1
+#define H3C_HEAT 2
+/* numerical flux tags: euler/tags.hpp:13-16 (AUSM, LLF); cns/tags.hpp:29
+ * (standard = AUSM + three-point viscous, selected by H3C_CNS + AUSM);
+ * heat/tags.hpp:13 (three_point, the only heat flux). */
+#define H3C_FLUX_AUSM 0
+#define H3C_FLUX_LLF 1
+/* time integration tags: solver/fv/tags.hpp:24-25 */
+#define H3C_EULER_FORWARD 0
+#define H3C_RUNGE_KUTTA_2 1
+/* arithmetic of the face fluxes (the state, residual and dt stay FP64) */
+#define H3C_FP64 0
+#define H3C_MIXED 1 /* FP32 reconstruction + face flux, FP64 update */
+
+/* Boundary / coupling conditions.  Values v[] per kind:
+ *  EULER_NEUMANN      surface flux per variable (euler/boundary_conditions.hpp:17-43)
+ *  EULER_DIRICHLET    surface state per variable (:47-67)
+ *  EULER_VORTEX       none; analytic isentropic vortex, overwrites the
+ *                     boundary cell too (:71-93, initial_conditions.hpp:343-368)
+ *  CNS_INFLOW         surface primitive state (u_0..u_{nd-1}, rho, p); u and
+ *                     rho imposed, zero normal pressure gradient (cns/boundary_conditions.hpp:28-65)
+ *  CNS_OUTFLOW        same layout, only p is used (:72-105)
+ *  CNS_ADIABATIC_NOSLIP / CNS_ADIABATIC_SLIP   none (:117-193)
+ *  CNS_ISOTHERMAL_NOSLIP  v[0] = wall temperature (:200-238)
+ *  HEAT_DIRICHLET     v[0] = surface temperature (heat/boundary_conditions.hpp:15-37)
+ *  HEAT_NEUMANN       v[0] = surface heat flux (:40-63)
+ *  CPL_*              coupling with the partner solver (h3c_set_partner):
+ *                     euler/coupling_conditions.hpp:17-35, cns/coupling_conditions.hpp:22-43,
+ *                     heat/coupling_conditions.hpp:18-61 */
+#define H3C_BC_EULER_NEUMANN 0
+#define H3C_BC_EULER_DIRICHLET 1
+#define H3C_BC_EULER_VORTEX 2
+#define H3C_BC_CNS_INFLOW 3
+#define H3C_BC_CNS_OUTFLOW 4
+#define H3C_BC_CNS_ADIABATIC_NOSLIP 5
+#define H3C_BC_CNS_ADIABATIC_SLIP 6
+#define H3C_BC_CNS_ISOTHERMAL_NOSLIP 7
+#define H3C_BC_HEAT_DIRICHLET 8
+#define H3C_BC_HEAT_NEUMANN 9
+#define H3C_BC_CPL_EULER_EULER 10
+#define H3C_BC_CPL_CNS_HEAT 11
+#define H3C_BC_CPL_HEAT_CNS 12
+#define H3C_BC_CPL_HEAT_HEAT 13
+/* EXTENSION (not in hom3): periodic pairing of opposite cube faces; the
+ * caller supplies the partner cell of each ghost through h3c_set_periodic. */
+#define H3C_BC_PERIODIC 14
+
+typedef struct h3c_solver_s* h3c_solver;
+
+/* Solver properties: the io::Properties keys hom3 reads on this path
+ * (solver.hpp:88-95,870; euler/physics.hpp:39-42; euler/quantities.hpp:23-29;
+ *  cns/physics.hpp:57-61; cns/quantities.hpp:23-30; heat/physics.hpp:36-39). */
+typedef struct {
+  int nd;               /* 2 or 3 */
+  int physics;          /* H3C_EULER / H3C_CNS / H3C_HEAT */
+  int flux;             /* H3C_FLUX_* */
+  int time_integration; /* H3C_EULER_FORWARD / H3C_RUNGE_KUTTA_2 */
+  int precision;        /* H3C_FP64 / H3C_MIXED */
+  double time_end;      /* "timeEnd" */
+  double cfl;           /* "CFL" */
+  double cfl_viscous;   /* "CFL_viscous" */
+  double gamma;         /* "gamma" */
+  double Rspecific;     /* "Rspecific" [J/(kg K)] */
+  double T0;            /* "T0" [K] */
+  double rho0;          /* "rho0" [kg/m^3] */
+  double Minfty;        /* "Minfty" */
+  double ReInfty;       /* "ReInfty" */
+  double Pr0;           /* "Pr0" */
+  double Sutherland0;   /* "Sutherland0" [K] */
+  double diffusivity;   /* "diffusivity" [m^2/s] (heat; does not enter the step) */
+  double T_ref;         /* "T_ref" [K] (heat; does not enter the step) */
+} h3c_desc;
+
+typedef struct {
+  int kind;     /* H3C_BC_* */
+  double v[8];  /* parameters, see above */
+} h3c_bc;
+
+/* The solver's cell container after Solver::initialize (container.hpp:58-66,
+ * solver.hpp:876-977).  Column-major arrays with leading dimension ld >= n_cells. */
+typedef struct {
+  int64_t n_cells;           /* cells().size(): internal + ghost */
+  int64_t first_ghost;       /* firstGC_ */
+  int64_t ld;                /* leading dimension of neighbors / x_center */
+  const int64_t* neighbors;  /* [2nd][ld]; no neighbour: any value outside [0, n_cells) */
+  const double* x_center;    /* [nd][ld] cell centres */
+  const double* length;      /* [n_cells] cell lengths */
+  const int32_t* bc_idx;     /* [n_cells] bc index of ghosts; internal cells: any value < 0 or >= n_bcs */
+  int n_bcs;                 /* number of appended boundary conditions, <= 64 */
+  const h3c_bc* bcs;         /* [n_bcs] in append_bc order (solver.hpp:159-169) */
+  /* EXTENSION (not in hom3, whose solver links same-level neighbours only,
+   * solver.hpp:899-908): coarse/fine faces of 2:1 balanced trees.  A
+   * neighbour entry v <= -2 names sub-face group k = -v - 2 whose 2^(nd-1)
+   * finer cells are subface_cells[j * n_subfaces + k] (j in increasing child
+   * position); a coarser neighbour is stored as a plain cell index.  Face
+   * fluxes through a group are area-weighted by 2^-(nd-1).  Zero / NULL for
+   * hom3 grids. */
+  int64_t n_subfaces;
+  const int64_t* subface_cells;
+} h3c_grid;
+
+/* ---- lifecycle: Solver(SolverIdx, io::Properties), solver.hpp:88-95 ---- */
+int h3c_create(const h3c_desc* desc, h3c_solver* out);
+int h3c_destroy(h3c_solver s);
+/* Copies the message of the last error on this solver (or a global one when
+ * s is NULL) into buf and returns its full length. */
+int h3c_last_error(h3c_solver s, char* buf, size_t n);
+
+/* ---- data: the tables create_local_cells/create_ghost_cells build
+ * (solver.hpp:876-977) and the state columns lhs/rhs (container.hpp:59-60) ---- */
+int h3c_set_grid(h3c_solver s, const h3c_grid* grid);
+/* which: 0 = lhs, 1 = rhs.  Host arrays, caller numbering, [nv][ld]. */
+int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld);
+int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld);
+/* Device-resident state in the internal (Morton) numbering: pointer, leading
+ * dimension and the internal index of every caller cell (perm[caller] = internal). */
+int h3c_state_device(h3c_solver s, int which, double** ptr, int64_t* ld);
+int h3c_device_order(h3c_solver s, int64_t* perm);
+int h3c_get_stream(h3c_solver s, void** stream);
+int h3c_sizes(h3c_solver s, int64_t* n_cells, int64_t* first_ghost, int* nv);
+
+/* ---- stepping: Solver::solve (solver.hpp:140-145), n times.  The step runs
+ * on the solver's stream and returns without waiting for it. ---- */
+int h3c_solve(h3c_solver s, int64_t nsteps);
+/* Solver::initialize's final set_dt (solver.hpp:137, 541-551): computes dt
+ * from the current lhs with time = 0, dt = 0. */
+int h3c_reset_time(h3c_solver s);
+/* Solver::apply_bcs on lhs (0) or rhs (1) (solver.hpp:561-586). */
+int h3c_apply_bcs(h3c_solver s, int which);
+/* Solver::min_dt (solver.hpp:109, 511-517): synchronous. */
+int h3c_min_dt(h3c_solver s, double* dt);
+/* Solver::dt() / dt(Num) (solver.hpp:112-115, 522-525). */
+int h3c_dt(h3c_solver s, double* dt);
+int h3c_force_dt(h3c_solver s, double dt);
+int h3c_time(h3c_solver s, double* t);
+int h3c_step(h3c_solver s, int64_t* step);
+/* Non-finite / non-positive dt seen by the device since the last call
+ * (utilities.hpp:74-76 checks dt in [1e-300, 1e300]); clears the flag. */
+int h3c_status(h3c_solver s, int* flags);
+
+/* ---- instrumentation (no hom3 counterpart: hom3 has no timers) ----
+ * h3c_launches: kernels this solver has launched since creation.
+ * h3c_profile(s, 1): bracket every subsequent launch with CUDA events on the
+ * solver's stream; h3c_profile_read sums the elapsed times per kernel kind
+ * (0 boundary conditions, 1 CFL reduction, 2 scalar step bookkeeping,
+ * 3 first stage / forward Euler, 4 second RK stage, 5 slopes) and resets. */
+int h3c_launches(h3c_solver s, int64_t* n);
+int h3c_profile(h3c_solver s, int enable);
+int h3c_profile_read(h3c_solver s, double* ms, int64_t* count, int nkinds);
+
+/* ---- coupling: coupling.hpp:24-73 ----
+ * partner_cells[g - first_ghost] = the partner solver's cell (caller
+ * numbering of the partner) that local_bndry_ids (coupling.hpp:24-39) finds
+ * for ghost g, or any negative value for ghosts of non-coupled conditions.
+ * Both solvers then share the partner's stream. */
+int h3c_set_partner(h3c_solver s, h3c_solver partner, const int64_t* partner_cells);
+/* coupling::apply(Tr0, cns, heat), coupling.hpp:167-183 */
+int h3c_couple_cht(h3c_solver cns, h3c_solver heat, double Tr0);
+/* coupling::apply(s1, s2), coupling.hpp:186-193 */
+int h3c_couple_equal(h3c_solver a, h3c_solver b);
+/* EXTENSION (not in hom3): partner cells (caller numbering, same solver) for
+ * the ghosts of H3C_BC_PERIODIC conditions. */
+int h3c_set_periodic(h3c_solver s, const int64_t* partner_cells);
+
+/* ---- grid builder (the device grid layer): builds hom3-equivalent tables
+ * for the MinLevel generator (grid/generation.hpp:355-376) and cube /
+ * box boundaries (grid/helpers.hpp:112-160, geometry/implicit.hpp:39-205),
+ * with leaves in Morton order.  EXTENSION (not in hom3): refinement of the
+ * cells that intersect spheres, 2:1 balanced, with coarse/fine faces. ---- */
+#define H3C_SDF_NONE 0
+#define H3C_SDF_EDGE 1   /* p = point[3], normal[3] */
+#define H3C_SDF_SQUARE 2 /* p = center[3], lengths[3] */
+#define H3C_SDF_SPHERE 3 /* p = center[3], radius */
+typedef struct {
+  int kind;
+  int inverted;
+  double p[6];
+} h3c_sdf;
+
+typedef struct {
+  int nd;
+  double xmin[3], xmax[3]; /* root cell (grid/grid.hpp:106-139) */
+  int min_level;           /* MinLevel "level" */
+  int n_refine;            /* EXTENSION: spheres refined to refine_level */
+  double refine_center[4][3];
+  double refine_radius[4];
+  int refine_level[4];
+  int domain_kind;         /* 0 all leaves, 1 leaves with sdf > 0, 2 with sdf < 0 */
+  h3c_sdf domain;          /* "initialDomain" predicate */
+  int n_bcs;               /* boundaries in append order */
+  h3c_sdf bc_geom[16];
+} h3c_grid_desc;
+
+typedef struct h3c_built_grid_s* h3c_built_grid;
+int h3c_grid_build(const h3c_grid_desc* desc, h3c_built_grid* out);
+/* Table views valid until h3c_grid_free; the layout is that of h3c_grid. */
+int h3c_grid_view(h3c_built_grid g, h3c_grid* view);
+/* cube faces of the root cell in hom3's order left,right,bottom,top,front,back;
+ * returns their number (2nd) or a negative error code */
+int h3c_cube_boundaries(const h3c_grid_desc* desc, h3c_sdf* out);
+int h3c_grid_free(h3c_built_grid g);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* H3C_H_ */

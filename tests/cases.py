@@ -1,0 +1,185 @@
+"""Test cases mirroring hom3's own solver tests, built in the oracle.
+
+Each builder returns (world, [solvers]) after initialize().  Cases follow
+src/solver/fv/euler/tests/euler_fv_solver_test.cpp, cns/tests/cns_fv_solver_test.cpp,
+heat/tests/heat_fv_solver_test.cpp, tests/coupled_cns_heat_test.cpp and
+euler/tests/coupled_euler_euler_test.cpp, at reduced refinement levels where
+noted so the oracle finishes in seconds.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from oracle import h3o  # noqa: E402
+
+EULER_PROPS = dict(gamma=1.4, Minfty=0.1, cfl=0.2, Rspecific=287.058, T0=273.15, rho0=1.225)
+SOD = [0, 0, 0.3, 1.0, 0.75, 1.0, 0.125, 0.0, 0.1]
+P123 = [0, 0, 0.5, 1.0, -2.0, 0.4, 1.0, 2.0, 0.4]
+
+
+def neumann_cube(w):
+    return [h3o.bc(h3o.BC_EULER_NEUMANN, g) for g in w.cube_boundaries()]
+
+
+def euler_case(name, nd=3, level=4, ti=h3o.EULER_FORWARD, flux=h3o.AUSM):
+    """euler_fv_solver_test.cpp:85-286 (3D cases at level 4 instead of 5)."""
+    if name == "vortex":
+        w = h3o.World(2, [-8, -8], [8, 8], level=level)
+        bcs = [h3o.bc(h3o.BC_EULER_VORTEX, g) for g in w.cube_boundaries()]
+        s = w.add_solver(h3o.EULER, flux, ti, bcs=bcs, ic_kind=h3o.IC_VORTEX, time_end=2.0, **EULER_PROPS)
+    else:
+        lo, hi = [0.0] * nd, [1.0] * nd
+        w = h3o.World(nd, lo, hi, level=level)
+        if name == "constant":
+            ic_kind, ic, tend = h3o.IC_CONSTANT_PV, [0.5] * nd + [1.0, 1.0], 0.25
+        elif name == "sod":
+            ic_kind, ic, tend = h3o.IC_SHOCK_TUBE, SOD, 0.2
+        elif name == "p123":
+            ic_kind, ic, tend = h3o.IC_SHOCK_TUBE, P123, 0.15
+        elif name == "explosion":
+            ic_kind, ic, tend = h3o.IC_EXPLOSION, [0.5, 0.5, 0.5, 0.2, 1.0, 1.0, 0.125, 0.1], 0.25
+        else:
+            raise KeyError(name)
+        s = w.add_solver(h3o.EULER, flux, ti, bcs=neumann_cube(w), ic_kind=ic_kind, ic=ic, time_end=tend,
+                         **EULER_PROPS)
+    s.initialize()
+    return w, [s]
+
+
+def euler_dirichlet_case(nd=2, level=5, ti=h3o.EULER_FORWARD):
+    """Dirichlet / non-zero Neumann conditions (euler/boundary_conditions.hpp:17-67)."""
+    w = h3o.World(nd, [0.0] * nd, [1.0] * nd, level=level)
+    g = w.cube_boundaries()
+    state = [0.1, 0.0, 1.0, 2.5] if nd == 2 else [0.1, 0.0, 0.0, 1.0, 2.5]
+    flux = [0.01 * (i + 1) for i in range(nd + 2)]
+    bcs = [h3o.bc(h3o.BC_EULER_DIRICHLET, g[0], state), h3o.bc(h3o.BC_EULER_NEUMANN, g[1], flux)]
+    bcs += [h3o.bc(h3o.BC_EULER_NEUMANN, x) for x in g[2:]]
+    s = w.add_solver(h3o.EULER, h3o.AUSM, ti, bcs=bcs, ic_kind=h3o.IC_SHOCK_TUBE, ic=SOD, time_end=0.2,
+                     **EULER_PROPS)
+    s.initialize()
+    return w, [s]
+
+
+CNS_PROPS = dict(gamma=1.4, cfl=0.4, cfl_viscous=0.4, Rspecific=287.058, T0=273.15, rho0=1.225, Pr0=0.72,
+                 Sutherland0=110.4)
+
+
+def cns_case(name, level=6, ti=h3o.EULER_FORWARD):
+    """cns_fv_solver_test.cpp:345-536 (level 6 instead of 8 for constant/sod)."""
+    if name in ("constant", "sod"):
+        w = h3o.World(2, [0, 0], [1, 1], level=level)
+        probe = w.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=neumann_cube(w), ic_kind=h3o.IC_CONSTANT_PV,
+                             ic=[0, 0, 1, 1], Minfty=0.1, ReInfty=100.0, time_end=0.25, **CNS_PROPS)
+        q = probe.quantities()
+        w = h3o.World(2, [0, 0], [1, 1], level=level)
+        if name == "constant":
+            s = w.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=neumann_cube(w), ic_kind=h3o.IC_CONSTANT_PV,
+                             ic=[q["u_inf"], 0.0, q["rho_inf"], q["p_inf"]], Minfty=0.1, ReInfty=100.0,
+                             time_end=0.25, **CNS_PROPS)
+        else:
+            ic = [0, 0, 0.3, 1.0 * q["rho_inf"], 0.75 * q["u_inf"], 1.0 * q["p_inf"], 0.125 * q["rho_inf"],
+                  0.0, 0.1 * q["p_inf"]]
+            s = w.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=neumann_cube(w), ic_kind=h3o.IC_SHOCK_TUBE, ic=ic,
+                             Minfty=0.1, ReInfty=1000.0, time_end=0.25, **CNS_PROPS)
+        s.initialize()
+        return w, [s]
+    if name in ("walls", "slip", "isothermal"):
+        # inflow / outflow + Neumann far field (cns_fv_solver_test.cpp:466-536 with the
+        # cube replaced by conditions on the cube faces so a small grid has all kinds)
+        w0 = h3o.World(2, [0, 0], [1, 1], level=level)
+        probe = w0.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=neumann_cube(w0), ic_kind=h3o.IC_CONSTANT_PV,
+                              ic=[0, 0, 1, 1], Minfty=0.2, ReInfty=200.0, **CNS_PROPS)
+        q = probe.quantities()
+        fs = [q["u_inf"], 0.0, q["rho_inf"], q["p_inf"]]
+        w = h3o.World(2, [0, 0], [1, 1], level=level)
+        g = w.cube_boundaries()
+        wall = {"walls": (h3o.BC_CNS_ADIABATIC_NOSLIP, []), "slip": (h3o.BC_CNS_ADIABATIC_SLIP, []),
+                "isothermal": (h3o.BC_CNS_ISOTHERMAL_NOSLIP, [1.05 * q["T_inf"]])}[name]
+        bcs = [h3o.bc(h3o.BC_CNS_INFLOW, g[0], fs), h3o.bc(h3o.BC_CNS_OUTFLOW, g[1], fs),
+               h3o.bc(wall[0], g[2], wall[1]), h3o.bc(h3o.BC_EULER_NEUMANN, g[3])]
+        ic = [0, 0, 0.5, 1.0 * q["rho_inf"], q["u_inf"], q["p_inf"], 0.9 * q["rho_inf"], q["u_inf"], q["p_inf"]]
+        s = w.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=bcs, ic_kind=h3o.IC_SHOCK_TUBE, ic=ic, Minfty=0.2,
+                         ReInfty=200.0, time_end=100.0, **CNS_PROPS)
+        s.initialize()
+        return w, [s]
+    raise KeyError(name)
+
+
+def heat_case(level=3, ti=h3o.EULER_FORWARD):
+    """heat_fv_solver_test.cpp:621-641 (level 3 instead of 4)."""
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=level)
+    g = w.cube_boundaries()
+    bcs = [h3o.bc(h3o.BC_HEAT_DIRICHLET, g[0], [1.0]), h3o.bc(h3o.BC_HEAT_DIRICHLET, g[1], [1.0])]
+    bcs += [h3o.bc(h3o.BC_HEAT_NEUMANN, x, [0.0]) for x in g[2:]]
+    s = w.add_solver(h3o.HEAT, 0, ti, bcs=bcs, ic_kind=h3o.IC_CONSTANT_CV, ic=[0.0], cfl=0.5, time_end=0.25)
+    s.initialize()
+    return w, [s]
+
+
+def cht_case(level=8):
+    """coupled_cns_heat_test.cpp:56-248: CNS (solver 0) around a heat-conducting cube (solver 1)."""
+    lo, hi = [-7.0, -7.0], [7.0, 7.0]
+    w = h3o.World(2, lo, hi, level=level, max_solvers=2)
+    h = w.cell_length_at_level(level)
+    c0, c1, c2 = h3o.make_cube(2, [-3.0, 0.0], [1.0, 1.0], h)
+    probe_w = h3o.World(2, lo, hi, level=1)
+    probe = probe_w.add_solver(h3o.CNS, h3o.AUSM, h3o.EULER_FORWARD, bcs=neumann_cube(probe_w),
+                               Minfty=0.2, ReInfty=100.0, **CNS_PROPS)
+    q = probe.quantities()
+    fs = [q["u_inf"], 0.0, q["rho_inf"], q["p_inf"]]
+    g = w.cube_boundaries()
+    cns_bcs = [h3o.bc(h3o.BC_CNS_INFLOW, g[0], fs), h3o.bc(h3o.BC_CNS_OUTFLOW, g[1], fs),
+               h3o.bc(h3o.BC_EULER_NEUMANN, g[2]), h3o.bc(h3o.BC_EULER_NEUMANN, g[3]),
+               h3o.bc(h3o.BC_CPL_CNS_HEAT, c1, partner=1)]
+    cns = w.add_solver(h3o.CNS, h3o.AUSM, h3o.EULER_FORWARD, bcs=cns_bcs, domain=c0, domain_kind=1,
+                       ic_kind=h3o.IC_CONSTANT_PV, ic=fs, Minfty=0.2, ReInfty=100.0, time_end=10.0,
+                       **dict(CNS_PROPS, cfl=0.4))
+    heat = w.add_solver(h3o.HEAT, 0, h3o.EULER_FORWARD, bcs=[h3o.bc(h3o.BC_CPL_HEAT_CNS, c2, partner=0)],
+                        domain=c0, domain_kind=2, ic_kind=h3o.IC_CONSTANT_CV, ic=[q["T_inf"]], cfl=0.5,
+                        time_end=10.0)
+    heat.initialize()  # initialize(hgrid, heatSolver, cnsSolver): coupled_cns_heat_test.cpp:231
+    cns.initialize()
+    return w, [cns, heat]
+
+
+def euler_euler_case(level=4):
+    """coupled_euler_euler_test.cpp:94-163 (level 4 instead of 5)."""
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=level, max_solvers=2)
+    h = w.cell_length_at_level(level)
+    c0, c1, c2 = h3o.make_cube(3, [0.5, 0.5, 0.5], [0.2, 0.2, 0.2], h, tol=0.5)
+    props = dict(EULER_PROPS, Minfty=0.2)
+    s0 = w.add_solver(h3o.EULER, h3o.AUSM, h3o.EULER_FORWARD,
+                      bcs=neumann_cube(w) + [h3o.bc(h3o.BC_CPL_EULER_EULER, c1, partner=1)],
+                      domain=c0, domain_kind=1, ic_kind=h3o.IC_SHOCK_TUBE, ic=SOD, time_end=0.25, **props)
+    s1 = w.add_solver(h3o.EULER, h3o.AUSM, h3o.EULER_FORWARD,
+                      bcs=[h3o.bc(h3o.BC_CPL_EULER_EULER, c2, partner=0)],
+                      domain=c0, domain_kind=2, ic_kind=h3o.IC_SHOCK_TUBE, ic=SOD, time_end=0.25, **props)
+    s0.initialize()
+    s1.initialize()
+    return w, [s0, s1]
+
+
+# ---------------------------------------------------------------------------
+def gpu_solver_from_oracle(o: "h3o.Solver", precision=0):
+    """Hand the oracle's (hom3-numbered) tables and initial state to the C ABI:
+    the drop-in path a hom3 Solver would take after Solver::initialize."""
+    import hom3_b200 as hb
+    from hom3_b200.solver import Condition
+
+    info = o.info()
+    props = {k: info[k] for k in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty", "ReInfty",
+                                  "Pr0", "Sutherland0", "time_end")}
+    s = hb.Solver(info["nd"], info["physics"], info["flux"], info["ti"], precision, **props)
+    t = o.tables()
+    s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
+               [Condition(k, v) for k, v in info["bcs"]], t["subface_cells"])
+    s.set_state(o.state(0), 0)
+    s.reset_time()
+    return s

@@ -1,0 +1,169 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle.
+
+The oracle builds hom3's grid and initial state; its hom3-numbered tables and
+state go through h3c_set_grid / h3c_set_state exactly as a hom3 Solver would
+hand them over, and both sides then step.  Tolerances: FP64 path <= 1e-12
+relative per step, multi-step runs <= 1e-10 (rounding of
+FMA-contracted kernels against the oracle's uncontracted arithmetic compounds
+over steps); mixed path (FP32 face fluxes) <= 1e-5 relative per step.
+"""
+import numpy as np
+import pytest
+
+import cases
+from oracle import h3o
+
+pytestmark = pytest.mark.gpu
+
+TOL_STEP = 1e-12
+TOL_MULTI = 1e-10
+
+
+def rel_err(a, b):
+    """max over variables of max|a - b| / max|b|"""
+    r = 0.0
+    for v in range(b.shape[0]):
+        scale = max(np.abs(b[v]).max(), 1e-300)
+        r = max(r, np.abs(a[v] - b[v]).max() / scale)
+    return r
+
+
+def check_pair(o, g, tol, what=""):
+    fg = o.first_ghost
+    qo, qg = o.state(0)[:, :fg], g.state(0)[:, :fg]
+    assert np.isfinite(qg).all(), what
+    e = rel_err(qg, qo)
+    assert e <= tol, f"{what}: rel err {e:.3e} > {tol:.1e}"
+    assert abs(g.dt() - o.dt()) <= tol * abs(o.dt()) + 1e-300, (what, g.dt(), o.dt())
+    assert abs(g.time() - o.time()) <= tol * max(abs(o.time()), 1e-300) + 1e-300, (what, g.time(), o.time())
+    assert g.step() == o.step()
+    return e
+
+
+def run_single(o, nsteps=(1, 4), precision=0, tol_step=TOL_STEP, tol_multi=TOL_MULTI):
+    g = cases.gpu_solver_from_oracle(o, precision)
+    assert abs(g.dt() - o.dt()) <= tol_step * o.dt()  # initialize()'s set_dt
+    o.solve(nsteps[0])
+    g.solve(nsteps[0])
+    check_pair(o, g, tol_step, "first step")
+    o.solve(nsteps[1])
+    g.solve(nsteps[1])
+    return check_pair(o, g, tol_multi, f"after {sum(nsteps)} steps")
+
+
+@pytest.mark.parametrize("name", ["constant", "sod", "p123", "explosion"])
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
+def test_euler_3d(name, ti):
+    _, (o,) = cases.euler_case(name, nd=3, level=4, ti=ti)
+    run_single(o)
+
+
+@pytest.mark.parametrize("flux", [h3o.AUSM, h3o.LLF])
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
+def test_euler_vortex_2d(flux, ti):
+    _, (o,) = cases.euler_case("vortex", level=6, ti=ti, flux=flux)
+    run_single(o)
+
+
+def test_euler_llf_sod_3d():
+    _, (o,) = cases.euler_case("sod", nd=3, level=4, flux=h3o.LLF)
+    run_single(o)
+
+
+@pytest.mark.parametrize("nd", [2, 3])
+def test_euler_dirichlet_neumann_flux(nd):
+    _, (o,) = cases.euler_dirichlet_case(nd=nd, level=5 if nd == 2 else 4)
+    run_single(o)
+
+
+def test_euler_constant_state_preserved():
+    """euler_fv_solver_test.cpp:82-112: the solution is the initial condition for all t."""
+    _, (o,) = cases.euler_case("constant", nd=3, level=4)
+    g = cases.gpu_solver_from_oracle(o)
+    q0 = g.state(0)[:, : o.first_ghost]
+    g.solve(10)
+    assert np.array_equal(g.state(0)[:, : o.first_ghost], q0)
+
+
+@pytest.mark.parametrize("name", ["constant", "sod", "walls", "slip", "isothermal"])
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
+def test_cns_2d(name, ti):
+    _, (o,) = cases.cns_case(name, level=5, ti=ti)
+    run_single(o, nsteps=(1, 3))
+
+
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
+def test_heat_3d(ti):
+    _, (o,) = cases.heat_case(level=3, ti=ti)
+    run_single(o, nsteps=(1, 6))
+
+
+def test_mixed_precision_euler():
+    _, (o,) = cases.euler_case("sod", nd=3, level=4, ti=h3o.RK2)
+    run_single(o, precision=1, tol_step=1e-5, tol_multi=1e-4)
+
+
+def _coupled(solvers, couple):
+    import hom3_b200 as hb
+    gs = [cases.gpu_solver_from_oracle(o) for o in solvers]
+    for o, g, other in zip(solvers, gs, reversed(gs)):
+        g.set_partner(other, o.partner_cells())
+    return gs
+
+
+def test_cht_coupled():
+    """coupled_cns_heat_test.cpp:235-248: coupling::apply, cns.solve, heat.solve."""
+    import hom3_b200 as hb
+    _, (cns, heat) = cases.cht_case(level=7)
+    gc, gh = _coupled([cns, heat], None)
+    for it in range(3):
+        h3o.couple_cht(cns, heat, 0.01)
+        hb.couple_cht(0.01, gc, gh)
+        cns.solve(); gc.solve()
+        heat.solve(); gh.solve()
+        check_pair(cns, gc, TOL_STEP if it == 0 else TOL_MULTI, f"cns step {it}")
+        check_pair(heat, gh, TOL_STEP if it == 0 else TOL_MULTI, f"heat step {it}")
+
+
+def test_euler_euler_coupled():
+    """coupled_euler_euler_test.cpp:155-162."""
+    import hom3_b200 as hb
+    _, (a, b) = cases.euler_euler_case(level=4)
+    ga, gb = _coupled([a, b], None)
+    for it in range(3):
+        h3o.couple_equal(a, b)
+        hb.couple_equal(ga, gb)
+        a.solve(); ga.solve()
+        b.solve(); gb.solve()
+        check_pair(a, ga, TOL_STEP if it == 0 else TOL_MULTI, f"s0 step {it}")
+        check_pair(b, gb, TOL_STEP if it == 0 else TOL_MULTI, f"s1 step {it}")
+
+
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
+def test_refined_tree_extension(ti):
+    """EXTENSION (not in hom3): coarse/fine faces on a 2:1 balanced tree."""
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=3)
+    w.refine_sphere([0.5, 0.5, 0.5], 0.25, 5)
+    o = w.add_solver(h3o.EULER, h3o.AUSM, ti, bcs=cases.neumann_cube(w), ic_kind=h3o.IC_SHOCK_TUBE,
+                     ic=[0, 0, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1], time_end=1.0, cfl=0.4)
+    o.initialize()
+    run_single(o)
+
+
+def test_device_order_is_morton_identity_for_minlevel():
+    """A MinLevel grid's hom3 leaf order is already the Morton order."""
+    _, (o,) = cases.euler_case("sod", nd=3, level=3)
+    g = cases.gpu_solver_from_oracle(o)
+    perm = g.device_order()
+    assert np.array_equal(perm, np.arange(o.ncells))
+
+
+def test_invalid_tables_rejected():
+    import hom3_b200 as hb
+    _, (o,) = cases.euler_case("sod", nd=2, level=3)
+    t = o.tables()
+    s = hb.Solver(2)
+    nb = t["neighbors"].copy()
+    nb[0, 5] = -7  # an internal cell without neighbour
+    with pytest.raises(hb.H3cError):
+        s.set_grid(nb, t["x_center"], t["length"], t["bc_idx"], t["first_ghost"], [])
