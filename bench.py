@@ -71,6 +71,10 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        t0 = time.time()  # wait for the first sample so the timed region is covered
+        while time.time() - t0 < 5.0 and os.path.getsize(self.path) == 0:
+            time.sleep(0.05)
         return self
 
     def __exit__(self, *exc):
@@ -218,7 +222,7 @@ def workload_config(args, t):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -242,23 +246,24 @@ def main():
     # ---- device-resident timing ('value') ----
     s.set_state(q0, 0)
     s.reset_time()
-    s.solve(args.warmup)
-    torch.cuda.synchronize()
-    barrier(ws)
-    l0 = s.launches()
-    s.profile(True)
     with ClockSampler(local) as clk:
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.solve(args.warmup)
         torch.cuda.synchronize()
         barrier(ws)
+        l0 = s.launches()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(stream)
         s.solve(args.steps)
         ev1.record(stream)
         torch.cuda.synchronize()
         ms = ev0.elapsed_time(ev1)
-    s.profile(False)
-    launches = s.launches() - l0
-    kern = s.profile_read()
+        launches = s.launches() - l0
+        # per-kernel durations: the same steps again with every launch bracketed by events
+        s.profile(True)
+        s.solve(min(args.steps, 100))
+        torch.cuda.synchronize()
+        s.profile(False)
+        kern = s.profile_read()
     barrier(ws)
     ms_max = allreduce_max(ms, ws)
     status = s.status()

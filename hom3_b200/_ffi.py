@@ -22,6 +22,7 @@ FP64, MIXED = 0, 1
  BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT,
  BC_PERIODIC) = range(15)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
+OPT_TILE_KERNEL, OPT_GRAPHS = 1, 2
 KERNEL_KINDS = ("bc", "cfl", "scalar", "stage1", "stage2", "slopes", "copy", "other")
 
 
@@ -82,6 +83,7 @@ SIGNATURES = {
     "h3c_couple_equal": (_i32, [_vp, _vp]),
     "h3c_set_periodic": (_i32, [_vp, _P(_i64)]),
     "h3c_launches": (_i32, [_vp, _P(_i64)]),
+    "h3c_set_option": (_i32, [_vp, _i32, _i32]),
     "h3c_profile": (_i32, [_vp, _i32]),
     "h3c_profile_read": (_i32, [_vp, _P(_dbl), _P(_i64), _i32]),
     "h3c_grid_build": (_i32, [_P(GridDesc), _P(_vp)]),

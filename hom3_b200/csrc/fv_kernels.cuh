@@ -700,6 +700,175 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
   if (FUSE) block_min_atomic(ord, dtmin);
 }
 
+// ---------------------------------------------------------------------------
+// Tile stage kernel (Euler).  A block owns kBlock consecutive cells of the
+// Morton order, which form a compact brick of the grid.  Primitive variables
+// are computed once per cell into shared memory, each cell evaluates the flux
+// of its plus face in every direction once, and a cell takes its minus-face
+// flux from the neighbour's plus-face result when that neighbour is in the
+// tile and links back to it (same-level face) -- the same F(l, r) evaluation
+// hom3's num_flux performs twice (solver.hpp:446-453), so results are
+// bit-identical to k_stage.  Faces leaving the tile, and coarse/fine faces,
+// are evaluated directly.
+// Shared memory (dynamic): prim [ND+4][kBlock] of R, plus-face flux
+// [ND][ND+2][kBlock] of double.
+// ---------------------------------------------------------------------------
+template <class R, int ND>
+__host__ __device__ constexpr size_t tile_smem_bytes() {
+  return sizeof(R) * (2 * ND + 4) * kBlock + sizeof(double) * ND * (ND + 2) * kBlock;
+}
+
+template <int ND, int FLUX, class R, int MODE, bool HANG, bool FUSE>
+__global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restrict__ qin, double* out, Geometry g,
+                                                       PhysConst pc, const Scalars* __restrict__ sc,
+                                                       long long* dtmin) {
+  constexpr int NV = ND + 2;
+  constexpr int NP = 2 * ND + 4;  // rows: q[ND+2], u[ND], p, a
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sprim = reinterpret_cast<R*>(smem_raw);
+  const long long c0 = (long long)blockIdx.x * kBlock;
+  const int tid = threadIdx.x;
+  const long long c = c0 + tid;
+  const bool live = c < g.n_int;
+  const long long ld = g.ld;
+  const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+  const double dt = sc->dt;
+  const double dx = live ? g.len[g.lvl[c]] : 1.0;
+  const R dx_dt = (R)(dx / dt);
+
+  // ---- phase A: own state and primitives -> shared memory ----
+  double qc[NV];
+  Prim<R, ND> Pc;
+  if (live) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Pc.q[v] = (R)qc[v];
+    make_prim<R, ND>(Pc, gamma, gm1);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sprim[v * kBlock + tid] = Pc.q[v];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) sprim[(NV + d) * kBlock + tid] = Pc.u[d];
+    sprim[(NV + ND) * kBlock + tid] = Pc.p;
+    sprim[(NV + ND + 1) * kBlock + tid] = Pc.a;
+  }
+  __syncthreads();
+
+  const long long tile_end = min(c0 + (long long)kBlock, g.n_int);
+  auto in_tile = [&](long long n) { return n >= c0 && n < tile_end; };
+  auto prim_of = [&](long long n, Prim<R, ND>& P) {
+    if (in_tile(n)) {
+      const int t = (int)(n - c0);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) P.q[v] = sprim[v * kBlock + t];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) P.u[d] = sprim[(NV + d) * kBlock + t];
+      P.p = sprim[(NV + ND) * kBlock + t];
+      P.a = sprim[(NV + ND + 1) * kBlock + t];
+    } else {
+      load_prim<R, ND>(P, qin, ld, (int)n, gamma, gm1);
+    }
+  };
+  auto flux = [&](const Prim<R, ND>& L, const Prim<R, ND>& Rt, int d, R* f) {
+    if (FLUX == LLF) llf<R, ND>(L, Rt, d, dx_dt, f);
+    else ausm<R, ND>(L, Rt, d, f);
+  };
+  constexpr int NS = 1 << (ND - 1);
+  constexpr double W = ND == 2 ? 0.5 : 0.25;
+  double* sf = reinterpret_cast<double*>(smem_raw + sizeof(R) * NP * kBlock);  // [ND][NV][kBlock]
+
+  // ---- phase B: plus-face fluxes ----
+  int nbm[ND];
+  if (live) {
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const int p = g.nbr[(2 * d + 1) * ld + c];
+      nbm[d] = g.nbr[(2 * d) * ld + c];
+      double fp[NV];
+      if (!HANG || p >= 0) {
+        Prim<R, ND> Pn;
+        prim_of(p, Pn);
+        R f[NV];
+        flux(Pc, Pn, d, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
+      } else {
+        const long long k = -p - 2;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+          Prim<R, ND> Pn;
+          prim_of(g.sub[j * g.nsub + k], Pn);
+          R f[NV];
+          flux(Pc, Pn, d, f);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fp[v] = W * fp[v];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) sf[(d * NV + v) * kBlock + tid] = fp[v];
+    }
+  }
+  __syncthreads();
+
+  // ---- phase C: minus faces, residual, update ----
+  long long ord = kOrdMax;
+  if (live) {
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const int m = nbm[d];
+      double fm[NV];
+      if (!HANG || m >= 0) {
+        if (in_tile(m) && g.nbr[(2 * d + 1) * ld + m] == (int)c) {
+          const int t = (int)(m - c0);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = sf[(d * NV + v) * kBlock + t];
+        } else {
+          Prim<R, ND> Pn;
+          prim_of(m, Pn);
+          R f[NV];
+          flux(Pn, Pc, d, f);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
+        }
+      } else {
+        const long long k = -m - 2;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+          Prim<R, ND> Pn;
+          prim_of(g.sub[j * g.nsub + k], Pn);
+          R f[NV];
+          flux(Pn, Pc, d, f);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fm[v] = W * fm[v];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);
+    }
+    const double k = dt / dx;
+    double o[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if (MODE == 0) o[v] = qc[v] + k * acc[v];
+      else o[v] = 0.5 * ((out[v * ld + c] + qc[v]) + k * acc[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
+    if (FUSE) {
+      const double cd = cell_dt<ND, EULER>(o, dx, pc);
+      if (!isnan(cd)) ord = dbl_to_ord(cd);
+    }
+  }
+  if (FUSE) block_min_atomic(ord, dtmin);
+}
+
 // gather / scatter between the caller's numbering and the internal one
 __global__ void k_gather(const double* __restrict__ src, long long src_ld, double* __restrict__ dst,
                          long long dst_ld, const long long* __restrict__ dev_to_caller, long long n, int nv) {

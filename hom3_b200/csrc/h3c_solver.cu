@@ -65,6 +65,13 @@ struct h3c_solver_s {
   bool unfused_dt = false;  // a condition rewrites interior cells (vortex)
   bool needs_partner = false, needs_periodic = false;  // coupling / periodic conditions present
   bool partner_set = false, periodic_set = false;
+  bool tile = true;  // Euler stages use the shared-memory tile kernel
+  // CUDA graph of `graph_steps` solver steps, replayed by h3c_solve
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+  const double* graph_q0 = nullptr;  // lhs buffer the capture started from
+  long long graph_launches = 0;
+  bool graphs = true;
   std::string err;
   // launch accounting and optional per-kernel CUDA-event timing (h3c_profile)
   long long launches = 0;
@@ -101,7 +108,14 @@ template <class T> void dfree(T*& p) {
   p = nullptr;
 }
 
+void drop_graph(h3c_solver s) {
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  s->graph = nullptr;
+  s->graph_steps = 0;
+}
+
 void free_grid(h3c_solver s) {
+  drop_graph(s);
   dfree(s->d_nbr); dfree(s->d_lvl); dfree(s->d_sub); dfree(s->d_gbndry); dfree(s->d_gpos);
   dfree(s->d_gapply); dfree(s->d_gown); dfree(s->d_gdx); dfree(s->d_gpartner); dfree(s->d_xc);
   dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_slopes); dfree(s->d_stage);
@@ -228,6 +242,18 @@ void launch_slopes(h3c_solver s, int which) {
 template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG, bool FUSE>
 void stage_t(h3c_solver s, const double* qin, double* out) {
   Launch L(s, MODE == 0 ? K_STAGE1 : K_STAGE2);
+  if (PHYS == EULER && s->tile) {
+    constexpr size_t smem = tile_smem_bytes<R, ND>();
+    static bool attr = false;  // one opt-in per instantiation (dynamic smem above 48 KB)
+    if (!attr) {
+      cudaFuncSetAttribute(k_stage_tile<ND, FLUX, R, MODE, HANG, FUSE>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr = true;
+    }
+    k_stage_tile<ND, FLUX, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, smem, s->stream>>>(
+        qin, out, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+    return;
+  }
   k_stage<ND, PHYS, FLUX, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
       qin, out, s->d_slopes, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
 }
@@ -686,9 +712,7 @@ int h3c_apply_bcs(h3c_solver s, int which) {
 }
 
 // Solver::solve (solver.hpp:140-145): apply_bcs(lhs), set_dt, evolve, advance.
-int h3c_solve(h3c_solver s, int64_t nsteps) {
-  if (!s || nsteps < 0) return H3C_E_INVALID;
-  if (int rc = ready(s, "h3c_solve")) return rc;
+static void enqueue_steps(h3c_solver s, int64_t nsteps) {
   const bool cns = s->desc.physics == H3C_CNS;
   const bool fuse = !s->unfused_dt;
   for (int64_t it = 0; it < nsteps; ++it) {
@@ -715,6 +739,65 @@ int h3c_solve(h3c_solver s, int64_t nsteps) {
       k_advance<<<1, 1, 0, s->stream>>>(s->d_sc);
     }
   }
+}
+
+// Steps per replayed graph: even, so forward Euler's buffer swap returns the
+// state pointers to where the capture started.
+constexpr int kGraphSteps = 8;
+
+static bool build_graph(h3c_solver s) {
+  drop_graph(s);
+  cudaGraph_t g = nullptr;
+  if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const long long l0 = s->launches;
+  enqueue_steps(s, kGraphSteps);
+  const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+  if (e != cudaSuccess || !g) {
+    cudaGetLastError();
+    s->launches = l0;
+    if (g) cudaGraphDestroy(g);
+    return false;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
+  cudaGraphDestroy(g);
+  s->launches = l0;
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    s->graph = nullptr;
+    return false;
+  }
+  s->graph_steps = kGraphSteps;
+  s->graph_launches = 0;
+  s->graph_q0 = s->d_q[0];
+  return true;
+}
+
+int h3c_solve(h3c_solver s, int64_t nsteps) {
+  if (!s || nsteps < 0) return H3C_E_INVALID;
+  if (int rc = ready(s, "h3c_solve")) return rc;
+  // Runs of steps replay a captured graph (no per-launch host cost); coupled
+  // solvers read their partner's current buffers and profiling brackets
+  // every launch, so those take the plain path.
+  const bool graphable = s->graphs && !s->prof && s->partner == nullptr;
+  if (graphable && nsteps >= kGraphSteps) {
+    if (s->graph && s->graph_q0 != s->d_q[0]) drop_graph(s);  // forward Euler swapped buffers since
+    if (!s->graph) {
+      const long long l0 = s->launches;
+      enqueue_steps(s, 1);  // one plain step first (sets kernel attributes outside capture)
+      const long long per_step = s->launches - l0;
+      nsteps -= 1;
+      if (build_graph(s)) s->graph_launches = per_step * kGraphSteps;
+    }
+    while (s->graph && nsteps >= kGraphSteps) {
+      H3C_CUDA(s, cudaGraphLaunch(s->graph, s->stream));
+      s->launches += s->graph_launches;
+      nsteps -= kGraphSteps;
+    }
+  }
+  enqueue_steps(s, nsteps);
   return s->cuda(cudaGetLastError(), "h3c_solve");
 }
 
@@ -852,6 +935,17 @@ int h3c_couple_equal(h3c_solver a, h3c_solver b) {
   launch_cfl(b, &b->d_sc->mindt_ord);
   k_couple_equal<<<1, 1, 0, a->stream>>>(a->d_sc, b->d_sc);
   return a->cuda(cudaGetLastError(), "h3c_couple_equal");
+}
+
+int h3c_set_option(h3c_solver s, int option, int value) {
+  if (!s) return H3C_E_INVALID;
+  switch (option) {
+    case H3C_OPT_TILE_KERNEL: s->tile = value != 0; break;
+    case H3C_OPT_GRAPHS: s->graphs = value != 0; break;
+    default: return s->fail(H3C_E_INVALID, "h3c_set_option: unknown option %d", option);
+  }
+  drop_graph(s);
+  return H3C_OK;
 }
 
 int h3c_launches(h3c_solver s, int64_t* n) {

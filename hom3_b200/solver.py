@@ -250,6 +250,9 @@ class Solver:
         self._check(lib().h3c_device_order(self.h, _lp(out)))
         return out
 
+    def set_option(self, option, value):
+        self._check(lib().h3c_set_option(self.h, int(option), int(value)))
+
     def launches(self):
         return self._get(lib().h3c_launches, C.c_int64)
 

@@ -191,6 +191,12 @@ int h3c_status(h3c_solver s, int* flags);
  * (0 boundary conditions, 1 CFL reduction, 2 scalar step bookkeeping,
  * 3 first stage / forward Euler, 4 second RK stage, 5 slopes) and resets. */
 int h3c_launches(h3c_solver s, int64_t* n);
+/* Execution options (no hom3 counterpart; results do not depend on them):
+ * H3C_OPT_TILE_KERNEL  Euler stages in the shared-memory tile kernel (default 1)
+ * H3C_OPT_GRAPHS       replay runs of steps from a captured CUDA graph (default 1) */
+#define H3C_OPT_TILE_KERNEL 1
+#define H3C_OPT_GRAPHS 2
+int h3c_set_option(h3c_solver s, int option, int value);
 int h3c_profile(h3c_solver s, int enable);
 int h3c_profile_read(h3c_solver s, double* ms, int64_t* count, int nkinds);
 
