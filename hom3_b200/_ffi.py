@@ -85,6 +85,7 @@ SIGNATURES = {
     "h3c_launches": (_i32, [_vp, _P(_i64)]),
     "h3c_set_option": (_i32, [_vp, _i32, _i32]),
     "h3c_selftest_nr": (_i32, [_P(_dbl), _i64, _P(_dbl), _P(_dbl)]),
+    "h3c_min_dt_noalloc": (_i32, [_P(Desc), _vp, _i64, _i64, _vp, _vp, _vp]),
     "h3c_profile": (_i32, [_vp, _i32]),
     "h3c_profile_read": (_i32, [_vp, _P(_dbl), _P(_i64), _i32]),
     "h3c_grid_build": (_i32, [_P(GridDesc), _P(_vp)]),

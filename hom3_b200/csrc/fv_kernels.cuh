@@ -337,6 +337,7 @@ __global__ void __launch_bounds__(kBlock) k_cfl(const double* __restrict__ q, Ge
   block_min_atomic(o, dst);
 }
 
+#ifndef H3C_DEVICE_FUNCTIONS_ONLY  // non-template kernels: defined in one translation unit
 // set_dt: solver.hpp:541-551 (dtmin_ord holds compute_dt of the current lhs)
 __global__ void k_set_dt(Scalars* s, int reset_after) {
   double dt;
@@ -355,6 +356,7 @@ __global__ void k_advance(Scalars* s) {
   s->step += 1;
 }
 __global__ void k_reset_slot(long long* slot) { *slot = kOrdMax; }
+#endif  // H3C_DEVICE_FUNCTIONS_ONLY
 
 // ---------------------------------------------------------------------------
 // isentropic vortex: euler/initial_conditions.hpp:343-368 (2D, hom3's fixed
@@ -1130,6 +1132,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
   if (FUSE) block_min_atomic(ord, dtmin);
 }
 
+#ifndef H3C_DEVICE_FUNCTIONS_ONLY  // non-template kernels: defined in one translation unit
 // gather / scatter between the caller's numbering and the internal one
 __global__ void k_gather(const double* __restrict__ src, long long src_ld, double* __restrict__ dst,
                          long long dst_ld, const long long* __restrict__ dev_to_caller, long long n, int nv) {
@@ -1145,5 +1148,6 @@ __global__ void k_scatter(const double* __restrict__ src, long long src_ld, doub
   const long long s = dev_to_caller[c];
   for (int v = 0; v < nv; ++v) dst[v * dst_ld + s] = src[v * src_ld + c];
 }
+#endif  // H3C_DEVICE_FUNCTIONS_ONLY
 
 }  // namespace h3c

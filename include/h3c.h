@@ -203,6 +203,22 @@ int h3c_selftest_nr(const double* x, int64_t n, double* rcp, double* rsqrt);
 int h3c_profile(h3c_solver s, int enable);
 int h3c_profile_read(h3c_solver s, double* ms, int64_t* count, int nkinds);
 
+/* ---- allocation-free time step (no counterpart in hom3) ----
+ * For callers that cannot allocate device memory -- code running inside a
+ * framework that owns all device memory through its own pool, or a step
+ * controller that must not call cudaMalloc because it synchronises the device
+ * and would serialise the caller's streams.  Computes the same minimum cell
+ * time step as h3c_min_dt (hom3's compute_dt) from caller-owned device
+ * buffers: q = interior-cell state [nv][ld], length = their cell lengths,
+ * dt_out = one device double; asynchronous on `stream`.  Allocates nothing:
+ * its scratch is a fixed 128 KiB array inside the library (held on every GPU
+ * that loads it until exit), so n_cells <= 4,194,304; larger sizes return
+ * H3C_E_INVALID.  The first call on a device looks up the array's address
+ * (make that first call before any stream capture).  Calls share the array:
+ * calls that overlap on the GPU race and must be serialised by the caller. */
+int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t ld, int64_t n_cells,
+                       const double* length, double* dt_out, void* stream);
+
 /* ---- coupling: coupling.hpp:24-73 ----
  * partner_cells[g - first_ghost] = the partner solver's cell (caller
  * numbering of the partner) that local_bndry_ids (coupling.hpp:24-39) finds
