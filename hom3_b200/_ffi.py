@@ -63,6 +63,9 @@ SIGNATURES = {
     "h3c_destroy": (_i32, [_vp]),
     "h3c_last_error": (_i32, [_vp, C.c_char_p, C.c_size_t]),
     "h3c_set_grid": (_i32, [_vp, _P(Grid)]),
+    "h3c_set_grids": (_i32, [_vp, _i32, _P(Grid)]),
+    "h3c_instances": (_i32, [_vp, _P(_dbl), _P(_dbl), _P(_i64)]),
+    "h3c_autotune": (_i32, [_vp, _i32, _P(_i32), _P(_dbl)]),
     "h3c_set_state": (_i32, [_vp, _i32, _P(_dbl), _i64]),
     "h3c_get_state": (_i32, [_vp, _i32, _P(_dbl), _i64]),
     "h3c_state_device": (_i32, [_vp, _i32, _P(_P(_dbl)), _P(_i64)]),

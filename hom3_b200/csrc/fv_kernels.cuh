@@ -65,7 +65,25 @@ struct Geometry {
   long long nsub;
   long long n_int, n_tot, ld;
   double len[kMaxLevels];
+  // Batches of independent grids: interior cells of instance k occupy
+  // [start_k, inst_end[k]) with start_k a multiple of kBlock, so every
+  // kBlock-cell tile belongs to one instance (blk_inst[tile]); the cells
+  // between inst_end[k] and the next start are padding.  nullptr: one grid.
+  const int* __restrict__ blk_inst;
+  const long long* __restrict__ inst_end;
+  long long ntiles;
 };
+
+__device__ __forceinline__ int tile_instance(const Geometry& g, long long tile) {
+  return g.blk_inst ? g.blk_inst[tile] : 0;
+}
+__device__ __forceinline__ long long instance_end(const Geometry& g, int inst) {
+  return g.blk_inst ? g.inst_end[inst] : g.n_int;
+}
+// the per-instance copy of a Scalars field (instances are consecutive Scalars)
+template <class T> __device__ __forceinline__ T* per_instance(T* slot0, int inst) {
+  return reinterpret_cast<T*>(reinterpret_cast<char*>(slot0) + (size_t)inst * sizeof(Scalars));
+}
 
 struct GhostTables {
   const int* __restrict__ bndry;          // [ng] boundary cell of each ghost
@@ -75,6 +93,7 @@ struct GhostTables {
   const double* __restrict__ dx;          // [ng] |x_b - x_g| (cell_dx, solver.hpp:590-592)
   const int* __restrict__ partner;        // [ng] partner cell (internal numbering) or -1
   const double* __restrict__ xc;          // [nd][ld] cell centres (vortex bc)
+  const int* __restrict__ ginst;          // [ng] instance of each ghost (nullptr: one grid)
   long long ng;
   const BcParam* bcs;                     // [n_bcs] device array
 };
@@ -326,20 +345,24 @@ __global__ void __launch_bounds__(kBlock) k_cfl(const double* __restrict__ q, Ge
                                                 long long* dst) {
   constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int inst = tile_instance(g, blockIdx.x);
   long long o = kOrdMax;
-  if (c < g.n_int) {
+  if (c < instance_end(g, inst)) {
     double qc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) qc[v] = __ldg(q + v * g.ld + c);
     const double dt = cell_dt<ND, PHYS>(qc, g.len[g.lvl[c]], pc);
     if (!isnan(dt)) o = dbl_to_ord(dt);
   }
-  block_min_atomic(o, dst);
+  block_min_atomic(o, per_instance(dst, inst));
 }
 
 #ifndef H3C_DEVICE_FUNCTIONS_ONLY  // non-template kernels: defined in one translation unit
 // set_dt: solver.hpp:541-551 (dtmin_ord holds compute_dt of the current lhs)
-__global__ void k_set_dt(Scalars* s, int reset_after) {
+__global__ void k_set_dt(Scalars* s0, int reset_after, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_inst) return;
+  Scalars* s = s0 + i;
   double dt;
   if (s->time + s->dt < s->tEnd) {
     dt = (s->step == s->forced_step) ? s->forced_dt : ord_to_dbl(s->dtmin_ord);
@@ -351,11 +374,17 @@ __global__ void k_set_dt(Scalars* s, int reset_after) {
   if (reset_after) s->dtmin_ord = kOrdMax;
 }
 // advance: solver.hpp:502-505
-__global__ void k_advance(Scalars* s) {
+__global__ void k_advance(Scalars* s0, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_inst) return;
+  Scalars* s = s0 + i;
   s->time += s->dt;
   s->step += 1;
 }
-__global__ void k_reset_slot(long long* slot) { *slot = kOrdMax; }
+__global__ void k_reset_slot(long long* slot, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_inst) *per_instance(slot, i) = kOrdMax;
+}
 #endif  // H3C_DEVICE_FUNCTIONS_ONLY
 
 // ---------------------------------------------------------------------------
@@ -434,7 +463,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
     case BC_EULER_VORTEX: {  // euler/boundary_conditions.hpp:304-316
       double vg[4] = {0, 0, 0, 0}, vb[4] = {0, 0, 0, 0};
       if (ND == 2) {
-        const double t = sc->time;
+        const double t = sc[gt.ginst ? gt.ginst[i] : 0].time;
         isentropic_vortex(gt.xc[gcell], gt.xc[ld + gcell], t, vg);
         isentropic_vortex(gt.xc[bc], gt.xc[ld + bc], t, vb);
       }
@@ -589,11 +618,12 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
                                                   const Scalars* __restrict__ sc, long long* dtmin) {
   constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = c < g.n_int;
+  const int inst = tile_instance(g, blockIdx.x);
+  const bool live = c < instance_end(g, inst);
   long long ord = kOrdMax;
   if (live) {
     const long long ld = g.ld;
-    const double dt = sc->dt;
+    const double dt = sc[inst].dt;
     const double dx = g.len[g.lvl[c]];
     double qc[NV];
 #pragma unroll
@@ -740,7 +770,7 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
       if (!isnan(cd)) ord = dbl_to_ord(cd);
     }
   }
-  if (FUSE) block_min_atomic(ord, dtmin);
+  if (FUSE) block_min_atomic(ord, per_instance(dtmin, inst));
 }
 
 // ---------------------------------------------------------------------------
@@ -772,10 +802,12 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
   const long long c0 = (long long)blockIdx.x * kBlock;
   const int tid = threadIdx.x;
   const long long c = c0 + tid;
-  const bool live = c < g.n_int;
+  const int inst = tile_instance(g, blockIdx.x);
+  const long long iend = instance_end(g, inst);
+  const bool live = c < iend;
   const long long ld = g.ld;
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
-  const double dt = sc->dt;
+  const double dt = sc[inst].dt;
   const double dx = live ? g.len[g.lvl[c]] : 1.0;
   const R dx_dt = (R)(dx / dt);
 
@@ -799,7 +831,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
   }
   __syncthreads();
 
-  const long long tile_end = min(c0 + (long long)kBlock, g.n_int);
+  const long long tile_end = min(c0 + (long long)kBlock, iend);
   auto in_tile = [&](long long n) { return n >= c0 && n < tile_end; };
   auto prim_of = [&](long long n, Prim<R, ND>& P) {
     if (in_tile(n)) {
@@ -915,7 +947,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
       if (!isnan(cd)) ord = dbl_to_ord(cd);
     }
   }
-  if (FUSE) block_min_atomic(ord, dtmin);
+  if (FUSE) block_min_atomic(ord, per_instance(dtmin, inst));
 }
 
 // ---------------------------------------------------------------------------
@@ -965,10 +997,13 @@ __device__ __forceinline__ void face_state_global(FaceState<R, ND>& F, const dou
 #ifndef H3C_AUSM_MINB
 #define H3C_AUSM_MINB 4  // blocks per SM the AUSM tile kernel is register-budgeted for
 #endif
+// Persistent: block b processes tiles b, b + gridDim.x, ... (the grid size is
+// a launch choice the batch autotuner makes; one block per tile by default).
 template <int ND, class R, int MODE, bool HANG, bool FUSE>
-__global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const double* __restrict__ qin, double* out, Geometry g,
-                                                          PhysConst pc, const Scalars* __restrict__ sc,
-                                                          long long* dtmin) {
+__global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const double* __restrict__ qin, double* out,
+                                                                      Geometry g, PhysConst pc,
+                                                                      const Scalars* __restrict__ sc,
+                                                                      long long* dtmin) {
   constexpr int NV = ND + 2;
   constexpr int NS = 1 << (ND - 1);
   constexpr double W = ND == 2 ? 0.5 : 0.25;
@@ -976,160 +1011,166 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
   R* sfs = reinterpret_cast<R*>(smem_raw);                                   // [NV + 1 + ND][kBlock]
   double* sf = reinterpret_cast<double*>(smem_raw + sizeof(R) * (2 * ND + 3) * kBlock);  // [ND][NV][kBlock]
   int* snp = reinterpret_cast<int*>(sf + ND * NV * kBlock);                  // [ND][kBlock]
-  const long long c0 = (long long)blockIdx.x * kBlock;
   const int tid = threadIdx.x;
-  const long long c = c0 + tid;
-  const bool live = c < g.n_int;
   const long long ld = g.ld;
-  const long long tile_end = min(c0 + (long long)kBlock, g.n_int);
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
 
-  // ---- own loads first: state, neighbours, level, (old state) ----
-  double qc[NV], qo[NV];
-  int nbp[ND], nbm[ND];
-  double dx = 1.0;
-  if (live) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
-#pragma unroll
-    for (int d = 0; d < ND; ++d) {
-      nbm[d] = __ldg(g.nbr + (2 * d) * ld + c);
-      nbp[d] = __ldg(g.nbr + (2 * d + 1) * ld + c);
-    }
-    dx = g.len[g.lvl[c]];
-  }
-  // ---- face state of the cell -> shared memory ----
-  Prim<R, ND> Pc;
-  if (live) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) Pc.q[v] = (R)qc[v];
-    make_prim<R, ND>(Pc, gamma, gm1);
-#pragma unroll
-    for (int v = 0; v < ND + 1; ++v) sfs[v * kBlock + tid] = Pc.q[v] * Pc.a;
-    sfs[(ND + 1) * kBlock + tid] = (Pc.q[ND + 1] + Pc.p) * Pc.a;
-    sfs[NV * kBlock + tid] = Pc.p;
-#pragma unroll
-    for (int d = 0; d < ND; ++d) sfs[(NV + 1 + d) * kBlock + tid] = Pc.M[d];
-#pragma unroll
-    for (int d = 0; d < ND; ++d) snp[d * kBlock + tid] = nbp[d];
-  }
-  __syncthreads();
+  for (long long tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
+    const long long c0 = tile * kBlock;
+    const long long c = c0 + tid;
+    const int inst = tile_instance(g, tile);
+    const long long tile_end = min(c0 + (long long)kBlock, instance_end(g, inst));
+    const bool live = c < tile_end;
 
-  auto in_tile = [&](long long n) { return n >= c0 && n < tile_end; };
-  auto fstate = [&](long long n, int d, FaceState<R, ND>& F) {
-    if (in_tile(n)) {
-      const int t = (int)(n - c0);
+    // ---- own loads first: state, neighbours, level ----
+    double qc[NV];
+    int nbp[ND], nbm[ND];
+    double dx = 1.0;
+    if (live) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + t];
-      F.p = sfs[NV * kBlock + t];
-      F.M = sfs[(NV + 1 + d) * kBlock + t];
-    } else {
-      face_state_global<R, ND>(F, qin, ld, (int)n, d, gamma, gm1);
+      for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        nbm[d] = __ldg(g.nbr + (2 * d) * ld + c);
+        nbp[d] = __ldg(g.nbr + (2 * d + 1) * ld + c);
+      }
+      dx = g.len[g.lvl[c]];
     }
-  };
-  auto own = [&](int d, FaceState<R, ND>& F) {
+    // ---- face state of the cell -> shared memory ----
+    if (live) {
+      Prim<R, ND> Pc;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + tid];
-    F.p = sfs[NV * kBlock + tid];
-    F.M = sfs[(NV + 1 + d) * kBlock + tid];
-  };
+      for (int v = 0; v < NV; ++v) Pc.q[v] = (R)qc[v];
+      make_prim<R, ND>(Pc, gamma, gm1);
+#pragma unroll
+      for (int v = 0; v < ND + 1; ++v) sfs[v * kBlock + tid] = Pc.q[v] * Pc.a;
+      sfs[(ND + 1) * kBlock + tid] = (Pc.q[ND + 1] + Pc.p) * Pc.a;
+      sfs[NV * kBlock + tid] = Pc.p;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) sfs[(NV + 1 + d) * kBlock + tid] = Pc.M[d];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) snp[d * kBlock + tid] = nbp[d];
+    }
+    __syncthreads();
 
-  // ---- plus faces ----
-  if (live) {
+    auto in_tile = [&](long long n) { return n >= c0 && n < tile_end; };
+    auto fstate = [&](long long n, int d, FaceState<R, ND>& F) {
+      if (in_tile(n)) {
+        const int t = (int)(n - c0);
 #pragma unroll
-    for (int d = 0; d < ND; ++d) {
-      FaceState<R, ND> Fc;
-      own(d, Fc);
-      const int p = nbp[d];
-      double fp[NV];
-      if (!HANG || p >= 0) {
-        FaceState<R, ND> Fn;
-        fstate(p, d, Fn);
-        R f[NV];
-        ausm_face<R, ND>(Fc, Fn, d, f);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
+        for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + t];
+        F.p = sfs[NV * kBlock + t];
+        F.M = sfs[(NV + 1 + d) * kBlock + t];
       } else {
-        const long long k = -p - 2;
+        face_state_global<R, ND>(F, qin, ld, (int)n, d, gamma, gm1);
+      }
+    };
+    auto own = [&](int d, FaceState<R, ND>& F) {
 #pragma unroll
-        for (int j = 0; j < NS; ++j) {
+      for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + tid];
+      F.p = sfs[NV * kBlock + tid];
+      F.M = sfs[(NV + 1 + d) * kBlock + tid];
+    };
+
+    // ---- plus faces ----
+    if (live) {
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        FaceState<R, ND> Fc;
+        own(d, Fc);
+        const int p = nbp[d];
+        double fp[NV];
+        if (!HANG || p >= 0) {
           FaceState<R, ND> Fn;
-          fstate(__ldg(g.sub + j * g.nsub + k), d, Fn);
+          fstate(p, d, Fn);
           R f[NV];
           ausm_face<R, ND>(Fc, Fn, d, f);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
+          for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
+        } else {
+          const long long k = -p - 2;
+#pragma unroll
+          for (int j = 0; j < NS; ++j) {
+            FaceState<R, ND> Fn;
+            fstate(__ldg(g.sub + j * g.nsub + k), d, Fn);
+            R f[NV];
+            ausm_face<R, ND>(Fc, Fn, d, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
+          }
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fp[v] = W * fp[v];
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fp[v] = W * fp[v];
+        for (int v = 0; v < NV; ++v) sf[(d * NV + v) * kBlock + tid] = fp[v];
       }
-#pragma unroll
-      for (int v = 0; v < NV; ++v) sf[(d * NV + v) * kBlock + tid] = fp[v];
     }
-  }
-  __syncthreads();
+    __syncthreads();
 
-  // ---- minus faces, residual, update ----
-  long long ord = kOrdMax;
-  if (live) {
-    double acc[NV];
+    // ---- minus faces, residual, update ----
+    long long ord = kOrdMax;
+    if (live) {
+      double acc[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+      for (int v = 0; v < NV; ++v) acc[v] = 0.0;
 #pragma unroll
-    for (int d = 0; d < ND; ++d) {
-      const int m = nbm[d];
-      double fm[NV];
-      if (in_tile(m) && snp[d * kBlock + (int)(m - c0)] == (int)c) {
-        const int t = (int)(m - c0);
+      for (int d = 0; d < ND; ++d) {
+        const int m = nbm[d];
+        double fm[NV];
+        if (in_tile(m) && snp[d * kBlock + (int)(m - c0)] == (int)c) {
+          const int t = (int)(m - c0);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fm[v] = sf[(d * NV + v) * kBlock + t];
-      } else if (!HANG || m >= 0) {
-        FaceState<R, ND> Fc, Fn;
-        own(d, Fc);
-        fstate(m, d, Fn);
-        R f[NV];
-        ausm_face<R, ND>(Fn, Fc, d, f);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
-      } else {
-        FaceState<R, ND> Fc;
-        own(d, Fc);
-        const long long k = -m - 2;
-#pragma unroll
-        for (int j = 0; j < NS; ++j) {
-          FaceState<R, ND> Fn;
-          fstate(__ldg(g.sub + j * g.nsub + k), d, Fn);
+          for (int v = 0; v < NV; ++v) fm[v] = sf[(d * NV + v) * kBlock + t];
+        } else if (!HANG || m >= 0) {
+          FaceState<R, ND> Fc, Fn;
+          own(d, Fc);
+          fstate(m, d, Fn);
           R f[NV];
           ausm_face<R, ND>(Fn, Fc, d, f);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
+          for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
+        } else {
+          FaceState<R, ND> Fc;
+          own(d, Fc);
+          const long long k = -m - 2;
+#pragma unroll
+          for (int j = 0; j < NS; ++j) {
+            FaceState<R, ND> Fn;
+            fstate(__ldg(g.sub + j * g.nsub + k), d, Fn);
+            R f[NV];
+            ausm_face<R, ND>(Fn, Fc, d, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
+          }
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = W * fm[v];
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fm[v] = W * fm[v];
+        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);
+      }
+      double qo[NV];
+      if (MODE == 2) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
+      }
+      const double dt = sc[inst].dt;
+      const double k = dt / dx;
+      double o[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        if (MODE == 0) o[v] = qc[v] + k * acc[v];
+        else o[v] = 0.5 * ((qo[v] + qc[v]) + k * acc[v]);
       }
 #pragma unroll
-      for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);
+      for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
+      if (FUSE) {
+        const double cd = cell_dt<ND, EULER>(o, dx, pc);
+        if (!isnan(cd)) ord = dbl_to_ord(cd);
+      }
     }
-    if (MODE == 2) {
-#pragma unroll
-      for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
-    }
-    const double dt = sc->dt;
-    const double k = dt / dx;
-    double o[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      if (MODE == 0) o[v] = qc[v] + k * acc[v];
-      else o[v] = 0.5 * ((qo[v] + qc[v]) + k * acc[v]);
-    }
-#pragma unroll
-    for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
-    if (FUSE) {
-      const double cd = cell_dt<ND, EULER>(o, dx, pc);
-      if (!isnan(cd)) ord = dbl_to_ord(cd);
-    }
+    if (FUSE) block_min_atomic(ord, per_instance(dtmin, inst));
+    __syncthreads();  // shared memory is rewritten by the next tile
   }
-  if (FUSE) block_min_atomic(ord, dtmin);
 }
 
 #ifndef H3C_DEVICE_FUNCTIONS_ONLY  // non-template kernels: defined in one translation unit
@@ -1139,6 +1180,7 @@ __global__ void k_gather(const double* __restrict__ src, long long src_ld, doubl
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   const long long s = dev_to_caller[c];
+  if (s < 0) return;  // padding between batch instances
   for (int v = 0; v < nv; ++v) dst[v * dst_ld + c] = src[v * src_ld + s];
 }
 __global__ void k_scatter(const double* __restrict__ src, long long src_ld, double* __restrict__ dst,
@@ -1146,6 +1188,7 @@ __global__ void k_scatter(const double* __restrict__ src, long long src_ld, doub
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   const long long s = dev_to_caller[c];
+  if (s < 0) return;  // padding between batch instances
   for (int v = 0; v < nv; ++v) dst[v * dst_ld + s] = src[v * src_ld + c];
 }
 #endif  // H3C_DEVICE_FUNCTIONS_ONLY

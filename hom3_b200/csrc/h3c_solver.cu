@@ -39,6 +39,13 @@ struct h3c_solver_s {
   // grid
   bool has_grid = false;
   long long n_int = 0, n_tot = 0, ng = 0, ld = 0, nsub = 0;
+  long long n_caller = 0;  // cells in the caller's numbering (all instances)
+  int n_inst = 1, sc_count = 1;
+  long long ntiles = 0;
+  int persist_blocks = 0;  // AUSM stage grid: 0 = one block per tile, else a persistent grid
+  int* d_blk_inst = nullptr;
+  long long* d_inst_end = nullptr;
+  int* d_ginst = nullptr;
   int* d_nbr = nullptr;
   unsigned char* d_lvl = nullptr;
   int* d_sub = nullptr;
@@ -120,6 +127,7 @@ void free_grid(h3c_solver s) {
   dfree(s->d_gapply); dfree(s->d_gown); dfree(s->d_gdx); dfree(s->d_gpartner); dfree(s->d_xc);
   dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_slopes); dfree(s->d_stage);
   dfree(s->d_dev2caller);
+  dfree(s->d_blk_inst); dfree(s->d_inst_end); dfree(s->d_ginst);
   s->has_grid = false;
 }
 
@@ -133,6 +141,9 @@ Geometry geometry(const h3c_solver s) {
   g.n_tot = s->n_tot;
   g.ld = s->ld;
   for (int i = 0; i < kMaxLevels; ++i) g.len[i] = s->lens[i];
+  g.blk_inst = s->n_inst > 1 ? s->d_blk_inst : nullptr;
+  g.inst_end = s->n_inst > 1 ? s->d_inst_end : nullptr;
+  g.ntiles = s->ntiles;
   return g;
 }
 
@@ -145,6 +156,7 @@ GhostTables ghosts(const h3c_solver s) {
   t.dx = s->d_gdx;
   t.partner = s->d_gpartner;
   t.xc = s->d_xc;
+  t.ginst = s->n_inst > 1 ? s->d_ginst : nullptr;
   t.ng = s->ng;
   t.bcs = s->d_bcs;
   return t;
@@ -218,7 +230,7 @@ void launch_cfl_t(h3c_solver s, long long* slot) {
 void launch_cfl(h3c_solver s, long long* slot) {
   {
     Launch L(s, K_SCALAR);
-    k_reset_slot<<<1, 1, 0, s->stream>>>(slot);
+    k_reset_slot<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(slot, s->n_inst);
   }
   if (s->nd == 2) {
     if (s->desc.physics == H3C_EULER) launch_cfl_t<2, EULER>(s, slot);
@@ -250,7 +262,8 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
                            (int)smem);
       attr = true;
     }
-    k_stage_ausm<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, smem, s->stream>>>(
+    const long long grid = s->persist_blocks > 0 ? std::min<long long>(s->persist_blocks, s->ntiles) : s->ntiles;
+    k_stage_ausm<ND, R, MODE, HANG, FUSE><<<(unsigned)std::max<long long>(1, grid), kBlock, smem, s->stream>>>(
         qin, out, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
     return;
   }
@@ -310,7 +323,10 @@ void launch_stage(h3c_solver s, int mode, const double* qin, double* out, bool f
   else stage_nd<3>(s, mode, qin, out, fuse);
 }
 
-__global__ void k_init_time(Scalars* sc, double tEnd) {
+__global__ void k_init_time(Scalars* sc0, double tEnd, int n_inst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_inst) return;
+  Scalars* sc = sc0 + i;
   sc->dt = 0;
   sc->time = 0;
   sc->tEnd = tEnd;
@@ -409,7 +425,7 @@ int h3c_create(const h3c_desc* d, h3c_solver* out) {
     g_last_error = std::string("h3c_create: cudaMalloc: ") + cudaGetErrorString(e);
     return H3C_E_NOMEM;
   }
-  k_init_time<<<1, 1, 0, s->stream>>>(s->d_sc, d->time_end);
+  k_init_time<<<1, 1, 0, s->stream>>>(s->d_sc, d->time_end, 1);
   *out = s.release();
   return H3C_OK;
 }
@@ -426,12 +442,19 @@ int h3c_destroy(h3c_solver s) {
   return H3C_OK;
 }
 
-int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
-  if (!s || !gr) return H3C_E_INVALID;
+// Per-instance table preparation shared by h3c_set_grid / h3c_set_grids.
+struct InstanceTables {
+  long long n = 0, fg = 0, ld = 0, nsub = 0;
+  std::vector<long long> order;          // interior cells in Morton order (caller numbering)
+  std::vector<int> gb, gbp;              // ghost -> boundary cell, boundary position
+  std::vector<unsigned char> apply, own; // per ghost, local bc indices (255: none)
+};
+
+static int prepare_instance(h3c_solver s, int k, const h3c_grid* gr, InstanceTables& T) {
   const int nd = s->nd, np = 2 * nd;
   const long long n = gr->n_cells, fg = gr->first_ghost, ld = gr->ld;
   if (n <= 0 || fg <= 0 || fg > n || ld < n || !gr->neighbors || !gr->x_center || !gr->length || !gr->bc_idx)
-    return s->fail(H3C_E_INVALID, "h3c_set_grid: bad sizes or null tables");
+    return s->fail(H3C_E_INVALID, "h3c_set_grid: instance %d: bad sizes or null tables", k);
   if (n >= (1LL << 31)) return s->fail(H3C_E_INVALID, "h3c_set_grid: more than 2^31 cells");
   if (gr->n_bcs < 0 || gr->n_bcs > kMaxBcs || (gr->n_bcs > 0 && !gr->bcs))
     return s->fail(H3C_E_INVALID, "h3c_set_grid: n_bcs must be in [0, %d]", kMaxBcs);
@@ -441,7 +464,6 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
   const int nsubc = 1 << (nd - 1);
   auto nb = [&](int p, long long c) { return gr->neighbors[p * ld + c]; };
   auto is_group = [&](long long v) { return nsub > 0 && v <= -2 && (-v - 2) < nsub; };
-  // ---- validation --------------------------------------------------------
   for (long long c = 0; c < fg; ++c) {
     for (int p = 0; p < np; ++p) {
       const long long v = nb(p, c);
@@ -450,7 +472,8 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
     }
     if (!(gr->length[c] > 0)) return s->fail(H3C_E_INVALID, "h3c_set_grid: cell %lld has length <= 0", c);
   }
-  std::vector<int> gb(n - fg), gbp(n - fg);
+  T.gb.assign(n - fg, 0);
+  T.gbp.assign(n - fg, 0);
   for (long long g = fg; g < n; ++g) {
     int cnt = 0, first = -1;
     for (int p = 0; p < np; ++p)
@@ -459,31 +482,21 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
       return s->fail(H3C_E_INVALID, "h3c_set_grid: ghost %lld has %d neighbours (expected 1)", g, cnt);
     const long long b = nb(first, g);
     if (b >= fg) return s->fail(H3C_E_INVALID, "h3c_set_grid: ghost %lld is linked to ghost %lld", g, b);
-    gb[g - fg] = (int)b;
-    gbp[g - fg] = first;
+    T.gb[g - fg] = (int)b;
+    T.gbp[g - fg] = first;
     const int bc = gr->bc_idx[g];
     if (bc < 0 || bc >= gr->n_bcs)
       return s->fail(H3C_E_INVALID, "h3c_set_grid: ghost %lld has bc index %d (n_bcs %d)", g, bc, gr->n_bcs);
   }
-  for (long long k = 0; k < nsub; ++k)
+  for (long long q = 0; q < nsub; ++q)
     for (int j = 0; j < nsubc; ++j) {
-      const long long v = gr->subface_cells[j * nsub + k];
-      if (!valid_cell(v, n)) return s->fail(H3C_E_INVALID, "h3c_set_grid: sub-face %lld has an invalid cell", k);
+      const long long v = gr->subface_cells[j * nsub + q];
+      if (!valid_cell(v, n)) return s->fail(H3C_E_INVALID, "h3c_set_grid: sub-face %lld has an invalid cell", q);
     }
-  // ---- length levels -------------------------------------------------------
-  std::vector<double> lens;
-  for (long long c = 0; c < n; ++c) {
-    const double l = gr->length[c];
-    if (std::find(lens.begin(), lens.end(), l) == lens.end()) {
-      if ((int)lens.size() == kMaxLevels)
-        return s->fail(H3C_E_INVALID, "h3c_set_grid: more than %d distinct cell lengths", kMaxLevels);
-      lens.push_back(l);
-    }
-  }
-  std::sort(lens.begin(), lens.end(), std::greater<double>());
-  // ---- Morton order of interior cells ---------------------------------------
+  // Morton order of interior cells (lower corners in units of the finest cell)
   double xmin[3] = {1e300, 1e300, 1e300};
-  double hmin = lens.back();
+  double hmin = 1e300;
+  for (long long c = 0; c < fg; ++c) hmin = std::min(hmin, gr->length[c]);
   for (long long c = 0; c < fg; ++c)
     for (int d = 0; d < nd; ++d) xmin[d] = std::min(xmin[d], gr->x_center[d * ld + c] - 0.5 * gr->length[c]);
   std::vector<std::pair<uint64_t, long long>> keys(fg);
@@ -497,83 +510,172 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
                    [](const std::pair<uint64_t, long long>& a, const std::pair<uint64_t, long long>& b) {
                      return a.first < b.first;
                    });
-  std::vector<long long> dev2caller(n), caller2dev(n);
-  for (long long i = 0; i < fg; ++i) dev2caller[i] = keys[i].second;
-  for (long long g = fg; g < n; ++g) dev2caller[g] = g;  // ghosts keep the caller's (bc-sorted) order
-  for (long long i = 0; i < n; ++i) caller2dev[dev2caller[i]] = i;
-  // ---- hom3's bc segment discovery (solver.hpp:561-586) -----------------------
-  std::vector<unsigned char> apply(n - fg, 255), own(n - fg);
-  {
-    auto valid_bc = [&](long long c) { return gr->bc_idx[c] >= 0 && gr->bc_idx[c] < gr->n_bcs; };
-    long long first = 0;
-    while (first < n && !valid_bc(first)) ++first;
-    if (first < n) {
-      int bcIdx = gr->bc_idx[first];
-      long long last = 0;
+  T.order.resize(fg);
+  for (long long c = 0; c < fg; ++c) T.order[c] = keys[c].second;
+  // hom3's bc segment discovery (solver.hpp:561-586)
+  T.apply.assign(n - fg, 255);
+  T.own.assign(n - fg, 0);
+  auto valid_bc = [&](long long c) { return gr->bc_idx[c] >= 0 && gr->bc_idx[c] < gr->n_bcs; };
+  long long first = 0;
+  while (first < n && !valid_bc(first)) ++first;
+  if (first < n) {
+    int bcIdx = gr->bc_idx[first];
+    long long last = 0;
+    while (last < n && gr->bc_idx[last] != bcIdx) ++last;
+    for (int q = 0; q < gr->n_bcs; ++q) {
+      ++bcIdx;
+      const long long f0 = last;
+      last = f0;
       while (last < n && gr->bc_idx[last] != bcIdx) ++last;
-      for (int k = 0; k < gr->n_bcs; ++k) {
-        ++bcIdx;
-        const long long f0 = last;
-        last = f0;
-        while (last < n && gr->bc_idx[last] != bcIdx) ++last;
-        for (long long c = std::max(f0, fg); c < last; ++c) apply[c - fg] = (unsigned char)k;
+      for (long long c = std::max(f0, fg); c < last; ++c) T.apply[c - fg] = (unsigned char)q;
+    }
+  }
+  for (long long g = fg; g < n; ++g) T.own[g - fg] = (unsigned char)gr->bc_idx[g];
+  T.n = n;
+  T.fg = fg;
+  T.ld = ld;
+  T.nsub = nsub;
+  return H3C_OK;
+}
+
+static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
+  if (!s || !grids || ninst < 1) return H3C_E_INVALID;
+  const int nd = s->nd, np = 2 * nd, nsubc = 1 << (nd - 1);
+  if (ninst > 1 && s->desc.physics == H3C_CNS)
+    return s->fail(H3C_E_INVALID, "h3c_set_grids: batches of CNS grids are not supported");
+  std::vector<InstanceTables> T(ninst);
+  for (int k = 0; k < ninst; ++k)
+    if (int rc = prepare_instance(s, k, &grids[k], T[k])) return rc;
+  // ---- merged conditions (identical conditions of different instances share one entry) ----
+  std::vector<h3c_bc> ubcs;
+  std::vector<std::vector<unsigned char>> bcmap(ninst);
+  for (int k = 0; k < ninst; ++k) {
+    for (int q = 0; q < grids[k].n_bcs; ++q) {
+      const h3c_bc& b = grids[k].bcs[q];
+      int found = -1;
+      for (size_t u = 0; u < ubcs.size(); ++u)
+        if (ubcs[u].kind == b.kind && std::memcmp(ubcs[u].v, b.v, sizeof(b.v)) == 0) { found = (int)u; break; }
+      if (found < 0) {
+        if ((int)ubcs.size() == kMaxBcs)
+          return s->fail(H3C_E_INVALID, "h3c_set_grids: more than %d distinct conditions", kMaxBcs);
+        ubcs.push_back(b);
+        found = (int)ubcs.size() - 1;
+      }
+      bcmap[k].push_back((unsigned char)found);
+    }
+  }
+  // ---- lengths -> level table ----
+  std::vector<double> lens;
+  for (int k = 0; k < ninst; ++k)
+    for (long long c = 0; c < T[k].n; ++c) {
+      const double l = grids[k].length[c];
+      if (std::find(lens.begin(), lens.end(), l) == lens.end()) {
+        if ((int)lens.size() == kMaxLevels)
+          return s->fail(H3C_E_INVALID, "h3c_set_grid: more than %d distinct cell lengths", kMaxLevels);
+        lens.push_back(l);
       }
     }
-    for (long long g = fg; g < n; ++g) own[g - fg] = (unsigned char)gr->bc_idx[g];
+  std::sort(lens.begin(), lens.end(), std::greater<double>());
+  // ---- device layout: interior ranges 256-aligned per instance, then all ghosts ----
+  std::vector<long long> int_start(ninst), int_end(ninst), ghost_start(ninst), caller_off(ninst), sub_off(ninst);
+  long long cur = 0, ncaller = 0, nsub = 0, ng = 0;
+  for (int k = 0; k < ninst; ++k) {
+    if (k > 0) cur = (cur + kBlock - 1) / kBlock * kBlock;
+    int_start[k] = cur;
+    cur += T[k].fg;
+    int_end[k] = cur;
+    caller_off[k] = ncaller;
+    ncaller += T[k].n;
+    sub_off[k] = nsub;
+    nsub += T[k].nsub;
+    ng += T[k].n - T[k].fg;
   }
-  // ---- device tables ---------------------------------------------------------
+  const long long n_int = cur;
+  for (int k = 0; k < ninst; ++k) {
+    ghost_start[k] = cur;
+    cur += T[k].n - T[k].fg;
+  }
+  const long long n_tot = cur;
+  if (n_tot >= (1LL << 31)) return s->fail(H3C_E_INVALID, "h3c_set_grids: more than 2^31 cells");
+  std::vector<long long> dev2caller(n_tot, -1), caller2dev(ncaller, -1);
+  for (int k = 0; k < ninst; ++k) {
+    for (long long i = 0; i < T[k].fg; ++i) dev2caller[int_start[k] + i] = caller_off[k] + T[k].order[i];
+    for (long long g = T[k].fg; g < T[k].n; ++g) dev2caller[ghost_start[k] + g - T[k].fg] = caller_off[k] + g;
+  }
+  for (long long i = 0; i < n_tot; ++i)
+    if (dev2caller[i] >= 0) caller2dev[dev2caller[i]] = i;
+  // ---- tables in device numbering ----
   free_grid(s);
-  s->n_int = fg;
-  s->n_tot = n;
-  s->ng = n - fg;
-  s->ld = (n + 31) / 32 * 32;
+  s->n_int = n_int;
+  s->n_tot = n_tot;
+  s->ng = ng;
+  s->n_caller = ncaller;
+  s->ld = (n_tot + 31) / 32 * 32;
   s->nsub = nsub;
   s->nlev = (int)lens.size();
+  s->n_inst = ninst;
+  s->ntiles = (n_int + kBlock - 1) / kBlock;
   for (int i = 0; i < kMaxLevels; ++i) s->lens[i] = i < s->nlev ? lens[i] : 0.0;
   const long long L = s->ld;
   std::vector<int> h_nbr(np * L, -1);
   std::vector<unsigned char> h_lvl(L, 0);
   std::vector<double> h_xc(nd * L, 0.0);
-  for (long long i = 0; i < n; ++i) {
-    const long long c = dev2caller[i];
-    h_lvl[i] = (unsigned char)(std::find(lens.begin(), lens.end(), gr->length[c]) - lens.begin());
-    for (int d = 0; d < nd; ++d) h_xc[d * L + i] = gr->x_center[d * ld + c];
-    for (int p = 0; p < np; ++p) {
-      const long long v = nb(p, c);
-      if (valid_cell(v, n)) h_nbr[p * L + i] = (int)caller2dev[v];
-      else if (i < fg && is_group(v)) h_nbr[p * L + i] = (int)v;
-    }
-  }
   std::vector<int> h_sub(nsubc * std::max<long long>(nsub, 1), 0);
-  for (long long k = 0; k < nsub; ++k)
-    for (int j = 0; j < nsubc; ++j) h_sub[j * nsub + k] = (int)caller2dev[gr->subface_cells[j * nsub + k]];
-  std::vector<int> h_gb(s->ng);
-  std::vector<unsigned char> h_gpos(s->ng);
-  std::vector<double> h_gdx(s->ng);
-  for (long long i = 0; i < s->ng; ++i) {
-    const long long g = fg + i;
-    const long long b = gb[i];
-    h_gb[i] = (int)caller2dev[b];
-    h_gpos[i] = (unsigned char)(gbp[i] ^ 1);  // ghost position w.r.t. its boundary cell
-    double s2 = 0;
-    for (int d = 0; d < nd; ++d) {
-      const double dd = gr->x_center[d * ld + b] - gr->x_center[d * ld + g];
-      s2 += dd * dd;
+  const long long ngm = std::max<long long>(1, ng);
+  std::vector<int> h_gb(ngm, 0), h_ginst(ngm, 0);
+  std::vector<unsigned char> h_gpos(ngm, 0), h_apply(ngm, 255), h_own(ngm, 0);
+  std::vector<double> h_gdx(ngm, 0.0);
+  std::vector<int> h_blk(std::max<long long>(1, s->ntiles), 0);
+  for (int k = 0; k < ninst; ++k) {
+    const h3c_grid& gr = grids[k];
+    const InstanceTables& I = T[k];
+    const long long co = caller_off[k];
+    auto to_dev = [&](long long v) -> int {
+      if (valid_cell(v, I.n)) return (int)caller2dev[co + v];
+      if (I.nsub > 0 && v <= -2 && (-v - 2) < I.nsub) return (int)(v - sub_off[k]);  // -2 - (local + offset)
+      return -1;
+    };
+    for (long long c = 0; c < I.n; ++c) {
+      const long long i = caller2dev[co + c];
+      h_lvl[i] = (unsigned char)(std::find(lens.begin(), lens.end(), gr.length[c]) - lens.begin());
+      for (int d = 0; d < nd; ++d) h_xc[d * L + i] = gr.x_center[d * I.ld + c];
+      for (int p = 0; p < np; ++p) {
+        const long long v = gr.neighbors[p * I.ld + c];
+        if (c < I.fg || valid_cell(v, I.n)) h_nbr[p * L + i] = to_dev(v);
+      }
     }
-    h_gdx[i] = std::sqrt(s2);
+    for (long long q = 0; q < I.nsub; ++q)
+      for (int j = 0; j < nsubc; ++j)
+        h_sub[j * nsub + sub_off[k] + q] = (int)caller2dev[co + gr.subface_cells[j * I.nsub + q]];
+    for (long long g = 0; g < I.n - I.fg; ++g) {
+      const long long gi = ghost_start[k] - n_int + g;
+      const long long b = I.gb[g];
+      h_gb[gi] = (int)caller2dev[co + b];
+      h_gpos[gi] = (unsigned char)(I.gbp[g] ^ 1);  // ghost position w.r.t. its boundary cell
+      h_apply[gi] = I.apply[g] == 255 ? 255 : bcmap[k][I.apply[g]];
+      h_own[gi] = bcmap[k][I.own[g]];
+      h_ginst[gi] = k;
+      double s2 = 0;
+      for (int d = 0; d < nd; ++d) {
+        const double dd = gr.x_center[d * I.ld + b] - gr.x_center[d * I.ld + I.fg + g];
+        s2 += dd * dd;
+      }
+      h_gdx[gi] = std::sqrt(s2);
+    }
+    for (long long t = int_start[k] / kBlock; t * kBlock < int_end[k]; ++t) h_blk[t] = k;
   }
-  s->needs_partner = s->needs_periodic = false;
-  s->bcs.assign(gr->bcs, gr->bcs + gr->n_bcs);
-  s->n_bcs = gr->n_bcs;
-  s->h_bcs.assign(std::max(1, gr->n_bcs), BcParam{});
+  s->bcs = ubcs;
+  s->n_bcs = (int)ubcs.size();
+  s->h_bcs.assign(std::max<size_t>(1, ubcs.size()), BcParam{});
   s->unfused_dt = false;
-  for (int k = 0; k < gr->n_bcs; ++k) {
-    BcParam& B = s->h_bcs[k];
-    B.kind = gr->bcs[k].kind;
-    if (B.kind < 0 || B.kind > H3C_BC_PERIODIC) return s->fail(H3C_E_INVALID, "h3c_set_grid: bc %d kind %d", k, B.kind);
+  s->needs_partner = s->needs_periodic = false;
+  for (size_t q = 0; q < ubcs.size(); ++q) {
+    BcParam& B = s->h_bcs[q];
+    B.kind = ubcs[q].kind;
+    if (B.kind < 0 || B.kind > H3C_BC_PERIODIC) return s->fail(H3C_E_INVALID, "h3c_set_grid: bc kind %d", B.kind);
     B.wall = (B.kind == H3C_BC_CNS_ADIABATIC_NOSLIP || B.kind == H3C_BC_CNS_ISOTHERMAL_NOSLIP ||
               B.kind == H3C_BC_CPL_CNS_HEAT);
-    for (int j = 0; j < 8; ++j) B.v[j] = gr->bcs[k].v[j];
+    for (int j = 0; j < 8; ++j) B.v[j] = ubcs[q].v[j];
     if (B.kind == H3C_BC_EULER_VORTEX) {
       if (nd != 2 || s->desc.physics == H3C_HEAT)
         return s->fail(H3C_E_INVALID, "h3c_set_grid: the isentropic vortex condition is 2D Euler/CNS only "
@@ -583,6 +685,8 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
     if (B.kind >= H3C_BC_CPL_EULER_EULER && B.kind <= H3C_BC_CPL_HEAT_HEAT) s->needs_partner = true;
     if (B.kind == H3C_BC_PERIODIC) s->needs_periodic = true;
   }
+  if (ninst > 1 && (s->needs_partner || s->needs_periodic))
+    return s->fail(H3C_E_INVALID, "h3c_set_grids: coupling and periodic conditions need a single grid");
   s->dev2caller = dev2caller;
   s->caller2dev = caller2dev;
   s->partner = nullptr;
@@ -592,7 +696,6 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
   H3C_CUDA(s, cudaMalloc(&s->d_lvl, L));
   H3C_CUDA(s, cudaMalloc(&s->d_sub, sizeof(int) * h_sub.size()));
   H3C_CUDA(s, cudaMalloc(&s->d_xc, sizeof(double) * nd * L));
-  const long long ngm = std::max<long long>(1, s->ng);
   H3C_CUDA(s, cudaMalloc(&s->d_gbndry, sizeof(int) * ngm));
   H3C_CUDA(s, cudaMalloc(&s->d_gpos, ngm));
   H3C_CUDA(s, cudaMalloc(&s->d_gapply, ngm));
@@ -603,27 +706,44 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* gr) {
   H3C_CUDA(s, cudaMalloc(&s->d_q[0], sizeof(double) * s->nv * L));
   H3C_CUDA(s, cudaMalloc(&s->d_q[1], sizeof(double) * s->nv * L));
   if (s->desc.physics == H3C_CNS) H3C_CUDA(s, cudaMalloc(&s->d_slopes, sizeof(double) * nd * s->nv * L));
-  H3C_CUDA(s, cudaMalloc(&s->d_dev2caller, sizeof(long long) * n));
-  // uploads (synchronous: tables are set once)
+  H3C_CUDA(s, cudaMalloc(&s->d_dev2caller, sizeof(long long) * n_tot));
+  if (ninst > 1) {
+    H3C_CUDA(s, cudaMalloc(&s->d_blk_inst, sizeof(int) * h_blk.size()));
+    H3C_CUDA(s, cudaMalloc(&s->d_inst_end, sizeof(long long) * ninst));
+    H3C_CUDA(s, cudaMalloc(&s->d_ginst, sizeof(int) * ngm));
+    H3C_CUDA(s, cudaMemcpy(s->d_blk_inst, h_blk.data(), sizeof(int) * h_blk.size(), cudaMemcpyHostToDevice));
+    H3C_CUDA(s, cudaMemcpy(s->d_inst_end, int_end.data(), sizeof(long long) * ninst, cudaMemcpyHostToDevice));
+    H3C_CUDA(s, cudaMemcpy(s->d_ginst, h_ginst.data(), sizeof(int) * ngm, cudaMemcpyHostToDevice));
+  }
+  if (ninst != s->sc_count) {  // one Scalars per instance
+    H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+    dfree(s->d_sc);
+    H3C_CUDA(s, cudaMalloc(&s->d_sc, sizeof(Scalars) * ninst));
+    s->sc_count = ninst;
+  }
   H3C_CUDA(s, cudaMemcpy(s->d_nbr, h_nbr.data(), sizeof(int) * np * L, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemcpy(s->d_lvl, h_lvl.data(), L, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemcpy(s->d_sub, h_sub.data(), sizeof(int) * h_sub.size(), cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemcpy(s->d_xc, h_xc.data(), sizeof(double) * nd * L, cudaMemcpyHostToDevice));
-  if (s->ng > 0) {
-    H3C_CUDA(s, cudaMemcpy(s->d_gbndry, h_gb.data(), sizeof(int) * s->ng, cudaMemcpyHostToDevice));
-    H3C_CUDA(s, cudaMemcpy(s->d_gpos, h_gpos.data(), s->ng, cudaMemcpyHostToDevice));
-    H3C_CUDA(s, cudaMemcpy(s->d_gapply, apply.data(), s->ng, cudaMemcpyHostToDevice));
-    H3C_CUDA(s, cudaMemcpy(s->d_gown, own.data(), s->ng, cudaMemcpyHostToDevice));
-    H3C_CUDA(s, cudaMemcpy(s->d_gdx, h_gdx.data(), sizeof(double) * s->ng, cudaMemcpyHostToDevice));
-  }
+  H3C_CUDA(s, cudaMemcpy(s->d_gbndry, h_gb.data(), sizeof(int) * ngm, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_gpos, h_gpos.data(), ngm, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_gapply, h_apply.data(), ngm, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_gown, h_own.data(), ngm, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_gdx, h_gdx.data(), sizeof(double) * ngm, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemset(s->d_gpartner, 0xff, sizeof(int) * ngm));
   H3C_CUDA(s, cudaMemcpy(s->d_bcs, s->h_bcs.data(), sizeof(BcParam) * s->h_bcs.size(), cudaMemcpyHostToDevice));
-  H3C_CUDA(s, cudaMemcpy(s->d_dev2caller, dev2caller.data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaMemcpy(s->d_dev2caller, dev2caller.data(), sizeof(long long) * n_tot, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemset(s->d_q[0], 0, sizeof(double) * s->nv * L));
   H3C_CUDA(s, cudaMemset(s->d_q[1], 0, sizeof(double) * s->nv * L));
+  k_init_time<<<blocks(ninst), kBlock, 0, s->stream>>>(s->d_sc, s->desc.time_end, ninst);
+  H3C_CUDA(s, cudaGetLastError());
   s->has_grid = true;
   return H3C_OK;
 }
+
+int h3c_set_grid(h3c_solver s, const h3c_grid* gr) { return set_grids(s, 1, gr); }
+
+int h3c_set_grids(h3c_solver s, int n, const h3c_grid* grids) { return set_grids(s, n, grids); }
 
 // Coupling and periodic conditions read partner cells: refuse to launch them
 // before the partner tables exist.
@@ -649,14 +769,15 @@ static int ensure_stage(h3c_solver s, long long ld) {
 int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld) {
   if (!s || !q || (which != 0 && which != 1)) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_set_state: no grid");
-  if (ld < s->n_tot) return s->fail(H3C_E_INVALID, "h3c_set_state: ld < n_cells");
-  int rc = ensure_stage(s, s->n_tot);
+  const long long nc = s->n_caller;
+  if (ld < nc) return s->fail(H3C_E_INVALID, "h3c_set_state: ld < n_cells");
+  int rc = ensure_stage(s, nc);
   if (rc) return rc;
   for (int v = 0; v < s->nv; ++v)
-    H3C_CUDA(s, cudaMemcpyAsync(s->d_stage + v * s->n_tot, q + v * ld, sizeof(double) * s->n_tot,
-                                cudaMemcpyHostToDevice, s->stream));
-  k_gather<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_stage, s->n_tot, s->d_q[which], s->ld,
-                                                       s->d_dev2caller, s->n_tot, s->nv);
+    H3C_CUDA(s, cudaMemcpyAsync(s->d_stage + v * nc, q + v * ld, sizeof(double) * nc, cudaMemcpyHostToDevice,
+                                s->stream));
+  k_gather<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_stage, nc, s->d_q[which], s->ld, s->d_dev2caller,
+                                                       s->n_tot, s->nv);
   if (which == 0) launch_cfl(s, &s->d_sc->dtmin_ord);
   H3C_CUDA(s, cudaStreamSynchronize(s->stream));
   return s->cuda(cudaGetLastError(), "h3c_set_state");
@@ -665,14 +786,15 @@ int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld) {
 int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld) {
   if (!s || !q || (which != 0 && which != 1)) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_get_state: no grid");
-  if (ld < s->n_tot) return s->fail(H3C_E_INVALID, "h3c_get_state: ld < n_cells");
-  int rc = ensure_stage(s, s->n_tot);
+  const long long nc = s->n_caller;
+  if (ld < nc) return s->fail(H3C_E_INVALID, "h3c_get_state: ld < n_cells");
+  int rc = ensure_stage(s, nc);
   if (rc) return rc;
-  k_scatter<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_q[which], s->ld, s->d_stage, s->n_tot,
-                                                        s->d_dev2caller, s->n_tot, s->nv);
+  k_scatter<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_q[which], s->ld, s->d_stage, nc, s->d_dev2caller,
+                                                        s->n_tot, s->nv);
   for (int v = 0; v < s->nv; ++v)
-    H3C_CUDA(s, cudaMemcpyAsync(q + v * ld, s->d_stage + v * s->n_tot, sizeof(double) * s->n_tot,
-                                cudaMemcpyDeviceToHost, s->stream));
+    H3C_CUDA(s, cudaMemcpyAsync(q + v * ld, s->d_stage + v * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost,
+                                s->stream));
   H3C_CUDA(s, cudaStreamSynchronize(s->stream));
   return s->cuda(cudaGetLastError(), "h3c_get_state");
 }
@@ -688,7 +810,7 @@ int h3c_state_device(h3c_solver s, int which, double** ptr, int64_t* ld) {
 int h3c_device_order(h3c_solver s, int64_t* perm) {
   if (!s || !perm) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_device_order: no grid");
-  for (long long c = 0; c < s->n_tot; ++c) perm[c] = s->caller2dev[c];
+  for (long long c = 0; c < s->n_caller; ++c) perm[c] = s->caller2dev[c];
   return H3C_OK;
 }
 
@@ -700,7 +822,7 @@ int h3c_get_stream(h3c_solver s, void** stream) {
 
 int h3c_sizes(h3c_solver s, int64_t* n_cells, int64_t* first_ghost, int* nv) {
   if (!s) return H3C_E_INVALID;
-  if (n_cells) *n_cells = s->n_tot;
+  if (n_cells) *n_cells = s->n_caller;
   if (first_ghost) *first_ghost = s->n_int;
   if (nv) *nv = s->nv;
   return H3C_OK;
@@ -710,9 +832,9 @@ int h3c_reset_time(h3c_solver s) {
   if (!s) return H3C_E_INVALID;
   if (s->ng < 0) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_reset_time: no grid");
-  k_init_time<<<1, 1, 0, s->stream>>>(s->d_sc, s->desc.time_end);
+  k_init_time<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, s->desc.time_end, s->n_inst);
   launch_cfl(s, &s->d_sc->dtmin_ord);
-  k_set_dt<<<1, 1, 0, s->stream>>>(s->d_sc, 0);
+  k_set_dt<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, 0, s->n_inst);
   return s->cuda(cudaGetLastError(), "h3c_reset_time");
 }
 
@@ -732,7 +854,7 @@ static void enqueue_steps(h3c_solver s, int64_t nsteps) {
     if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
     {
       Launch L(s, K_SCALAR);
-      k_set_dt<<<1, 1, 0, s->stream>>>(s->d_sc, 1);
+      k_set_dt<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, 1, s->n_inst);
     }
     if (cns) launch_slopes(s, 0);
     if (s->desc.time_integration == H3C_EULER_FORWARD) {
@@ -748,7 +870,7 @@ static void enqueue_steps(h3c_solver s, int64_t nsteps) {
     }
     {
       Launch L(s, K_SCALAR);
-      k_advance<<<1, 1, 0, s->stream>>>(s->d_sc);
+      k_advance<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, s->n_inst);
     }
   }
 }
@@ -878,7 +1000,7 @@ int h3c_set_partner(h3c_solver s, h3c_solver partner, const int64_t* partner_cel
   std::vector<int> h(std::max<long long>(1, s->ng), -1);
   for (long long i = 0; i < s->ng; ++i) {
     const long long o = partner_cells[i];
-    if (o >= 0 && o < partner->n_tot) h[i] = (int)partner->caller2dev[o];
+    if (o >= 0 && o < partner->n_caller) h[i] = (int)partner->caller2dev[o];
   }
   // every ghost of a coupling condition needs a partner cell
   std::vector<unsigned char> own(s->ng);
@@ -981,6 +1103,86 @@ int h3c_set_option(h3c_solver s, int option, int value) {
   }
   drop_graph(s);
   return H3C_OK;
+}
+
+int h3c_instances(h3c_solver s, double* dt, double* time, int64_t* step) {
+  if (!s) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_instances: no grid");
+  std::vector<Scalars> h(s->n_inst);
+  H3C_CUDA(s, cudaMemcpyAsync(h.data(), s->d_sc, sizeof(Scalars) * s->n_inst, cudaMemcpyDeviceToHost, s->stream));
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  for (int i = 0; i < s->n_inst; ++i) {
+    if (dt) dt[i] = h[i].dt;
+    if (time) time[i] = h[i].time;
+    if (step) step[i] = h[i].step;
+  }
+  return H3C_OK;
+}
+
+// Times `nsteps` steps for each launch configuration (stage kernel variant x
+// persistent grid size) from the same saved state and keeps the fastest.
+int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_out) {
+  if (!s || nsteps < 1) return H3C_E_INVALID;
+  if (int rc = ready(s, "h3c_autotune")) return rc;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int cand_persist[5] = {0, sms, 2 * sms, 3 * sms, 4 * sms};
+  const size_t qbytes = sizeof(double) * s->nv * s->ld;
+  double* save = nullptr;
+  Scalars* save_sc = nullptr;
+  H3C_CUDA(s, cudaMalloc(&save, 2 * qbytes));
+  H3C_CUDA(s, cudaMalloc(&save_sc, sizeof(Scalars) * s->n_inst));
+  double* const q0 = s->d_q[0];
+  double* const q1 = s->d_q[1];
+  cudaMemcpyAsync(save, q0, qbytes, cudaMemcpyDeviceToDevice, s->stream);
+  cudaMemcpyAsync(save + s->nv * s->ld, q1, qbytes, cudaMemcpyDeviceToDevice, s->stream);
+  cudaMemcpyAsync(save_sc, s->d_sc, sizeof(Scalars) * s->n_inst, cudaMemcpyDeviceToDevice, s->stream);
+  auto restore = [&]() {
+    s->d_q[0] = q0;  // forward Euler swaps the buffers
+    s->d_q[1] = q1;
+    cudaMemcpyAsync(q0, save, qbytes, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(q1, save + s->nv * s->ld, qbytes, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(s->d_sc, save_sc, sizeof(Scalars) * s->n_inst, cudaMemcpyDeviceToDevice, s->stream);
+  };
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  int best = 0;
+  double best_ms = 1e300;
+  const bool prof = s->prof;
+  s->prof = false;
+  for (int tile = 1; tile >= 0; --tile) {
+    for (int k = 0; k < 5; ++k) {
+      const int idx = (1 - tile) * 5 + k;
+      if (!tile && k > 0) continue;  // the per-cell kernel has no persistent variant
+      restore();
+      s->tile = tile != 0;
+      s->persist_blocks = cand_persist[k];
+      drop_graph(s);
+      h3c_solve(s, 1);  // warm-up (kernel attributes, graph capture below)
+      cudaEventRecord(a, s->stream);
+      h3c_solve(s, nsteps);
+      cudaEventRecord(b, s->stream);
+      cudaEventSynchronize(b);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      if (ms < best_ms) { best_ms = ms; best = idx; }
+    }
+  }
+  s->prof = prof;
+  restore();
+  s->tile = best < 5;
+  s->persist_blocks = best < 5 ? cand_persist[best] : 0;
+  drop_graph(s);
+  cudaStreamSynchronize(s->stream);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(save);
+  cudaFree(save_sc);
+  if (choice) *choice = best;
+  if (ms_out) *ms_out = best_ms / nsteps;
+  return s->cuda(cudaGetLastError(), "h3c_autotune");
 }
 
 int h3c_launches(h3c_solver s, int64_t* n) {

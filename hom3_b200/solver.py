@@ -275,6 +275,56 @@ class Solver:
         self._check(lib().h3c_set_periodic(self.h, _lp(pc)))
 
 
+class Batch(Solver):
+    """Independent grids of one solver description advanced together
+    (h3c_set_grids): one launch per stage over all instances, per-instance
+    dt / time / step.  State arrays are the instances' cells concatenated."""
+
+    def set_grids(self, tables: Sequence[dict], conditions: Sequence[Sequence[Condition]]):
+        keep = []
+        grids = (F.Grid * len(tables))()
+        for k, (t, conds) in enumerate(zip(tables, conditions)):
+            nb = np.ascontiguousarray(t["neighbors"], np.int64)
+            xc = np.ascontiguousarray(t["x_center"], np.float64)
+            ln = np.ascontiguousarray(t["length"], np.float64)
+            bc = np.ascontiguousarray(t["bc_idx"], np.int32)
+            arr = (F.Bc * max(1, len(conds)))()
+            for i, c in enumerate(conds):
+                arr[i] = c.to_c()
+            g = grids[k]
+            n = ln.shape[0]
+            g.n_cells, g.first_ghost, g.ld = n, int(t["first_ghost"]), n
+            g.neighbors, g.x_center, g.length = _lp(nb), _dp(xc), _dp(ln)
+            g.bc_idx = bc.ctypes.data_as(C.POINTER(C.c_int32))
+            g.n_bcs, g.bcs = len(conds), arr
+            sub = t.get("subface_cells")
+            if sub is not None and np.asarray(sub).size:
+                sub = np.ascontiguousarray(sub, np.int64)
+                g.n_subfaces, g.subface_cells = sub.shape[1], _lp(sub)
+                keep.append(sub)
+            keep += [nb, xc, ln, bc, arr]
+        self._check(lib().h3c_set_grids(self.h, len(tables), grids))
+        self.sizes = [int(t["ncells"]) for t in tables]
+        self.offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+        self.n_cells = int(self.offsets[-1])
+        self.first_ghost = sum(int(t["first_ghost"]) for t in tables)
+        self.n_instances = len(tables)
+
+    def instance_state(self, q, k):
+        return q[:, self.offsets[k]:self.offsets[k + 1]]
+
+    def instances(self):
+        n = self.n_instances
+        dt, tm, st = np.empty(n), np.empty(n), np.empty(n, np.int64)
+        self._check(lib().h3c_instances(self.h, _dp(dt), _dp(tm), _lp(st)))
+        return dt, tm, st
+
+    def autotune(self, nsteps=20):
+        ch, ms = C.c_int(), C.c_double()
+        self._check(lib().h3c_autotune(self.h, nsteps, C.byref(ch), C.byref(ms)))
+        return ch.value, ms.value
+
+
 def couple_cht(Tr0, cns: Solver, heat: Solver):
     """coupling::apply(Tr0, cns, heat) -- coupling.hpp:167-183."""
     check(lib().h3c_couple_cht(cns.h, heat.h, float(Tr0)), cns.h)

@@ -65,3 +65,60 @@ def riemann3d_oracle_ic(modes, amp=0.01):
 
 def riemann3d_conditions(nd=3):
     return [euler_neumann() for _ in range(2 * nd)]
+
+
+# ---------------------------------------------------------------------------
+# Ensemble of independent 2D isentropic vortices (batched workload).
+# ---------------------------------------------------------------------------
+def vortex_ic(beta, cx, cy, u=1.0, v=1.0, gamma=1.4):
+    """hom3's isentropic vortex (euler/initial_conditions.hpp:343-368) with the
+    strength and centre as parameters (hom3 fixes beta = 5, centre (-5, -5))."""
+    def f(x):
+        dx, dy = x[0] - cx, x[1] - cy
+        r2 = dx * dx + dy * dy
+        e1 = np.exp(1 - r2)
+        e2 = np.exp(2 * (1 - r2))
+        uu = u - beta * e1 * dy / (2 * math.pi)
+        vv = v + beta * e1 * dx / (2 * math.pi)
+        rho = (1 - ((gamma - 1) * beta ** 2 * e2) / (16 * gamma * math.pi ** 2)) ** (1 / (gamma - 1))
+        p = rho ** gamma
+        q = np.empty((4, x.shape[1]))
+        q[0], q[1], q[2] = rho * uu, rho * vv, rho
+        q[3] = p / (gamma - 1.0) + 0.5 * rho * (uu * uu + vv * vv)
+        return q
+    return f
+
+
+def ensemble_members(n=256, seed=3, nmin=32, nmax=512, patch_max=0.3, h=10.0 / 512):
+    """Per-instance parameters: grid nx x ny in U{nmin..nmax}^2 embedded in a
+    square root cell at level ceil(log2(max(nx, ny))) with a box domain, a
+    refinement patch (+1 level disc) covering U[0, patch_max] of the box, and a
+    vortex of strength U[1, 5] centred uniformly in the box."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(n):
+        nx, ny = (int(v) for v in rng.integers(nmin, nmax + 1, size=2))
+        level = int(math.ceil(math.log2(max(nx, ny))))
+        frac = float(rng.uniform(0.0, patch_max))
+        area = frac * nx * ny * h * h
+        pr = math.sqrt(area / math.pi)
+        pc = (float(rng.uniform(0, nx * h)), float(rng.uniform(0, ny * h)))
+        beta = float(rng.uniform(1.0, 5.0))
+        cc = (float(rng.uniform(0, nx * h)), float(rng.uniform(0, ny * h)))
+        out.append(dict(nx=nx, ny=ny, level=level, h=h, patch=(pc, pr), patch_frac=frac, beta=beta, centre=cc))
+    return out
+
+
+def ensemble_member_tables(m):
+    """Grid tables of one ensemble member from the library's builder."""
+    from .solver import GridSpec, build_tables, edge, square
+    h, nx, ny, level = m["h"], m["nx"], m["ny"], m["level"]
+    side = h * 2 ** level
+    (px, py), pr = m["patch"]
+    refine = [([px, py], pr, level + 1)] if pr > 0.5 * h else []
+    spec = GridSpec(2, [0.0, 0.0], [side, side], level, refine=refine)
+    lx, ly = nx * h, ny * h
+    eps = side * 1e-15
+    geoms = [edge([eps, 0], [1, 0]), edge([lx - eps, 0], [-1, 0]), edge([0, eps], [0, 1]), edge([0, ly - eps], [0, -1])]
+    dom = square([0.5 * lx, 0.5 * ly], [lx, ly])
+    return build_tables(spec, geoms, dom, 2)

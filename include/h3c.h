@@ -152,6 +152,23 @@ int h3c_destroy(h3c_solver s);
  * s is NULL) into buf and returns its full length. */
 int h3c_last_error(h3c_solver s, char* buf, size_t n);
 
+/* ---- batches (no hom3 counterpart: hom3 steps one solver at a time) ----
+ * h3c_set_grids: n independent grids (instances) of one solver description
+ * advanced together: every stage is one launch over all instances' cells, each
+ * instance keeps its own dt / time / step.  The caller numbering is the
+ * concatenation of the instances' cells (instance k's cell c is caller cell
+ * sum_{j<k} n_cells_j + c) for h3c_set_state / h3c_get_state / h3c_device_order.
+ * Euler and heat only; no coupling or periodic conditions.  h3c_dt / h3c_time /
+ * h3c_step / h3c_min_dt / h3c_force_dt refer to instance 0. */
+int h3c_set_grids(h3c_solver s, int n, const h3c_grid* grids);
+/* per-instance dt, time and step (arrays of n; any may be NULL) */
+int h3c_instances(h3c_solver s, double* dt, double* time, int64_t* step);
+/* Times nsteps steps for each launch configuration -- stage kernel variant
+ * (shared-memory tile or per cell) x persistent grid size (one block per tile,
+ * or 1-4 blocks per SM) -- from the same saved state, restores the state and
+ * keeps the fastest; returns its index and its time per step (ms). */
+int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_per_step);
+
 /* ---- data: the tables create_local_cells/create_ghost_cells build
  * (solver.hpp:876-977) and the state columns lhs/rhs (container.hpp:59-60) ---- */
 int h3c_set_grid(h3c_solver s, const h3c_grid* grid);

@@ -1,0 +1,69 @@
+"""Batched independent grids (h3c_set_grids): every instance of a batch must
+evolve exactly as the same grid stepped alone, each with its own dt."""
+import numpy as np
+import pytest
+
+import hom3_b200 as hb
+from hom3_b200 import _ffi as F
+from hom3_b200 import workloads as W
+from hom3_b200.solver import euler_neumann
+
+pytestmark = pytest.mark.gpu
+
+
+def members(n=6):
+    ms = W.ensemble_members(n, seed=11, nmin=12, nmax=40)
+    tables = [W.ensemble_member_tables(m) for m in ms]
+    states = []
+    for m, t in zip(ms, tables):
+        fg = t["first_ghost"]
+        q = np.zeros((4, t["ncells"]))
+        q[:, :fg] = hb.cell_average(W.vortex_ic(m["beta"], *m["centre"]), t["x_center"][:, :fg], t["length"][:fg], 2)
+        states.append(q)
+    return ms, tables, states
+
+
+@pytest.mark.parametrize("ti", [F.EULER_FORWARD, F.RUNGE_KUTTA_2])
+@pytest.mark.parametrize("precision", [F.FP64, F.MIXED])
+def test_batch_matches_single_instances(ti, precision):
+    ms, tables, states = members()
+    conds = [[euler_neumann() for _ in range(4)] for _ in tables]
+    b = hb.Batch(2, F.EULER, F.FLUX_AUSM, ti, precision, cfl=0.4, time_end=1e9)
+    b.set_grids(tables, conds)
+    b.set_state(np.concatenate(states, axis=1), 0)
+    b.reset_time()
+    b.solve(7)
+    qb = b.state(0)
+    dtb, tb, sb = b.instances()
+    assert np.all(sb == 7)
+    assert len(set(np.round(dtb, 15))) > 1  # instances keep their own time step
+    for k, (t, q0) in enumerate(zip(tables, states)):
+        s = hb.Solver(2, F.EULER, F.FLUX_AUSM, ti, precision, cfl=0.4, time_end=1e9)
+        s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"], conds[k],
+                   t["subface_cells"])
+        s.set_state(q0, 0)
+        s.reset_time()
+        s.solve(7)
+        fg = t["first_ghost"]
+        assert np.array_equal(b.instance_state(qb, k)[:, :fg], s.state(0)[:, :fg]), k
+        assert dtb[k] == s.dt() and tb[k] == s.time()
+
+
+def test_autotune_keeps_the_state():
+    ms, tables, states = members(5)
+    conds = [[euler_neumann() for _ in range(4)] for _ in tables]
+
+    def make():
+        b = hb.Batch(2, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, F.FP64, cfl=0.4, time_end=1e9)
+        b.set_grids(tables, conds)
+        b.set_state(np.concatenate(states, axis=1), 0)
+        b.reset_time()
+        return b
+
+    a, b = make(), make()
+    choice, ms_step = a.autotune(4)
+    assert 0 <= choice < 10 and ms_step > 0
+    a.solve(9)
+    b.solve(9)
+    assert np.array_equal(a.state(0), b.state(0))
+    assert np.array_equal(a.instances()[1], b.instances()[1])
