@@ -219,6 +219,100 @@ def workload_config(args, t):
     return cfg
 
 
+def run_ensemble(args, ws, rank, local):
+    """Batched workload: 256 independent 2D isentropic-vortex grids of uneven
+    size (nx, ny in U{32..512}, +1-level patches on 0-30% of each box), one
+    launch per stage over all of them, launch shape from the autotuner."""
+    import concurrent.futures as cf
+
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200 import workloads as W
+    from hom3_b200.solver import euler_neumann
+
+    torch.cuda.set_device(local)
+    ms = W.ensemble_members(args.members)
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:  # the builder releases the GIL
+        tables = list(ex.map(W.ensemble_member_tables, ms))
+
+    def ic(mt):
+        m, t = mt
+        fg = t["first_ghost"]
+        q = np.zeros((4, t["ncells"]))
+        q[:, :fg] = hb.cell_average(W.vortex_ic(m["beta"], *m["centre"]), t["x_center"][:, :fg], t["length"][:fg], 2)
+        return q
+
+    with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        states = list(ex.map(ic, zip(ms, tables)))
+    q0 = np.concatenate(states, axis=1)
+    cells = sum(t["first_ghost"] for t in tables)
+    results = {}
+    for prec_name in ("mixed", "fp64"):
+        prec = F.MIXED if prec_name == "mixed" else F.FP64
+        b = hb.Batch(2, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, prec, cfl=args.cfl, time_end=1e30)
+        b.set_grids(tables, [[euler_neumann() for _ in range(4)] for _ in tables])
+        b.set_state(q0, 0)
+        b.reset_time()
+        choice, _ = b.autotune(10)
+        stream = torch.cuda.ExternalStream(b.stream())
+        b.solve(args.warmup)
+        torch.cuda.synchronize()
+        barrier(ws)
+        l0 = b.launches()
+        with ClockSampler(local) as clk:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            b.solve(args.steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        ms_ = allreduce_max(ev0.elapsed_time(ev1), ws)
+        results[prec_name] = dict(value=cells * args.steps * ws / (ms_ * 1e-3), ms=ms_, choice=choice,
+                                  launches=b.launches() - l0, clocks=clk.summary(), state=b.state(0))
+        del b
+    # the plain FP64 path without batching: one solver per grid, stepped one after another
+    seq = []
+    for t, q in zip(tables, states):
+        s1 = hb.Solver(2, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, F.FP64, cfl=args.cfl, time_end=1e30)
+        s1.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
+                    [euler_neumann() for _ in range(4)], t["subface_cells"])
+        s1.set_state(q, 0)
+        s1.reset_time()
+        s1.solve(args.warmup)
+        seq.append(s1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s1 in seq:
+        s1.solve(args.steps)
+    torch.cuda.synchronize()
+    seq_s = allreduce_max(time.perf_counter() - t0, ws)
+    seq_value = cells * args.steps * ws / seq_s
+    del seq
+    # accuracy of the mixed path against the FP64 path after the same steps (L2, relative)
+    qa, qb = results["mixed"].pop("state"), results["fp64"].pop("state")
+    l2 = float(np.sqrt(((qa - qb) ** 2).sum() / (qb ** 2).sum()))
+    peak, peak_kind = peaks()
+    r = results["mixed"]
+    line = {
+        "metric": "cell-updates/s", "value": r["value"], "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-flux/f64-state", "data": "synthetic",
+        "config": {"workload": f"{args.members} independent 2D isentropic vortices (nx, ny in U{{32..512}}, "
+                               "+1-level patches on 0-30% of each box, beta in U[1,5]), Neumann outflow, AUSM, RK2, "
+                               "one launch per stage over all instances",
+                   "leaf_cells": int(cells), "autotune_choice": r["choice"], "parallelism": f"replicas x{ws}"},
+        "fp64_value": results["fp64"]["value"], "mixed_over_fp64": r["value"] / results["fp64"]["value"],
+        "plain_fp64_one_grid_at_a_time_value": seq_value, "batched_mixed_over_plain_fp64": r["value"] / seq_value,
+        "l2_rel_mixed_vs_fp64": l2, "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
+        "roofline": {"bound": "hbm", "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
+                     "achieved": cells * (2 * 4 * 8 + 3 * 4 * 8 + 2 * (4 * 4 + 1)) / (r["ms"] / args.steps * 1e-3) / 1e9},
+    }
+    line["roofline"]["frac"] = line["roofline"]["achieved"] / peak
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,9 +324,14 @@ def main():
     ap.add_argument("--extra-levels", type=int, default=2)
     ap.add_argument("--cfl", type=float, default=0.4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble"])
+    ap.add_argument("--members", type=int, default=256)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()
+    if args.workload == "ensemble" and args.impl == "ours":
+        run_ensemble(args, ws, rank, local)
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
         return

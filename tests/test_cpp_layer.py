@@ -25,8 +25,9 @@ def test_cpp_cases_compile_and_link(tmp_path):
 @pytest.mark.gpu
 def test_cpp_cases_run(tmp_path):
     exe = build(tmp_path)
-    out = subprocess.run([exe, "4"], check=True, capture_output=True, text=True, timeout=600).stdout
-    rows = [l.split() for l in out.strip().splitlines()]
+    res = subprocess.run([exe, "4"], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0, res.stdout + res.stderr
+    rows = [l.split() for l in res.stdout.strip().splitlines()]
     names = [r[0] for r in rows]
     assert names == ["euler_constant_ic", "euler_sod_shock_tube_ic", "euler_problem123_ic", "euler_explosion_ic",
                      "euler_isentropic_vortex_ic", "heat_one_dimensional_dirichlet"]
