@@ -283,8 +283,9 @@ def run_ensemble(args, ws, rank, local):
         seq.append(s1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for s1 in seq:
+    for s1 in seq:  # each grid finishes before the next starts (dt read-back synchronises)
         s1.solve(args.steps)
+        s1.dt()
     torch.cuda.synchronize()
     seq_s = allreduce_max(time.perf_counter() - t0, ws)
     seq_value = cells * args.steps * ws / seq_s
@@ -313,6 +314,73 @@ def run_ensemble(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_tgv(args, ws, rank, local):
+    """3D compressible Navier-Stokes Taylor-Green vortex (periodic [0, 2pi]^3,
+    Re 1600, Mach 0.1, Pr 0.71) on a uniform grid, FP64 and mixed precision;
+    kinetic-energy dissipation rate of the mixed path against the FP64 path."""
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200.solver import Condition
+
+    torch.cuda.set_device(local)
+    spec = hb.GridSpec(3, [0.0] * 3, [2 * math.pi] * 3, args.tgv_level)
+    t = hb.build_tables(spec, spec.cube_boundaries())
+    partners = hb.periodic_partners(t, spec)
+    fg = t["first_ghost"]
+    U, r0, p0 = 0.1, 1.0, 1 / 1.4
+
+    def ic(x):
+        u = U * np.sin(x[0]) * np.cos(x[1]) * np.cos(x[2])
+        v = -U * np.cos(x[0]) * np.sin(x[1]) * np.cos(x[2])
+        p = p0 + r0 * U * U / 16.0 * (np.cos(2 * x[0]) + np.cos(2 * x[1])) * (np.cos(2 * x[2]) + 2.0)
+        rho = r0 * p / p0
+        q = np.zeros((5, x.shape[1]))
+        q[0], q[1], q[3] = rho * u, rho * v, rho
+        q[4] = p / 0.4 + 0.5 * rho * (u * u + v * v)
+        return q
+
+    q0 = np.zeros((5, t["ncells"]))
+    q0[:, :fg] = hb.cell_average(ic, t["x_center"][:, :fg], t["length"][:fg], 3)
+    out = {}
+    for name, prec in (("fp64", F.FP64), ("mixed", F.MIXED)):
+        s = hb.Solver(3, F.CNS, F.FLUX_AUSM, F.RUNGE_KUTTA_2, prec, cfl=0.5, cfl_viscous=0.4, Minfty=0.1,
+                      ReInfty=1600.0, Pr0=0.71, time_end=1e30)
+        s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg,
+                   [Condition(F.BC_PERIODIC) for _ in range(6)])
+        s.set_periodic(partners)
+        s.set_state(q0, 0)
+        s.reset_time()
+        stream = torch.cuda.ExternalStream(s.stream())
+        s.solve(args.warmup)
+        torch.cuda.synchronize()
+        ke0 = None
+        with ClockSampler(local) as clk:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            s.solve(args.steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        ms = allreduce_max(ev0.elapsed_time(ev1), ws)
+        q = s.state(0)[:, :fg]
+        ke = 0.5 * ((q[0] ** 2 + q[1] ** 2 + q[2] ** 2) / q[3]).mean()
+        out[name] = dict(value=fg * args.steps * ws / (ms * 1e-3), ms=ms, ke=float(ke), time=s.time(),
+                         clocks=clk.summary())
+    ke_init = float((0.5 * (q0[0, :fg] ** 2 + q0[1, :fg] ** 2) / q0[3, :fg]).mean())
+    line = {"metric": "cell-updates/s", "value": out["fp64"]["value"], "unit": "cell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["fp64"]["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"3D CNS Taylor-Green vortex, periodic [0,2pi]^3, uniform {2 ** args.tgv_level}^3, "
+                                   "Re 1600, Mach 0.1, Pr 0.71, AUSM + three-point viscous, RK2", "leaf_cells": int(fg)},
+            "mixed_value": out["mixed"]["value"], "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
+            "ke_fp64": out["fp64"]["ke"], "ke_mixed": out["mixed"]["ke"], "ke_initial": ke_init,
+            "ke_rel_diff": abs(out["mixed"]["ke"] - out["fp64"]["ke"]) / out["fp64"]["ke"],
+            "sim_time": out["fp64"]["time"], "clocks": out["fp64"]["clocks"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -324,13 +392,17 @@ def main():
     ap.add_argument("--extra-levels", type=int, default=2)
     ap.add_argument("--cfl", type=float, default=0.4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble"])
+    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble", "tgv"])
+    ap.add_argument("--tgv-level", type=int, default=7)
     ap.add_argument("--members", type=int, default=256)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()
     if args.workload == "ensemble" and args.impl == "ours":
         run_ensemble(args, ws, rank, local)
+        return
+    if args.workload == "tgv" and args.impl == "ours":
+        run_tgv(args, ws, rank, local)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)

@@ -128,6 +128,7 @@ void free_grid(h3c_solver s) {
   dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_slopes); dfree(s->d_stage);
   dfree(s->d_dev2caller);
   dfree(s->d_blk_inst); dfree(s->d_inst_end); dfree(s->d_ginst);
+  s->stage_cap = 0;
   s->has_grid = false;
 }
 

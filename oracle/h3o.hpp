@@ -310,6 +310,7 @@ enum BcKind {
   BC_CPL_CNS_HEAT = 11,        // cns/coupling_conditions.hpp:22-43 (CNS side)
   BC_CPL_HEAT_CNS = 12,        // heat/coupling_conditions.hpp:18-38 (heat side)
   BC_CPL_HEAT_HEAT = 13,       // heat/coupling_conditions.hpp:41-61
+  BC_PERIODIC = 14,            // EXTENSION (not in hom3): copy of the cell on the opposite face
 };
 
 struct Bc {
@@ -328,6 +329,7 @@ enum IcKind {
   IC_CONSTANT_CV = 4,   // constant conservative state (heat: T)
   IC_RIEMANN3D_PERTURBED = 5,  // EXTENSION (not in hom3): 3D Riemann + Fourier modes
   IC_VORTEX_PARAM = 6,  // EXTENSION (not in hom3): vortex with centre/strength params
+  IC_TAYLOR_GREEN = 7,  // EXTENSION (not in hom3): 3D Taylor-Green vortex
 };
 
 template <class T> struct World;
@@ -359,6 +361,8 @@ template <class T> struct Solver {
   // trees.  nbr < -1 encodes group k = -nbr - 2 whose 2^(nd-1) finer cells are
   // subs[k * 2^(nd-1) + j], j in increasing child position.
   std::vector<Ind> subs;
+  // EXTENSION: interior cell paired with each periodic ghost (index g - firstGC)
+  std::vector<Ind> periodic_partner;
   // numerical data: solver.hpp:406-416
   T dt_ = 0;
   double time_ = 0, tEnd_ = 0;
@@ -490,6 +494,8 @@ template <class T> struct Solver {
     if (m != INV && pp != INV) return (q(t, pp, v) - q(t, m, v)) / (2. * len[c]);
     if (m != INV) return slope(t, m, v, dir);
     if (pp != INV) return slope(t, pp, v, dir);
+    // EXTENSION: a periodic ghost takes the slope of its paired interior cell
+    if (bcs[bc_idx[c]].kind == BC_PERIODIC) return slope(t, periodic_partner[c - firstGC], v, dir);
     // ghost cell: BC slope of its boundary cell (boundary_condition.hpp:45-67)
     const Ind b = boundary_cell(c);
     const T s = slope(t, b, v, dir);
@@ -801,6 +807,19 @@ template <class T> void Solver<T>::eval_ic(const double* x, State& out) const {
     pvars[nd] = inside ? ic[4] : ic[6];
     pvars[nd + 1] = inside ? ic[5] : ic[7];
     out = cv(pvars);
+  } else if (ic_kind == IC_TAYLOR_GREEN) {
+    // EXTENSION (not in hom3): ic = {U, rho0, p0}; u = U sin x cos y cos z,
+    // v = -U cos x sin y cos z, w = 0, p = p0 + rho0 U^2/16 (cos 2x + cos 2y)(cos 2z + 2),
+    // rho = rho0 p / p0 (isothermal start)
+    const double U = ic[0], r0 = ic[1], p0 = ic[2];
+    const double z = nd == 3 ? x[2] : 0.0;
+    pvars[0] = U * std::sin(x[0]) * std::cos(x[1]) * std::cos(z);
+    pvars[1] = -U * std::cos(x[0]) * std::sin(x[1]) * std::cos(z);
+    if (nd == 3) pvars[2] = 0.0;
+    const double p = p0 + r0 * U * U / 16.0 * (std::cos(2 * x[0]) + std::cos(2 * x[1])) * (std::cos(2 * z) + 2.0);
+    pvars[nd] = r0 * p / p0;
+    pvars[nd + 1] = p;
+    out = cv(pvars);
   } else if (ic_kind == IC_RIEMANN3D_PERTURBED) {
     // EXTENSION (not in hom3).  ic = {x0, rhoL, pL, rhoR, pR, amp, nmodes,
     // then per mode (kx, ky, kz, phase) starting at ic[8]} -- at most 16 modes.
@@ -936,6 +955,11 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
         q(t, g, 0) = 2.0 * Ts - q(t, b, 0);
         break;
       }
+      case BC_PERIODIC: {  // EXTENSION
+        const Ind o = periodic_partner[g - firstGC];
+        for (int v = 0; v < nv; ++v) q(t, g, v) = q(t, o, v);
+        break;
+      }
       case BC_CPL_EULER_EULER: {  // euler/coupling_conditions.hpp:452-460
         const Ind o = partner_cell(g);
         const Solver<T>& os = *w->solvers[B.partner];
@@ -1039,6 +1063,42 @@ template <class T> void Solver<T>::initialize() {
     for (Ind g = first; g < size(); ++g)
       for (int p = 0; p < 2 * nd; ++p)
         if (nbr[p][g] != INV) nbr[opposite_pos[p]][nbr[p][g]] = g;
+  }
+  // EXTENSION: periodic partners -- the interior cell at the ghost's position
+  // wrapped into the root cell
+  {
+    periodic_partner.assign(size() - firstGC, INV);
+    bool any = false;
+    for (auto& b : bcs) any = any || b.kind == BC_PERIODIC;
+    if (any) {
+      const double L = tr.rootLength;
+      double lo[3];
+      for (int d = 0; d < nd; ++d) lo[d] = tr.rootCoords[d] - 0.5 * L;
+      auto key = [&](const double* x, double h) {
+        long long k = 0;
+        for (int d = 0; d < nd; ++d) {
+          double w = x[d] - lo[d];
+          w = w - L * std::floor(w / L);
+          k = k * 4194304LL + (long long)std::floor(w / h);
+        }
+        return k;
+      };
+      std::unordered_map<long long, Ind> cellAt;
+      for (Ind c = 0; c < firstGC; ++c) {
+        double x[3];
+        for (int d = 0; d < nd; ++d) x[d] = xc[d][c];
+        cellAt[key(x, len[c]) * 32 + tr.level(node[c])] = c;
+      }
+      for (Ind g = firstGC; g < size(); ++g) {
+        if (bcs[bc_idx[g]].kind != BC_PERIODIC) continue;
+        double x[3];
+        for (int d = 0; d < nd; ++d) x[d] = xc[d][g];
+        const Ind b = boundary_cell(g);
+        auto it = cellAt.find(key(x, len[g]) * 32 + tr.level(node[b]));
+        if (it == cellAt.end()) throw std::runtime_error("periodic ghost without partner");
+        periodic_partner[g - firstGC] = it->second;
+      }
+    }
   }
   // 5) initial condition: cell average by 2^nd Gauss points
   const double gp = 1 / std::sqrt(3);

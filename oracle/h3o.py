@@ -28,9 +28,10 @@ AUSM, LLF = 0, 1
 EULER_FORWARD, RK2 = 0, 1
 (BC_EULER_NEUMANN, BC_EULER_DIRICHLET, BC_EULER_VORTEX, BC_CNS_INFLOW, BC_CNS_OUTFLOW,
  BC_CNS_ADIABATIC_NOSLIP, BC_CNS_ADIABATIC_SLIP, BC_CNS_ISOTHERMAL_NOSLIP, BC_HEAT_DIRICHLET,
- BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT) = range(14)
+ BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT,
+ BC_PERIODIC) = range(15)
 (IC_CONSTANT_PV, IC_SHOCK_TUBE, IC_VORTEX, IC_EXPLOSION, IC_CONSTANT_CV,
- IC_RIEMANN3D_PERTURBED, IC_VORTEX_PARAM) = range(7)
+ IC_RIEMANN3D_PERTURBED, IC_VORTEX_PARAM, IC_TAYLOR_GREEN) = range(8)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
 
 

@@ -169,7 +169,7 @@ int h3o_partner_cells(void* w, int s, int64_t* out) {
     const int k = so.bcs[so.bc_idx[g]].kind;
     const bool cpl = k == BC_CPL_EULER_EULER || k == BC_CPL_CNS_HEAT || k == BC_CPL_HEAT_CNS ||
                      k == BC_CPL_HEAT_HEAT;
-    out[g - so.firstGC] = cpl ? so.partner_cell(g) : INV;
+    out[g - so.firstGC] = cpl ? so.partner_cell(g) : k == BC_PERIODIC ? so.periodic_partner[g - so.firstGC] : INV;
   }
   return 0;
 }

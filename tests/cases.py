@@ -180,6 +180,32 @@ def gpu_solver_from_oracle(o: "h3o.Solver", precision=0):
     t = o.tables()
     s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
                [Condition(k, v) for k, v in info["bcs"]], t["subface_cells"])
+    if any(k == h3o.BC_PERIODIC for k, _ in info["bcs"]):
+        s.set_periodic(o.partner_cells())
     s.set_state(o.state(0), 0)
     s.reset_time()
     return s
+
+
+def tgv_case(level=4, ti=h3o.RK2):
+    """EXTENSION (not in hom3): 3D Taylor-Green vortex, periodic [0, 2pi]^3,
+    Re = 1600, Mach 0.1, Pr = 0.71 (the CNS benchmark configuration)."""
+    import math
+    w = h3o.World(3, [0, 0, 0], [2 * math.pi] * 3, level=level)
+    bcs = [h3o.bc(h3o.BC_PERIODIC, g) for g in w.cube_boundaries()]
+    s = w.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=bcs, ic_kind=h3o.IC_TAYLOR_GREEN, ic=[0.1, 1.0, 1 / 1.4],
+                     Minfty=0.1, ReInfty=1600.0, Pr0=0.71, cfl=0.5, cfl_viscous=0.4, time_end=10.0,
+                     **{k: v for k, v in CNS_PROPS.items() if k not in ("cfl", "cfl_viscous", "Pr0")})
+    s.initialize()
+    return w, [s]
+
+
+def periodic_vortex_case(level=6, ti=h3o.RK2, flux=h3o.AUSM):
+    """EXTENSION (not in hom3): the 2D isentropic vortex of the first benchmark
+    configuration -- [0, 10]^2, centre (5, 5), beta 5, periodic."""
+    w = h3o.World(2, [0, 0], [10, 10], level=level)
+    bcs = [h3o.bc(h3o.BC_PERIODIC, g) for g in w.cube_boundaries()]
+    s = w.add_solver(h3o.EULER, flux, ti, bcs=bcs, ic_kind=h3o.IC_VORTEX_PARAM, ic=[5.0, 5.0, 5.0, 1.0, 1.0],
+                     time_end=10.0, **dict(EULER_PROPS, cfl=0.5))
+    s.initialize()
+    return w, [s]

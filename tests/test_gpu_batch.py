@@ -65,5 +65,10 @@ def test_autotune_keeps_the_state():
     assert 0 <= choice < 10 and ms_step > 0
     a.solve(9)
     b.solve(9)
-    assert np.array_equal(a.state(0), b.state(0))
-    assert np.array_equal(a.instances()[1], b.instances()[1])
+    # the chosen launch configuration may be the other kernel variant, which
+    # rounds differently (FMA placement), so compare to rounding
+    qa, qb = a.state(0), b.state(0)
+    assert np.max(np.abs(qa - qb)) <= 1e-12 * np.max(np.abs(qb))
+    ta, tb = a.instances()[1], b.instances()[1]
+    assert np.allclose(ta, tb, rtol=1e-12, atol=0)
+    assert np.array_equal(a.instances()[2], b.instances()[2])

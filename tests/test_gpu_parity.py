@@ -228,3 +228,35 @@ def test_newton_reciprocals_within_2ulp():
     assert np.max(np.abs(r - 1.0 / x) / ulp(1.0 / x)) <= 2.0
     ref = 1.0 / np.sqrt(x)
     assert np.max(np.abs(rs - ref) / ulp(ref)) <= 2.0
+
+
+def test_set_grid_twice_reuses_solver():
+    """Re-initialising a solver (a second h3c_set_grid) must leave it usable."""
+    _, (o,) = cases.euler_case("sod", nd=3, level=3)
+    g = cases.gpu_solver_from_oracle(o)
+    g.solve(2)
+    g2 = cases.gpu_solver_from_oracle(o)
+    t = o.tables()
+    from hom3_b200.solver import Condition
+    info = o.info()
+    g.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
+               [Condition(k, v) for k, v in info["bcs"]])
+    g.set_state(o.state(0), 0)
+    g.reset_time()
+    g.solve(3)
+    g2.solve(3)
+    assert np.array_equal(g.state(0), g2.state(0))
+
+
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
+def test_taylor_green_cns_periodic(ti):
+    """EXTENSION: CNS with periodic conditions (Taylor-Green vortex)."""
+    _, (o,) = cases.tgv_case(level=4, ti=ti)
+    run_single(o, nsteps=(1, 3))
+
+
+@pytest.mark.parametrize("flux", [h3o.AUSM, h3o.LLF])
+def test_periodic_vortex_euler(flux):
+    """EXTENSION: periodic 2D isentropic vortex (first benchmark configuration's setup)."""
+    _, (o,) = cases.periodic_vortex_case(level=6, flux=flux)
+    run_single(o)

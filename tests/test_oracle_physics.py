@@ -1,0 +1,146 @@
+"""Known-answer checks of the oracle's finite-volume arithmetic (hom3's own
+solver tests carry no numeric assertions, so these pin the restatement)."""
+import math
+
+import numpy as np
+import pytest
+
+import cases
+from oracle import h3o
+
+
+def test_constant_state_preserved_exactly():
+    """euler_fv_solver_test.cpp:82-84: the solution is the initial condition for all t."""
+    _, (o,) = cases.euler_case("constant", nd=3, level=3)
+    q0 = o.state(0)[:, : o.first_ghost].copy()
+    o.solve(20)
+    assert np.array_equal(o.state(0)[:, : o.first_ghost], q0)
+
+
+def test_cns_free_stream_preserved():
+    """cns_fv_solver_test.cpp:345-383: free-stream state with Neumann conditions."""
+    _, (o,) = cases.cns_case("constant", level=4)
+    q0 = o.state(0)[:, : o.first_ghost].copy()
+    o.solve(10)
+    assert np.max(np.abs(o.state(0)[:, : o.first_ghost] - q0)) <= 1e-14
+
+
+@pytest.mark.parametrize("case", ["tgv", "periodic_vortex"])
+def test_periodic_conservation(case):
+    """A periodic domain exchanges no flux with the outside: the sums of the
+    conserved variables stay constant to rounding."""
+    _, (o,) = cases.tgv_case(level=3) if case == "tgv" else cases.periodic_vortex_case(level=5)
+    fg = o.first_ghost
+    vol = o.tables()["length"][:fg] ** o.w.nd
+    s0 = (o.state(0)[:, :fg] * vol).sum(1)
+    o.solve(6)
+    s1 = (o.state(0)[:, :fg] * vol).sum(1)
+    scale = np.abs(o.state(0)[:, :fg] * vol).sum(1)
+    assert np.all(np.abs(s1 - s0) <= 1e-13 * scale)
+
+
+def test_refined_tree_conserves():
+    """EXTENSION: coarse/fine faces are conservative (both sides use one flux):
+    while the cells next to the outer faces are still untouched (no flux
+    through the domain boundary), the conserved sums do not change."""
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=3)
+    w.refine_sphere([0.5, 0.5, 0.5], 0.25, 5)
+    bcs = [h3o.bc(h3o.BC_EULER_NEUMANN, g) for g in w.cube_boundaries()]
+    o = w.add_solver(h3o.EULER, h3o.AUSM, h3o.EULER_FORWARD, bcs=bcs, ic_kind=h3o.IC_EXPLOSION,
+                     ic=[0.5, 0.5, 0.5, 0.2, 1.0, 1.0, 0.125, 0.1], time_end=1.0, cfl=0.4)
+    o.initialize()
+    fg = o.first_ghost
+    t = o.tables()
+    vol = t["length"][:fg] ** 3
+    outer = (t["neighbors"][:, :fg] >= fg).any(0) & (t["neighbors"][:, :fg] < t["ncells"]).any(0)
+    q0 = o.state(0)[:, :fg].copy()
+    s0 = (q0 * vol).sum(1)
+    checked = 0
+    for _ in range(6):
+        o.solve(1)
+        q = o.state(0)[:, :fg]
+        if not np.array_equal(q[:, outer], q0[:, outer]):
+            break
+        s1 = (q * vol).sum(1)
+        scale = np.abs(q * vol).sum(1)
+        assert np.all(np.abs(s1 - s0) <= 1e-14 * scale)
+        checked += 1
+    assert checked >= 2
+
+
+def _exact_sod(x, t, x0=0.3, L=(1.0, 0.75, 1.0), R=(0.125, 0.0, 0.1), g=1.4):
+    """Exact Riemann solution (Toro, Riemann Solvers and Numerical Methods for
+    Fluid Dynamics, ch. 4: pressure function and Newton iteration for p*)."""
+    rl, ul, pl = L
+    rr, ur, pr = R
+    al, ar = math.sqrt(g * pl / rl), math.sqrt(g * pr / rr)
+
+    def f(p, rk, pk, ak):
+        if p > pk:
+            A, B = 2 / ((g + 1) * rk), (g - 1) / (g + 1) * pk
+            return (p - pk) * math.sqrt(A / (p + B)), math.sqrt(A / (B + p)) * (1 - (p - pk) / (2 * (B + p)))
+        r = p / pk
+        return 2 * ak / (g - 1) * (r ** ((g - 1) / (2 * g)) - 1), 1 / (rk * ak) * r ** (-(g + 1) / (2 * g))
+
+    p = 0.5 * (pl + pr)
+    for _ in range(100):
+        fl, dl = f(p, rl, pl, al)
+        fr, dr = f(p, rr, pr, ar)
+        dp = (fl + fr + ur - ul) / (dl + dr)
+        p = max(1e-8, p - dp)
+        if abs(dp) < 1e-14 * p:
+            break
+    fl, _ = f(p, rl, pl, al)
+    fr, _ = f(p, rr, pr, ar)
+    u = 0.5 * (ul + ur) + 0.5 * (fr - fl)
+    out = np.empty_like(x)
+    for i, xi in enumerate(x):
+        s = (xi - x0) / t
+        if s < u:  # left of contact
+            if p > pl:
+                sl = ul - al * math.sqrt((g + 1) / (2 * g) * p / pl + (g - 1) / (2 * g))
+                out[i] = rl if s < sl else rl * ((p / pl + (g - 1) / (g + 1)) / ((g - 1) / (g + 1) * p / pl + 1))
+            else:
+                shl, stl = ul - al, u - al * (p / pl) ** ((g - 1) / (2 * g))
+                if s < shl:
+                    out[i] = rl
+                elif s > stl:
+                    out[i] = rl * (p / pl) ** (1 / g)
+                else:
+                    out[i] = rl * (2 / (g + 1) + (g - 1) / ((g + 1) * al) * (ul - s)) ** (2 / (g - 1))
+        else:
+            if p > pr:
+                sr = ur + ar * math.sqrt((g + 1) / (2 * g) * p / pr + (g - 1) / (2 * g))
+                out[i] = rr if s > sr else rr * ((p / pr + (g - 1) / (g + 1)) / ((g - 1) / (g + 1) * p / pr + 1))
+            else:
+                shr, str_ = ur + ar, u + ar * (p / pr) ** ((g - 1) / (2 * g))
+                if s > shr:
+                    out[i] = rr
+                elif s < str_:
+                    out[i] = rr * (p / pr) ** (1 / g)
+                else:
+                    out[i] = rr * (2 / (g + 1) - (g - 1) / ((g + 1) * ar) * (ur - s)) ** (2 / (g - 1))
+    return out
+
+
+def test_sod_converges_to_exact_riemann_solution():
+    """euler_fv_solver_test.cpp:114-156 cite Toro's modified Sod problem; the
+    first-order AUSM solution's L1 density error against the exact solution
+    must fall with refinement (first-order rate)."""
+    errs = []
+    for level in (5, 6, 7):
+        w = h3o.World(2, [0, 0], [1, 1], level=level)
+        bcs = [h3o.bc(h3o.BC_EULER_NEUMANN, g) for g in w.cube_boundaries()]
+        o = w.add_solver(h3o.EULER, h3o.AUSM, h3o.RK2, bcs=bcs, ic_kind=h3o.IC_SHOCK_TUBE, ic=cases.SOD,
+                         time_end=0.2, cfl=0.4)
+        o.initialize()
+        while o.time() < 0.2:
+            o.solve(1)
+        fg = o.first_ghost
+        t = o.tables()
+        x = t["x_center"][0, :fg]
+        rho = o.state(0)[2, :fg]
+        errs.append(np.mean(np.abs(rho - _exact_sod(x, o.time()))))
+    assert errs[0] > errs[1] > errs[2]
+    assert errs[2] < 0.02
+    assert errs[1] / errs[2] > 1.4
