@@ -23,7 +23,7 @@ FP64, MIXED = 0, 1
  BC_PERIODIC) = range(15)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
 OPT_TILE_KERNEL, OPT_GRAPHS = 1, 2
-KERNEL_KINDS = ("bc", "cfl", "scalar", "stage1", "stage2", "slopes", "copy", "other")
+KERNEL_KINDS = ("bc", "cfl", "scalar", "stage1", "stage2", "slopes", "copy", "adjoint")
 
 
 class Desc(C.Structure):
@@ -85,6 +85,8 @@ SIGNATURES = {
     "h3c_couple_cht": (_i32, [_vp, _vp, _dbl]),
     "h3c_couple_equal": (_i32, [_vp, _vp]),
     "h3c_set_periodic": (_i32, [_vp, _P(_i64)]),
+    "h3c_solve_dt": (_i32, [_vp, _i64, _P(_dbl)]),
+    "h3c_adjoint": (_i32, [_vp, _i64, _i64, _P(_dbl), _P(_dbl), _P(_dbl)]),
     "h3c_launches": (_i32, [_vp, _P(_i64)]),
     "h3c_set_option": (_i32, [_vp, _i32, _i32]),
     "h3c_selftest_nr": (_i32, [_P(_dbl), _i64, _P(_dbl), _P(_dbl)]),

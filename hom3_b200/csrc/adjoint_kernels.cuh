@@ -1,0 +1,250 @@
+// adjoint_kernels.cuh -- discrete adjoint of the explicit stage (no hom3
+// counterpart: hom3 has no adjoint).
+//
+// A stage maps q -> q + k R(q), k = dt / h per cell, R the num_flux sum of
+// face fluxes (solver.hpp:440-460).  Its vector-Jacobian product for a
+// cotangent lambda is gathered per cell: every face (L, R) of the cell adds
+// w^T dF/dq_cell with w = k_R' lambda_R - k_L' lambda_L (the face enters the
+// left residual with a minus sign, the right one with a plus; k' carries the
+// 2^-(nd-1) area weight on the coarse side of a coarse/fine face).  Ghost
+// states depend on their boundary cell through the condition (Neumann: I,
+// Dirichlet: -I), periodic ghosts are their paired interior cell.  The AUSM
+// flux is differentiated by hand in reverse mode; its upwind choice (sign of
+// the interface Mach number) and the |M| > 1 branches of the split functions
+// are frozen at the forward values.  The time step is frozen too.
+#pragma once
+#include "fv_kernels.cuh"
+
+namespace h3c {
+
+// derivatives of the split functions (euler/physics.hpp:297-310), |M| > 1 branches frozen
+__device__ __forceinline__ double dm_int(double s, double M) {
+  if (fabs(M) > 1.0) return (s * M > 0.0) ? 1.0 : 0.0;
+  return s * 0.5 * (M + s);
+}
+__device__ __forceinline__ double dp_int(double s, double M) {
+  if (fabs(M) > 1.0) return 0.0;
+  return 0.5 * (M + s) * (2.0 - s * M) - s * 0.25 * (M + s) * (M + s);
+}
+__device__ __forceinline__ double m_int_d(double s, double M) {
+  if (fabs(M) > 1.0) return (s * M > 0.0) ? M : 0.0;
+  return (s * 0.25) * ((M + s) * (M + s));
+}
+__device__ __forceinline__ double p_int_d(double s, double M) {
+  if (fabs(M) > 1.0) return (s * M > 0.0) ? 1.0 : 0.0;
+  return (0.25 * ((M + s) * (M + s))) * (2.0 - s * M);
+}
+
+template <int ND> struct SideAD {
+  double rinv, u[ND], um2, p, a2, a, M;
+};
+
+template <int ND>
+__device__ __forceinline__ void side_forward(const double* q, int d, double gamma, double gm1, SideAD<ND>& S) {
+  S.rinv = 1.0 / q[ND];
+  S.um2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    S.u[k] = q[k] * S.rinv;
+    S.um2 += S.u[k] * S.u[k];
+  }
+  S.p = gm1 * (q[ND + 1] - 0.5 * q[ND] * S.um2);
+  S.a2 = gamma * S.p * S.rinv;
+  S.a = sqrt(S.a2);
+  S.M = S.u[d] / S.a;
+}
+
+// reverse through p(q), a(q), M(q) of one side; adds to g[ND + 2]
+template <int ND>
+__device__ __forceinline__ void side_reverse(const double* q, int d, double gamma, double gm1, const SideAD<ND>& S,
+                                             double Mbar, double abar, double pbar, double* g) {
+  double ubar[ND];
+#pragma unroll
+  for (int k = 0; k < ND; ++k) ubar[k] = 0.0;
+  ubar[d] += Mbar / S.a;
+  abar += -Mbar * S.M / S.a;
+  const double a2bar = abar / (2.0 * S.a);
+  pbar += a2bar * gamma * S.rinv;
+  double rinvbar = a2bar * gamma * S.p;
+  g[ND + 1] += gm1 * pbar;
+  g[ND] += -0.5 * gm1 * S.um2 * pbar;
+  const double um2bar = -0.5 * gm1 * q[ND] * pbar;
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    ubar[k] += 2.0 * S.u[k] * um2bar;
+    g[k] += S.rinv * ubar[k];
+    rinvbar += q[k] * ubar[k];
+  }
+  g[ND] += -S.rinv * S.rinv * rinvbar;
+}
+
+// gL += w^T dF/dq_L, gR += w^T dF/dq_R for the AUSM flux F(q_L, q_R) along d
+template <int ND>
+__device__ __forceinline__ void ausm_vjp(const double* qL, const double* qR, int d, const double* w, double gamma,
+                                         double gm1, double* gL, double* gR) {
+  constexpr int NV = ND + 2;
+  SideAD<ND> SL, SR;
+  side_forward<ND>(qL, d, gamma, gm1, SL);
+  side_forward<ND>(qR, d, gamma, gm1, SR);
+  const double mi = m_int_d(1.0, SL.M) + m_int_d(-1.0, SR.M);
+  const bool left = mi >= 0.0;
+  const double* qu = left ? qL : qR;
+  const SideAD<ND>& Su = left ? SL : SR;
+  double theta[NV];
+#pragma unroll
+  for (int v = 0; v < ND + 1; ++v) theta[v] = Su.a * qu[v];
+  theta[ND + 1] = Su.a * (qu[ND + 1] + Su.p);
+  // F_v = mi theta_v + [v == d] pi
+  double mbar = 0.0;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) mbar += w[v] * theta[v];
+  const double pibar = w[d];
+  double MLbar = dm_int(1.0, SL.M) * mbar + dp_int(1.0, SL.M) * SL.p * pibar;
+  double MRbar = dm_int(-1.0, SR.M) * mbar + dp_int(-1.0, SR.M) * SR.p * pibar;
+  double pLbar = p_int_d(1.0, SL.M) * pibar;
+  double pRbar = p_int_d(-1.0, SR.M) * pibar;
+  double aLbar = 0.0, aRbar = 0.0;
+  // theta of the upwind side
+  double abar_u = 0.0;
+  double* gu = left ? gL : gR;
+#pragma unroll
+  for (int v = 0; v < ND + 1; ++v) {
+    const double tb = mi * w[v];
+    abar_u += tb * qu[v];
+    gu[v] += Su.a * tb;
+  }
+  {
+    const double tb = mi * w[ND + 1];
+    abar_u += tb * (qu[ND + 1] + Su.p);
+    gu[ND + 1] += Su.a * tb;
+    if (left) pLbar += Su.a * tb;
+    else pRbar += Su.a * tb;
+  }
+  if (left) aLbar += abar_u;
+  else aRbar += abar_u;
+  side_reverse<ND>(qL, d, gamma, gm1, SL, MLbar, aLbar, pLbar, gL);
+  side_reverse<ND>(qR, d, gamma, gm1, SR, MRbar, aRbar, pRbar, gR);
+}
+
+// Per-cell adjoint of one stage:
+//   gout_c = beta lam_c + [VJP of (q -> alpha k R(q)) with cotangent lam]_c + gamma_e extra_c
+// q is the stage input with its ghosts filled by the conditions.
+template <int ND, int PHYS>
+__global__ void __launch_bounds__(kBlock) k_adj_stage(const double* __restrict__ q, const double* __restrict__ lam,
+                                                      double* __restrict__ gout, const double* __restrict__ extra,
+                                                      double alpha, double beta, double gamma_e, Geometry g,
+                                                      GhostTables gt, PhysConst pc, const Scalars* __restrict__ sc) {
+  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  constexpr int NS = 1 << (ND - 1);
+  constexpr double W = ND == 2 ? 0.5 : 0.25;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= g.n_int) return;
+  const long long ld = g.ld;
+  const double dt = sc->dt;
+  const double hc = g.len[g.lvl[c]];
+  const double kc = alpha * dt / hc;
+  double qc[NV], lc[NV], acc[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    qc[v] = q[v * ld + c];
+    lc[v] = lam[v * ld + c];
+    acc[v] = 0.0;
+  }
+  // resolve a neighbour entry: interior cell (its own residual) or ghost (condition Jacobian)
+  // returns the residual-owning cell for the cotangent and the Jacobian sign of the ghost
+  auto face = [&](int nb_cell, bool c_is_left, double kc_face, double kn_face, int d) {
+    // nb_cell: neighbour index (interior or ghost)
+    double qn[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qn[v] = q[v * ld + nb_cell];
+    double w[NV];
+    double jac = 0.0;  // ghost: dq_ghost/dq_c = jac I; interior: 0
+    long long own = nb_cell;
+    double kn = kn_face;
+    if (nb_cell >= g.n_int) {
+      const long long i = nb_cell - g.n_int;
+      const int b = gt.bc_apply[i];
+      own = -1;
+      kn = 0.0;
+      if (b != 255) {
+        const int kind = gt.bcs[b].kind;
+        if (kind == BC_PERIODIC) {
+          // the ghost is a copy of its paired cell, whose residual holds the same face
+          own = gt.partner[i];
+          if (own >= 0) kn = alpha * dt / g.len[g.lvl[own]];
+        } else {
+          jac = (kind == BC_EULER_DIRICHLET || kind == BC_HEAT_DIRICHLET) ? -1.0 : 1.0;
+        }
+      }
+    }
+    double ln[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) ln[v] = own >= 0 ? lam[v * ld + own] : 0.0;
+    // w = k_R lambda_R - k_L lambda_L
+#pragma unroll
+    for (int v = 0; v < NV; ++v) w[v] = c_is_left ? (kn * ln[v] - kc_face * lc[v]) : (kc_face * lc[v] - kn * ln[v]);
+    double gc[NV], gn[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { gc[v] = 0.0; gn[v] = 0.0; }
+    if (PHYS == HEAT) {
+      // F = (T_L - T_R) / dx_owner (heat/physics.hpp:113-119): the two residuals use their own dx
+      const double hn = own >= 0 ? g.len[g.lvl[own]] : hc;
+      const double wl = c_is_left ? -kc_face * lc[0] / hc : kc_face * lc[0] / hc;  // c's residual term
+      const double wn = own >= 0 ? (c_is_left ? kn * ln[0] / hn : -kn * ln[0] / hn) : 0.0;
+      // d/dT_c of (+-F): c is L -> +1, c is R -> -1 ; ghost chain: d/dT_g -> opposite sign times jac
+      const double sgn = c_is_left ? 1.0 : -1.0;
+      gc[0] = (wl + wn) * sgn;
+      if (own < 0) gc[0] += wl * (-sgn) * jac;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[v] += gc[v];
+      return;
+    }
+    if (c_is_left) ausm_vjp<ND>(qc, qn, d, w, pc.gamma, pc.gm1, gc, gn);
+    else ausm_vjp<ND>(qn, qc, d, w, pc.gamma, pc.gm1, gn, gc);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] += gc[v] + jac * gn[v];
+  };
+#pragma unroll
+  for (int d = 0; d < ND; ++d) {
+    const int m = g.nbr[(2 * d) * ld + c];
+    const int p = g.nbr[(2 * d + 1) * ld + c];
+    // minus side: c is the right cell of F(m, c)
+    if (m >= 0) {
+      const bool coarser = m < g.n_int && g.len[g.lvl[m]] > hc;
+      const double km = m < g.n_int ? alpha * dt / g.len[g.lvl[m]] : 0.0;
+      face(m, false, kc, coarser ? W * km : km, d);
+    } else {
+      const long long k = -m - 2;
+#pragma unroll
+      for (int j = 0; j < NS; ++j) {
+        const int f = g.sub[j * g.nsub + k];
+        face(f, false, W * kc, alpha * dt / g.len[g.lvl[f]], d);
+      }
+    }
+    // plus side: c is the left cell of F(c, p)
+    if (p >= 0) {
+      const bool coarser = p < g.n_int && g.len[g.lvl[p]] > hc;
+      const double kp = p < g.n_int ? alpha * dt / g.len[g.lvl[p]] : 0.0;
+      face(p, true, kc, coarser ? W * kp : kp, d);
+    } else {
+      const long long k = -p - 2;
+#pragma unroll
+      for (int j = 0; j < NS; ++j) {
+        const int f = g.sub[j * g.nsub + k];
+        face(f, true, W * kc, alpha * dt / g.len[g.lvl[f]], d);
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    double o = beta * lc[v] + acc[v];
+    if (extra) o += gamma_e * extra[v * ld + c];
+    gout[v * ld + c] = o;
+  }
+}
+
+// frozen time step of step i
+__global__ void k_set_dt_from(Scalars* sc, const double* dts, long long i) { sc->dt = dts[i]; }
+__global__ void k_record_dt(const Scalars* sc, double* dts, long long i) { dts[i] = sc->dt; }
+
+}  // namespace h3c

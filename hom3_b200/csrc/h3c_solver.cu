@@ -20,6 +20,7 @@
 
 #include "../../include/h3c.h"
 #include "fv_kernels.cuh"
+#include "adjoint_kernels.cuh"
 
 using namespace h3c;
 
@@ -70,6 +71,7 @@ struct h3c_solver_s {
   std::vector<long long> dev2caller, caller2dev;
   Scalars* d_sc = nullptr;
   bool unfused_dt = false;  // a condition rewrites interior cells (vortex)
+  bool ghost_unapplied = false;  // some ghost gets no condition (hom3's find_if segments)
   bool needs_partner = false, needs_periodic = false;  // coupling / periodic conditions present
   bool partner_set = false, periodic_set = false;
   bool tile = true;  // Euler stages use the shared-memory tile kernel
@@ -166,7 +168,7 @@ GhostTables ghosts(const h3c_solver s) {
 unsigned blocks(long long n) { return (unsigned)std::max<long long>(1, (n + kBlock - 1) / kBlock); }
 
 // kernel kinds reported by h3c_profile_read
-enum { K_BC = 0, K_CFL = 1, K_SCALAR = 2, K_STAGE1 = 3, K_STAGE2 = 4, K_SLOPES = 5, K_COPY = 6, K_NKINDS = 8 };
+enum { K_BC = 0, K_CFL = 1, K_SCALAR = 2, K_STAGE1 = 3, K_STAGE2 = 4, K_SLOPES = 5, K_COPY = 6, K_OTHER = 7, K_NKINDS = 8 };
 
 cudaEvent_t take_event(h3c_solver s) {
   cudaEvent_t e;
@@ -203,25 +205,26 @@ struct Launch {
 
 // ---- kernel dispatch -------------------------------------------------------
 template <int ND, int PHYS>
-void launch_bc_t(h3c_solver s, int which) {
+void launch_bc_t(h3c_solver s, double* q, const double* qlhs) {
   PartnerView pv{nullptr, 0};
   if (s->partner) pv = PartnerView{s->partner->d_q[0], s->partner->ld};
   Launch L(s, K_BC);
-  k_bc<ND, PHYS><<<blocks(s->ng), kBlock, 0, s->stream>>>(s->d_q[which], s->d_q[0], geometry(s), ghosts(s),
-                                                          s->pc, s->d_sc, pv);
+  k_bc<ND, PHYS><<<blocks(s->ng), kBlock, 0, s->stream>>>(q, qlhs, geometry(s), ghosts(s), s->pc, s->d_sc, pv);
 }
-void launch_bc(h3c_solver s, int which) {
+// conditions applied to q; coupling conditions read temperatures from qlhs
+void launch_bc_ptr(h3c_solver s, double* q, const double* qlhs) {
   if (s->ng == 0) return;
   if (s->nd == 2) {
-    if (s->desc.physics == H3C_EULER) launch_bc_t<2, EULER>(s, which);
-    else if (s->desc.physics == H3C_CNS) launch_bc_t<2, CNS>(s, which);
-    else launch_bc_t<2, HEAT>(s, which);
+    if (s->desc.physics == H3C_EULER) launch_bc_t<2, EULER>(s, q, qlhs);
+    else if (s->desc.physics == H3C_CNS) launch_bc_t<2, CNS>(s, q, qlhs);
+    else launch_bc_t<2, HEAT>(s, q, qlhs);
   } else {
-    if (s->desc.physics == H3C_EULER) launch_bc_t<3, EULER>(s, which);
-    else if (s->desc.physics == H3C_CNS) launch_bc_t<3, CNS>(s, which);
-    else launch_bc_t<3, HEAT>(s, which);
+    if (s->desc.physics == H3C_EULER) launch_bc_t<3, EULER>(s, q, qlhs);
+    else if (s->desc.physics == H3C_CNS) launch_bc_t<3, CNS>(s, q, qlhs);
+    else launch_bc_t<3, HEAT>(s, q, qlhs);
   }
 }
+void launch_bc(h3c_solver s, int which) { launch_bc_ptr(s, s->d_q[which], s->d_q[0]); }
 
 template <int ND, int PHYS>
 void launch_cfl_t(h3c_solver s, long long* slot) {
@@ -627,6 +630,7 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   std::vector<unsigned char> h_gpos(ngm, 0), h_apply(ngm, 255), h_own(ngm, 0);
   std::vector<double> h_gdx(ngm, 0.0);
   std::vector<int> h_blk(std::max<long long>(1, s->ntiles), 0);
+  s->ghost_unapplied = false;
   for (int k = 0; k < ninst; ++k) {
     const h3c_grid& gr = grids[k];
     const InstanceTables& I = T[k];
@@ -654,6 +658,7 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
       h_gb[gi] = (int)caller2dev[co + b];
       h_gpos[gi] = (unsigned char)(I.gbp[g] ^ 1);  // ghost position w.r.t. its boundary cell
       h_apply[gi] = I.apply[g] == 255 ? 255 : bcmap[k][I.apply[g]];
+      if (I.apply[g] == 255) s->ghost_unapplied = true;
       h_own[gi] = bcmap[k][I.own[g]];
       h_ginst[gi] = k;
       double s2 = 0;
@@ -1184,6 +1189,192 @@ int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_out) {
   if (choice) *choice = best;
   if (ms_out) *ms_out = best_ms / nsteps;
   return s->cuda(cudaGetLastError(), "h3c_autotune");
+}
+
+// ---- frozen-dt stepping and the discrete adjoint ----------------------------
+static int adjoint_supported(h3c_solver s, const char* what) {
+  if (int rc = ready(s, what)) return rc;
+  if (s->n_inst != 1) return s->fail(H3C_E_INVALID, "%s: single grids only", what);
+  const bool ok_phys = (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM) ||
+                       s->desc.physics == H3C_HEAT;
+  if (!ok_phys) return s->fail(H3C_E_INVALID, "%s: Euler/AUSM and heat only", what);
+  if (s->ghost_unapplied) return s->fail(H3C_E_INVALID, "%s: a ghost cell gets no condition", what);
+  for (int k = 0; k < s->n_bcs; ++k) {
+    const int kind = s->h_bcs[k].kind;
+    if (kind != H3C_BC_EULER_NEUMANN && kind != H3C_BC_EULER_DIRICHLET && kind != H3C_BC_HEAT_NEUMANN &&
+        kind != H3C_BC_HEAT_DIRICHLET && kind != H3C_BC_PERIODIC)
+      return s->fail(H3C_E_INVALID, "%s: condition kind %d has no adjoint", what, kind);
+  }
+  return H3C_OK;
+}
+
+// One step with the given time step on explicit buffers: the stage inputs
+// (ghosts filled) are left in in0 (and in1 for RK2); the new state in out.
+// For forward Euler out may not alias in0; for RK2 out == in0 is allowed.
+static void frozen_step(h3c_solver s, double* in0, double* in1, double* out, const double* d_dts, long long i) {
+  launch_bc_ptr(s, in0, in0);
+  {
+    Launch L(s, K_SCALAR);
+    k_set_dt_from<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
+  }
+  if (s->desc.time_integration == H3C_EULER_FORWARD) {
+    launch_stage(s, 0, in0, out, false);
+  } else {
+    launch_stage(s, 0, in0, in1, false);
+    launch_bc_ptr(s, in1, in0);
+    if (out != in0) cudaMemcpyAsync(out, in0, sizeof(double) * s->nv * s->ld, cudaMemcpyDeviceToDevice, s->stream);
+    launch_stage(s, 2, in1, out, false);
+  }
+  {
+    Launch L(s, K_SCALAR);
+    k_advance<<<1, 1, 0, s->stream>>>(s->d_sc, 1);
+  }
+}
+
+int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts) {
+  if (!s || nsteps < 0 || (nsteps > 0 && !dts)) return H3C_E_INVALID;
+  if (int rc = ready(s, "h3c_solve_dt")) return rc;
+  if (s->n_inst != 1) return s->fail(H3C_E_INVALID, "h3c_solve_dt: single grids only");
+  if (nsteps == 0) return H3C_OK;
+  double* d_dts = nullptr;
+  H3C_CUDA(s, cudaMalloc(&d_dts, sizeof(double) * nsteps));
+  cudaMemcpyAsync(d_dts, dts, sizeof(double) * nsteps, cudaMemcpyHostToDevice, s->stream);
+  for (int64_t i = 0; i < nsteps; ++i) {
+    if (s->desc.time_integration == H3C_EULER_FORWARD) {
+      frozen_step(s, s->d_q[0], nullptr, s->d_q[1], d_dts, i);
+      std::swap(s->d_q[0], s->d_q[1]);
+    } else {
+      frozen_step(s, s->d_q[0], s->d_q[1], s->d_q[0], d_dts, i);
+    }
+  }
+  launch_cfl(s, &s->d_sc->dtmin_ord);  // the next h3c_solve computes dt from this state
+  cudaStreamSynchronize(s->stream);
+  cudaFree(d_dts);
+  return s->cuda(cudaGetLastError(), "h3c_solve_dt");
+}
+
+int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dqN, double* dJ_dq0, double* dts_out) {
+  if (!s || nsteps < 1 || every < 1 || !dJ_dqN || !dJ_dq0) return H3C_E_INVALID;
+  if (int rc = adjoint_supported(s, "h3c_adjoint")) return rc;
+  const long long L = s->ld, nv = s->nv, Q = nv * L;
+  const bool rk2 = s->desc.time_integration == H3C_RUNGE_KUTTA_2;
+  const long long nck = (nsteps + every - 1) / every;
+  const long long per = rk2 ? 2 : 1;
+  double *ck = nullptr, *seg = nullptr, *work = nullptr, *lam = nullptr, *d_dts = nullptr;
+  auto cleanup = [&]() {
+    cudaStreamSynchronize(s->stream);
+    cudaFree(ck); cudaFree(seg); cudaFree(work); cudaFree(lam); cudaFree(d_dts);
+  };
+  if (cudaMalloc(&ck, sizeof(double) * Q * nck) != cudaSuccess || cudaMalloc(&seg, sizeof(double) * Q * per * every) != cudaSuccess ||
+      cudaMalloc(&work, sizeof(double) * Q * 3) != cudaSuccess || cudaMalloc(&lam, sizeof(double) * Q * 3) != cudaSuccess ||
+      cudaMalloc(&d_dts, sizeof(double) * nsteps) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return s->fail(H3C_E_NOMEM, "h3c_adjoint: checkpoints do not fit (%lld checkpoints + %lld stage states)", nck, per * every);
+  }
+  // ---- forward: the solver's own step (CFL dt), checkpoint every `every` steps, record dt ----
+  const bool fuse = !s->unfused_dt;
+  for (int64_t i = 0; i < nsteps; ++i) {
+    if (i % every == 0)
+      cudaMemcpyAsync(ck + Q * (i / every), s->d_q[0], sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+    launch_bc(s, 0);
+    if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
+    {
+      Launch L1(s, K_SCALAR);
+      k_set_dt<<<1, 1, 0, s->stream>>>(s->d_sc, 1, 1);
+    }
+    k_record_dt<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
+    if (!rk2) {
+      launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
+      std::swap(s->d_q[0], s->d_q[1]);
+    } else {
+      launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
+      launch_bc(s, 1);
+      launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
+    }
+    {
+      Launch L2(s, K_SCALAR);
+      k_advance<<<1, 1, 0, s->stream>>>(s->d_sc, 1);
+    }
+  }
+  Scalars saved;
+  cudaMemcpyAsync(&saved, s->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream);
+  // ---- cotangent of the final state (caller numbering -> internal) ----
+  double* lamA = lam;          // lambda^{n+1}
+  double* lamB = lam + Q;      // scratch
+  double* lamC = lam + 2 * Q;  // lambda* (RK2)
+  cudaMemsetAsync(lam, 0, sizeof(double) * Q * 3, s->stream);
+  if (int rc = ensure_stage(s, s->n_caller)) { cleanup(); return rc; }
+  for (int v = 0; v < nv; ++v)
+    cudaMemcpyAsync(s->d_stage + v * s->n_caller, dJ_dqN + v * s->n_caller, sizeof(double) * s->n_caller,
+                    cudaMemcpyHostToDevice, s->stream);
+  k_gather<<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_stage, s->n_caller, lamA, L, s->d_dev2caller, s->n_int, (int)nv);
+  // ---- backward over segments, recomputing each segment's stage inputs ----
+  auto adj = [&](const double* qin, const double* lamin, double* gout, const double* extra, double alpha, double beta,
+                 double gam) {
+    Launch La(s, K_OTHER);
+    const Geometry g = geometry(s);
+    const GhostTables gt = ghosts(s);
+    if (s->nd == 2) {
+      if (s->desc.physics == H3C_HEAT)
+        k_adj_stage<2, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+      else
+        k_adj_stage<2, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+    } else {
+      if (s->desc.physics == H3C_HEAT)
+        k_adj_stage<3, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+      else
+        k_adj_stage<3, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+    }
+  };
+  for (long long k = nck - 1; k >= 0; --k) {
+    const long long i0 = k * every, i1 = std::min<long long>(nsteps, i0 + every);
+    // recompute: work[0] <- checkpoint, keep every stage input in seg
+    double* cur = work;
+    cudaMemcpyAsync(cur, ck + Q * k, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+    for (long long i = i0; i < i1; ++i) {
+      double* s0 = seg + Q * per * (i - i0);
+      cudaMemcpyAsync(s0, cur, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+      double* nxt = (cur == work) ? work + Q : work;
+      frozen_step(s, s0, rk2 ? s0 + Q : nullptr, rk2 ? s0 : nxt, d_dts, i);
+      if (rk2) {
+        // s0 now holds the new state (in-place second stage); restore the stage input into s0
+        cudaMemcpyAsync(nxt, s0, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+        cudaMemcpyAsync(s0, cur, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+        launch_bc_ptr(s, s0, s0);
+      }
+      cur = nxt;
+    }
+    for (long long i = i1 - 1; i >= i0; --i) {
+      double* s0 = seg + Q * per * (i - i0);
+      {
+        Launch L3(s, K_SCALAR);
+        k_set_dt_from<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
+      }
+      if (!rk2) {
+        adj(s0, lamA, lamB, nullptr, 1.0, 1.0, 0.0);
+        std::swap(lamA, lamB);
+      } else {
+        // lambda* = 0.5 lambda + VJP(q*; 0.5 lambda); lambda^n = 0.5 lambda + lambda* + VJP(q^n; lambda*)
+        adj(s0 + Q, lamA, lamC, nullptr, 0.5, 0.5, 0.0);
+        adj(s0, lamC, lamB, lamA, 1.0, 1.0, 0.5);
+        std::swap(lamA, lamB);
+      }
+    }
+  }
+  // ---- gradient (internal -> caller numbering), dt sequence ----
+  cudaMemsetAsync(s->d_stage, 0, sizeof(double) * nv * s->n_caller, s->stream);
+  k_scatter<<<blocks(s->n_int), kBlock, 0, s->stream>>>(lamA, L, s->d_stage, s->n_caller, s->d_dev2caller, s->n_int, (int)nv);
+  for (int v = 0; v < nv; ++v)
+    cudaMemcpyAsync(dJ_dq0 + v * s->n_caller, s->d_stage + v * s->n_caller, sizeof(double) * s->n_caller,
+                    cudaMemcpyDeviceToHost, s->stream);
+  if (dts_out) cudaMemcpyAsync(dts_out, d_dts, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, s->stream);
+  cudaStreamSynchronize(s->stream);
+  // the solver is left at step N with the scalars of the forward run
+  cudaMemcpy(s->d_sc, &saved, sizeof(Scalars), cudaMemcpyHostToDevice);
+  const cudaError_t e = cudaGetLastError();
+  cleanup();
+  return s->cuda(e, "h3c_adjoint");
 }
 
 int h3c_launches(h3c_solver s, int64_t* n) {

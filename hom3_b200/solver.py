@@ -253,6 +253,21 @@ class Solver:
     def set_option(self, option, value):
         self._check(lib().h3c_set_option(self.h, int(option), int(value)))
 
+    def solve_dt(self, dts):
+        """Steps with the given time steps (the frozen-dt forward map)."""
+        d = np.ascontiguousarray(dts, np.float64)
+        self._check(lib().h3c_solve_dt(self.h, d.size, _dp(d)))
+
+    def adjoint(self, nsteps, dJ_dqN, every=None):
+        """Run nsteps steps (CFL dt) and return (dJ/dq0, dts) for J = <dJ_dqN, q_N>."""
+        lam = np.ascontiguousarray(dJ_dqN, np.float64)
+        assert lam.shape == (self.nv, self.n_cells)
+        grad = np.empty_like(lam)
+        dts = np.empty(nsteps)
+        every = every or max(1, int(round(nsteps ** 0.5)))
+        self._check(lib().h3c_adjoint(self.h, nsteps, every, _dp(lam), _dp(grad), _dp(dts)))
+        return grad, dts
+
     def launches(self):
         return self._get(lib().h3c_launches, C.c_int64)
 

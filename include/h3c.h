@@ -206,7 +206,7 @@ int h3c_status(h3c_solver s, int* flags);
  * h3c_profile(s, 1): bracket every subsequent launch with CUDA events on the
  * solver's stream; h3c_profile_read sums the elapsed times per kernel kind
  * (0 boundary conditions, 1 CFL reduction, 2 scalar step bookkeeping,
- * 3 first stage / forward Euler, 4 second RK stage, 5 slopes) and resets. */
+ * 3 first stage / forward Euler, 4 second RK stage, 5 slopes, 7 adjoint stages) and resets. */
 int h3c_launches(h3c_solver s, int64_t* n);
 /* Execution options (no hom3 counterpart; results do not depend on them):
  * H3C_OPT_TILE_KERNEL  Euler stages in the shared-memory tile kernel (default 1)
@@ -235,6 +235,19 @@ int h3c_profile_read(h3c_solver s, double* ms, int64_t* count, int nkinds);
  * calls that overlap on the GPU race and must be serialised by the caller. */
 int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t ld, int64_t n_cells,
                        const double* length, double* dt_out, void* stream);
+
+/* ---- discrete adjoint (no hom3 counterpart) ----
+ * h3c_solve_dt: nsteps steps with the given time steps (host array) instead
+ * of the CFL time step -- the forward map the adjoint differentiates.
+ * h3c_adjoint: runs nsteps steps from the current state (leaving the solver
+ * at step N, like h3c_solve) with checkpoints every `every` steps, then
+ * returns dJ/dq0 for J = <dJ_dqN, q_N> (host arrays, caller numbering,
+ * [nv][n_cells]; ghost entries of dJ_dqN are ignored, of dJ_dq0 zero) with the
+ * time steps frozen at the forward values (returned in dts, may be NULL).
+ * Each segment of `every` steps is recomputed from its checkpoint.  Euler
+ * with the AUSM flux and heat, Neumann / Dirichlet / periodic conditions. */
+int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts);
+int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dqN, double* dJ_dq0, double* dts);
 
 /* ---- coupling: coupling.hpp:24-73 ----
  * partner_cells[g - first_ghost] = the partner solver's cell (caller

@@ -44,6 +44,41 @@ constexpr Ind INV = std::numeric_limits<Ind>::max();    // misc/constants.hpp:42
 constexpr SInd SINV = std::numeric_limits<SInd>::max();
 constexpr double PI = 3.141592653589793238462643383279502884;  // misc/constants.hpp:67
 
+// Forward-mode dual number (value, derivative) for the derivative build of the
+// oracle (Solver<Dual>): every operation propagates d(x) by the chain rule;
+// comparisons look at values only, so branches are those of the double build.
+struct Dual {
+  double v = 0, d = 0;
+  Dual() {}
+  Dual(double x) : v(x) {}
+  Dual(double x, double y) : v(x), d(y) {}
+};
+inline Dual operator+(Dual a, Dual b) { return {a.v + b.v, a.d + b.d}; }
+inline Dual operator-(Dual a, Dual b) { return {a.v - b.v, a.d - b.d}; }
+inline Dual operator*(Dual a, Dual b) { return {a.v * b.v, a.d * b.v + a.v * b.d}; }
+inline Dual operator/(Dual a, Dual b) { return {a.v / b.v, (a.d * b.v - a.v * b.d) / (b.v * b.v)}; }
+inline Dual operator-(Dual a) { return {-a.v, -a.d}; }
+inline Dual operator+(Dual a, double b) { return {a.v + b, a.d}; }
+inline Dual operator+(double a, Dual b) { return {a + b.v, b.d}; }
+inline Dual operator-(Dual a, double b) { return {a.v - b, a.d}; }
+inline Dual operator-(double a, Dual b) { return {a - b.v, -b.d}; }
+inline Dual operator*(Dual a, double b) { return {a.v * b, a.d * b}; }
+inline Dual operator*(double a, Dual b) { return {a * b.v, a * b.d}; }
+inline Dual operator/(Dual a, double b) { return {a.v / b, a.d / b}; }
+inline Dual operator/(double a, Dual b) { return {a / b.v, -a * b.d / (b.v * b.v)}; }
+inline Dual& operator+=(Dual& a, Dual b) { a = a + b; return a; }
+#define H3O_DUAL_CMP(op)                                                  \
+  inline bool operator op(Dual a, Dual b) { return a.v op b.v; }         \
+  inline bool operator op(Dual a, double b) { return a.v op b; }         \
+  inline bool operator op(double a, Dual b) { return a op b.v; }
+H3O_DUAL_CMP(<) H3O_DUAL_CMP(>) H3O_DUAL_CMP(<=) H3O_DUAL_CMP(>=) H3O_DUAL_CMP(==) H3O_DUAL_CMP(!=)
+#undef H3O_DUAL_CMP
+inline Dual sqrt(Dual a) { const double r = std::sqrt(a.v); return {r, a.d / (2 * r)}; }
+inline Dual abs(Dual a) { return a.v < 0 ? -a : a; }
+inline Dual pow(Dual a, double e) { const double r = std::pow(a.v, e); return {r, e * std::pow(a.v, e - 1) * a.d}; }
+inline double value(double x) { return x; }
+inline double value(Dual x) { return x.v; }
+
 // ---------------------------------------------------------------------------
 // Stencils: grid/grid.hpp:41-81, containers/hierarchical/implementation.hpp:46-65
 // ---------------------------------------------------------------------------
@@ -339,6 +374,7 @@ template <class T> struct World;
 // ---------------------------------------------------------------------------
 template <class T> struct Solver {
   using State = std::array<T, 5>;
+  using ICState = std::array<double, 5>;  // initial conditions are evaluated in double
   World<T>* w = nullptr;
   int idx = 0;
   int nd = 2, nv = 4;
@@ -406,10 +442,10 @@ template <class T> struct Solver {
     return P.gamma * p(t, c) / rho(t, c);
   }
   // cv / pv: euler/quantities.hpp:153-189
-  State cv(const State& pvs) const {
-    State c{};
+  template <class S> S cv(const S& pvs) const {
+    S c{};
     c[nd] = pvs[nd];
-    T velMag2 = 0;
+    typename S::value_type velMag2 = 0;
     for (int d = 0; d < nd; ++d) {
       c[d] = pvs[nd] * pvs[d];
       velMag2 = velMag2 + pvs[d] * pvs[d];
@@ -662,7 +698,7 @@ template <class T> struct Solver {
   void force_dt(T dt) { forced_step_ = step_; forced_dt_ = dt; }  // :522-525
 
   // ---- boundary conditions ----
-  void isentropic_vortex(const double* x, double t, State& out) const;
+  void isentropic_vortex(const double* x, double t, ICState& out) const;
   Ind partner_cell(Ind g) const;  // coupling.hpp:24-39
   void apply_bc(int t, int b, Ind g0, Ind g1);
   // apply_bcs: solver.hpp:561-586 (segment discovery by find_if, as in hom3)
@@ -713,7 +749,7 @@ template <class T> struct Solver {
     apply_bcs(0);
     set_dt();
     evolve();
-    time_ += dt_;
+    time_ += value(dt_);
     ++step_;
   }
 
@@ -722,7 +758,7 @@ template <class T> struct Solver {
     const double s = domain(nd, x);
     return domain_kind == 1 ? (s > 0.) : (s < 0.);
   }
-  void eval_ic(const double* x, State& out) const;
+  void eval_ic(const double* x, ICState& out) const;
   void initialize();
 };
 
@@ -738,21 +774,21 @@ template <class T> struct World {
 // isentropic_vortex: euler/initial_conditions.hpp:343-368 (hard-coded
 // beta=5, gamma=1.4, x0=(-5,-5), u=v=1 in hom3).
 template <class T>
-void Solver<T>::isentropic_vortex(const double* x, double t, State& out) const {
+void Solver<T>::isentropic_vortex(const double* x, double t, ICState& out) const {
   double beta = 5, gamma = 1.4, x00 = -5.0, x01 = -5.0, uu = 1, vv = 1;
   if (ic_kind == IC_VORTEX_PARAM) { beta = ic[0]; x00 = ic[1]; x01 = ic[2]; uu = ic[3]; vv = ic[4]; }
   const double x_t = x[0] - uu * t, y_t = x[1] - vv * t;
   const double r = std::sqrt(std::pow(x_t - x00, 2) + std::pow(y_t - x01, 2));
   const double eT1mr2 = std::exp(1 - std::pow(r, 2));
   const double eT21mr2 = std::exp(2 * (1 - std::pow(r, 2)));
-  State pvars{};
+  ICState pvars{};
   pvars[0] = uu - beta * eT1mr2 * (y_t - x01) / (2 * PI);
   pvars[1] = vv + beta * eT1mr2 * (x_t - x00) / (2 * PI);
   pvars[2] = std::pow((1 - ((gamma - 1) * std::pow(beta, 2) * eT21mr2) / (16 * gamma * std::pow(PI, 2))),
                       1 / (gamma - 1));
   pvars[3] = std::pow(pvars[2], gamma);
   // cv<nd>(pvars, 1.4): euler/quantities.hpp:153-166 with gamma = 1.4
-  State c{};
+  ICState c{};
   c[2] = pvars[2];
   double vm2 = 0;
   for (int d = 0; d < 2; ++d) { c[d] = pvars[2] * pvars[d]; vm2 += pvars[d] * pvars[d]; }
@@ -760,8 +796,8 @@ void Solver<T>::isentropic_vortex(const double* x, double t, State& out) const {
   out = c;
 }
 
-template <class T> void Solver<T>::eval_ic(const double* x, State& out) const {
-  State pvars{};
+template <class T> void Solver<T>::eval_ic(const double* x, ICState& out) const {
+  ICState pvars{};
   if (ic_kind == IC_CONSTANT_PV) {
     for (int v = 0; v < nv; ++v) pvars[v] = ic[v];
     out = cv(pvars);
@@ -790,7 +826,7 @@ template <class T> void Solver<T>::eval_ic(const double* x, State& out) const {
       pvars[nd + 1] = ic[8];
     }
     // shock_tube converts with gamma = 1.4 hard-coded (initial_conditions.hpp:387)
-    State c{};
+    ICState c{};
     c[nd] = pvars[nd];
     double vm2 = 0;
     for (int d = 0; d < nd; ++d) { c[d] = pvars[nd] * pvars[d]; vm2 += pvars[d] * pvars[d]; }
@@ -870,11 +906,10 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
       case BC_EULER_VORTEX: {  // :304-316 (also overwrites the boundary cell)
         double xg[3], xb[3];
         for (int d = 0; d < nd; ++d) { xg[d] = xc[d][g]; xb[d] = xc[d][b]; }
-        State sg, sb;
+        ICState sg, sb;
         isentropic_vortex(xg, time_, sg);
         isentropic_vortex(xb, time_, sb);
-        setQ(t, g, sg);
-        setQ(t, b, sb);
+        for (int v = 0; v < nv; ++v) { q(t, g, v) = sg[v]; q(t, b, v) = sb[v]; }
         break;
       }
       case BC_CNS_INFLOW: {  // cns/boundary_conditions.hpp:37-61; v = surface pv (u.., rho, p)
@@ -1104,13 +1139,13 @@ template <class T> void Solver<T>::initialize() {
   const double gp = 1 / std::sqrt(3);
   for (Ind c = 0; c < firstGC; ++c) {
     const double l = tr.length(node[c]);
-    State sum{};
+    ICState sum{};
     for (int k = 0; k < (1 << nd); ++k) {
       double x[3];
       for (int d = 0; d < nd; ++d) x[d] = xc[d][c] + 0.5 * l * ((double)child_rel(nd, k, d) * gp);
-      State f{};
+      ICState f{};
       eval_ic(x, f);
-      for (int v = 0; v < nv; ++v) sum[v] = k == 0 ? f[v] : T(sum[v] + f[v]);
+      for (int v = 0; v < nv; ++v) sum[v] = k == 0 ? f[v] : sum[v] + f[v];
     }
     double vol = l;
     for (int d = 1; d < nd; ++d) vol = l * vol;

@@ -114,6 +114,13 @@ def lib():
             "h3o_couple_equal": (None, [vp, i32, i32]),
             "h3o_num_threads": (i32, []),
             "h3o_solver_info": (None, [vp, i32, P(Info)]),
+            "h3o_dual_clone": (vp, [vp, i32]),
+            "h3o_dual_world_destroy": (None, [vp]),
+            "h3o_dual_initialize": (i32, [vp]),
+            "h3o_dual_set_state": (None, [vp, P(dbl), P(dbl)]),
+            "h3o_dual_get_state": (None, [vp, P(dbl), P(dbl)]),
+            "h3o_dual_solve_dt": (None, [vp, i32, P(dbl)]),
+            "h3o_dual_ncells": (i64, [vp]),
             "h3o_set_num_threads": (None, [i32]),
         }
         for name, (res, args) in sig.items():
@@ -314,25 +321,8 @@ class World:
 
     def add_solver(self, physics=EULER, flux=AUSM, time_integration=EULER_FORWARD, *, bcs=(),
                    domain=None, domain_kind=0, ic_kind=IC_CONSTANT_PV, ic=(), **props) -> Solver:
-        d = SolverDesc()
-        defaults = dict(cfl=0.2, cfl_viscous=0.4, gamma=1.4, Rspecific=287.058, T0=273.15, rho0=1.225,
-                        Minfty=0.1, ReInfty=100.0, Pr0=0.72, Sutherland0=110.4, diffusivity=1.0,
-                        T_ref=273.15, time_end=1.0)
-        defaults.update(props)
-        d.physics, d.flux, d.time_integration = physics, flux, time_integration
-        for k, v in defaults.items():
-            setattr(d, k, float(v))
-        d.domain_kind = domain_kind
-        if domain is not None:
-            d.domain = domain
-        d.ic_kind = ic_kind
-        for i, v in enumerate(ic):
-            d.ic[i] = v
-        arr = (BcDesc * max(1, len(bcs)))()
-        for i, b in enumerate(bcs):
-            arr[i] = b
-        d.n_bcs = len(bcs)
-        d.bcs = arr
+        d, arr = _pack_desc(physics, flux, time_integration, bcs=bcs, domain=domain, domain_kind=domain_kind,
+                            ic_kind=ic_kind, ic=ic, **props)
         self._keep = getattr(self, "_keep", []) + [arr]
         idx = lib().h3o_add_solver(self.h, C.byref(d))
         assert idx >= 0, "too many solvers for this grid"
@@ -365,3 +355,62 @@ def set_num_threads(n: int):
 
 def num_threads() -> int:
     return lib().h3o_num_threads()
+
+
+class DualSolver:
+    """Forward-mode derivative twin of an oracle solver (Solver<Dual>): the
+    same tree, description and initial condition; the state carries a
+    direction and steps run with given (frozen) time steps, so state() returns
+    the state and its directional derivative d q_N / d q_0 . dot."""
+
+    def __init__(self, src: Solver):
+        self.h = lib().h3o_dual_clone(src.w.h, src.idx)
+        assert lib().h3o_dual_initialize(self.h) == 0
+        self.nv = src.nv
+        self.n = lib().h3o_dual_ncells(self.h)
+        assert self.n == src.ncells
+
+    def __del__(self):
+        try:
+            lib().h3o_dual_world_destroy(self.h)
+        except Exception:
+            pass
+
+    def set_state(self, val, dot):
+        val = np.ascontiguousarray(val, np.float64)
+        dot = np.ascontiguousarray(dot, np.float64)
+        assert val.shape == dot.shape == (self.nv, self.n)
+        lib().h3o_dual_set_state(self.h, _dp(val), _dp(dot))
+
+    def state(self):
+        val = np.empty((self.nv, self.n))
+        dot = np.empty((self.nv, self.n))
+        lib().h3o_dual_get_state(self.h, _dp(val), _dp(dot))
+        return val, dot
+
+    def solve_dt(self, dts):
+        d = np.ascontiguousarray(dts, np.float64)
+        lib().h3o_dual_solve_dt(self.h, d.size, _dp(d))
+
+
+def _pack_desc(physics=EULER, flux=AUSM, time_integration=EULER_FORWARD, *, bcs=(), domain=None, domain_kind=0,
+               ic_kind=IC_CONSTANT_PV, ic=(), **props):
+    d = SolverDesc()
+    defaults = dict(cfl=0.2, cfl_viscous=0.4, gamma=1.4, Rspecific=287.058, T0=273.15, rho0=1.225, Minfty=0.1,
+                    ReInfty=100.0, Pr0=0.72, Sutherland0=110.4, diffusivity=1.0, T_ref=273.15, time_end=1.0)
+    defaults.update(props)
+    d.physics, d.flux, d.time_integration = physics, flux, time_integration
+    for k, v in defaults.items():
+        setattr(d, k, float(v))
+    d.domain_kind = domain_kind
+    if domain is not None:
+        d.domain = domain
+    d.ic_kind = ic_kind
+    for i, v in enumerate(ic):
+        d.ic[i] = v
+    arr = (BcDesc * max(1, len(bcs)))()
+    for i, b in enumerate(bcs):
+        arr[i] = b
+    d.n_bcs = len(bcs)
+    d.bcs = arr
+    return d, arr

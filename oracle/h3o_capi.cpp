@@ -223,6 +223,57 @@ void h3o_solver_info(void* w, int s, h3o_info* o) {
   }
 }
 
+// ---- forward-mode derivative build (Solver<Dual>): same grid and physics, the
+// state carries a direction; steps run with frozen time steps ----
+using WD = World<Dual>;
+// a derivative twin of solver s of world w: same tree, description and initial state
+void* h3o_dual_clone(void* w, int s) {
+  W* src = (W*)w;
+  const Solver<double>& so = *src->solvers[s];
+  auto* wd = new WD();
+  wd->nd = src->nd;
+  wd->tree.reset(new Tree(*src->tree));
+  wd->tree->node2cell.assign(1, std::vector<Ind>(wd->tree->size(), INV));
+  auto d = std::make_unique<Solver<Dual>>();
+  d->w = wd;
+  d->idx = 0;
+  d->nd = so.nd;
+  d->nv = so.nv;
+  d->P = so.P;
+  d->bcs = so.bcs;
+  d->domain_kind = so.domain_kind;
+  d->domain = so.domain;
+  d->ic_kind = so.ic_kind;
+  std::memcpy(d->ic, so.ic, sizeof(d->ic));
+  wd->solvers.push_back(std::move(d));
+  return wd;
+}
+void h3o_dual_world_destroy(void* w) { delete (WD*)w; }
+int h3o_dual_initialize(void* w) {
+  try { ((WD*)w)->solvers[0]->initialize(); } catch (...) { return -1; }
+  return 0;
+}
+void h3o_dual_set_state(void* w, const double* val, const double* dot) {
+  auto& so = *((WD*)w)->solvers[0];
+  const int64_t n = so.size();
+  for (int v = 0; v < so.nv; ++v)
+    for (int64_t c = 0; c < n; ++c) so.Q[0][v][c] = Dual(val[v * n + c], dot[v * n + c]);
+}
+void h3o_dual_get_state(void* w, double* val, double* dot) {
+  auto& so = *((WD*)w)->solvers[0];
+  const int64_t n = so.size();
+  for (int v = 0; v < so.nv; ++v)
+    for (int64_t c = 0; c < n; ++c) { val[v * n + c] = so.Q[0][v][c].v; dot[v * n + c] = so.Q[0][v][c].d; }
+}
+void h3o_dual_solve_dt(void* w, int nsteps, const double* dts) {
+  auto& so = *((WD*)w)->solvers[0];
+  for (int i = 0; i < nsteps; ++i) {
+    so.force_dt(Dual(dts[i]));
+    so.solve();
+  }
+}
+int64_t h3o_dual_ncells(void* w) { return ((WD*)w)->solvers[0]->size(); }
+
 int h3o_num_threads(void) {
 #ifdef _OPENMP
   return omp_get_max_threads();

@@ -209,3 +209,39 @@ def periodic_vortex_case(level=6, ti=h3o.RK2, flux=h3o.AUSM):
                      time_end=10.0, **dict(EULER_PROPS, cfl=0.5))
     s.initialize()
     return w, [s]
+
+
+def refined_case(ti=h3o.RK2, level=2, fine=4):
+    """EXTENSION (not in hom3): 3D Sod tube on a tree refined +2 levels in a sphere."""
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=level)
+    w.refine_sphere([0.5, 0.5, 0.5], 0.3, fine)
+    s = w.add_solver(h3o.EULER, h3o.AUSM, ti, bcs=neumann_cube(w), ic_kind=h3o.IC_SHOCK_TUBE,
+                     ic=[0, 0, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1], time_end=1.0, cfl=0.4)
+    s.initialize()
+    return w, [s]
+
+
+def smooth_state(o: "h3o.Solver", seed=0):
+    """A state on which the discrete map is smooth, for derivative checks: the
+    case's state plus a uniform subsonic drift (Euler; no face sits at the
+    interface-Mach-number switch m = 0) or 1 + a smooth random field (heat)."""
+    q = o.state(0).copy()
+    fg = o.first_ghost
+    nd = o.w.nd
+    rng = np.random.default_rng(seed)
+    if o.nv == 1:
+        x = o.tables()["x_center"]
+        k = rng.integers(1, 4, size=(4, nd))
+        ph = rng.uniform(0, 2 * np.pi, size=4)
+        f = sum(np.sin(2 * np.pi * (k[m] @ x) + ph[m]) for m in range(4))
+        q[0] = 1.0 + 0.1 * f
+        return q
+    drift = np.array([0.3, 0.1, 0.05][:nd])
+    rho = q[nd]
+    u = q[:nd] / rho
+    ke_old = 0.5 * rho * (u * u).sum(axis=0)
+    u = u + drift[:, None]
+    q[:nd] = rho * u
+    q[nd + 1] = q[nd + 1] - ke_old + 0.5 * rho * (u * u).sum(axis=0)
+    q[:, fg:] = 0.0
+    return q

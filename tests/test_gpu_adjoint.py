@@ -1,0 +1,164 @@
+"""Discrete adjoint (h3c_adjoint) on the GPU, through the C ABI.
+
+J(q0) = <lambda, q_N> with the forward time steps frozen.  The gradient is
+checked against (a) the forward-mode dual-number build of the oracle
+(directional derivatives, to rounding), (b) central finite differences of the
+GPU's own frozen-dt forward map (h3c_solve_dt) in 32 random directions, to
+1e-6 relative, and (c) itself under different checkpoint intervals.  The
+states are made smooth first (cases.smooth_state) so that no face sits on a
+switch of the AUSM flux, where the derivative does not exist.
+"""
+import numpy as np
+import pytest
+
+import cases
+from oracle import h3o
+
+pytestmark = pytest.mark.gpu
+
+BUILDERS = {
+    "euler2d_fe": lambda: cases.euler_case("sod", nd=2, level=5, ti=h3o.EULER_FORWARD),
+    "euler2d_rk2": lambda: cases.euler_case("sod", nd=2, level=5, ti=h3o.RK2),
+    "euler3d_rk2": lambda: cases.euler_case("sod", nd=3, level=3, ti=h3o.RK2),
+    "euler_dirichlet_rk2": lambda: cases.euler_dirichlet_case(nd=2, level=4, ti=h3o.RK2),
+    "heat3d_fe": lambda: cases.heat_case(level=3),
+    "heat3d_rk2": lambda: cases.heat_case(level=3, ti=h3o.RK2),
+    "periodic_vortex_rk2": lambda: cases.periodic_vortex_case(level=5),
+    "refined_fe": lambda: cases.refined_case(ti=h3o.EULER_FORWARD),
+    "refined_rk2": lambda: cases.refined_case(ti=h3o.RK2),
+}
+NSTEPS = 12
+
+
+def setup(name, seed=0):
+    _, (o,) = BUILDERS[name]()
+    q1 = cases.smooth_state(o)
+    o.set_state(q1)
+    g = cases.gpu_solver_from_oracle(o)
+    rng = np.random.default_rng(seed)
+    lam = np.zeros_like(q1)
+    lam[:, :o.first_ghost] = rng.standard_normal((q1.shape[0], o.first_ghost))
+    return o, g, q1, lam
+
+
+def frozen_J(g, q, dts, lam):
+    g.set_state(q, 0)
+    g.reset_time()
+    g.solve_dt(dts)
+    return float((g.state(0) * lam).sum())
+
+
+@pytest.mark.parametrize("name", sorted(BUILDERS))
+def test_adjoint_matches_dual_oracle(name):
+    o, g, q1, lam = setup(name)
+    fg = o.first_ghost
+    grad, dts = g.adjoint(NSTEPS, lam, every=5)
+    assert np.isfinite(grad).all()
+    assert np.all(grad[:, fg:] == 0.0)
+    # the forward of the adjoint took the solver's own CFL steps
+    for i in range(NSTEPS):
+        o.solve(1)
+        assert abs(dts[i] - o.dt()) <= 1e-12 * o.dt(), (i, dts[i], o.dt())
+    rng = np.random.default_rng(11)
+    for _ in range(3):
+        dq = np.zeros_like(q1)
+        dq[:, :fg] = rng.standard_normal((q1.shape[0], fg))
+        _, (o2,) = BUILDERS[name]()
+        ds = h3o.DualSolver(o2)
+        ds.set_state(q1, dq)
+        ds.solve_dt(dts)
+        _, dot = ds.state()
+        jvp = (lam[:, :fg] * dot[:, :fg]).sum()
+        vjp = (grad[:, :fg] * dq[:, :fg]).sum()
+        scale = np.abs(lam[:, :fg] * dot[:, :fg]).sum()
+        assert abs(jvp - vjp) <= 1e-11 * scale, (jvp, vjp, scale)
+
+
+@pytest.mark.parametrize("name", ["euler2d_rk2", "heat3d_fe", "periodic_vortex_rk2", "refined_rk2"])
+def test_adjoint_matches_finite_differences(name):
+    """32 random directions, central differences of the GPU frozen-dt map."""
+    o, g, q1, lam = setup(name, seed=2)
+    fg = o.first_ghost
+    grad, dts = g.adjoint(NSTEPS, lam, every=4)
+    rng = np.random.default_rng(2)
+    worst = 0.0
+    for _ in range(32):
+        dq = np.zeros_like(q1)
+        dq[:, :fg] = rng.standard_normal((q1.shape[0], fg))
+        eps = 1e-6
+        fd = (frozen_J(g, q1 + eps * dq, dts, lam) - frozen_J(g, q1 - eps * dq, dts, lam)) / (2 * eps)
+        ad = (grad * dq).sum()
+        scale = np.abs(grad * dq).sum()
+        worst = max(worst, abs(fd - ad) / scale)
+    assert worst <= 1e-6, worst
+
+
+@pytest.mark.parametrize("name", ["euler2d_fe", "euler3d_rk2", "heat3d_rk2"])
+def test_checkpoint_interval_does_not_change_gradient(name):
+    _, g, q1, lam = setup(name)
+    grads = []
+    for every in (1, 4, NSTEPS):
+        g.set_state(q1, 0)
+        g.reset_time()
+        grads.append(g.adjoint(NSTEPS, lam, every=every)[0])
+    for gr in grads[1:]:
+        assert np.array_equal(gr, grads[0])
+
+
+@pytest.mark.parametrize("name", ["euler2d_rk2", "euler2d_fe"])
+def test_adjoint_leaves_solver_at_step_n(name):
+    """h3c_adjoint's forward is the solver's own step: the state, time and
+    step afterwards equal those of h3c_solve."""
+    o, g, q1, lam = setup(name)
+    g.adjoint(NSTEPS, lam, every=3)
+    _, g2, _, _ = setup(name)
+    g2.solve(NSTEPS)
+    fg = o.first_ghost
+    assert np.abs(g.state(0)[:, :fg] - g2.state(0)[:, :fg]).max() <= 1e-13 * np.abs(g2.state(0)).max()
+    assert g.step() == g2.step() == NSTEPS
+    assert abs(g.time() - g2.time()) <= 1e-15 * g2.time()
+    g.solve(2)
+    g2.solve(2)
+    assert abs(g.dt() - g2.dt()) <= 1e-13 * g2.dt()
+
+
+def test_solve_dt_matches_oracle_forced_steps():
+    o, g, q1, _ = setup("euler3d_rk2")
+    dts = [2e-3, 1.5e-3, 2.5e-3, 1e-3]
+    g.solve_dt(dts)
+    for d in dts:
+        o.force_dt(d)
+        o.solve(1)
+    fg = o.first_ghost
+    a, b = g.state(0)[:, :fg], o.state(0)[:, :fg]
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+def test_autograd_function():
+    import torch
+    from hom3_b200.autograd import solve
+    o, g, q1, lam = setup("euler2d_rk2")
+    fg = o.first_ghost
+    q0 = torch.tensor(q1, requires_grad=True)
+    qn = solve(q0, g, NSTEPS, every=4)
+    loss = (qn * torch.from_numpy(lam)).sum()
+    loss.backward()
+    _, g2, _, _ = setup("euler2d_rk2")
+    grad, _ = g2.adjoint(NSTEPS, lam, every=4)
+    assert np.array_equal(q0.grad.numpy(), grad)
+    _, g3, _, _ = setup("euler2d_rk2")
+    g3.solve(NSTEPS)
+    assert np.abs(qn.detach().numpy()[:, :fg] - g3.state(0)[:, :fg]).max() <= 1e-13 * np.abs(q1).max()
+
+
+def test_unsupported_configurations_are_rejected():
+    import hom3_b200 as hb
+    _, (o,) = cases.cns_case("constant", level=4)
+    g = cases.gpu_solver_from_oracle(o)
+    lam = np.zeros((o.nv, o.ncells))
+    with pytest.raises(hb.H3cError):
+        g.adjoint(2, lam)
+    _, (o,) = cases.euler_case("sod", nd=2, level=4, flux=h3o.LLF)
+    g = cases.gpu_solver_from_oracle(o)
+    with pytest.raises(hb.H3cError):
+        g.adjoint(2, np.zeros((o.nv, o.ncells)))

@@ -1,0 +1,55 @@
+"""The forward-mode dual-number build of the oracle (Solver<Dual>, the
+checker of the discrete adjoint) against central finite differences of the
+double build: same values bit for bit, derivatives to second order in the
+finite-difference step.  Time steps are frozen (forced) in both."""
+import numpy as np
+import pytest
+
+import cases
+from oracle import h3o
+
+BUILDERS = {
+    "euler2d_rk2": lambda: cases.euler_case("sod", nd=2, level=4, ti=h3o.RK2),
+    "euler_dirichlet_fe": lambda: cases.euler_dirichlet_case(nd=2, level=4),
+    "heat3d_fe": lambda: cases.heat_case(level=3),
+    "periodic_vortex_rk2": lambda: cases.periodic_vortex_case(level=4),
+    "refined_rk2": lambda: cases.refined_case(level=2, fine=3),
+}
+
+
+def frozen_run(build, q, dts):
+    _, (s,) = build()
+    s.set_state(q)
+    for d in dts:
+        s.force_dt(d)
+        s.solve(1)
+    return s.state(0)
+
+
+@pytest.mark.parametrize("name", sorted(BUILDERS))
+def test_dual_oracle_matches_finite_differences(name):
+    build = BUILDERS[name]
+    _, (o,) = build()
+    q1 = cases.smooth_state(o)
+    fg = o.first_ghost
+    o.set_state(q1)
+    dts = []
+    for _ in range(4):
+        o.solve(1)
+        dts.append(o.dt())
+    rng = np.random.default_rng(7)
+    dq = np.zeros_like(q1)
+    dq[:, :fg] = rng.standard_normal((q1.shape[0], fg))
+    _, (o2,) = build()
+    ds = h3o.DualSolver(o2)
+    ds.set_state(q1, dq)
+    ds.solve_dt(np.array(dts))
+    val, dot = ds.state()
+    ref = frozen_run(build, q1, dts)
+    assert np.array_equal(val[:, :fg], ref[:, :fg])
+    errs = []
+    for eps in (1e-4, 1e-5):
+        fd = (frozen_run(build, q1 + eps * dq, dts) - frozen_run(build, q1 - eps * dq, dts)) / (2 * eps)
+        errs.append(np.abs(dot[:, :fg] - fd[:, :fg]).max() / np.abs(fd[:, :fg]).max())
+    assert errs[1] < 1e-7, errs
+    assert errs[1] < errs[0] / 30 or errs[1] < 1e-9, errs  # second-order convergence
