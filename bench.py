@@ -381,6 +381,50 @@ def run_tgv(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def measure_adjoint(s, q0, nsteps, stream, fg):
+    """Time h3c_adjoint of J = <lambda, q_N> over nsteps RK2 steps against the
+    same nsteps of h3c_solve (CUDA events on the solver's stream, both from the
+    same initial state; cotangent and gradient are device arrays)."""
+    import torch
+    rng = np.random.default_rng(5)
+    lam = torch.from_numpy(rng.standard_normal(q0.shape)).cuda()
+    grad = torch.empty_like(lam)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    # warm-up: allocates the workspace once
+    s.set_state(q0, 0)
+    s.reset_time()
+    s.adjoint(nsteps, lam, every=0, out=grad)
+    s.set_state(q0, 0)
+    s.reset_time()
+    torch.cuda.synchronize()
+    ev[0].record(stream)
+    s.solve(nsteps)
+    ev[1].record(stream)
+    torch.cuda.synchronize()
+    s.set_state(q0, 0)
+    s.reset_time()
+    torch.cuda.synchronize()
+    s.profile(True)
+    ev[2].record(stream)
+    s.adjoint(nsteps, lam, every=0, out=grad)
+    ev[3].record(stream)
+    torch.cuda.synchronize()
+    s.profile(False)
+    kern = s.profile_read()
+    fwd_ms = ev[0].elapsed_time(ev[1])
+    adj_ms = ev[2].elapsed_time(ev[3])
+    ak_ms, ak_n = kern.get("adjoint", (0.0, 0))
+    # algorithmic bytes of one adjoint-stage launch: stage state + cotangent in, cotangent out
+    # (+ the extra cotangent of the second launch of a step, counted in the mean) and the tables
+    b_launch = fg * (3 * 5 * 8 + 6 * 4 + 1) + 0.5 * fg * 5 * 8
+    return {"steps": nsteps, "forward_ms": fwd_ms, "adjoint_ms": adj_ms, "ratio": adj_ms / fwd_ms,
+            "what": "h3c_adjoint (forward with checkpoints + backward sweep, device cotangent) / h3c_solve of "
+                    "the same steps; the library chose the checkpoint interval",
+            "adjoint_kernel_ms": ak_ms / max(ak_n, 1), "adjoint_launches": ak_n,
+            "adjoint_kernel_gbs": b_launch / (ak_ms / max(ak_n, 1) * 1e-3) / 1e9 if ak_n else None,
+            "grad_finite": bool(torch.isfinite(grad).all().item())}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -395,6 +439,7 @@ def main():
     ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble", "tgv"])
     ap.add_argument("--tgv-level", type=int, default=7)
     ap.add_argument("--members", type=int, default=256)
+    ap.add_argument("--adjoint-steps", type=int, default=50)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_setup()
@@ -457,6 +502,10 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_s = allreduce_max(e2e_s, ws)
     e2e = fg * args.steps * ws / e2e_s
+    # ---- discrete adjoint: time of h3c_adjoint (its forward included) over the forward alone ----
+    adj = None
+    if args.adjoint_steps > 0:
+        adj = measure_adjoint(s, q0, args.adjoint_steps, stream, fg)
     # ---- roofline of the dominant kernel (second RK stage) ----
     peak, peak_kind = peaks()
     st2_ms, st2_n = kern.get("stage2", (0.0, 0))
@@ -497,6 +546,8 @@ def main():
         "l2": "no flush: the working set (both states + tables) exceeds the 126 MB L2",
         "device_status": status,
     }
+    if adj is not None:
+        line["adjoint"] = adj
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         ups, cells, nst, threads, el = cpu_oracle_run(args)
         line["cpu_baseline"] = {"value": ups, "unit": "cell-updates/s", "cores": threads, "kind": "port",

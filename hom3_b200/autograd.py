@@ -39,6 +39,6 @@ class _Solve(torch.autograd.Function):
         return torch.from_numpy(np.ascontiguousarray(grad)).to(grad_out.device), None, None, None
 
 
-def solve(q0: torch.Tensor, solver: Solver, nsteps: int, every: int | None = None) -> torch.Tensor:
+def solve(q0: torch.Tensor, solver: Solver, nsteps: int, every: int = 0) -> torch.Tensor:
     """q_N = solve(q0): nsteps steps of `solver` from q0 at time 0, differentiable in q0."""
     return _Solve.apply(q0, solver, nsteps, every)

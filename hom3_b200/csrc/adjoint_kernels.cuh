@@ -15,6 +15,10 @@
 #pragma once
 #include "fv_kernels.cuh"
 
+#ifndef H3C_ADJ_MINB
+#define H3C_ADJ_MINB 2  // resident blocks per SM the adjoint stage is compiled for
+#endif
+
 namespace h3c {
 
 // derivatives of the split functions (euler/physics.hpp:297-310), |M| > 1 branches frozen
@@ -35,102 +39,95 @@ __device__ __forceinline__ double p_int_d(double s, double M) {
   return (0.25 * ((M + s) * (M + s))) * (2.0 - s * M);
 }
 
+// primitive state of one side, all directions (Newton reciprocals as in make_prim)
 template <int ND> struct SideAD {
-  double rinv, u[ND], um2, p, a2, a, M;
+  double q[ND + 2];
+  double rinv, u[ND], um2, p, a, ainv, M[ND];
 };
 
 template <int ND>
-__device__ __forceinline__ void side_forward(const double* q, int d, double gamma, double gm1, SideAD<ND>& S) {
-  S.rinv = 1.0 / q[ND];
+__device__ __forceinline__ void side_forward(SideAD<ND>& S, double gamma, double gm1) {
+  S.rinv = nr_rcp(S.q[ND]);
   S.um2 = 0.0;
 #pragma unroll
   for (int k = 0; k < ND; ++k) {
-    S.u[k] = q[k] * S.rinv;
-    S.um2 += S.u[k] * S.u[k];
+    S.u[k] = S.q[k] * S.rinv;
+    S.um2 = k == 0 ? S.u[k] * S.u[k] : S.um2 + S.u[k] * S.u[k];
   }
-  S.p = gm1 * (q[ND + 1] - 0.5 * q[ND] * S.um2);
-  S.a2 = gamma * S.p * S.rinv;
-  S.a = sqrt(S.a2);
-  S.M = S.u[d] / S.a;
+  S.p = gm1 * (S.q[ND + 1] - 0.5 * S.q[ND] * S.um2);
+  const double a2 = gamma * S.p * S.rinv;
+  S.ainv = nr_rsqrt(a2);
+  S.a = a2 * S.ainv;
+#pragma unroll
+  for (int k = 0; k < ND; ++k) S.M[k] = S.u[k] * S.ainv;
 }
 
-// reverse through p(q), a(q), M(q) of one side; adds to g[ND + 2]
+// reverse through p(q), a(q), M_d(q) of one side; adds to g[ND + 2]
 template <int ND>
-__device__ __forceinline__ void side_reverse(const double* q, int d, double gamma, double gm1, const SideAD<ND>& S,
-                                             double Mbar, double abar, double pbar, double* g) {
+__device__ __forceinline__ void side_reverse(const SideAD<ND>& S, int d, double gamma, double gm1, double Mbar,
+                                             double abar, double pbar, double* g) {
   double ubar[ND];
 #pragma unroll
-  for (int k = 0; k < ND; ++k) ubar[k] = 0.0;
-  ubar[d] += Mbar / S.a;
-  abar += -Mbar * S.M / S.a;
-  const double a2bar = abar / (2.0 * S.a);
+  for (int k = 0; k < ND; ++k) ubar[k] = k == d ? Mbar * S.ainv : 0.0;
+  abar -= Mbar * S.M[d] * S.ainv;
+  const double a2bar = 0.5 * abar * S.ainv;
   pbar += a2bar * gamma * S.rinv;
   double rinvbar = a2bar * gamma * S.p;
   g[ND + 1] += gm1 * pbar;
-  g[ND] += -0.5 * gm1 * S.um2 * pbar;
-  const double um2bar = -0.5 * gm1 * q[ND] * pbar;
+  g[ND] -= 0.5 * gm1 * S.um2 * pbar;
+  const double um2bar = -0.5 * gm1 * S.q[ND] * pbar;
 #pragma unroll
   for (int k = 0; k < ND; ++k) {
     ubar[k] += 2.0 * S.u[k] * um2bar;
     g[k] += S.rinv * ubar[k];
-    rinvbar += q[k] * ubar[k];
+    rinvbar += S.q[k] * ubar[k];
   }
-  g[ND] += -S.rinv * S.rinv * rinvbar;
+  g[ND] -= S.rinv * S.rinv * rinvbar;
 }
 
 // gL += w^T dF/dq_L, gR += w^T dF/dq_R for the AUSM flux F(q_L, q_R) along d
 template <int ND>
-__device__ __forceinline__ void ausm_vjp(const double* qL, const double* qR, int d, const double* w, double gamma,
-                                         double gm1, double* gL, double* gR) {
+__device__ __forceinline__ void ausm_vjp(const SideAD<ND>& SL, const SideAD<ND>& SR, int d, const double* w,
+                                         double gamma, double gm1, double* gL, double* gR) {
   constexpr int NV = ND + 2;
-  SideAD<ND> SL, SR;
-  side_forward<ND>(qL, d, gamma, gm1, SL);
-  side_forward<ND>(qR, d, gamma, gm1, SR);
-  const double mi = m_int_d(1.0, SL.M) + m_int_d(-1.0, SR.M);
+  const double ML = SL.M[d], MR = SR.M[d];
+  const double mi = m_int_d(1.0, ML) + m_int_d(-1.0, MR);
   const bool left = mi >= 0.0;
-  const double* qu = left ? qL : qR;
   const SideAD<ND>& Su = left ? SL : SR;
-  double theta[NV];
+  // F_v = mi theta_v + [v == d] pi, theta = a (q_0 .. q_ND, q_E + p) of the upwind side
+  double wq = 0.0;
 #pragma unroll
-  for (int v = 0; v < ND + 1; ++v) theta[v] = Su.a * qu[v];
-  theta[ND + 1] = Su.a * (qu[ND + 1] + Su.p);
-  // F_v = mi theta_v + [v == d] pi
-  double mbar = 0.0;
-#pragma unroll
-  for (int v = 0; v < NV; ++v) mbar += w[v] * theta[v];
+  for (int v = 0; v < NV - 1; ++v) wq += w[v] * Su.q[v];
+  wq += w[NV - 1] * (Su.q[NV - 1] + Su.p);
+  const double mbar = Su.a * wq;
   const double pibar = w[d];
-  double MLbar = dm_int(1.0, SL.M) * mbar + dp_int(1.0, SL.M) * SL.p * pibar;
-  double MRbar = dm_int(-1.0, SR.M) * mbar + dp_int(-1.0, SR.M) * SR.p * pibar;
-  double pLbar = p_int_d(1.0, SL.M) * pibar;
-  double pRbar = p_int_d(-1.0, SR.M) * pibar;
+  const double MLbar = dm_int(1.0, ML) * mbar + dp_int(1.0, ML) * SL.p * pibar;
+  const double MRbar = dm_int(-1.0, MR) * mbar + dp_int(-1.0, MR) * SR.p * pibar;
+  double pLbar = p_int_d(1.0, ML) * pibar;
+  double pRbar = p_int_d(-1.0, MR) * pibar;
+  const double abar_u = mi * wq;
+  const double am = Su.a * mi;
   double aLbar = 0.0, aRbar = 0.0;
-  // theta of the upwind side
-  double abar_u = 0.0;
-  double* gu = left ? gL : gR;
+  if (left) {
 #pragma unroll
-  for (int v = 0; v < ND + 1; ++v) {
-    const double tb = mi * w[v];
-    abar_u += tb * qu[v];
-    gu[v] += Su.a * tb;
+    for (int v = 0; v < NV; ++v) gL[v] += am * w[v];
+    pLbar += am * w[NV - 1];
+    aLbar = abar_u;
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) gR[v] += am * w[v];
+    pRbar += am * w[NV - 1];
+    aRbar = abar_u;
   }
-  {
-    const double tb = mi * w[ND + 1];
-    abar_u += tb * (qu[ND + 1] + Su.p);
-    gu[ND + 1] += Su.a * tb;
-    if (left) pLbar += Su.a * tb;
-    else pRbar += Su.a * tb;
-  }
-  if (left) aLbar += abar_u;
-  else aRbar += abar_u;
-  side_reverse<ND>(qL, d, gamma, gm1, SL, MLbar, aLbar, pLbar, gL);
-  side_reverse<ND>(qR, d, gamma, gm1, SR, MRbar, aRbar, pRbar, gR);
+  side_reverse<ND>(SL, d, gamma, gm1, MLbar, aLbar, pLbar, gL);
+  side_reverse<ND>(SR, d, gamma, gm1, MRbar, aRbar, pRbar, gR);
 }
 
 // Per-cell adjoint of one stage:
 //   gout_c = beta lam_c + [VJP of (q -> alpha k R(q)) with cotangent lam]_c + gamma_e extra_c
 // q is the stage input with its ghosts filled by the conditions.
 template <int ND, int PHYS>
-__global__ void __launch_bounds__(kBlock) k_adj_stage(const double* __restrict__ q, const double* __restrict__ lam,
+__global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double* __restrict__ q, const double* __restrict__ lam,
                                                       double* __restrict__ gout, const double* __restrict__ extra,
                                                       double alpha, double beta, double gamma_e, Geometry g,
                                                       GhostTables gt, PhysConst pc, const Scalars* __restrict__ sc) {
@@ -143,20 +140,24 @@ __global__ void __launch_bounds__(kBlock) k_adj_stage(const double* __restrict__
   const double dt = sc->dt;
   const double hc = g.len[g.lvl[c]];
   const double kc = alpha * dt / hc;
-  double qc[NV], lc[NV], acc[NV];
+  double lc[NV], acc[NV];
+  SideAD<ND> Sc;
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    qc[v] = q[v * ld + c];
     lc[v] = lam[v * ld + c];
     acc[v] = 0.0;
+  }
+  if (PHYS == HEAT) {
+    Sc.q[0] = q[c];
+  } else {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Sc.q[v] = q[v * ld + c];
+    side_forward<ND>(Sc, pc.gamma, pc.gm1);
   }
   // resolve a neighbour entry: interior cell (its own residual) or ghost (condition Jacobian)
   // returns the residual-owning cell for the cotangent and the Jacobian sign of the ghost
   auto face = [&](int nb_cell, bool c_is_left, double kc_face, double kn_face, int d) {
     // nb_cell: neighbour index (interior or ghost)
-    double qn[NV];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) qn[v] = q[v * ld + nb_cell];
     double w[NV];
     double jac = 0.0;  // ghost: dq_ghost/dq_c = jac I; interior: 0
     long long own = nb_cell;
@@ -199,8 +200,12 @@ __global__ void __launch_bounds__(kBlock) k_adj_stage(const double* __restrict__
       for (int v = 0; v < NV; ++v) acc[v] += gc[v];
       return;
     }
-    if (c_is_left) ausm_vjp<ND>(qc, qn, d, w, pc.gamma, pc.gm1, gc, gn);
-    else ausm_vjp<ND>(qn, qc, d, w, pc.gamma, pc.gm1, gn, gc);
+    SideAD<ND> Sn;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Sn.q[v] = q[v * ld + nb_cell];
+    side_forward<ND>(Sn, pc.gamma, pc.gm1);
+    if (c_is_left) ausm_vjp<ND>(Sc, Sn, d, w, pc.gamma, pc.gm1, gc, gn);
+    else ausm_vjp<ND>(Sn, Sc, d, w, pc.gamma, pc.gm1, gn, gc);
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] += gc[v] + jac * gn[v];
   };

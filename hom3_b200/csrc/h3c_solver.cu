@@ -67,6 +67,8 @@ struct h3c_solver_s {
   double* d_slopes = nullptr;
   double* d_stage = nullptr;  // host<->device staging in caller numbering
   long long stage_cap = 0;
+  double* d_adj = nullptr;  // adjoint workspace (checkpoints, stage states, cotangents), kept between calls
+  size_t adj_cap = 0;
   long long* d_dev2caller = nullptr;
   std::vector<long long> dev2caller, caller2dev;
   Scalars* d_sc = nullptr;
@@ -130,6 +132,8 @@ void free_grid(h3c_solver s) {
   dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_slopes); dfree(s->d_stage);
   dfree(s->d_dev2caller);
   dfree(s->d_blk_inst); dfree(s->d_inst_end); dfree(s->d_ginst);
+  dfree(s->d_adj);
+  s->adj_cap = 0;
   s->stage_cap = 0;
   s->has_grid = false;
 }
@@ -1253,43 +1257,72 @@ int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts) {
   return s->cuda(cudaGetLastError(), "h3c_solve_dt");
 }
 
+// Backward sweep of the discrete adjoint.  Memory: nck checkpoints + the
+// stage states of one segment + 3 work + 3 cotangent states.  The forward
+// stores the stage states of the last segment as it goes, so that segment
+// (all of them when every >= nsteps) needs no recomputation.
 int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dqN, double* dJ_dq0, double* dts_out) {
-  if (!s || nsteps < 1 || every < 1 || !dJ_dqN || !dJ_dq0) return H3C_E_INVALID;
+  if (!s || nsteps < 1 || every < 0 || !dJ_dqN || !dJ_dq0) return H3C_E_INVALID;
   if (int rc = adjoint_supported(s, "h3c_adjoint")) return rc;
   const long long L = s->ld, nv = s->nv, Q = nv * L;
   const bool rk2 = s->desc.time_integration == H3C_RUNGE_KUTTA_2;
-  const long long nck = (nsteps + every - 1) / every;
   const long long per = rk2 ? 2 : 1;
-  double *ck = nullptr, *seg = nullptr, *work = nullptr, *lam = nullptr, *d_dts = nullptr;
-  auto cleanup = [&]() {
-    cudaStreamSynchronize(s->stream);
-    cudaFree(ck); cudaFree(seg); cudaFree(work); cudaFree(lam); cudaFree(d_dts);
+  auto need = [&](long long ev) {
+    const long long nck = (nsteps + ev - 1) / ev;
+    return sizeof(double) * ((size_t)Q * (nck + per * ev + 6) + nsteps);
   };
-  if (cudaMalloc(&ck, sizeof(double) * Q * nck) != cudaSuccess || cudaMalloc(&seg, sizeof(double) * Q * per * every) != cudaSuccess ||
-      cudaMalloc(&work, sizeof(double) * Q * 3) != cudaSuccess || cudaMalloc(&lam, sizeof(double) * Q * 3) != cudaSuccess ||
-      cudaMalloc(&d_dts, sizeof(double) * nsteps) != cudaSuccess) {
-    cudaGetLastError();
-    cleanup();
-    return s->fail(H3C_E_NOMEM, "h3c_adjoint: checkpoints do not fit (%lld checkpoints + %lld stage states)", nck, per * every);
+  if (every > nsteps) every = nsteps;
+  if (every == 0) {  // no recomputation if that fits in half of the free memory, else ~sqrt(N) segments
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    const size_t budget = fr / 2 + s->adj_cap;
+    every = nsteps;
+    if (need(every) > budget) every = std::max<long long>(1, (long long)std::sqrt((double)nsteps));
+    while (every > 1 && need(every) > budget) --every;
   }
-  // ---- forward: the solver's own step (CFL dt), checkpoint every `every` steps, record dt ----
+  const long long nck = (nsteps + every - 1) / every;
+  const size_t bytes = need(every);
+  if (bytes > s->adj_cap) {
+    dfree(s->d_adj);
+    s->adj_cap = 0;
+    if (cudaMalloc(&s->d_adj, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      s->d_adj = nullptr;
+      return s->fail(H3C_E_NOMEM, "h3c_adjoint: %zu bytes of checkpoints do not fit (%lld checkpoints + %lld stage states)",
+                     bytes, nck, per * every);
+    }
+    s->adj_cap = bytes;
+  }
+  double* ck = s->d_adj;
+  double* seg = ck + Q * nck;
+  double* work = seg + Q * per * every;
+  double* lam = work + Q * 3;
+  double* d_dts = lam + Q * 3;
+  const long long last0 = (nck - 1) * every;  // first step of the last segment
+  // ---- forward: the solver's own step (CFL dt), checkpoints, dt record ----
   const bool fuse = !s->unfused_dt;
   for (int64_t i = 0; i < nsteps; ++i) {
     if (i % every == 0)
       cudaMemcpyAsync(ck + Q * (i / every), s->d_q[0], sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+    double* s0 = i >= last0 ? seg + Q * per * (i - last0) : nullptr;
     launch_bc(s, 0);
     if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
     {
       Launch L1(s, K_SCALAR);
       k_set_dt<<<1, 1, 0, s->stream>>>(s->d_sc, 1, 1);
     }
-    k_record_dt<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
+    {
+      Launch L1(s, K_SCALAR);
+      k_record_dt<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
+    }
+    if (s0) cudaMemcpyAsync(s0, s->d_q[0], sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
     if (!rk2) {
       launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
       std::swap(s->d_q[0], s->d_q[1]);
     } else {
       launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
       launch_bc(s, 1);
+      if (s0) cudaMemcpyAsync(s0 + Q, s->d_q[1], sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
       launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
     }
     {
@@ -1304,12 +1337,13 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   double* lamB = lam + Q;      // scratch
   double* lamC = lam + 2 * Q;  // lambda* (RK2)
   cudaMemsetAsync(lam, 0, sizeof(double) * Q * 3, s->stream);
-  if (int rc = ensure_stage(s, s->n_caller)) { cleanup(); return rc; }
+  if (int rc = ensure_stage(s, s->n_caller)) return rc;
+  // host or device arrays (unified addressing)
   for (int v = 0; v < nv; ++v)
     cudaMemcpyAsync(s->d_stage + v * s->n_caller, dJ_dqN + v * s->n_caller, sizeof(double) * s->n_caller,
-                    cudaMemcpyHostToDevice, s->stream);
+                    cudaMemcpyDefault, s->stream);
   k_gather<<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_stage, s->n_caller, lamA, L, s->d_dev2caller, s->n_int, (int)nv);
-  // ---- backward over segments, recomputing each segment's stage inputs ----
+  ++s->launches;
   auto adj = [&](const double* qin, const double* lamin, double* gout, const double* extra, double alpha, double beta,
                  double gam) {
     Launch La(s, K_OTHER);
@@ -1327,23 +1361,25 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
         k_adj_stage<3, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
     }
   };
+  // ---- backward over segments; all but the last recompute their stage states from the checkpoint ----
   for (long long k = nck - 1; k >= 0; --k) {
     const long long i0 = k * every, i1 = std::min<long long>(nsteps, i0 + every);
-    // recompute: work[0] <- checkpoint, keep every stage input in seg
-    double* cur = work;
-    cudaMemcpyAsync(cur, ck + Q * k, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-    for (long long i = i0; i < i1; ++i) {
-      double* s0 = seg + Q * per * (i - i0);
-      cudaMemcpyAsync(s0, cur, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-      double* nxt = (cur == work) ? work + Q : work;
-      frozen_step(s, s0, rk2 ? s0 + Q : nullptr, rk2 ? s0 : nxt, d_dts, i);
-      if (rk2) {
-        // s0 now holds the new state (in-place second stage); restore the stage input into s0
-        cudaMemcpyAsync(nxt, s0, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+    if (k != nck - 1) {
+      double* cur = work;
+      cudaMemcpyAsync(cur, ck + Q * k, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+      for (long long i = i0; i < i1; ++i) {
+        double* s0 = seg + Q * per * (i - i0);
         cudaMemcpyAsync(s0, cur, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-        launch_bc_ptr(s, s0, s0);
+        double* nxt = (cur == work) ? work + Q : work;
+        frozen_step(s, s0, rk2 ? s0 + Q : nullptr, rk2 ? s0 : nxt, d_dts, i);
+        if (rk2) {
+          // s0 now holds the new state (in-place second stage); restore the stage input into s0
+          cudaMemcpyAsync(nxt, s0, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+          cudaMemcpyAsync(s0, cur, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
+          launch_bc_ptr(s, s0, s0);
+        }
+        cur = nxt;
       }
-      cur = nxt;
     }
     for (long long i = i1 - 1; i >= i0; --i) {
       double* s0 = seg + Q * per * (i - i0);
@@ -1365,16 +1401,16 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   // ---- gradient (internal -> caller numbering), dt sequence ----
   cudaMemsetAsync(s->d_stage, 0, sizeof(double) * nv * s->n_caller, s->stream);
   k_scatter<<<blocks(s->n_int), kBlock, 0, s->stream>>>(lamA, L, s->d_stage, s->n_caller, s->d_dev2caller, s->n_int, (int)nv);
+  ++s->launches;
   for (int v = 0; v < nv; ++v)
     cudaMemcpyAsync(dJ_dq0 + v * s->n_caller, s->d_stage + v * s->n_caller, sizeof(double) * s->n_caller,
-                    cudaMemcpyDeviceToHost, s->stream);
-  if (dts_out) cudaMemcpyAsync(dts_out, d_dts, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, s->stream);
-  cudaStreamSynchronize(s->stream);
+                    cudaMemcpyDefault, s->stream);
+  if (dts_out) cudaMemcpyAsync(dts_out, d_dts, sizeof(double) * nsteps, cudaMemcpyDefault, s->stream);
   // the solver is left at step N with the scalars of the forward run
-  cudaMemcpy(s->d_sc, &saved, sizeof(Scalars), cudaMemcpyHostToDevice);
-  const cudaError_t e = cudaGetLastError();
-  cleanup();
-  return s->cuda(e, "h3c_adjoint");
+  cudaStreamSynchronize(s->stream);
+  cudaMemcpyAsync(s->d_sc, &saved, sizeof(Scalars), cudaMemcpyHostToDevice, s->stream);
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  return s->cuda(cudaGetLastError(), "h3c_adjoint");
 }
 
 int h3c_launches(h3c_solver s, int64_t* n) {

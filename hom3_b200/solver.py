@@ -258,13 +258,24 @@ class Solver:
         d = np.ascontiguousarray(dts, np.float64)
         self._check(lib().h3c_solve_dt(self.h, d.size, _dp(d)))
 
-    def adjoint(self, nsteps, dJ_dqN, every=None):
-        """Run nsteps steps (CFL dt) and return (dJ/dq0, dts) for J = <dJ_dqN, q_N>."""
+    def adjoint(self, nsteps, dJ_dqN, every=0, out=None):
+        """Run nsteps steps (CFL dt) and return (dJ/dq0, dts) for J = <dJ_dqN, q_N>.
+
+        every: checkpoint interval (0: chosen by the library).  dJ_dqN may be a
+        numpy array or a float64 CUDA tensor of shape [nv][n_cells]; with a CUDA
+        tensor the gradient is returned as one (or written into `out`)."""
+        dts = np.empty(nsteps)
+        if hasattr(dJ_dqN, "is_cuda") and dJ_dqN.is_cuda:
+            import torch
+            lam = dJ_dqN.contiguous()
+            assert lam.dtype == torch.float64 and tuple(lam.shape) == (self.nv, self.n_cells)
+            grad = torch.empty_like(lam) if out is None else out
+            self._check(lib().h3c_adjoint(self.h, nsteps, every, C.cast(lam.data_ptr(), C.POINTER(C.c_double)),
+                                          C.cast(grad.data_ptr(), C.POINTER(C.c_double)), _dp(dts)))
+            return grad, dts
         lam = np.ascontiguousarray(dJ_dqN, np.float64)
         assert lam.shape == (self.nv, self.n_cells)
-        grad = np.empty_like(lam)
-        dts = np.empty(nsteps)
-        every = every or max(1, int(round(nsteps ** 0.5)))
+        grad = np.empty_like(lam) if out is None else out
         self._check(lib().h3c_adjoint(self.h, nsteps, every, _dp(lam), _dp(grad), _dp(dts)))
         return grad, dts
 

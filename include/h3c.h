@@ -240,12 +240,16 @@ int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t ld, int64_
  * h3c_solve_dt: nsteps steps with the given time steps (host array) instead
  * of the CFL time step -- the forward map the adjoint differentiates.
  * h3c_adjoint: runs nsteps steps from the current state (leaving the solver
- * at step N, like h3c_solve) with checkpoints every `every` steps, then
- * returns dJ/dq0 for J = <dJ_dqN, q_N> (host arrays, caller numbering,
- * [nv][n_cells]; ghost entries of dJ_dqN are ignored, of dJ_dq0 zero) with the
- * time steps frozen at the forward values (returned in dts, may be NULL).
- * Each segment of `every` steps is recomputed from its checkpoint.  Euler
- * with the AUSM flux and heat, Neumann / Dirichlet / periodic conditions. */
+ * at step N, like h3c_solve) with a checkpoint every `every` steps (0: the
+ * library picks -- no recomputation when that fits in half of the free device
+ * memory), then returns dJ/dq0 for J = <dJ_dqN, q_N> with the time steps
+ * frozen at the forward values (returned in dts, may be NULL).  dJ_dqN,
+ * dJ_dq0 and dts are [nv][n_cells] / [nsteps] arrays in caller numbering, in
+ * host or device memory; ghost entries of dJ_dqN are ignored, of dJ_dq0 zero.
+ * The last segment's stage states are kept from the forward run; the other
+ * segments are recomputed from their checkpoints.  The workspace stays
+ * allocated for the next call.  Euler with the AUSM flux and heat;
+ * Neumann / Dirichlet / periodic conditions. */
 int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts);
 int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dqN, double* dJ_dq0, double* dts);
 

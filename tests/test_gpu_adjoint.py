@@ -122,6 +122,20 @@ def test_adjoint_leaves_solver_at_step_n(name):
     assert abs(g.dt() - g2.dt()) <= 1e-13 * g2.dt()
 
 
+def test_device_cotangent_and_automatic_interval():
+    """CUDA-tensor cotangent/gradient (device pointers through the ABI) and
+    the library-chosen checkpoint interval give the host-array result."""
+    import torch
+    _, g, q1, lam = setup("euler3d_rk2")
+    ref, dts_ref = g.adjoint(NSTEPS, lam, every=3)
+    g.set_state(q1, 0)
+    g.reset_time()
+    grad, dts = g.adjoint(NSTEPS, torch.from_numpy(lam).cuda(), every=0)
+    assert grad.is_cuda
+    assert np.array_equal(grad.cpu().numpy(), ref)
+    assert np.array_equal(dts, dts_ref)
+
+
 def test_solve_dt_matches_oracle_forced_steps():
     o, g, q1, _ = setup("euler3d_rk2")
     dts = [2e-3, 1.5e-3, 2.5e-3, 1e-3]
