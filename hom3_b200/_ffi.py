@@ -15,7 +15,8 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libhom3_b200.so")
 OK, E_INVALID, E_CUDA, E_NONFINITE, E_STATE, E_TIMEOUT, E_NOMEM = 0, -1, -2, -3, -4, -5, -6
 EULER, CNS, HEAT = 0, 1, 2
 FLUX_AUSM, FLUX_LLF = 0, 1
-EULER_FORWARD, RUNGE_KUTTA_2 = 0, 1
+EULER_FORWARD, RUNGE_KUTTA_2, SSPRK3 = 0, 1, 2
+RECON_NONE, RECON_MUSCL = 0, 1
 FP64, MIXED = 0, 1
 (BC_EULER_NEUMANN, BC_EULER_DIRICHLET, BC_EULER_VORTEX, BC_CNS_INFLOW, BC_CNS_OUTFLOW,
  BC_CNS_ADIABATIC_NOSLIP, BC_CNS_ADIABATIC_SLIP, BC_CNS_ISOTHERMAL_NOSLIP, BC_HEAT_DIRICHLET,
@@ -30,7 +31,8 @@ class Desc(C.Structure):
     _fields_ = [("nd", C.c_int), ("physics", C.c_int), ("flux", C.c_int), ("time_integration", C.c_int),
                 ("precision", C.c_int)] + [
         (n, C.c_double) for n in ("time_end", "cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0",
-                                  "Minfty", "ReInfty", "Pr0", "Sutherland0", "diffusivity", "T_ref")]
+                                  "Minfty", "ReInfty", "Pr0", "Sutherland0", "diffusivity", "T_ref")] + [
+        ("reconstruction", C.c_int), ("limiter_k", C.c_double)]
 
 
 class Bc(C.Structure):

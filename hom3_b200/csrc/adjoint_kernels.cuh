@@ -124,12 +124,14 @@ __device__ __forceinline__ void ausm_vjp(const SideAD<ND>& SL, const SideAD<ND>&
 }
 
 // Per-cell adjoint of one stage:
-//   gout_c = beta lam_c + [VJP of (q -> alpha k R(q)) with cotangent lam]_c + gamma_e extra_c
+//   gout_c = beta lam_c + [VJP of (q -> alpha k R(q)) with cotangent lam]_c
+//            + gamma_e extra_c + gamma_e2 extra2_c
 // q is the stage input with its ghosts filled by the conditions.
 template <int ND, int PHYS>
 __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double* __restrict__ q, const double* __restrict__ lam,
                                                       double* __restrict__ gout, const double* __restrict__ extra,
-                                                      double alpha, double beta, double gamma_e, Geometry g,
+                                                      const double* __restrict__ extra2, double alpha, double beta,
+                                                      double gamma_e, double gamma_e2, Geometry g,
                                                       GhostTables gt, PhysConst pc, const Scalars* __restrict__ sc) {
   constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
   constexpr int NS = 1 << (ND - 1);
@@ -244,6 +246,7 @@ __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double
   for (int v = 0; v < NV; ++v) {
     double o = beta * lc[v] + acc[v];
     if (extra) o += gamma_e * extra[v * ld + c];
+    if (extra2) o += gamma_e2 * extra2[v * ld + c];
     gout[v * ld + c] = o;
   }
 }

@@ -603,11 +603,23 @@ __global__ void __launch_bounds__(kBlock) k_slopes(const double* __restrict__ q,
   }
 }
 
+// Explicit stage update from q0 (the step's start state, in `out` for the
+// in-place stages), the stage input qc and r = dt/dx R(qc):
+//   MODE 0: qc + r (FE, first stage of RK2 / SSP-RK3)
+//   MODE 2: 0.5 ((q0 + qc) + r) (RK2 second stage, solver.hpp:483-494)
+//   MODE 3: 3/4 q0 + 1/4 (qc + r), MODE 4: 1/3 q0 + 2/3 (qc + r) (EXTENSION: SSP-RK3)
+template <int MODE> __device__ __forceinline__ double rk_combine(double q0, double qc, double r) {
+  if (MODE == 0) return qc + r;
+  if (MODE == 2) return 0.5 * ((q0 + qc) + r);
+  if (MODE == 3) return 0.75 * q0 + 0.25 * (qc + r);
+  return (1.0 / 3.0) * q0 + (2.0 / 3.0) * (qc + r);
+}
+
 // ---------------------------------------------------------------------------
 // Stage kernel: num_flux (solver.hpp:440-460) + the explicit update of evolve
 // (solver.hpp:470-494).
-//   MODE 0:  out = qin + dt/dx * R(qin)                 (FE, RK2 stage 1)
-//   MODE 2:  out = 0.5 * ((out + qin) + dt/dx * R(qin))  (RK2 stage 2, in place on lhs)
+//   out = rk_combine<MODE>(out, qin, dt/dx R(qin)); MODE 2, 3 and 4 read the
+//   start state from `out` (in place).
 // FUSE: also reduce the next step's cell dt of `out` into *dtmin (the
 // compute_dt of the next set_dt; valid when no condition rewrites interior cells).
 // HANG: the grid has coarse/fine faces (EXTENSION, not in hom3).
@@ -759,10 +771,7 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
     const double k = dt / dx;
     double o[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      if (MODE == 0) o[v] = qc[v] + k * acc[v];
-      else o[v] = 0.5 * ((out[v * ld + c] + qc[v]) + k * acc[v]);
-    }
+    for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : out[v * ld + c], qc[v], k * acc[v]);
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
     if (FUSE) {
@@ -936,10 +945,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
     const double k = dt / dx;
     double o[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) {
-      if (MODE == 0) o[v] = qc[v] + k * acc[v];
-      else o[v] = 0.5 * ((out[v * ld + c] + qc[v]) + k * acc[v]);
-    }
+    for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : out[v * ld + c], qc[v], k * acc[v]);
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
     if (FUSE) {
@@ -1149,7 +1155,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
         for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);
       }
       double qo[NV];
-      if (MODE == 2) {
+      if (MODE != 0) {
 #pragma unroll
         for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
       }
@@ -1157,10 +1163,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
       const double k = dt / dx;
       double o[NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        if (MODE == 0) o[v] = qc[v] + k * acc[v];
-        else o[v] = 0.5 * ((qo[v] + qc[v]) + k * acc[v]);
-      }
+      for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], qc[v], k * acc[v]);
 #pragma unroll
       for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
       if (FUSE) {

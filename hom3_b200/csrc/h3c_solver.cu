@@ -21,6 +21,7 @@
 #include "../../include/h3c.h"
 #include "fv_kernels.cuh"
 #include "adjoint_kernels.cuh"
+#include "muscl_kernels.cuh"
 
 using namespace h3c;
 
@@ -63,7 +64,7 @@ struct h3c_solver_s {
   BcParam* d_bcs = nullptr;
   h3c_solver partner = nullptr;
   // state
-  double* d_q[2] = {nullptr, nullptr};
+  double* d_q[3] = {nullptr, nullptr, nullptr};  // lhs, rhs, second SSP-RK3 stage
   double* d_slopes = nullptr;
   double* d_stage = nullptr;  // host<->device staging in caller numbering
   long long stage_cap = 0;
@@ -129,7 +130,7 @@ void free_grid(h3c_solver s) {
   drop_graph(s);
   dfree(s->d_nbr); dfree(s->d_lvl); dfree(s->d_sub); dfree(s->d_gbndry); dfree(s->d_gpos);
   dfree(s->d_gapply); dfree(s->d_gown); dfree(s->d_gdx); dfree(s->d_gpartner); dfree(s->d_xc);
-  dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_slopes); dfree(s->d_stage);
+  dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_q[2]); dfree(s->d_slopes); dfree(s->d_stage);
   dfree(s->d_dev2caller);
   dfree(s->d_blk_inst); dfree(s->d_inst_end); dfree(s->d_ginst);
   dfree(s->d_adj);
@@ -259,9 +260,29 @@ void launch_slopes(h3c_solver s, int which) {
     k_slopes<3><<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_q[which], geometry(s), ghosts(s), s->d_slopes);
 }
 
+// EXTENSION: limited least-squares gradients of the stage input (MUSCL)
+void launch_grad(h3c_solver s, const double* q) {
+  Launch L(s, K_SLOPES);
+  const double K = s->desc.limiter_k;
+  if (s->nd == 2) {
+    if (s->nsub > 0) k_muscl_grad<2, true><<<blocks(s->n_int), kBlock, 0, s->stream>>>(q, s->d_xc, geometry(s), s->pc, K, s->d_slopes);
+    else k_muscl_grad<2, false><<<blocks(s->n_int), kBlock, 0, s->stream>>>(q, s->d_xc, geometry(s), s->pc, K, s->d_slopes);
+    if (s->needs_periodic) k_muscl_ghosts<2><<<blocks(s->ng), kBlock, 0, s->stream>>>(s->d_slopes, geometry(s), ghosts(s));
+  } else {
+    if (s->nsub > 0) k_muscl_grad<3, true><<<blocks(s->n_int), kBlock, 0, s->stream>>>(q, s->d_xc, geometry(s), s->pc, K, s->d_slopes);
+    else k_muscl_grad<3, false><<<blocks(s->n_int), kBlock, 0, s->stream>>>(q, s->d_xc, geometry(s), s->pc, K, s->d_slopes);
+    if (s->needs_periodic) k_muscl_ghosts<3><<<blocks(s->ng), kBlock, 0, s->stream>>>(s->d_slopes, geometry(s), ghosts(s));
+  }
+}
+
 template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG, bool FUSE>
 void stage_t(h3c_solver s, const double* qin, double* out) {
   Launch L(s, MODE == 0 ? K_STAGE1 : K_STAGE2);
+  if (PHYS == EULER && FLUX == AUSM && s->desc.reconstruction == H3C_RECON_MUSCL) {
+    k_stage_muscl<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
+        qin, out, s->d_slopes, s->d_xc, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+    return;
+  }
   if (PHYS == EULER && FLUX == AUSM && s->tile) {
     constexpr size_t smem = ausm_smem_bytes<R, ND>();
     static bool attr = false;  // one opt-in per instantiation (dynamic smem above 48 KB)
@@ -303,7 +324,9 @@ void stage_h(h3c_solver s, const double* qin, double* out, bool fuse) {
 template <int ND, int PHYS, int FLUX, class R>
 void stage_m(h3c_solver s, int mode, const double* qin, double* out, bool fuse) {
   if (mode == 0) stage_h<ND, PHYS, FLUX, R, 0>(s, qin, out, fuse);
-  else stage_h<ND, PHYS, FLUX, R, 2>(s, qin, out, fuse);
+  else if (mode == 2) stage_h<ND, PHYS, FLUX, R, 2>(s, qin, out, fuse);
+  else if (mode == 3) stage_h<ND, PHYS, FLUX, R, 3>(s, qin, out, fuse);
+  else stage_h<ND, PHYS, FLUX, R, 4>(s, qin, out, fuse);
 }
 template <int ND>
 void stage_nd(h3c_solver s, int mode, const double* qin, double* out, bool fuse) {
@@ -399,8 +422,13 @@ int h3c_create(const h3c_desc* d, h3c_solver* out) {
   if (!d || !out) { g_last_error = "h3c_create: null argument"; return H3C_E_INVALID; }
   if (d->nd != 2 && d->nd != 3) { g_last_error = "h3c_create: nd must be 2 or 3"; return H3C_E_INVALID; }
   if (d->physics < 0 || d->physics > 2 || d->flux < 0 || d->flux > 1 || d->time_integration < 0 ||
-      d->time_integration > 1 || d->precision < 0 || d->precision > 1) {
+      d->time_integration > 2 || d->precision < 0 || d->precision > 1 || d->reconstruction < 0 ||
+      d->reconstruction > 1) {
     g_last_error = "h3c_create: unknown physics / flux / time integration / precision";
+    return H3C_E_INVALID;
+  }
+  if (d->reconstruction == H3C_RECON_MUSCL && (d->physics != H3C_EULER || d->flux != H3C_FLUX_AUSM)) {
+    g_last_error = "h3c_create: MUSCL reconstruction is implemented for Euler with the AUSM flux";
     return H3C_E_INVALID;
   }
   if (d->physics == H3C_CNS && d->flux != H3C_FLUX_AUSM) {
@@ -715,7 +743,9 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   H3C_CUDA(s, cudaMalloc(&s->d_bcs, sizeof(BcParam) * s->h_bcs.size()));
   H3C_CUDA(s, cudaMalloc(&s->d_q[0], sizeof(double) * s->nv * L));
   H3C_CUDA(s, cudaMalloc(&s->d_q[1], sizeof(double) * s->nv * L));
-  if (s->desc.physics == H3C_CNS) H3C_CUDA(s, cudaMalloc(&s->d_slopes, sizeof(double) * nd * s->nv * L));
+  if (s->desc.time_integration == H3C_SSPRK3) H3C_CUDA(s, cudaMalloc(&s->d_q[2], sizeof(double) * s->nv * L));
+  if (s->desc.physics == H3C_CNS || s->desc.reconstruction == H3C_RECON_MUSCL)
+    H3C_CUDA(s, cudaMalloc(&s->d_slopes, sizeof(double) * nd * s->nv * L));
   H3C_CUDA(s, cudaMalloc(&s->d_dev2caller, sizeof(long long) * n_tot));
   if (ninst > 1) {
     H3C_CUDA(s, cudaMalloc(&s->d_blk_inst, sizeof(int) * h_blk.size()));
@@ -745,6 +775,8 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   H3C_CUDA(s, cudaMemcpy(s->d_dev2caller, dev2caller.data(), sizeof(long long) * n_tot, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemset(s->d_q[0], 0, sizeof(double) * s->nv * L));
   H3C_CUDA(s, cudaMemset(s->d_q[1], 0, sizeof(double) * s->nv * L));
+  if (s->d_q[2]) H3C_CUDA(s, cudaMemset(s->d_q[2], 0, sizeof(double) * s->nv * L));
+  if (s->d_slopes) H3C_CUDA(s, cudaMemset(s->d_slopes, 0, sizeof(double) * nd * s->nv * L));
   k_init_time<<<blocks(ninst), kBlock, 0, s->stream>>>(s->d_sc, s->desc.time_end, ninst);
   H3C_CUDA(s, cudaGetLastError());
   s->has_grid = true;
@@ -856,33 +888,64 @@ int h3c_apply_bcs(h3c_solver s, int which) {
 }
 
 // Solver::solve (solver.hpp:140-145): apply_bcs(lhs), set_dt, evolve, advance.
-static void enqueue_steps(h3c_solver s, int64_t nsteps) {
-  const bool cns = s->desc.physics == H3C_CNS;
-  const bool fuse = !s->unfused_dt;
-  for (int64_t it = 0; it < nsteps; ++it) {
-    launch_bc(s, 0);
-    if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
-    {
-      Launch L(s, K_SCALAR);
-      k_set_dt<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, 1, s->n_inst);
-    }
-    if (cns) launch_slopes(s, 0);
-    if (s->desc.time_integration == H3C_EULER_FORWARD) {
-      // evolve(euler_forward): solver.hpp:470-479 (rhs = lhs + R; lhs = rhs as a buffer swap)
-      launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
-      std::swap(s->d_q[0], s->d_q[1]);
-    } else {
-      // evolve(runge_kutta_2): solver.hpp:483-494
-      launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
-      launch_bc(s, 1);
-      if (cns) launch_slopes(s, 1);
-      launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
-    }
-    {
-      Launch L(s, K_SCALAR);
-      k_advance<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, s->n_inst);
-    }
+// Per-stage preparation of a stage input q: CNS cell slopes or MUSCL gradients.
+static void prepare_stage(h3c_solver s, const double* q, int which) {
+  if (s->desc.physics == H3C_CNS) launch_slopes(s, which);
+  else if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, q);
+}
+
+// One solver step (solver.hpp:140-145) on the solver's buffers.  keep (may be
+// null) receives copies of the ghost-filled stage inputs in consecutive
+// nv * ld slots; dts (may be null) records the step's dt at index i.
+static void enqueue_step(h3c_solver s, bool fuse, double* keep, double* dts, long long i) {
+  const size_t Qb = sizeof(double) * s->nv * s->ld;
+  const long long Q = s->nv * s->ld;
+  launch_bc(s, 0);
+  if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
+  {
+    Launch L(s, K_SCALAR);
+    k_set_dt<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, 1, s->n_inst);
   }
+  if (dts) {
+    Launch L(s, K_SCALAR);
+    k_record_dt<<<1, 1, 0, s->stream>>>(s->d_sc, dts, i);
+  }
+  if (keep) cudaMemcpyAsync(keep, s->d_q[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
+  prepare_stage(s, s->d_q[0], 0);
+  const int ti = s->desc.time_integration;
+  if (ti == H3C_EULER_FORWARD) {
+    // evolve(euler_forward): solver.hpp:470-479 (rhs = lhs + R; lhs = rhs as a buffer swap)
+    launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
+    std::swap(s->d_q[0], s->d_q[1]);
+  } else if (ti == H3C_RUNGE_KUTTA_2) {
+    // evolve(runge_kutta_2): solver.hpp:483-494
+    launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
+    launch_bc(s, 1);
+    if (keep) cudaMemcpyAsync(keep + Q, s->d_q[1], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    prepare_stage(s, s->d_q[1], 1);
+    launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
+  } else {
+    // EXTENSION: SSP-RK3, conditions before every stage
+    launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
+    launch_bc(s, 1);
+    if (keep) cudaMemcpyAsync(keep + Q, s->d_q[1], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    cudaMemcpyAsync(s->d_q[2], s->d_q[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    prepare_stage(s, s->d_q[1], 1);
+    launch_stage(s, 3, s->d_q[1], s->d_q[2], false);
+    launch_bc(s, 2);
+    if (keep) cudaMemcpyAsync(keep + 2 * Q, s->d_q[2], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    prepare_stage(s, s->d_q[2], 2);
+    launch_stage(s, 4, s->d_q[2], s->d_q[0], fuse);
+  }
+  {
+    Launch L(s, K_SCALAR);
+    k_advance<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, s->n_inst);
+  }
+}
+
+static void enqueue_steps(h3c_solver s, int64_t nsteps) {
+  const bool fuse = !s->unfused_dt;
+  for (int64_t it = 0; it < nsteps; ++it) enqueue_step(s, fuse, nullptr, nullptr, 0);
 }
 
 // Steps per replayed graph: even, so forward Euler's buffer swap returns the
@@ -1202,6 +1265,8 @@ static int adjoint_supported(h3c_solver s, const char* what) {
   const bool ok_phys = (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM) ||
                        s->desc.physics == H3C_HEAT;
   if (!ok_phys) return s->fail(H3C_E_INVALID, "%s: Euler/AUSM and heat only", what);
+  if (s->desc.reconstruction != H3C_RECON_NONE)
+    return s->fail(H3C_E_INVALID, "%s: the adjoint covers the first-order scheme only", what);
   if (s->ghost_unapplied) return s->fail(H3C_E_INVALID, "%s: a ghost cell gets no condition", what);
   for (int k = 0; k < s->n_bcs; ++k) {
     const int kind = s->h_bcs[k].kind;
@@ -1212,22 +1277,38 @@ static int adjoint_supported(h3c_solver s, const char* what) {
   return H3C_OK;
 }
 
-// One step with the given time step on explicit buffers: the stage inputs
-// (ghosts filled) are left in in0 (and in1 for RK2); the new state in out.
-// For forward Euler out may not alias in0; for RK2 out == in0 is allowed.
-static void frozen_step(h3c_solver s, double* in0, double* in1, double* out, const double* d_dts, long long i) {
-  launch_bc_ptr(s, in0, in0);
+// One step with the given time step on explicit buffers.  st[0] is the
+// step's start state; the stage inputs (ghosts filled) are left in st[0..]
+// (RK2: st[1]; SSP-RK3: st[1], st[2]) and the new state in out.  For forward
+// Euler out must not alias st[0]; for the Runge-Kutta schemes out == st[0] is
+// allowed (in-place last stage), otherwise st[0] is copied to out first.
+static void frozen_step(h3c_solver s, double* const* st, double* out, const double* d_dts, long long i) {
+  const size_t Qb = sizeof(double) * s->nv * s->ld;
+  launch_bc_ptr(s, st[0], st[0]);
   {
     Launch L(s, K_SCALAR);
     k_set_dt_from<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
   }
-  if (s->desc.time_integration == H3C_EULER_FORWARD) {
-    launch_stage(s, 0, in0, out, false);
+  const int ti = s->desc.time_integration;
+  if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[0]);
+  if (ti == H3C_EULER_FORWARD) {
+    launch_stage(s, 0, st[0], out, false);
+  } else if (ti == H3C_RUNGE_KUTTA_2) {
+    launch_stage(s, 0, st[0], st[1], false);
+    launch_bc_ptr(s, st[1], st[0]);
+    if (out != st[0]) cudaMemcpyAsync(out, st[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[1]);
+    launch_stage(s, 2, st[1], out, false);
   } else {
-    launch_stage(s, 0, in0, in1, false);
-    launch_bc_ptr(s, in1, in0);
-    if (out != in0) cudaMemcpyAsync(out, in0, sizeof(double) * s->nv * s->ld, cudaMemcpyDeviceToDevice, s->stream);
-    launch_stage(s, 2, in1, out, false);
+    launch_stage(s, 0, st[0], st[1], false);
+    launch_bc_ptr(s, st[1], st[0]);
+    cudaMemcpyAsync(st[2], st[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[1]);
+    launch_stage(s, 3, st[1], st[2], false);
+    launch_bc_ptr(s, st[2], st[0]);
+    if (out != st[0]) cudaMemcpyAsync(out, st[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[2]);
+    launch_stage(s, 4, st[2], out, false);
   }
   {
     Launch L(s, K_SCALAR);
@@ -1245,10 +1326,12 @@ int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts) {
   cudaMemcpyAsync(d_dts, dts, sizeof(double) * nsteps, cudaMemcpyHostToDevice, s->stream);
   for (int64_t i = 0; i < nsteps; ++i) {
     if (s->desc.time_integration == H3C_EULER_FORWARD) {
-      frozen_step(s, s->d_q[0], nullptr, s->d_q[1], d_dts, i);
+      double* st[1] = {s->d_q[0]};
+      frozen_step(s, st, s->d_q[1], d_dts, i);
       std::swap(s->d_q[0], s->d_q[1]);
     } else {
-      frozen_step(s, s->d_q[0], s->d_q[1], s->d_q[0], d_dts, i);
+      double* st[3] = {s->d_q[0], s->d_q[1], s->d_q[2]};
+      frozen_step(s, st, s->d_q[0], d_dts, i);
     }
   }
   launch_cfl(s, &s->d_sc->dtmin_ord);  // the next h3c_solve computes dt from this state
@@ -1265,11 +1348,11 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   if (!s || nsteps < 1 || every < 0 || !dJ_dqN || !dJ_dq0) return H3C_E_INVALID;
   if (int rc = adjoint_supported(s, "h3c_adjoint")) return rc;
   const long long L = s->ld, nv = s->nv, Q = nv * L;
-  const bool rk2 = s->desc.time_integration == H3C_RUNGE_KUTTA_2;
-  const long long per = rk2 ? 2 : 1;
+  const int ti = s->desc.time_integration;
+  const long long per = ti == H3C_EULER_FORWARD ? 1 : ti == H3C_RUNGE_KUTTA_2 ? 2 : 3;  // stages per step
   auto need = [&](long long ev) {
     const long long nck = (nsteps + ev - 1) / ev;
-    return sizeof(double) * ((size_t)Q * (nck + per * ev + 6) + nsteps);
+    return sizeof(double) * ((size_t)Q * (nck + per * ev + 7) + nsteps);
   };
   if (every > nsteps) every = nsteps;
   if (every == 0) {  // no recomputation if that fits in half of the free memory, else ~sqrt(N) segments
@@ -1297,46 +1380,23 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   double* seg = ck + Q * nck;
   double* work = seg + Q * per * every;
   double* lam = work + Q * 3;
-  double* d_dts = lam + Q * 3;
+  double* d_dts = lam + Q * 4;
   const long long last0 = (nck - 1) * every;  // first step of the last segment
   // ---- forward: the solver's own step (CFL dt), checkpoints, dt record ----
   const bool fuse = !s->unfused_dt;
   for (int64_t i = 0; i < nsteps; ++i) {
     if (i % every == 0)
       cudaMemcpyAsync(ck + Q * (i / every), s->d_q[0], sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-    double* s0 = i >= last0 ? seg + Q * per * (i - last0) : nullptr;
-    launch_bc(s, 0);
-    if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
-    {
-      Launch L1(s, K_SCALAR);
-      k_set_dt<<<1, 1, 0, s->stream>>>(s->d_sc, 1, 1);
-    }
-    {
-      Launch L1(s, K_SCALAR);
-      k_record_dt<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
-    }
-    if (s0) cudaMemcpyAsync(s0, s->d_q[0], sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-    if (!rk2) {
-      launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
-      std::swap(s->d_q[0], s->d_q[1]);
-    } else {
-      launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
-      launch_bc(s, 1);
-      if (s0) cudaMemcpyAsync(s0 + Q, s->d_q[1], sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-      launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
-    }
-    {
-      Launch L2(s, K_SCALAR);
-      k_advance<<<1, 1, 0, s->stream>>>(s->d_sc, 1);
-    }
+    enqueue_step(s, fuse, i >= last0 ? seg + Q * per * (i - last0) : nullptr, d_dts, i);
   }
   Scalars saved;
   cudaMemcpyAsync(&saved, s->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream);
   // ---- cotangent of the final state (caller numbering -> internal) ----
   double* lamA = lam;          // lambda^{n+1}
-  double* lamB = lam + Q;      // scratch
-  double* lamC = lam + 2 * Q;  // lambda* (RK2)
-  cudaMemsetAsync(lam, 0, sizeof(double) * Q * 3, s->stream);
+  double* lamB = lam + Q;      // lambda^n
+  double* lamC = lam + 2 * Q;  // last-stage input cotangent (RK2, SSP-RK3)
+  double* lamD = lam + 3 * Q;  // first-stage output cotangent (SSP-RK3)
+  cudaMemsetAsync(lam, 0, sizeof(double) * Q * 4, s->stream);
   if (int rc = ensure_stage(s, s->n_caller)) return rc;
   // host or device arrays (unified addressing)
   for (int v = 0; v < nv; ++v)
@@ -1344,21 +1404,22 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
                     cudaMemcpyDefault, s->stream);
   k_gather<<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_stage, s->n_caller, lamA, L, s->d_dev2caller, s->n_int, (int)nv);
   ++s->launches;
-  auto adj = [&](const double* qin, const double* lamin, double* gout, const double* extra, double alpha, double beta,
-                 double gam) {
+  auto adj = [&](const double* qin, const double* lamin, double* gout, double alpha, double beta,
+                 const double* extra = nullptr, double gam = 0.0, const double* extra2 = nullptr,
+                 double gam2 = 0.0) {
     Launch La(s, K_OTHER);
     const Geometry g = geometry(s);
     const GhostTables gt = ghosts(s);
     if (s->nd == 2) {
       if (s->desc.physics == H3C_HEAT)
-        k_adj_stage<2, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+        k_adj_stage<2, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
       else
-        k_adj_stage<2, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+        k_adj_stage<2, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
     } else {
       if (s->desc.physics == H3C_HEAT)
-        k_adj_stage<3, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+        k_adj_stage<3, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
       else
-        k_adj_stage<3, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, alpha, beta, gam, g, gt, s->pc, s->d_sc);
+        k_adj_stage<3, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
     }
   };
   // ---- backward over segments; all but the last recompute their stage states from the checkpoint ----
@@ -1371,13 +1432,8 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
         double* s0 = seg + Q * per * (i - i0);
         cudaMemcpyAsync(s0, cur, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
         double* nxt = (cur == work) ? work + Q : work;
-        frozen_step(s, s0, rk2 ? s0 + Q : nullptr, rk2 ? s0 : nxt, d_dts, i);
-        if (rk2) {
-          // s0 now holds the new state (in-place second stage); restore the stage input into s0
-          cudaMemcpyAsync(nxt, s0, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-          cudaMemcpyAsync(s0, cur, sizeof(double) * Q, cudaMemcpyDeviceToDevice, s->stream);
-          launch_bc_ptr(s, s0, s0);
-        }
+        double* st[3] = {s0, s0 + Q, s0 + 2 * Q};
+        frozen_step(s, st, nxt, d_dts, i);
         cur = nxt;
       }
     }
@@ -1387,15 +1443,20 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
         Launch L3(s, K_SCALAR);
         k_set_dt_from<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
       }
-      if (!rk2) {
-        adj(s0, lamA, lamB, nullptr, 1.0, 1.0, 0.0);
-        std::swap(lamA, lamB);
-      } else {
+      if (ti == H3C_EULER_FORWARD) {
+        adj(s0, lamA, lamB, 1.0, 1.0);
+      } else if (ti == H3C_RUNGE_KUTTA_2) {
         // lambda* = 0.5 lambda + VJP(q*; 0.5 lambda); lambda^n = 0.5 lambda + lambda* + VJP(q^n; lambda*)
-        adj(s0 + Q, lamA, lamC, nullptr, 0.5, 0.5, 0.0);
-        adj(s0, lamC, lamB, lamA, 1.0, 1.0, 0.5);
-        std::swap(lamA, lamB);
+        adj(s0 + Q, lamA, lamC, 0.5, 0.5);
+        adj(s0, lamC, lamB, 1.0, 1.0, lamA, 0.5);
+      } else {
+        // q' = 1/3 q + 2/3 (q2 + R(q2)), q2 = 3/4 q + 1/4 (q1 + R(q1)), q1 = q + R(q):
+        // l2 = 2/3 (l + VJP(q2; l)), l1 = 1/4 (l2 + VJP(q1; l2)), l^n = l1 + VJP(q; l1) + 1/3 l + 3/4 l2
+        adj(s0 + 2 * Q, lamA, lamC, 2.0 / 3.0, 2.0 / 3.0);
+        adj(s0 + Q, lamC, lamD, 0.25, 0.25);
+        adj(s0, lamD, lamB, 1.0, 1.0, lamA, 1.0 / 3.0, lamC, 0.75);
       }
+      std::swap(lamA, lamB);
     }
   }
   // ---- gradient (internal -> caller numbering), dt sequence ----

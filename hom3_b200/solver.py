@@ -24,7 +24,8 @@ INV64 = np.iinfo(np.int64).max
 INV32 = np.iinfo(np.int32).max
 
 _DEFAULTS = dict(time_end=1.0, cfl=0.2, cfl_viscous=0.4, gamma=1.4, Rspecific=287.058, T0=273.15, rho0=1.225,
-                 Minfty=0.1, ReInfty=100.0, Pr0=0.72, Sutherland0=110.4, diffusivity=1.0, T_ref=273.15)
+                 Minfty=0.1, ReInfty=100.0, Pr0=0.72, Sutherland0=110.4, diffusivity=1.0, T_ref=273.15,
+                 limiter_k=1.0)
 # hom3 property names -> desc fields
 _PROP_KEYS = {"timeEnd": "time_end", "CFL": "cfl", "CFL_viscous": "cfl_viscous", "gamma": "gamma",
               "Rspecific": "Rspecific", "T0": "T0", "rho0": "rho0", "Minfty": "Minfty", "ReInfty": "ReInfty",
@@ -134,9 +135,10 @@ class Solver:
     """One h3c solver: tables in the caller's numbering, state columns [nv, n_cells]."""
 
     def __init__(self, nd=2, physics=F.EULER, flux=F.FLUX_AUSM, time_integration=F.EULER_FORWARD,
-                 precision=F.FP64, **props):
+                 precision=F.FP64, reconstruction=F.RECON_NONE, **props):
         d = F.Desc()
         d.nd, d.physics, d.flux, d.time_integration, d.precision = nd, physics, flux, time_integration, precision
+        d.reconstruction = reconstruction
         vals = dict(_DEFAULTS)
         for k, v in props.items():
             vals[_PROP_KEYS.get(k, k)] = v

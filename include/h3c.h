@@ -54,6 +54,17 @@ extern "C" {
 /* time integration tags: solver/fv/tags.hpp:24-25 */
 #define H3C_EULER_FORWARD 0
 #define H3C_RUNGE_KUTTA_2 1
+/* EXTENSION (not in hom3): three-stage strong-stability-preserving
+ * Runge-Kutta in Shu-Osher form, q1 = q + dt R(q),
+ * q2 = 3/4 q + 1/4 (q1 + dt R(q1)), q' = 1/3 q + 2/3 (q2 + dt R(q2)),
+ * conditions applied before every stage. */
+#define H3C_SSPRK3 2
+/* reconstruction of the face states.  EXTENSION (not in hom3, which is
+ * first order, solver.hpp:45-49): MUSCL on the primitive variables
+ * (u, rho, p) with least-squares gradients over the face neighbours and
+ * Venkatakrishnan's limiter, eps^2 = (limiter_k h)^3.  Euler with AUSM. */
+#define H3C_RECON_NONE 0
+#define H3C_RECON_MUSCL 1
 /* arithmetic of the face fluxes (the state, residual and dt stay FP64) */
 #define H3C_FP64 0
 #define H3C_MIXED 1 /* FP32 reconstruction + face flux, FP64 update */
@@ -100,7 +111,7 @@ typedef struct {
   int nd;               /* 2 or 3 */
   int physics;          /* H3C_EULER / H3C_CNS / H3C_HEAT */
   int flux;             /* H3C_FLUX_* */
-  int time_integration; /* H3C_EULER_FORWARD / H3C_RUNGE_KUTTA_2 */
+  int time_integration; /* H3C_EULER_FORWARD / H3C_RUNGE_KUTTA_2 / H3C_SSPRK3 */
   int precision;        /* H3C_FP64 / H3C_MIXED */
   double time_end;      /* "timeEnd" */
   double cfl;           /* "CFL" */
@@ -115,6 +126,8 @@ typedef struct {
   double Sutherland0;   /* "Sutherland0" [K] */
   double diffusivity;   /* "diffusivity" [m^2/s] (heat; does not enter the step) */
   double T_ref;         /* "T_ref" [K] (heat; does not enter the step) */
+  int reconstruction;   /* H3C_RECON_NONE (hom3) / H3C_RECON_MUSCL (EXTENSION) */
+  double limiter_k;     /* Venkatakrishnan constant K of H3C_RECON_MUSCL */
 } h3c_desc;
 
 typedef struct {

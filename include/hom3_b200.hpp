@@ -44,6 +44,8 @@ struct Properties {
          T_ref = 273.15;
   int domain_kind = 0;  // "initialDomain": 0 all, 1 sdf > 0, 2 sdf < 0
   h3c_sdf domain{};
+  int reconstruction = H3C_RECON_NONE;  // EXTENSION: H3C_RECON_MUSCL
+  double limiter_k = 1.0;               // Venkatakrishnan K
 };
 
 // Root cell + MinLevel generator (grid/helpers.hpp:163-179); refine: EXTENSION.
@@ -114,6 +116,8 @@ class Solver {
     d.gamma = p.gamma; d.Rspecific = p.Rspecific; d.T0 = p.T0; d.rho0 = p.rho0; d.Minfty = p.Minfty;
     d.ReInfty = p.ReInfty; d.Pr0 = p.Pr0; d.Sutherland0 = p.Sutherland0; d.diffusivity = p.diffusivity;
     d.T_ref = p.T_ref;
+    d.reconstruction = p.reconstruction;
+    d.limiter_k = p.limiter_k;
     nv_ = p.physics == H3C_HEAT ? 1 : grid.nd + 2;
     check(h3c_create(&d, &s_));
   }

@@ -300,10 +300,13 @@ inline std::vector<Sdf> cube_boundaries(int nd, const Tree& t) {
 // ---------------------------------------------------------------------------
 enum PhysicsKind { PHYS_EULER = 0, PHYS_CNS = 1, PHYS_HEAT = 2 };
 enum FluxKind { FLUX_AUSM = 0, FLUX_LLF = 1 };
-enum TimeKind { TI_EULER_FORWARD = 0, TI_RK2 = 1 };
+enum TimeKind { TI_EULER_FORWARD = 0, TI_RK2 = 1, TI_SSPRK3 = 2 /* EXTENSION: Shu-Osher SSP-RK3 */ };
+enum ReconKind { RECON_NONE = 0, RECON_MUSCL = 1 /* EXTENSION: LSQ + MUSCL + Venkatakrishnan */ };
 
 struct Params {
   int physics = PHYS_EULER, flux = FLUX_AUSM, ti = TI_EULER_FORWARD;
+  int recon = RECON_NONE;
+  double limiter_k = 1.0;  // Venkatakrishnan: eps^2 = (limiter_k h)^3
   double cfl = 0.2, cfl_viscous = 0.4;
   double gamma = 1.4, Rspecific = 287.058, T0 = 273.15, rho0 = 1.225, Minfty = 0.1;
   double ReInfty = 100, Pr0 = 0.72, Sutherland0 = 110.4;
@@ -386,7 +389,7 @@ template <class T> struct Solver {
   int ic_kind = IC_CONSTANT_PV;
   double ic[80] = {0};
   // Container columns: container.hpp:58-66
-  std::vector<T> Q[2][5];
+  std::vector<T> Q[3][5];  // lhs, rhs, and the second SSP-RK3 stage
   std::vector<Ind> nbr[6];
   std::vector<double> xc[3];
   std::vector<double> len;
@@ -415,7 +418,7 @@ template <class T> struct Solver {
   bool is_ghost(Ind c) const { return node[c] == INV; }
 
   Ind push_cell() {
-    for (int t = 0; t < 2; ++t)
+    for (int t = 0; t < 3; ++t)
       for (int v = 0; v < nv; ++v) Q[t][v].push_back(T(std::numeric_limits<double>::quiet_NaN()));
     for (int p = 0; p < 2 * nd; ++p) nbr[p].push_back(INV);
     for (int d = 0; d < nd; ++d) xc[d].push_back(std::numeric_limits<double>::quiet_NaN());
@@ -603,6 +606,176 @@ template <class T> struct Solver {
   }
   T sutherland(T Tt) const { using std::pow; return pow(Tt, 1.5) * P.sOverTrefP1 / (Tt + P.sOverTref); }
 
+  // ---- EXTENSION (not in hom3): second-order MUSCL reconstruction ----
+  // Primitive variables w = (u_0..u_{nd-1}, rho, p) (velocity in the momentum
+  // slots).  Per interior cell: least-squares gradient over the face
+  // neighbours (same-level, coarser, the finer cells of a sub-face group and
+  // ghosts at their mirrored centres), weights 1/|dx|^2, normal equations
+  // solved by the adjugate; then Venkatakrishnan's limiter per variable,
+  // psi = min(1, min over faces phi), eps^2 = (K h)^3.  Ghost cells carry no
+  // gradient (first order on the ghost side) except periodic ghosts, which
+  // take their paired cell's.  A face uses one point for both sides: on the
+  // face plane (from the minus-side cell), transverse coordinates of the
+  // smaller cell.  A face whose reconstructed density or pressure is not
+  // positive on either side falls back to the cell values.
+  std::vector<T> Wg[5][3];  // limited gradients [v][d] per cell
+  using WState = std::array<T, 5>;
+  WState prim_w(int t, Ind c) const {
+    WState w{};
+    for (int d = 0; d < nd; ++d) w[d] = u(t, c, d);
+    w[nd] = rho(t, c);
+    w[nd + 1] = p(t, c);
+    return w;
+  }
+  // the face neighbours of interior cell c: f(n, d, side), side -1 / +1
+  template <class F> void for_each_face(Ind c, F f) const {
+    const int ns = 1 << (nd - 1);
+    for (int d = 0; d < nd; ++d)
+      for (int sd = 0; sd < 2; ++sd) {
+        const Ind n = nbr[2 * d + sd][c];
+        const int side = sd == 0 ? -1 : 1;
+        if (n >= 0) f(n, d, side);
+        else
+          for (int j = 0; j < ns; ++j) f(subs[(-n - 2) * ns + j], d, side);
+      }
+  }
+  // the face point of the face between L (minus side) and R along d
+  void face_point(Ind L, Ind R, int d, double* xf) const {
+    const Ind sm = len[R] < len[L] ? R : L;
+    for (int k = 0; k < nd; ++k) xf[k] = xc[k][sm];
+    xf[d] = xc[d][L] + 0.5 * len[L];
+  }
+  static T vk_phi(T a, T b, T e2) {
+    return ((a * a + e2) * b + 2. * b * b * a) / (b * (a * a + 2. * b * b + a * b + e2));
+  }
+  void compute_gradients(int t) {
+    const Ind n = n_internal();
+    for (int v = 0; v < 5; ++v)
+      for (int d = 0; d < 3; ++d) Wg[v][d].assign(size(), T(0));
+#pragma omp parallel for schedule(static)
+    for (Ind c = 0; c < n; ++c) {
+      const WState wc = prim_w(t, c);
+      T M[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      T b[5][3] = {};
+      WState wmax = wc, wmin = wc;
+      for_each_face(c, [&](Ind nb, int, int) {
+        const WState wn = prim_w(t, nb);
+        double dx[3];
+        double r2 = 0;
+        for (int k = 0; k < nd; ++k) {
+          dx[k] = xc[k][nb] - xc[k][c];
+          r2 = k == 0 ? dx[k] * dx[k] : r2 + dx[k] * dx[k];
+        }
+        const double wgt = 1.0 / r2;
+        for (int i = 0; i < nd; ++i)
+          for (int j = 0; j < nd; ++j) M[i][j] = M[i][j] + (wgt * dx[i]) * dx[j];
+        for (int v = 0; v < nv; ++v) {
+          const T dw = wn[v] - wc[v];
+          for (int i = 0; i < nd; ++i) b[v][i] = b[v][i] + (wgt * dx[i]) * dw;
+          wmax[v] = wn[v] > wmax[v] ? wn[v] : wmax[v];
+          wmin[v] = wn[v] < wmin[v] ? wn[v] : wmin[v];
+        }
+      });
+      // adjugate inverse of the symmetric normal matrix
+      T inv[3][3];
+      if (nd == 2) {
+        const T id = 1.0 / (M[0][0] * M[1][1] - M[0][1] * M[1][0]);
+        inv[0][0] = M[1][1] * id;
+        inv[1][1] = M[0][0] * id;
+        inv[0][1] = -M[0][1] * id;
+        inv[1][0] = -M[1][0] * id;
+      } else {
+        const T c00 = M[1][1] * M[2][2] - M[1][2] * M[2][1];
+        const T c01 = M[1][2] * M[2][0] - M[1][0] * M[2][2];
+        const T c02 = M[1][0] * M[2][1] - M[1][1] * M[2][0];
+        const T id = 1.0 / (M[0][0] * c00 + M[0][1] * c01 + M[0][2] * c02);
+        inv[0][0] = c00 * id;
+        inv[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * id;
+        inv[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * id;
+        inv[1][0] = c01 * id;
+        inv[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * id;
+        inv[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * id;
+        inv[2][0] = c02 * id;
+        inv[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * id;
+        inv[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * id;
+      }
+      const double kh = P.limiter_k * len[c];
+      const T e2 = kh * kh * kh;
+      for (int v = 0; v < nv; ++v) {
+        T G[3];
+        for (int i = 0; i < nd; ++i) {
+          T s = inv[i][0] * b[v][0];
+          for (int j = 1; j < nd; ++j) s = s + inv[i][j] * b[v][j];
+          G[i] = s;
+        }
+        const T dmax = wmax[v] - wc[v], dmin = wmin[v] - wc[v];
+        T psi = 1.0;
+        for_each_face(c, [&](Ind nb, int d, int side) {
+          double xf[3];
+          if (side < 0) face_point(nb, c, d, xf);
+          else face_point(c, nb, d, xf);
+          T d2 = G[0] * (xf[0] - xc[0][c]);
+          for (int k = 1; k < nd; ++k) d2 = d2 + G[k] * (xf[k] - xc[k][c]);
+          T phi = 1.0;
+          if (d2 > 0) phi = vk_phi(dmax, d2, e2);
+          else if (d2 < 0) phi = vk_phi(dmin, d2, e2);
+          psi = phi < psi ? phi : psi;
+        });
+        for (int i = 0; i < nd; ++i) Wg[v][i][c] = psi * G[i];
+      }
+    }
+    // periodic ghosts take their paired cell's gradient
+    for (Ind g = firstGC; g < size(); ++g)
+      if (bcs[bc_idx[g]].kind == BC_PERIODIC)
+        for (int v = 0; v < nv; ++v)
+          for (int d = 0; d < nd; ++d) Wg[v][d][g] = Wg[v][d][periodic_partner[g - firstGC]];
+  }
+  // reconstructed primitive state of cell X at the face point xf
+  WState recon_w(int t, Ind X, const double* xf) const {
+    WState w = prim_w(t, X);
+    for (int v = 0; v < nv; ++v) {
+      T s = w[v];
+      for (int k = 0; k < nd; ++k) s = s + Wg[v][k][X] * (xf[k] - xc[k][X]);
+      w[v] = s;
+    }
+    return w;
+  }
+  // AUSM (euler/physics.hpp:276-325) of two primitive states
+  State ausm_w(const WState& wl, const WState& wr, int d) const {
+    auto side = [&](const WState& w, State& th, T& pp, T& M) {
+      using std::sqrt;
+      const T rh = w[nd];
+      pp = w[nd + 1];
+      const T a_ = sqrt(P.gamma * pp / rh);
+      M = w[d] / a_;
+      T um2 = w[0] * w[0];
+      for (int k = 1; k < nd; ++k) um2 = um2 + w[k] * w[k];
+      for (int k = 0; k < nd; ++k) th[k] = (rh * w[k]) * a_;
+      th[nd] = rh * a_;
+      th[nd + 1] = ((pp / P.gm1 + 0.5 * rh * um2) + pp) * a_;
+    };
+    State tl{}, tr{};
+    T pl, pr, ML, MR;
+    side(wl, tl, pl, ML);
+    side(wr, tr, pr, MR);
+    const T m_i = m_int(+1, ML) + m_int(-1, MR);
+    const T p_i = p_int(+1, ML) * pl + p_int(-1, MR) * pr;
+    State f = m_i >= 0 ? tl : tr;
+    for (int v = 0; v < nv; ++v) f[v] = f[v] * m_i;
+    f[d] = f[d] + p_i;
+    return f;
+  }
+  State muscl_flux(int t, Ind l, Ind r, int d) const {
+    double xf[3];
+    face_point(l, r, d, xf);
+    WState wl = recon_w(t, l, xf), wr = recon_w(t, r, xf);
+    if (!(wl[nd] > 0) || !(wl[nd + 1] > 0) || !(wr[nd] > 0) || !(wr[nd + 1] > 0)) {
+      wl = prim_w(t, l);
+      wr = prim_w(t, r);
+    }
+    return ausm_w(wl, wr, d);
+  }
+
   // compute_num_flux dispatch (physics.hpp:175-178, cns 155-161, heat 113-119)
   State face_flux(int t, Ind l, Ind r, int d, double dx, T dt) const {
     if (P.physics == PHYS_HEAT) {
@@ -610,6 +783,7 @@ template <class T> struct Solver {
       f[0] = 1 / dx * (q(t, l, 0) - q(t, r, 0));
       return f;
     }
+    if (P.recon == RECON_MUSCL) return muscl_flux(t, l, r, d);
     State f = P.flux == FLUX_LLF ? llf(t, l, r, d, dx, dt) : ausm(t, l, r, d);
     if (P.physics == PHYS_CNS) {
       const State fv = viscous(t, l, r, d);
@@ -722,6 +896,7 @@ template <class T> struct Solver {
   void evolve() {
     const Ind n = n_internal();
     if (P.ti == TI_EULER_FORWARD) {
+      if (P.recon == RECON_MUSCL) compute_gradients(0);
 #pragma omp parallel for schedule(static)
       for (Ind c = 0; c < n; ++c) {
         const State nf = num_flux(0, c);
@@ -730,17 +905,40 @@ template <class T> struct Solver {
 #pragma omp parallel for schedule(static)
       for (Ind c = 0; c < n; ++c)
         for (int v = 0; v < nv; ++v) q(0, c, v) = q(1, c, v);
-    } else {
+    } else if (P.ti == TI_RK2) {
+      if (P.recon == RECON_MUSCL) compute_gradients(0);
 #pragma omp parallel for schedule(static)
       for (Ind c = 0; c < n; ++c) {
         const State nf = num_flux(0, c);
         for (int v = 0; v < nv; ++v) q(1, c, v) = q(0, c, v) + nf[v];
       }
       apply_bcs(1);
+      if (P.recon == RECON_MUSCL) compute_gradients(1);
 #pragma omp parallel for schedule(static)
       for (Ind c = 0; c < n; ++c) {
         const State nf = num_flux(1, c);
         for (int v = 0; v < nv; ++v) q(0, c, v) = 0.5 * ((q(0, c, v) + q(1, c, v)) + nf[v]);
+      }
+    } else {  // EXTENSION (not in hom3): SSP-RK3 in Shu-Osher form
+      if (P.recon == RECON_MUSCL) compute_gradients(0);
+#pragma omp parallel for schedule(static)
+      for (Ind c = 0; c < n; ++c) {
+        const State nf = num_flux(0, c);
+        for (int v = 0; v < nv; ++v) q(1, c, v) = q(0, c, v) + nf[v];
+      }
+      apply_bcs(1);
+      if (P.recon == RECON_MUSCL) compute_gradients(1);
+#pragma omp parallel for schedule(static)
+      for (Ind c = 0; c < n; ++c) {
+        const State nf = num_flux(1, c);
+        for (int v = 0; v < nv; ++v) q(2, c, v) = 0.75 * q(0, c, v) + 0.25 * (q(1, c, v) + nf[v]);
+      }
+      apply_bcs(2);
+      if (P.recon == RECON_MUSCL) compute_gradients(2);
+#pragma omp parallel for schedule(static)
+      for (Ind c = 0; c < n; ++c) {
+        const State nf = num_flux(2, c);
+        for (int v = 0; v < nv; ++v) q(0, c, v) = (1.0 / 3.0) * q(0, c, v) + (2.0 / 3.0) * (q(2, c, v) + nf[v]);
       }
     }
   }

@@ -25,7 +25,8 @@ SINV = np.iinfo(np.int32).max
 # physics / flux / time integration / bc / ic kinds (oracle/h3o.hpp)
 EULER, CNS, HEAT = 0, 1, 2
 AUSM, LLF = 0, 1
-EULER_FORWARD, RK2 = 0, 1
+EULER_FORWARD, RK2, SSPRK3 = 0, 1, 2  # SSPRK3: EXTENSION (not in hom3)
+RECON_NONE, RECON_MUSCL = 0, 1  # MUSCL: EXTENSION (not in hom3)
 (BC_EULER_NEUMANN, BC_EULER_DIRICHLET, BC_EULER_VORTEX, BC_CNS_INFLOW, BC_CNS_OUTFLOW,
  BC_CNS_ADIABATIC_NOSLIP, BC_CNS_ADIABATIC_SLIP, BC_CNS_ISOTHERMAL_NOSLIP, BC_HEAT_DIRICHLET,
  BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT,
@@ -48,14 +49,14 @@ class SolverDesc(C.Structure):
         (n, C.c_double) for n in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty",
                                   "ReInfty", "Pr0", "Sutherland0", "diffusivity", "T_ref", "time_end")
     ] + [("domain_kind", C.c_int), ("domain", Sdf), ("ic_kind", C.c_int), ("ic", C.c_double * 80),
-         ("n_bcs", C.c_int), ("bcs", C.POINTER(BcDesc))]
+         ("n_bcs", C.c_int), ("bcs", C.POINTER(BcDesc)), ("recon", C.c_int), ("limiter_k", C.c_double)]
 
 
 class Info(C.Structure):
     _fields_ = [("physics", C.c_int), ("flux", C.c_int), ("ti", C.c_int), ("nd", C.c_int), ("n_bcs", C.c_int)] + [
         (n, C.c_double) for n in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty", "ReInfty",
                                   "Pr0", "Sutherland0", "time_end")
-    ] + [("bc_kind", C.c_int * 16), ("bc_v", (C.c_double * 8) * 16)]
+    ] + [("bc_kind", C.c_int * 16), ("bc_v", (C.c_double * 8) * 16), ("recon", C.c_int), ("limiter_k", C.c_double)]
 
 
 def build() -> str:
@@ -251,6 +252,7 @@ class Solver:
         lib().h3o_solver_info(self._h, self.idx, C.byref(i))
         d = {f: getattr(i, f) for f, _ in Info._fields_[:16]}
         d["bcs"] = [(i.bc_kind[k], list(i.bc_v[k])) for k in range(i.n_bcs)]
+        d["recon"], d["limiter_k"] = i.recon, i.limiter_k
         return d
 
     def quantities(self):
@@ -394,8 +396,9 @@ class DualSolver:
 
 
 def _pack_desc(physics=EULER, flux=AUSM, time_integration=EULER_FORWARD, *, bcs=(), domain=None, domain_kind=0,
-               ic_kind=IC_CONSTANT_PV, ic=(), **props):
+               ic_kind=IC_CONSTANT_PV, ic=(), recon=RECON_NONE, limiter_k=1.0, **props):
     d = SolverDesc()
+    d.recon, d.limiter_k = recon, float(limiter_k)
     defaults = dict(cfl=0.2, cfl_viscous=0.4, gamma=1.4, Rspecific=287.058, T0=273.15, rho0=1.225, Minfty=0.1,
                     ReInfty=100.0, Pr0=0.72, Sutherland0=110.4, diffusivity=1.0, T_ref=273.15, time_end=1.0)
     defaults.update(props)

@@ -37,6 +37,8 @@ typedef struct {
   double ic[80];
   int n_bcs;
   const h3o_bc* bcs;
+  int recon;         // EXTENSION: 0 none (hom3), 1 MUSCL (LSQ gradients, Venkatakrishnan limiter)
+  double limiter_k;  // Venkatakrishnan constant K
 } h3o_solver_desc;
 
 static Sdf to_sdf(const h3o_sdf& s) {
@@ -99,6 +101,8 @@ int h3o_add_solver(void* w, const h3o_solver_desc* d) {
   P.T0 = d->T0; P.rho0 = d->rho0; P.Minfty = d->Minfty; P.ReInfty = d->ReInfty; P.Pr0 = d->Pr0;
   P.Sutherland0 = d->Sutherland0; P.diffusivity = d->diffusivity; P.T_ref = d->T_ref;
   P.time_end = d->time_end;
+  P.recon = d->recon;
+  P.limiter_k = d->limiter_k;
   P.derive();
   s->nv = P.physics == PHYS_HEAT ? 1 : ww->nd + 2;
   s->domain_kind = d->domain_kind;
@@ -207,6 +211,8 @@ typedef struct {
   double cfl, cfl_viscous, gamma, Rspecific, T0, rho0, Minfty, ReInfty, Pr0, Sutherland0, time_end;
   int bc_kind[16];
   double bc_v[16][8];
+  int recon;
+  double limiter_k;
 } h3o_info;
 
 void h3o_solver_info(void* w, int s, h3o_info* o) {
@@ -217,6 +223,8 @@ void h3o_solver_info(void* w, int s, h3o_info* o) {
   o->cfl = P.cfl; o->cfl_viscous = P.cfl_viscous; o->gamma = P.gamma; o->Rspecific = P.Rspecific;
   o->T0 = P.T0; o->rho0 = P.rho0; o->Minfty = P.Minfty; o->ReInfty = P.ReInfty; o->Pr0 = P.Pr0;
   o->Sutherland0 = P.Sutherland0; o->time_end = P.time_end;
+  o->recon = P.recon;
+  o->limiter_k = P.limiter_k;
   for (int k = 0; k < (int)so.bcs.size() && k < 16; ++k) {
     o->bc_kind[k] = so.bcs[k].kind;
     for (int j = 0; j < 8; ++j) o->bc_v[k][j] = so.bcs[k].v[j];

@@ -28,12 +28,13 @@ def neumann_cube(w):
     return [h3o.bc(h3o.BC_EULER_NEUMANN, g) for g in w.cube_boundaries()]
 
 
-def euler_case(name, nd=3, level=4, ti=h3o.EULER_FORWARD, flux=h3o.AUSM):
-    """euler_fv_solver_test.cpp:85-286 (3D cases at level 4 instead of 5)."""
+def euler_case(name, nd=3, level=4, ti=h3o.EULER_FORWARD, flux=h3o.AUSM, **extra):
+    """euler_fv_solver_test.cpp:85-286 (3D cases at level 4 instead of 5).
+    extra: EXTENSION keywords (recon, limiter_k)."""
     if name == "vortex":
         w = h3o.World(2, [-8, -8], [8, 8], level=level)
         bcs = [h3o.bc(h3o.BC_EULER_VORTEX, g) for g in w.cube_boundaries()]
-        s = w.add_solver(h3o.EULER, flux, ti, bcs=bcs, ic_kind=h3o.IC_VORTEX, time_end=2.0, **EULER_PROPS)
+        s = w.add_solver(h3o.EULER, flux, ti, bcs=bcs, ic_kind=h3o.IC_VORTEX, time_end=2.0, **EULER_PROPS, **extra)
     else:
         lo, hi = [0.0] * nd, [1.0] * nd
         w = h3o.World(nd, lo, hi, level=level)
@@ -48,12 +49,12 @@ def euler_case(name, nd=3, level=4, ti=h3o.EULER_FORWARD, flux=h3o.AUSM):
         else:
             raise KeyError(name)
         s = w.add_solver(h3o.EULER, flux, ti, bcs=neumann_cube(w), ic_kind=ic_kind, ic=ic, time_end=tend,
-                         **EULER_PROPS)
+                         **EULER_PROPS, **extra)
     s.initialize()
     return w, [s]
 
 
-def euler_dirichlet_case(nd=2, level=5, ti=h3o.EULER_FORWARD):
+def euler_dirichlet_case(nd=2, level=5, ti=h3o.EULER_FORWARD, **extra):
     """Dirichlet / non-zero Neumann conditions (euler/boundary_conditions.hpp:17-67)."""
     w = h3o.World(nd, [0.0] * nd, [1.0] * nd, level=level)
     g = w.cube_boundaries()
@@ -62,7 +63,7 @@ def euler_dirichlet_case(nd=2, level=5, ti=h3o.EULER_FORWARD):
     bcs = [h3o.bc(h3o.BC_EULER_DIRICHLET, g[0], state), h3o.bc(h3o.BC_EULER_NEUMANN, g[1], flux)]
     bcs += [h3o.bc(h3o.BC_EULER_NEUMANN, x) for x in g[2:]]
     s = w.add_solver(h3o.EULER, h3o.AUSM, ti, bcs=bcs, ic_kind=h3o.IC_SHOCK_TUBE, ic=SOD, time_end=0.2,
-                     **EULER_PROPS)
+                     **EULER_PROPS, **extra)
     s.initialize()
     return w, [s]
 
@@ -176,7 +177,8 @@ def gpu_solver_from_oracle(o: "h3o.Solver", precision=0):
     info = o.info()
     props = {k: info[k] for k in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty", "ReInfty",
                                   "Pr0", "Sutherland0", "time_end")}
-    s = hb.Solver(info["nd"], info["physics"], info["flux"], info["ti"], precision, **props)
+    s = hb.Solver(info["nd"], info["physics"], info["flux"], info["ti"], precision, reconstruction=info["recon"],
+                  limiter_k=info["limiter_k"], **props)
     t = o.tables()
     s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
                [Condition(k, v) for k, v in info["bcs"]], t["subface_cells"])
@@ -200,23 +202,23 @@ def tgv_case(level=4, ti=h3o.RK2):
     return w, [s]
 
 
-def periodic_vortex_case(level=6, ti=h3o.RK2, flux=h3o.AUSM):
+def periodic_vortex_case(level=6, ti=h3o.RK2, flux=h3o.AUSM, **extra):
     """EXTENSION (not in hom3): the 2D isentropic vortex of the first benchmark
     configuration -- [0, 10]^2, centre (5, 5), beta 5, periodic."""
     w = h3o.World(2, [0, 0], [10, 10], level=level)
     bcs = [h3o.bc(h3o.BC_PERIODIC, g) for g in w.cube_boundaries()]
     s = w.add_solver(h3o.EULER, flux, ti, bcs=bcs, ic_kind=h3o.IC_VORTEX_PARAM, ic=[5.0, 5.0, 5.0, 1.0, 1.0],
-                     time_end=10.0, **dict(EULER_PROPS, cfl=0.5))
+                     time_end=10.0, **dict(EULER_PROPS, cfl=0.5), **extra)
     s.initialize()
     return w, [s]
 
 
-def refined_case(ti=h3o.RK2, level=2, fine=4):
+def refined_case(ti=h3o.RK2, level=2, fine=4, **extra):
     """EXTENSION (not in hom3): 3D Sod tube on a tree refined +2 levels in a sphere."""
     w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=level)
     w.refine_sphere([0.5, 0.5, 0.5], 0.3, fine)
     s = w.add_solver(h3o.EULER, h3o.AUSM, ti, bcs=neumann_cube(w), ic_kind=h3o.IC_SHOCK_TUBE,
-                     ic=[0, 0, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1], time_end=1.0, cfl=0.4)
+                     ic=[0, 0, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1], time_end=1.0, cfl=0.4, **extra)
     s.initialize()
     return w, [s]
 

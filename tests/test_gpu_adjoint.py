@@ -176,3 +176,22 @@ def test_unsupported_configurations_are_rejected():
     g = cases.gpu_solver_from_oracle(o)
     with pytest.raises(hb.H3cError):
         g.adjoint(2, np.zeros((o.nv, o.ncells)))
+
+
+@pytest.mark.parametrize("name", ["euler2d_rk3", "heat3d_rk3", "periodic_vortex_rk3"])
+def test_ssprk3_adjoint_matches_dual_oracle(name):
+    """EXTENSION: the adjoint of the three SSP-RK3 stages."""
+    BUILDERS.update({
+        "euler2d_rk3": lambda: cases.euler_case("sod", nd=2, level=5, ti=h3o.SSPRK3),
+        "heat3d_rk3": lambda: cases.heat_case(level=3, ti=h3o.SSPRK3),
+        "periodic_vortex_rk3": lambda: cases.periodic_vortex_case(level=5, ti=h3o.SSPRK3),
+    })
+    test_adjoint_matches_dual_oracle(name)
+
+
+def test_muscl_adjoint_is_rejected():
+    import hom3_b200 as hb
+    _, (o,) = cases.periodic_vortex_case(level=4, recon=h3o.RECON_MUSCL)
+    g = cases.gpu_solver_from_oracle(o)
+    with pytest.raises(hb.H3cError):
+        g.adjoint(2, np.zeros((o.nv, o.ncells)))

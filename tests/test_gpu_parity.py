@@ -260,3 +260,63 @@ def test_periodic_vortex_euler(flux):
     """EXTENSION: periodic 2D isentropic vortex (first benchmark configuration's setup)."""
     _, (o,) = cases.periodic_vortex_case(level=6, flux=flux)
     run_single(o)
+
+
+# ---- EXTENSION (not in hom3): SSP-RK3 and MUSCL reconstruction ----
+MUSCL = dict(recon=h3o.RECON_MUSCL, limiter_k=1.0)
+
+
+@pytest.mark.parametrize("name", ["sod", "explosion"])
+def test_ssprk3_euler_3d(name):
+    _, (o,) = cases.euler_case(name, nd=3, level=4, ti=h3o.SSPRK3)
+    run_single(o)
+
+
+def test_ssprk3_heat_and_cns():
+    _, (o,) = cases.heat_case(level=3, ti=h3o.SSPRK3)
+    run_single(o, nsteps=(1, 6))
+    _, (o,) = cases.cns_case("sod", level=5, ti=h3o.SSPRK3)
+    run_single(o, nsteps=(1, 3))
+
+
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2, h3o.SSPRK3])
+def test_muscl_periodic_vortex(ti):
+    _, (o,) = cases.periodic_vortex_case(level=6, ti=ti, **MUSCL)
+    run_single(o, nsteps=(1, 6))
+
+
+@pytest.mark.parametrize("name", ["sod", "explosion"])
+def test_muscl_euler_3d(name):
+    _, (o,) = cases.euler_case(name, nd=3, level=4, ti=h3o.SSPRK3, **MUSCL)
+    run_single(o)
+
+
+def test_muscl_dirichlet_neumann():
+    _, (o,) = cases.euler_dirichlet_case(nd=2, level=5, ti=h3o.RK2, **MUSCL)
+    run_single(o)
+
+
+@pytest.mark.parametrize("ti", [h3o.RK2, h3o.SSPRK3])
+def test_muscl_refined_tree(ti):
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=3)
+    w.refine_sphere([0.5, 0.5, 0.5], 0.25, 5)
+    o = w.add_solver(h3o.EULER, h3o.AUSM, ti, bcs=cases.neumann_cube(w), ic_kind=h3o.IC_EXPLOSION,
+                     ic=[0.5, 0.5, 0.5, 0.2, 1.0, 1.0, 0.125, 0.1], time_end=1.0, cfl=0.4, **MUSCL)
+    o.initialize()
+    run_single(o)
+
+
+def test_muscl_mixed_precision():
+    _, (o,) = cases.periodic_vortex_case(level=6, ti=h3o.SSPRK3, **MUSCL)
+    run_single(o, precision=1, tol_step=1e-5, tol_multi=1e-4)
+
+
+def test_muscl_graph_replay_matches_single_steps():
+    _, (o,) = cases.periodic_vortex_case(level=5, ti=h3o.SSPRK3, **MUSCL)
+    a = cases.gpu_solver_from_oracle(o)
+    b = cases.gpu_solver_from_oracle(o)
+    a.solve(19)
+    for _ in range(19):
+        b.solve(1)
+    fg = o.first_ghost
+    assert np.array_equal(a.state(0)[:, :fg], b.state(0)[:, :fg])
