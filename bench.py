@@ -381,6 +381,89 @@ def run_tgv(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_vortex(args, ws, rank, local):
+    """2D Euler isentropic vortex on a uniform 256^2 grid over [0, 10]^2,
+    periodic, beta 5, centre (5, 5), free stream rho = u = v = p = 1, CFL 0.5:
+    the second-order scheme (LSQ gradients + MUSCL + Venkatakrishnan limiter,
+    SSP-RK3) in FP64 and mixed precision, and hom3's first-order AUSM/RK2 for
+    comparison.  Each result's density L2 error against the exact solution
+    (the initial vortex advected by (t, t)) is reported beside its speed."""
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200 import workloads as W
+    from hom3_b200.solver import Condition
+
+    torch.cuda.set_device(local)
+    level = args.vortex_level
+    spec = hb.GridSpec(2, [0.0, 0.0], [10.0, 10.0], level)
+    t = hb.build_tables(spec, spec.cube_boundaries())
+    partners = hb.periodic_partners(t, spec)
+    fg = t["first_ghost"]
+    f0 = W.vortex_ic(5.0, 5.0, 5.0)
+    q0 = np.zeros((4, t["ncells"]))
+    q0[:, :fg] = hb.cell_average(f0, t["x_center"][:, :fg], t["length"][:fg], 2)
+
+    def exact(time_):
+        def f(x):
+            return f0(np.mod(x - time_, 10.0))
+        return hb.cell_average(f, t["x_center"][:, :fg], t["length"][:fg], 2)
+
+    runs = (("muscl_rk3_fp64", F.SSPRK3, F.RECON_MUSCL, F.FP64), ("muscl_rk3_mixed", F.SSPRK3, F.RECON_MUSCL, F.MIXED),
+            ("first_order_rk2_fp64", F.RUNGE_KUTTA_2, F.RECON_NONE, F.FP64))
+    out = {}
+    for name, ti, rec, prec in runs:
+        s = hb.Solver(2, F.EULER, F.FLUX_AUSM, ti, prec, reconstruction=rec, limiter_k=1.0, cfl=0.5,
+                      time_end=1e30)
+        s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg,
+                   [Condition(F.BC_PERIODIC) for _ in range(4)])
+        s.set_periodic(partners)
+        stream = torch.cuda.ExternalStream(s.stream())
+        s.set_state(q0, 0)
+        s.reset_time()
+        s.solve(args.warmup)  # warm-up (graph capture), then the timed run from the initial state
+        s.set_state(q0, 0)
+        s.reset_time()
+        torch.cuda.synchronize()
+        l0 = s.launches()
+        with ClockSampler(local) as clk:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            s.solve(args.steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        ms = allreduce_max(ev0.elapsed_time(ev1), ws)
+        launches = s.launches() - l0
+        q = s.state(0)[:, :fg]
+        tt = s.time()
+        ex = exact(tt)
+        s.profile(True)
+        s.solve(min(args.steps, 50))
+        torch.cuda.synchronize()
+        s.profile(False)
+        kern = s.profile_read()
+        out[name] = dict(value=fg * args.steps * ws / (ms * 1e-3), ms=ms, time=tt, launches=int(launches),
+                         l2_rho=float(np.sqrt(((q[2] - ex[2]) ** 2).mean())), q=q, clocks=clk.summary(),
+                         kernels_ms={k: {"total_ms": v[0], "launches": v[1]} for k, v in kern.items()})
+    d = out["muscl_rk3_mixed"]["q"] - out["muscl_rk3_fp64"]["q"]
+    l2_mixed_vs_fp64 = float(np.sqrt((d ** 2).mean() / (out["muscl_rk3_fp64"]["q"] ** 2).mean()))
+    a = out["muscl_rk3_fp64"]
+    line = {"metric": "cell-updates/s", "value": a["value"], "unit": "cell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": a["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"2D Euler isentropic vortex, uniform {2 ** level}^2 on [0,10]^2, periodic, "
+                                   "beta 5, centre (5,5), LSQ gradients + MUSCL + Venkatakrishnan (K 1), "
+                                   "SSP-RK3, CFL 0.5", "leaf_cells": int(fg),
+                       "l2": "working set (3 states + gradients) is L2-resident; no flush"},
+            "gpu_launches": a["launches"], "sim_time": a["time"], "l2_rho_error": a["l2_rho"],
+            "runs": {k: {kk: vv for kk, vv in v.items() if kk != "q"} for k, v in out.items()},
+            "mixed_over_fp64": out["muscl_rk3_mixed"]["value"] / a["value"],
+            "mixed_vs_fp64_rel_l2": l2_mixed_vs_fp64, "clocks": a["clocks"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def measure_adjoint(s, q0, nsteps, stream, fg):
     """Time h3c_adjoint of J = <lambda, q_N> over nsteps RK2 steps against the
     same nsteps of h3c_solve (CUDA events on the solver's stream, both from the
@@ -436,7 +519,8 @@ def main():
     ap.add_argument("--extra-levels", type=int, default=2)
     ap.add_argument("--cfl", type=float, default=0.4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble", "tgv"])
+    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble", "tgv", "vortex"])
+    ap.add_argument("--vortex-level", type=int, default=8)
     ap.add_argument("--tgv-level", type=int, default=7)
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--adjoint-steps", type=int, default=50)
@@ -448,6 +532,9 @@ def main():
         return
     if args.workload == "tgv" and args.impl == "ours":
         run_tgv(args, ws, rank, local)
+        return
+    if args.workload == "vortex" and args.impl == "ours":
+        run_vortex(args, ws, rank, local)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)

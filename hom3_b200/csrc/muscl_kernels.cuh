@@ -69,7 +69,7 @@ __device__ __forceinline__ void face_point(const Geometry& g, const double* __re
 }
 
 __device__ __forceinline__ double vk_phi(double a, double b, double e2) {
-  return ((a * a + e2) * b + 2. * b * b * a) / (b * (a * a + 2. * b * b + a * b + e2));
+  return ((a * a + e2) * b + 2. * b * b * a) * nr_rcp(b * (a * a + 2. * b * b + a * b + e2));
 }
 
 template <int ND, bool HANG>
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(kBlock) k_muscl_grad(const double* __restrict_
       dx[k] = __ldg(xc + k * ld + n) - xcc[k];
       r2 = k == 0 ? dx[k] * dx[k] : r2 + dx[k] * dx[k];
     }
-    const double wgt = 1.0 / r2;
+    const double wgt = nr_rcp(r2);
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
 #pragma unroll
@@ -126,7 +126,7 @@ __global__ void __launch_bounds__(kBlock) k_muscl_grad(const double* __restrict_
   });
   double inv[ND][ND];
   if (ND == 2) {
-    const double id = 1.0 / (M[0][0] * M[1][1] - M[0][1] * M[1][0]);
+    const double id = nr_rcp(M[0][0] * M[1][1] - M[0][1] * M[1][0]);
     inv[0][0] = M[1][1] * id;
     inv[1][1] = M[0][0] * id;
     inv[0][1] = -M[0][1] * id;
@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kBlock) k_muscl_grad(const double* __restrict_
     const double c00 = M[1][1] * M[i2][i2] - M[1][i2] * M[i2][1];
     const double c01 = M[1][i2] * M[i2][0] - M[1][0] * M[i2][i2];
     const double c02 = M[1][0] * M[i2][1] - M[1][1] * M[i2][0];
-    const double id = 1.0 / (M[0][0] * c00 + M[0][1] * c01 + M[0][i2] * c02);
+    const double id = nr_rcp(M[0][0] * c00 + M[0][1] * c01 + M[0][i2] * c02);
     inv[0][0] = c00 * id;
     inv[0][1] = (M[0][i2] * M[i2][1] - M[0][1] * M[i2][i2]) * id;
     inv[0][i2] = (M[0][1] * M[1][i2] - M[0][i2] * M[1][1]) * id;
@@ -149,32 +149,42 @@ __global__ void __launch_bounds__(kBlock) k_muscl_grad(const double* __restrict_
   }
   const double kh = limiter_k * g.len[g.lvl[c]];
   const double e2 = kh * kh * kh;
+  double G[NV][ND], psi[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    double G[ND];
 #pragma unroll
     for (int i = 0; i < ND; ++i) {
       double s = inv[i][0] * b[v][0];
 #pragma unroll
       for (int j = 1; j < ND; ++j) s = s + inv[i][j] * b[v][j];
-      G[i] = s;
+      G[v][i] = s;
     }
-    const double dmax = wmax[v] - wc[v], dmin = wmin[v] - wc[v];
-    double psi = 1.0;
-    for_each_face<ND, HANG>(g, c, [&](int n, int d, int side) {
-      double xf[ND];
-      if (side < 0) face_point<ND>(g, xc, n, (int)c, d, xf);
-      else face_point<ND>(g, xc, (int)c, n, d, xf);
-      double d2 = G[0] * (xf[0] - xcc[0]);
+    psi[v] = 1.0;
+    wmax[v] = wmax[v] - wc[v];  // largest / smallest neighbour difference
+    wmin[v] = wmin[v] - wc[v];
+  }
+  // one pass over the faces for all variables: the face offset is loaded once
+  for_each_face<ND, HANG>(g, c, [&](int n, int d, int side) {
+    double xf[ND];
+    if (side < 0) face_point<ND>(g, xc, n, (int)c, d, xf);
+    else face_point<ND>(g, xc, (int)c, n, d, xf);
 #pragma unroll
-      for (int k = 1; k < ND; ++k) d2 = d2 + G[k] * (xf[k] - xcc[k]);
+    for (int k = 0; k < ND; ++k) xf[k] = xf[k] - xcc[k];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double d2 = G[v][0] * xf[0];
+#pragma unroll
+      for (int k = 1; k < ND; ++k) d2 = d2 + G[v][k] * xf[k];
       double phi = 1.0;
-      if (d2 > 0) phi = vk_phi(dmax, d2, e2);
-      else if (d2 < 0) phi = vk_phi(dmin, d2, e2);
-      psi = phi < psi ? phi : psi;
-    });
+      if (d2 > 0) phi = vk_phi(wmax[v], d2, e2);
+      else if (d2 < 0) phi = vk_phi(wmin[v], d2, e2);
+      psi[v] = phi < psi[v] ? phi : psi[v];
+    }
+  });
 #pragma unroll
-    for (int i = 0; i < ND; ++i) grad[(v * ND + i) * ld + c] = psi * G[i];
+  for (int v = 0; v < NV; ++v) {
+#pragma unroll
+    for (int i = 0; i < ND; ++i) grad[(v * ND + i) * ld + c] = psi[v] * G[v][i];
   }
 }
 
