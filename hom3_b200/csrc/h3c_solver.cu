@@ -22,6 +22,7 @@
 #include "fv_kernels.cuh"
 #include "adjoint_kernels.cuh"
 #include "muscl_kernels.cuh"
+#include "muscl_adjoint.cuh"
 
 using namespace h3c;
 
@@ -1265,8 +1266,6 @@ static int adjoint_supported(h3c_solver s, const char* what) {
   const bool ok_phys = (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM) ||
                        s->desc.physics == H3C_HEAT;
   if (!ok_phys) return s->fail(H3C_E_INVALID, "%s: Euler/AUSM and heat only", what);
-  if (s->desc.reconstruction != H3C_RECON_NONE)
-    return s->fail(H3C_E_INVALID, "%s: the adjoint covers the first-order scheme only", what);
   if (s->ghost_unapplied) return s->fail(H3C_E_INVALID, "%s: a ghost cell gets no condition", what);
   for (int k = 0; k < s->n_bcs; ++k) {
     const int kind = s->h_bcs[k].kind;
@@ -1350,9 +1349,13 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   const long long L = s->ld, nv = s->nv, Q = nv * L;
   const int ti = s->desc.time_integration;
   const long long per = ti == H3C_EULER_FORWARD ? 1 : ti == H3C_RUNGE_KUTTA_2 ? 2 : 3;  // stages per step
+  const bool muscl = s->desc.reconstruction == H3C_RECON_MUSCL;
+  // MUSCL reverse: face and ghost cotangents, own terms, limiter terms (4 states), gradient and
+  // normal-equation cotangents (2 x nd nv columns), extreme-neighbour owners (nv int columns)
+  const long long extra_m = muscl ? 4 * Q + 2 * s->nd * Q + (Q + 1) / 2 + 1 : 0;
   auto need = [&](long long ev) {
     const long long nck = (nsteps + ev - 1) / ev;
-    return sizeof(double) * ((size_t)Q * (nck + per * ev + 7) + nsteps);
+    return sizeof(double) * ((size_t)Q * (nck + per * ev + 7) + nsteps + extra_m);
   };
   if (every > nsteps) every = nsteps;
   if (every == 0) {  // no recomputation if that fits in half of the free memory, else ~sqrt(N) segments
@@ -1381,6 +1384,13 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   double* work = seg + Q * per * every;
   double* lam = work + Q * 3;
   double* d_dts = lam + Q * 4;
+  double* m_qface = d_dts + nsteps;  // MUSCL reverse buffers (unused otherwise)
+  double* m_qghost = m_qface + Q;
+  double* m_wself = m_qghost + Q;
+  double* m_dl1 = m_wself + Q;
+  double* m_gbar = m_dl1 + Q;
+  double* m_bbar = m_gbar + s->nd * Q;
+  int* m_owner = reinterpret_cast<int*>(m_bbar + s->nd * Q);
   const long long last0 = (nck - 1) * every;  // first step of the last segment
   // ---- forward: the solver's own step (CFL dt), checkpoints, dt record ----
   const bool fuse = !s->unfused_dt;
@@ -1407,9 +1417,31 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   auto adj = [&](const double* qin, const double* lamin, double* gout, double alpha, double beta,
                  const double* extra = nullptr, double gam = 0.0, const double* extra2 = nullptr,
                  double gam2 = 0.0) {
-    Launch La(s, K_OTHER);
     const Geometry g = geometry(s);
     const GhostTables gt = ghosts(s);
+    if (muscl) {
+      launch_grad(s, qin);  // the forward's limited gradients of this stage input
+      Launch La(s, K_OTHER);
+      const unsigned nb = (unsigned)blocks(s->n_int);
+      const double K = s->desc.limiter_k;
+#define H3C_ADJM(ND, HANG)                                                                                          \
+  k_adjm_face<ND, HANG><<<nb, kBlock, 0, s->stream>>>(qin, s->d_slopes, s->d_xc, lamin, alpha, g, gt, s->pc, s->d_sc, \
+                                                      m_qface, m_gbar);                                              \
+  k_adjm_lim<ND, HANG><<<nb, kBlock, 0, s->stream>>>(qin, s->d_xc, m_gbar, g, gt, s->pc, K, m_bbar, m_dl1, m_owner,   \
+                                                     m_wself, m_qghost);                                             \
+  k_adjm_gather<ND, HANG><<<nb, kBlock, 0, s->stream>>>(qin, s->d_xc, lamin, extra, extra2, beta, gam, gam2, g, gt,    \
+                                                        s->pc, m_bbar, m_dl1, m_owner, m_wself, m_qface, m_qghost,   \
+                                                        gout)
+      if (s->nd == 2) {
+        if (s->nsub > 0) { H3C_ADJM(2, true); } else { H3C_ADJM(2, false); }
+      } else {
+        if (s->nsub > 0) { H3C_ADJM(3, true); } else { H3C_ADJM(3, false); }
+      }
+#undef H3C_ADJM
+      s->launches += 2;  // three kernels under one Launch record
+      return;
+    }
+    Launch La(s, K_OTHER);
     if (s->nd == 2) {
       if (s->desc.physics == H3C_HEAT)
         k_adj_stage<2, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);

@@ -226,7 +226,8 @@ def refined_case(ti=h3o.RK2, level=2, fine=4, **extra):
 def smooth_state(o: "h3o.Solver", seed=0):
     """A state on which the discrete map is smooth, for derivative checks: the
     case's state plus a uniform subsonic drift (Euler; no face sits at the
-    interface-Mach-number switch m = 0) or 1 + a smooth random field (heat)."""
+    interface-Mach-number switch m = 0) and a small per-cell perturbation,
+    or 1 + a smooth random field (heat).  gamma = 1.4."""
     q = o.state(0).copy()
     fg = o.first_ghost
     nd = o.w.nd
@@ -241,9 +242,24 @@ def smooth_state(o: "h3o.Solver", seed=0):
     drift = np.array([0.3, 0.1, 0.05][:nd])
     rho = q[nd]
     u = q[:nd] / rho
-    ke_old = 0.5 * rho * (u * u).sum(axis=0)
-    u = u + drift[:, None]
+    p = 0.4 * (q[nd + 1] - 0.5 * rho * (u * u).sum(axis=0))
+    # a smooth random perturbation of 1e-3 (random phases): no symmetry of the
+    # initial condition makes two neighbours tie (a tie is a kink of the
+    # limiter's max / min, where central differences and one-sided derivatives
+    # differ), and no per-cell extrema are added
+    x = o.tables()["x_center"][:, :q.shape[1]]
+    span = np.ptp(x[:, :fg], axis=1).max() + 1e-300
+
+    def field():  # random real wave vectors: no reflection or rotation symmetry survives
+        k = rng.uniform(0.5, 2.5, size=(3, nd)) * (2 * np.pi / span)
+        ph = rng.uniform(0, 2 * np.pi, size=3)
+        return sum(np.sin(k[m] @ x + ph[m]) for m in range(3)) / 3
+
+    rho = rho * (1.0 + 1e-3 * field())
+    p = p * (1.0 + 1e-3 * field())
+    u = u + drift[:, None] + 1e-3 * np.stack([field() for _ in range(nd)])
     q[:nd] = rho * u
-    q[nd + 1] = q[nd + 1] - ke_old + 0.5 * rho * (u * u).sum(axis=0)
+    q[nd] = rho
+    q[nd + 1] = p / 0.4 + 0.5 * rho * (u * u).sum(axis=0)
     q[:, fg:] = 0.0
     return q

@@ -14,6 +14,8 @@ BUILDERS = {
     "heat3d_fe": lambda: cases.heat_case(level=3),
     "periodic_vortex_rk2": lambda: cases.periodic_vortex_case(level=4),
     "refined_rk2": lambda: cases.refined_case(level=2, fine=3),
+    "vortex_muscl_rk3": lambda: cases.periodic_vortex_case(level=4, ti=h3o.SSPRK3, recon=h3o.RECON_MUSCL),
+    "vortex_muscl_fe": lambda: cases.periodic_vortex_case(level=5, ti=h3o.EULER_FORWARD, recon=h3o.RECON_MUSCL),
 }
 
 
@@ -48,8 +50,14 @@ def test_dual_oracle_matches_finite_differences(name):
     ref = frozen_run(build, q1, dts)
     assert np.array_equal(val[:, :fg], ref[:, :fg])
     errs = []
-    for eps in (1e-4, 1e-5):
+    # the limited reconstruction is differentiable only closer to the state than
+    # its nearest switch (limiter face, extreme neighbour): smaller steps there
+    steps = (1e-7, 1e-8) if "muscl" in name else (1e-4, 1e-5)
+    for eps in steps:
         fd = (frozen_run(build, q1 + eps * dq, dts) - frozen_run(build, q1 - eps * dq, dts)) / (2 * eps)
         errs.append(np.abs(dot[:, :fg] - fd[:, :fg]).max() / np.abs(fd[:, :fg]).max())
-    assert errs[1] < 1e-7, errs
-    assert errs[1] < errs[0] / 30 or errs[1] < 1e-9, errs  # second-order convergence
+    if "muscl" in name:
+        assert max(errs) < 1e-6, errs
+    else:
+        assert errs[1] < 1e-7, errs
+        assert errs[1] < errs[0] / 30 or errs[1] < 1e-9, errs  # second-order convergence
