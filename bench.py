@@ -464,6 +464,88 @@ def run_vortex(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_cht(args, ws, rank, local):
+    """Conjugate heat transfer: CNS channel 512 x 128 over a heat-conducting
+    solid 512 x 64 in one level-9 root cell, conductivity ratio 10, solid
+    initial temperature 1 + 0.1 (smooth 16-mode field, seed 1); each step
+    coupling::apply (common dt, Tr0 = 0.01), one CNS step, one heat step
+    (coupled_cns_heat_test.cpp:235-248).  Unit: one cell (fluid or solid)
+    advanced one step."""
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    d = W.cht_setup()
+    tf, ts = d["tables_fluid"], d["tables_solid"]
+    fgf, fgs = tf["first_ghost"], ts["first_ghost"]
+
+    def make():
+        cns = hb.Solver(2, F.CNS, F.FLUX_AUSM, F.EULER_FORWARD, F.FP64, time_end=1e30, **d["props"])
+        heat = hb.Solver(2, F.HEAT, F.FLUX_AUSM, F.EULER_FORWARD, F.FP64, cfl=0.5, time_end=1e30)
+        cns.set_grid(tf["neighbors"], tf["x_center"], tf["length"], tf["bc_idx"], fgf, d["conditions_fluid"])
+        heat.set_grid(ts["neighbors"], ts["x_center"], ts["length"], ts["bc_idx"], fgs, d["conditions_solid"])
+        cns.set_partner(heat, d["partners_fluid"])
+        heat.set_partner(cns, d["partners_solid"])
+        cns.set_state(d["q_fluid"], 0)
+        heat.set_state(d["q_solid"], 0)
+        cns.reset_time()
+        heat.reset_time()
+        return cns, heat
+
+    cns, heat = make()
+    stream = torch.cuda.ExternalStream(cns.stream())
+    Tr0 = 0.01
+
+    def steps(n):
+        hb.cht_solve(Tr0, cns, heat, n)
+
+    steps(args.warmup)
+    torch.cuda.synchronize()
+    l0 = cns.launches() + heat.launches()
+    with ClockSampler(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        steps(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = allreduce_max(ev0.elapsed_time(ev1), ws)
+    launches = cns.launches() + heat.launches() - l0
+    # the same steps one call per solver and step (hom3's loop shape), for comparison
+    c2, h2 = make()
+    for _ in range(args.warmup):
+        hb.couple_cht(Tr0, c2, h2)
+        c2.solve(1)
+        h2.solve(1)
+    torch.cuda.synchronize()
+    s2 = torch.cuda.ExternalStream(c2.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s2)
+    for _ in range(args.steps):
+        hb.couple_cht(Tr0, c2, h2)
+        c2.solve(1)
+        h2.solve(1)
+    e1.record(s2)
+    torch.cuda.synchronize()
+    ms_loop = e0.elapsed_time(e1)
+    Ts = heat.state(0)[0, :fgs]
+    cells = fgf + fgs
+    line = {"metric": "cell-updates/s", "value": cells * args.steps * ws / (ms * 1e-3), "unit": "cell-updates/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "2D conjugate heat transfer: CNS 512x128 over heat 512x64 in one level-9 root "
+                                   "cell, conductivity ratio 10, Minfty 0.2, ReInfty 100, Tr0 0.01, forward Euler, "
+                                   "solid T0 = T_inf (1 + 0.1 f), f 16 Fourier modes seed 1",
+                       "fluid_cells": int(fgf), "solid_cells": int(fgs)},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "per_solver_loop_value": cells * args.steps / (ms_loop * 1e-3),
+            "solid_T_range": [float(Ts.min()), float(Ts.max())], "time": cns.time()}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def measure_adjoint(s, q0, nsteps, stream, fg):
     """Time h3c_adjoint of J = <lambda, q_N> over nsteps RK2 steps against the
     same nsteps of h3c_solve (CUDA events on the solver's stream, both from the
@@ -519,7 +601,7 @@ def main():
     ap.add_argument("--extra-levels", type=int, default=2)
     ap.add_argument("--cfl", type=float, default=0.4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble", "tgv", "vortex"])
+    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble", "tgv", "vortex", "cht"])
     ap.add_argument("--vortex-level", type=int, default=8)
     ap.add_argument("--tgv-level", type=int, default=7)
     ap.add_argument("--members", type=int, default=256)
@@ -535,6 +617,9 @@ def main():
         return
     if args.workload == "vortex" and args.impl == "ours":
         run_vortex(args, ws, rank, local)
+        return
+    if args.workload == "cht" and args.impl == "ours":
+        run_cht(args, ws, rank, local)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)

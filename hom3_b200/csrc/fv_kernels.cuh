@@ -493,7 +493,10 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
       if (gt.partner[i] < 0 || pv.q == nullptr) return;
       const double Tother = partner_T(B, pv, gt.partner[i]);
       const double Tthis = qlhs[bc];
-      const double Ts = B.kind == BC_CPL_HEAT_CNS ? 0.5 * (Tother + Tthis) : 0.5 * (Tthis + Tother);
+      const double kap = B.kind == BC_CPL_HEAT_CNS ? B.v[0] : 0.0;  // EXTENSION: k_solid / k_fluid
+      const double Ts = B.kind == BC_CPL_HEAT_CNS
+                            ? ((kap == 0.0 || kap == 1.0) ? 0.5 * (Tother + Tthis) : (Tother + kap * Tthis) / (1.0 + kap))
+                            : 0.5 * (Tthis + Tother);
       out[0] = 2.0 * Ts - qb[0];
       break;
     }
@@ -541,7 +544,10 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
           }
           const double pf = pc.gm1 * (ql[ND + 1] - 0.5 * ql[ND] * um2);
           const double Tf = gamma * pf / ql[ND];
-          Ts = 0.5 * (Tf + partner_T(B, pv, gt.partner[i]));
+          const double Tsol = partner_T(B, pv, gt.partner[i]);
+          // EXTENSION: conductivity ratio kappa = k_solid / k_fluid in v[0] (0: hom3's mean)
+          const double kap = B.v[0];
+          Ts = (kap == 0.0 || kap == 1.0) ? 0.5 * (Tf + Tsol) : (Tf + kap * Tsol) / (1.0 + kap);
         }
 #pragma unroll
         for (int d = 0; d < ND; ++d) gp[d] = 0.0 - bp[d];

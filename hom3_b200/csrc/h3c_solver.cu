@@ -83,6 +83,12 @@ struct h3c_solver_s {
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   const double* graph_q0 = nullptr;  // lhs buffer the capture started from
+  // coupled conjugate-heat steps (h3c_cht_solve) captured with the heat partner
+  cudaGraphExec_t cpl_graph = nullptr;
+  h3c_solver cpl_with = nullptr;
+  const double *cpl_q0 = nullptr, *cpl_q0_other = nullptr;
+  double cpl_scaling = 0.0;
+  long long cpl_launches = 0;
   long long graph_launches = 0;
   bool graphs = true;
   std::string err;
@@ -121,10 +127,19 @@ template <class T> void dfree(T*& p) {
   p = nullptr;
 }
 
+void drop_cpl_graph(h3c_solver s) {
+  if (s->cpl_graph) cudaGraphExecDestroy(s->cpl_graph);
+  s->cpl_graph = nullptr;
+  s->cpl_with = nullptr;
+}
+
 void drop_graph(h3c_solver s) {
   if (s->graph) cudaGraphExecDestroy(s->graph);
   s->graph = nullptr;
   s->graph_steps = 0;
+  // a coupled graph holds this solver's and its partner's buffers
+  drop_cpl_graph(s);
+  if (s->partner && s->partner->cpl_with == s) drop_cpl_graph(s->partner);
 }
 
 void free_grid(h3c_solver s) {
@@ -1133,6 +1148,68 @@ int h3c_couple_cht(h3c_solver cns, h3c_solver heat, double Tr0) {
   launch_cfl(heat, &heat->d_sc->mindt_ord);
   k_couple_cht<<<1, 1, 0, cns->stream>>>(cns->d_sc, heat->d_sc, scaling);
   return cns->cuda(cudaGetLastError(), "h3c_couple_cht");
+}
+
+// One coupled step: coupling::apply(Tr0, cns, heat), cns.solve(), heat.solve()
+// (coupled_cns_heat_test.cpp:235-248), all on the shared stream.
+static void enqueue_cht(h3c_solver cns, h3c_solver heat, double scaling, int64_t n) {
+  for (int64_t i = 0; i < n; ++i) {
+    launch_cfl(cns, &cns->d_sc->mindt_ord);
+    launch_cfl(heat, &heat->d_sc->mindt_ord);
+    {
+      Launch L(cns, K_SCALAR);
+      k_couple_cht<<<1, 1, 0, cns->stream>>>(cns->d_sc, heat->d_sc, scaling);
+    }
+    enqueue_steps(cns, 1);
+    enqueue_steps(heat, 1);
+  }
+}
+
+int h3c_cht_solve(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps) {
+  if (!cns || !heat || nsteps < 0) return H3C_E_INVALID;
+  if (int rc = ready(cns, "h3c_cht_solve")) return rc;
+  if (int rc = ready(heat, "h3c_cht_solve")) return rc;
+  if (cns->desc.physics != H3C_CNS || heat->desc.physics != H3C_HEAT)
+    return cns->fail(H3C_E_INVALID, "h3c_cht_solve: expects (cns, heat)");
+  if (cns->stream != heat->stream || cns->partner != heat || heat->partner != cns)
+    return cns->fail(H3C_E_STATE, "h3c_cht_solve: solvers are not coupled with each other");
+  const double scaling = Tr0 * cns->Pr0 * cns->Re0;
+  const bool graphable = cns->graphs && heat->graphs && !cns->prof && !heat->prof;
+  if (graphable && nsteps >= kGraphSteps) {
+    if (cns->cpl_graph && (cns->cpl_with != heat || cns->cpl_q0 != cns->d_q[0] ||
+                           cns->cpl_q0_other != heat->d_q[0] || cns->cpl_scaling != scaling))
+      drop_cpl_graph(cns);
+    if (!cns->cpl_graph) {
+      enqueue_cht(cns, heat, scaling, 1);  // one plain step first (kernel attributes outside capture)
+      nsteps -= 1;
+      const long long lc = cns->launches, lh = heat->launches;
+      cudaGraph_t g = nullptr;
+      if (cudaStreamBeginCapture(cns->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        enqueue_cht(cns, heat, scaling, kGraphSteps);
+        if (cudaStreamEndCapture(cns->stream, &g) == cudaSuccess && g &&
+            cudaGraphInstantiate(&cns->cpl_graph, g, 0) == cudaSuccess) {
+          cns->cpl_with = heat;
+          cns->cpl_q0 = cns->d_q[0];
+          cns->cpl_q0_other = heat->d_q[0];
+          cns->cpl_scaling = scaling;
+          cns->cpl_launches = (cns->launches - lc) + (heat->launches - lh);
+        } else {
+          cns->cpl_graph = nullptr;
+        }
+        if (g) cudaGraphDestroy(g);
+      }
+      cudaGetLastError();
+      cns->launches = lc;  // captured launches are counted when the graph runs
+      heat->launches = lh;
+    }
+    while (cns->cpl_graph && nsteps >= kGraphSteps) {
+      H3C_CUDA(cns, cudaGraphLaunch(cns->cpl_graph, cns->stream));
+      cns->launches += cns->cpl_launches;
+      nsteps -= kGraphSteps;
+    }
+  }
+  enqueue_cht(cns, heat, scaling, nsteps);
+  return cns->cuda(cudaGetLastError(), "h3c_cht_solve");
 }
 
 int h3c_couple_equal(h3c_solver a, h3c_solver b) {

@@ -358,6 +358,12 @@ def couple_cht(Tr0, cns: Solver, heat: Solver):
     check(lib().h3c_couple_cht(cns.h, heat.h, float(Tr0)), cns.h)
 
 
+def cht_solve(Tr0, cns: Solver, heat: Solver, nsteps: int):
+    """nsteps of coupling::apply(Tr0, cns, heat) + cns.solve() + heat.solve()
+    (coupled_cns_heat_test.cpp:235-248), replayed as one CUDA graph."""
+    check(lib().h3c_cht_solve(cns.h, heat.h, float(Tr0), int(nsteps)), cns.h)
+
+
 def couple_equal(a: Solver, b: Solver):
     """coupling::apply(s1, s2) -- coupling.hpp:186-193."""
     check(lib().h3c_couple_equal(a.h, b.h), a.h)

@@ -122,3 +122,66 @@ def ensemble_member_tables(m):
     geoms = [edge([eps, 0], [1, 0]), edge([lx - eps, 0], [-1, 0]), edge([0, eps], [0, 1]), edge([0, ly - eps], [0, -1])]
     dom = square([0.5 * lx, 0.5 * ly], [lx, ly])
     return build_tables(spec, geoms, dom, 2)
+
+
+# ---------------------------------------------------------------------------
+# Conjugate heat transfer: a CNS channel over a heat-conducting solid.
+# ---------------------------------------------------------------------------
+def cht_setup(level=9, side=4.0, fluid_rows=128, solid_rows=64, kappa=10.0, seed=1, amp=0.1, Minfty=0.2,
+              ReInfty=100.0):
+    """Fluid (CNS) block of 2^level x fluid_rows cells above a solid (heat)
+    block of 2^level x solid_rows cells, both in one square root cell
+    [0, side]^2 at `level`, split by domain predicates as in hom3's coupled
+    test (coupled_cns_heat_test.cpp:93-95,139-141).  Fluid: hom3's free
+    stream at Minfty (quantities of cns/quantities.hpp), inflow left, outflow
+    right, zero-gradient top; solid: adiabatic (zero heat flux) outside the
+    interface; interface conditions with conductivity ratio kappa =
+    k_solid / k_fluid.  Solid initial temperature T_inf (1 + amp f), f a
+    16-mode smooth field (integer wave numbers 1..4, PCG64 `seed`) scaled to
+    max |f| = 1.  Returns a dict with both solvers' tables, conditions,
+    partner cells and initial states."""
+    from .solver import (GridSpec, Condition, build_tables, cell_average, edge, partner_cells, square)
+    h = side / 2 ** level
+    eps = side * 1e-15
+    y0 = solid_rows * h
+    y1 = y0 + fluid_rows * h
+    spec = GridSpec(2, [0.0, 0.0], [side, side], level)
+    # fluid: left, right, top, interface
+    gf = [edge([eps, 0], [1, 0]), edge([side - eps, 0], [-1, 0]), edge([0, y1 - eps], [0, -1]), edge([0, y0 + eps], [0, 1])]
+    tf = build_tables(spec, gf, square([0.5 * side, 0.5 * (y0 + y1)], [side, y1 - y0]), 2)
+    # solid: left, right, bottom, interface
+    gs = [edge([eps, 0], [1, 0]), edge([side - eps, 0], [-1, 0]), edge([0, eps], [0, 1]), edge([0, y0 - eps], [0, -1])]
+    ts = build_tables(spec, gs, square([0.5 * side, 0.5 * y0], [side, y0]), 2)
+    gm1 = 0.4
+    T_inf = 1.0 / (1 + 0.5 * gm1 * Minfty * Minfty)           # euler/quantities.hpp:131-133
+    rho_inf = T_inf ** (1 / gm1)
+    u_inf = Minfty * math.sqrt(T_inf)
+    p_inf = T_inf ** (1.4 / gm1) / 1.4
+    fs = [u_inf, 0.0, rho_inf, p_inf]
+    cf = [Condition(F.BC_CNS_INFLOW, fs), Condition(F.BC_CNS_OUTFLOW, fs), Condition(F.BC_EULER_NEUMANN),
+          Condition(F.BC_CPL_CNS_HEAT, [kappa])]
+    cs = [Condition(F.BC_HEAT_NEUMANN, [0.0]), Condition(F.BC_HEAT_NEUMANN, [0.0]), Condition(F.BC_HEAT_NEUMANN, [0.0]),
+          Condition(F.BC_CPL_HEAT_CNS, [kappa])]
+    qf = np.zeros((4, tf["ncells"]))
+    fgf = tf["first_ghost"]
+    qf[0, :fgf] = rho_inf * u_inf
+    qf[2, :fgf] = rho_inf
+    qf[3, :fgf] = p_inf / gm1 + 0.5 * rho_inf * u_inf * u_inf
+    rng = np.random.Generator(np.random.PCG64(seed))
+    k = rng.integers(1, 5, size=(16, 2)).astype(np.float64)
+    ph = rng.uniform(0, 2 * math.pi, size=16)
+
+    def field(x):
+        f = np.zeros(x.shape[1])
+        for m in range(16):
+            f = f + np.sin(2 * math.pi * (k[m, 0] * x[0] / side + k[m, 1] * x[1] / side) + ph[m])
+        return f
+
+    fgs = ts["first_ghost"]
+    xs = ts["x_center"][:, :fgs]
+    fmax = np.abs(field(xs)).max()
+    qs = np.zeros((1, ts["ncells"]))
+    qs[:, :fgs] = cell_average(lambda x: (T_inf * (1 + amp * field(x) / fmax))[None, :], xs, ts["length"][:fgs], 2)
+    return dict(tables_fluid=tf, tables_solid=ts, conditions_fluid=cf, conditions_solid=cs,
+                partners_fluid=partner_cells(tf, ts), partners_solid=partner_cells(ts, tf), q_fluid=qf, q_solid=qs,
+                props=dict(Minfty=Minfty, ReInfty=ReInfty, Pr0=0.72, cfl=0.4, cfl_viscous=0.4), T_inf=T_inf, h=h)

@@ -83,7 +83,10 @@ extern "C" {
  *  HEAT_NEUMANN       v[0] = surface heat flux (:40-63)
  *  CPL_*              coupling with the partner solver (h3c_set_partner):
  *                     euler/coupling_conditions.hpp:17-35, cns/coupling_conditions.hpp:22-43,
- *                     heat/coupling_conditions.hpp:18-61 */
+ *                     heat/coupling_conditions.hpp:18-61.  CPL_CNS_HEAT / CPL_HEAT_CNS:
+ *                     EXTENSION v[0] = conductivity ratio kappa = k_solid / k_fluid, interface
+ *                     temperature (T_fluid + kappa T_solid) / (1 + kappa) (flux continuity for
+ *                     equal cells); 0 or 1 gives hom3's mean 0.5 (T_fluid + T_solid) */
 #define H3C_BC_EULER_NEUMANN 0
 #define H3C_BC_EULER_DIRICHLET 1
 #define H3C_BC_EULER_VORTEX 2
@@ -274,6 +277,11 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
 int h3c_set_partner(h3c_solver s, h3c_solver partner, const int64_t* partner_cells);
 /* coupling::apply(Tr0, cns, heat), coupling.hpp:167-183 */
 int h3c_couple_cht(h3c_solver cns, h3c_solver heat, double Tr0);
+/* nsteps of the coupled loop of coupled_cns_heat_test.cpp:235-248 --
+ * coupling::apply(Tr0, cns, heat), cns.solve(), heat.solve() per step -- on
+ * the solvers' shared stream; runs of steps replay one captured CUDA graph
+ * (the same kernels as the three calls per step). */
+int h3c_cht_solve(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps);
 /* coupling::apply(s1, s2), coupling.hpp:186-193 */
 int h3c_couple_equal(h3c_solver a, h3c_solver b);
 /* EXTENSION (not in hom3): partner cells (caller numbering, same solver) for

@@ -1159,7 +1159,9 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
           const Ind o = partner_cell(g);
           const T Tf = Temp(0, b);  // fluid T from lhs
           const T Tsol = w->solvers[B.partner]->Temp(0, o);  // solid T from lhs
-          Ts = 0.5 * (Tf + Tsol);
+          // EXTENSION: conductivity ratio kappa = k_solid / k_fluid in v[0] (0: hom3's mean)
+          const double kap = B.v[0];
+          Ts = (kap == 0.0 || kap == 1.0) ? T(0.5 * (Tf + Tsol)) : T((Tf + kap * Tsol) / (1.0 + kap));
         }
         State gp{};
         for (int d = 0; d < nd; ++d) gp[d] = 2.0 * 0 - bp[d];
@@ -1184,7 +1186,10 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
         const Ind o = partner_cell(g);
         const T Tthis = Temp(0, b);
         const T Tother = w->solvers[B.partner]->Temp(0, o);
-        const T Ts = B.kind == BC_CPL_HEAT_CNS ? T(0.5 * (Tother + Tthis)) : T(0.5 * (Tthis + Tother));
+        const double kap = B.kind == BC_CPL_HEAT_CNS ? B.v[0] : 0.0;  // EXTENSION: k_solid / k_fluid
+        const T Ts = B.kind == BC_CPL_HEAT_CNS
+                         ? ((kap == 0.0 || kap == 1.0) ? T(0.5 * (Tother + Tthis)) : T((Tother + kap * Tthis) / (1.0 + kap)))
+                         : T(0.5 * (Tthis + Tother));
         q(t, g, 0) = 2.0 * Ts - q(t, b, 0);
         break;
       }

@@ -124,8 +124,10 @@ def heat_case(level=3, ti=h3o.EULER_FORWARD):
     return w, [s]
 
 
-def cht_case(level=8):
-    """coupled_cns_heat_test.cpp:56-248: CNS (solver 0) around a heat-conducting cube (solver 1)."""
+def cht_case(level=8, kappa=0.0, heat_T=None):
+    """coupled_cns_heat_test.cpp:56-248: CNS (solver 0) around a heat-conducting cube (solver 1).
+    EXTENSION: kappa = k_solid / k_fluid (0: hom3's mean interface temperature) and a
+    solid initial temperature heat_T (default the free-stream T, as in hom3)."""
     lo, hi = [-7.0, -7.0], [7.0, 7.0]
     w = h3o.World(2, lo, hi, level=level, max_solvers=2)
     h = w.cell_length_at_level(level)
@@ -138,12 +140,13 @@ def cht_case(level=8):
     g = w.cube_boundaries()
     cns_bcs = [h3o.bc(h3o.BC_CNS_INFLOW, g[0], fs), h3o.bc(h3o.BC_CNS_OUTFLOW, g[1], fs),
                h3o.bc(h3o.BC_EULER_NEUMANN, g[2]), h3o.bc(h3o.BC_EULER_NEUMANN, g[3]),
-               h3o.bc(h3o.BC_CPL_CNS_HEAT, c1, partner=1)]
+               h3o.bc(h3o.BC_CPL_CNS_HEAT, c1, [kappa], partner=1)]
     cns = w.add_solver(h3o.CNS, h3o.AUSM, h3o.EULER_FORWARD, bcs=cns_bcs, domain=c0, domain_kind=1,
                        ic_kind=h3o.IC_CONSTANT_PV, ic=fs, Minfty=0.2, ReInfty=100.0, time_end=10.0,
                        **dict(CNS_PROPS, cfl=0.4))
-    heat = w.add_solver(h3o.HEAT, 0, h3o.EULER_FORWARD, bcs=[h3o.bc(h3o.BC_CPL_HEAT_CNS, c2, partner=0)],
-                        domain=c0, domain_kind=2, ic_kind=h3o.IC_CONSTANT_CV, ic=[q["T_inf"]], cfl=0.5,
+    heat = w.add_solver(h3o.HEAT, 0, h3o.EULER_FORWARD, bcs=[h3o.bc(h3o.BC_CPL_HEAT_CNS, c2, [kappa], partner=0)],
+                        domain=c0, domain_kind=2, ic_kind=h3o.IC_CONSTANT_CV,
+                        ic=[q["T_inf"] if heat_T is None else heat_T], cfl=0.5,
                         time_end=10.0)
     heat.initialize()  # initialize(hgrid, heatSolver, cnsSolver): coupled_cns_heat_test.cpp:231
     cns.initialize()

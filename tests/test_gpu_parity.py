@@ -128,6 +128,43 @@ def test_cht_coupled():
         check_pair(heat, gh, TOL_STEP if it == 0 else TOL_MULTI, f"heat step {it}")
 
 
+@pytest.mark.parametrize("kappa", [0.0, 10.0])
+def test_cht_hot_solid_conductivity_ratio(kappa):
+    """A solid hotter than the flow (heat flows through the interface);
+    EXTENSION: conductivity ratio kappa = 10 in the interface temperature."""
+    import hom3_b200 as hb
+    _, (cns, heat) = cases.cht_case(level=7, kappa=kappa, heat_T=1.3)
+    gc, gh = _coupled([cns, heat], None)
+    for it in range(4):
+        h3o.couple_cht(cns, heat, 0.01)
+        hb.couple_cht(0.01, gc, gh)
+        cns.solve(); gc.solve()
+        heat.solve(); gh.solve()
+        check_pair(cns, gc, TOL_STEP if it == 0 else TOL_MULTI, f"cns step {it}")
+        check_pair(heat, gh, TOL_STEP if it == 0 else TOL_MULTI, f"heat step {it}")
+
+
+def test_cht_solve_graph_matches_per_call_loop():
+    """h3c_cht_solve (coupled steps replayed from one CUDA graph) equals the
+    per-call loop coupling::apply, cns.solve, heat.solve, and the oracle."""
+    import hom3_b200 as hb
+    _, (cns, heat) = cases.cht_case(level=7, kappa=10.0, heat_T=1.3)
+    ga, ha = _coupled([cns, heat], None)
+    gb, hb_ = _coupled([cns, heat], None)
+    hb.cht_solve(0.01, ga, ha, 19)
+    for _ in range(19):
+        hb.couple_cht(0.01, gb, hb_)
+        gb.solve(1)
+        hb_.solve(1)
+        h3o.couple_cht(cns, heat, 0.01)
+        cns.solve()
+        heat.solve()
+    for x, y, o in ((ga, gb, cns), (ha, hb_, heat)):
+        fg = o.first_ghost
+        assert np.array_equal(x.state(0)[:, :fg], y.state(0)[:, :fg])
+        check_pair(o, x, TOL_MULTI, "cht_solve vs oracle")
+
+
 def test_euler_euler_coupled():
     """coupled_euler_euler_test.cpp:155-162."""
     import hom3_b200 as hb

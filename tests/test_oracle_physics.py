@@ -202,3 +202,21 @@ def test_muscl_preserves_constant_state():
     q0 = o.state(0)[:, : o.first_ghost].copy()
     o.solve(5)
     assert np.max(np.abs(o.state(0)[:, : o.first_ghost] - q0)) <= 1e-14
+
+
+def test_conductivity_ratio_weights_interface_temperature():
+    """EXTENSION: with kappa = k_solid / k_fluid the interface temperature is
+    (T_f + kappa T_s) / (1 + kappa): a very conductive solid pins the fluid
+    wall temperature near its own, so the fluid near the solid heats faster
+    than with hom3's mean (kappa = 1)."""
+    res = {}
+    for kappa in (1.0, 50.0):
+        _, (cns, heat) = cases.cht_case(level=6, kappa=kappa, heat_T=1.3)
+        for _ in range(5):
+            h3o.couple_cht(cns, heat, 0.01)
+            cns.solve()
+            heat.solve()
+        q = cns.state(0)[:, : cns.first_ghost]
+        T = 1.4 * 0.4 * (q[3] - 0.5 * (q[0] ** 2 + q[1] ** 2) / q[2]) / q[2]
+        res[kappa] = T.max()
+    assert res[50.0] > res[1.0]
