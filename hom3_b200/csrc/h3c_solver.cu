@@ -23,6 +23,7 @@
 #include "adjoint_kernels.cuh"
 #include "muscl_kernels.cuh"
 #include "muscl_adjoint.cuh"
+#include "cns_adjoint.cuh"
 
 using namespace h3c;
 
@@ -64,6 +65,7 @@ struct h3c_solver_s {
   std::vector<BcParam> h_bcs;
   BcParam* d_bcs = nullptr;
   h3c_solver partner = nullptr;
+  const double* partner_override = nullptr;  // partner state the coupling conditions read (adjoint recompute)
   // state
   double* d_q[3] = {nullptr, nullptr, nullptr};  // lhs, rhs, second SSP-RK3 stage
   double* d_slopes = nullptr;
@@ -228,7 +230,7 @@ struct Launch {
 template <int ND, int PHYS>
 void launch_bc_t(h3c_solver s, double* q, const double* qlhs) {
   PartnerView pv{nullptr, 0};
-  if (s->partner) pv = PartnerView{s->partner->d_q[0], s->partner->ld};
+  if (s->partner) pv = PartnerView{s->partner_override ? s->partner_override : s->partner->d_q[0], s->partner->ld};
   Launch L(s, K_BC);
   k_bc<ND, PHYS><<<blocks(s->ng), kBlock, 0, s->stream>>>(q, qlhs, geometry(s), ghosts(s), s->pc, s->d_sc, pv);
 }
@@ -266,6 +268,14 @@ void launch_cfl(h3c_solver s, long long* slot) {
     else if (s->desc.physics == H3C_CNS) launch_cfl_t<3, CNS>(s, slot);
     else launch_cfl_t<3, HEAT>(s, slot);
   }
+}
+
+void launch_slopes_ptr(h3c_solver s, const double* q) {
+  Launch L(s, K_SLOPES);
+  if (s->nd == 2)
+    k_slopes<2><<<blocks(s->n_tot), kBlock, 0, s->stream>>>(q, geometry(s), ghosts(s), s->d_slopes);
+  else
+    k_slopes<3><<<blocks(s->n_tot), kBlock, 0, s->stream>>>(q, geometry(s), ghosts(s), s->d_slopes);
 }
 
 void launch_slopes(h3c_solver s, int which) {
@@ -1337,18 +1347,23 @@ int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_out) {
 }
 
 // ---- frozen-dt stepping and the discrete adjoint ----------------------------
-static int adjoint_supported(h3c_solver s, const char* what) {
+static int adjoint_supported(h3c_solver s, const char* what, bool coupled = false) {
   if (int rc = ready(s, what)) return rc;
   if (s->n_inst != 1) return s->fail(H3C_E_INVALID, "%s: single grids only", what);
-  const bool ok_phys = (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM) ||
+  const bool ok_phys = ((s->desc.physics == H3C_EULER || s->desc.physics == H3C_CNS) && s->desc.flux == H3C_FLUX_AUSM) ||
                        s->desc.physics == H3C_HEAT;
-  if (!ok_phys) return s->fail(H3C_E_INVALID, "%s: Euler/AUSM and heat only", what);
+  if (!ok_phys) return s->fail(H3C_E_INVALID, "%s: Euler and CNS with AUSM, and heat only", what);
+  if (s->desc.physics == H3C_CNS && s->nsub > 0)
+    return s->fail(H3C_E_INVALID, "%s: CNS on coarse/fine faces has no adjoint", what);
   if (s->ghost_unapplied) return s->fail(H3C_E_INVALID, "%s: a ghost cell gets no condition", what);
   for (int k = 0; k < s->n_bcs; ++k) {
     const int kind = s->h_bcs[k].kind;
-    if (kind != H3C_BC_EULER_NEUMANN && kind != H3C_BC_EULER_DIRICHLET && kind != H3C_BC_HEAT_NEUMANN &&
-        kind != H3C_BC_HEAT_DIRICHLET && kind != H3C_BC_PERIODIC)
-      return s->fail(H3C_E_INVALID, "%s: condition kind %d has no adjoint", what, kind);
+    const bool cns_kind = kind >= H3C_BC_CNS_INFLOW && kind <= H3C_BC_CNS_ISOTHERMAL_NOSLIP;
+    const bool cpl = kind == H3C_BC_CPL_CNS_HEAT || kind == H3C_BC_CPL_HEAT_CNS;
+    if (!(kind == H3C_BC_EULER_NEUMANN || kind == H3C_BC_EULER_DIRICHLET || kind == H3C_BC_HEAT_NEUMANN ||
+          kind == H3C_BC_HEAT_DIRICHLET || kind == H3C_BC_PERIODIC || (cns_kind && s->desc.physics == H3C_CNS) ||
+          (cpl && coupled)))
+      return s->fail(H3C_E_INVALID, "%s: condition kind %d has no adjoint here", what, kind);
   }
   return H3C_OK;
 }
@@ -1366,7 +1381,9 @@ static void frozen_step(h3c_solver s, double* const* st, double* out, const doub
     k_set_dt_from<<<1, 1, 0, s->stream>>>(s->d_sc, d_dts, i);
   }
   const int ti = s->desc.time_integration;
+  const bool cns = s->desc.physics == H3C_CNS;
   if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[0]);
+  if (cns) launch_slopes_ptr(s, st[0]);
   if (ti == H3C_EULER_FORWARD) {
     launch_stage(s, 0, st[0], out, false);
   } else if (ti == H3C_RUNGE_KUTTA_2) {
@@ -1374,16 +1391,19 @@ static void frozen_step(h3c_solver s, double* const* st, double* out, const doub
     launch_bc_ptr(s, st[1], st[0]);
     if (out != st[0]) cudaMemcpyAsync(out, st[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
     if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[1]);
+    if (cns) launch_slopes_ptr(s, st[1]);
     launch_stage(s, 2, st[1], out, false);
   } else {
     launch_stage(s, 0, st[0], st[1], false);
     launch_bc_ptr(s, st[1], st[0]);
     cudaMemcpyAsync(st[2], st[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
     if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[1]);
+    if (cns) launch_slopes_ptr(s, st[1]);
     launch_stage(s, 3, st[1], st[2], false);
     launch_bc_ptr(s, st[2], st[0]);
     if (out != st[0]) cudaMemcpyAsync(out, st[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
     if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, st[2]);
+    if (cns) launch_slopes_ptr(s, st[2]);
     launch_stage(s, 4, st[2], out, false);
   }
   {
@@ -1429,7 +1449,9 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   const bool muscl = s->desc.reconstruction == H3C_RECON_MUSCL;
   // MUSCL reverse: face and ghost cotangents, own terms, limiter terms (4 states), gradient and
   // normal-equation cotangents (2 x nd nv columns), extreme-neighbour owners (nv int columns)
-  const long long extra_m = muscl ? 4 * Q + 2 * s->nd * Q + (Q + 1) / 2 + 1 : 0;
+  const bool cnsphys = s->desc.physics == H3C_CNS;
+  // CNS reverse: face cotangents (at the MUSCL face slot) and slope cotangents (at the gradient slot)
+  const long long extra_m = muscl ? 4 * Q + 2 * s->nd * Q + (Q + 1) / 2 + 1 : cnsphys ? 4 * Q + s->nd * Q : 0;
   auto need = [&](long long ev) {
     const long long nck = (nsteps + ev - 1) / ev;
     return sizeof(double) * ((size_t)Q * (nck + per * ev + 7) + nsteps + extra_m);
@@ -1496,6 +1518,24 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
                  double gam2 = 0.0) {
     const Geometry g = geometry(s);
     const GhostTables gt = ghosts(s);
+    if (cnsphys) {
+      launch_slopes_ptr(s, qin);  // the forward's cell slopes of this stage input
+      Launch La(s, K_OTHER);
+      const unsigned nb = (unsigned)blocks(s->n_int);
+      if (s->nd == 2) {
+        k_adjc_face<2><<<nb, kBlock, 0, s->stream>>>(qin, s->d_slopes, lamin, alpha, g, gt, s->pc, s->d_sc, nullptr,
+                                                     m_qface, m_gbar, nullptr);
+        k_adjc_slopes<2><<<nb, kBlock, 0, s->stream>>>(qin, lamin, extra, extra2, beta, gam, gam2, g, gt, s->pc,
+                                                       nullptr, m_qface, m_gbar, nullptr, gout);
+      } else {
+        k_adjc_face<3><<<nb, kBlock, 0, s->stream>>>(qin, s->d_slopes, lamin, alpha, g, gt, s->pc, s->d_sc, nullptr,
+                                                     m_qface, m_gbar, nullptr);
+        k_adjc_slopes<3><<<nb, kBlock, 0, s->stream>>>(qin, lamin, extra, extra2, beta, gam, gam2, g, gt, s->pc,
+                                                       nullptr, m_qface, m_gbar, nullptr, gout);
+      }
+      s->launches += 1;  // two kernels under one Launch record
+      return;
+    }
     if (muscl) {
       launch_grad(s, qin);  // the forward's limited gradients of this stage input
       Launch La(s, K_OTHER);

@@ -15,6 +15,10 @@ BUILDERS = {
     "periodic_vortex_rk2": lambda: cases.periodic_vortex_case(level=4),
     "refined_rk2": lambda: cases.refined_case(level=2, fine=3),
     "vortex_muscl_rk3": lambda: cases.periodic_vortex_case(level=4, ti=h3o.SSPRK3, recon=h3o.RECON_MUSCL),
+    "cns_walls_fe": lambda: cases.cns_case("walls", level=4),
+    "cns_slip_rk2": lambda: cases.cns_case("slip", level=4, ti=h3o.RK2),
+    "cns_isothermal_fe": lambda: cases.cns_case("isothermal", level=4),
+    "tgv_cns_rk2": lambda: cases.tgv_case(level=3),
     "vortex_muscl_fe": lambda: cases.periodic_vortex_case(level=5, ti=h3o.EULER_FORWARD, recon=h3o.RECON_MUSCL),
 }
 
