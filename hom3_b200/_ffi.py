@@ -86,6 +86,7 @@ SIGNATURES = {
     "h3c_set_partner": (_i32, [_vp, _vp, _P(_i64)]),
     "h3c_couple_cht": (_i32, [_vp, _vp, _dbl]),
     "h3c_cht_solve": (_i32, [_vp, _vp, _dbl, _i64]),
+    "h3c_cht_adjoint": (_i32, [_vp, _vp, _dbl, _i64, _i64, _P(_dbl), _P(_dbl), _P(_dbl), _P(_dbl), _P(_dbl)]),
     "h3c_couple_equal": (_i32, [_vp, _vp]),
     "h3c_set_periodic": (_i32, [_vp, _P(_i64)]),
     "h3c_solve_dt": (_i32, [_vp, _i64, _P(_dbl)]),

@@ -131,7 +131,8 @@ template <int ND, int PHYS>
 __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double* __restrict__ q, const double* __restrict__ lam,
                                                       double* __restrict__ gout, const double* __restrict__ extra,
                                                       const double* __restrict__ extra2, double alpha, double beta,
-                                                      double gamma_e, double gamma_e2, Geometry g,
+                                                      double gamma_e, double gamma_e2, double* __restrict__ xbar,
+                                                      Geometry g,
                                                       GhostTables gt, PhysConst pc, const Scalars* __restrict__ sc) {
   constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
   constexpr int NS = 1 << (ND - 1);
@@ -162,6 +163,8 @@ __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double
     // nb_cell: neighbour index (interior or ghost)
     double w[NV];
     double jac = 0.0;  // ghost: dq_ghost/dq_c = jac I; interior: 0
+    double xjac = 0.0;  // conjugate heat ghost: dT_ghost / dT_partner
+    long long gi = -1;
     long long own = nb_cell;
     double kn = kn_face;
     if (nb_cell >= g.n_int) {
@@ -175,6 +178,13 @@ __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double
           // the ghost is a copy of its paired cell, whose residual holds the same face
           own = gt.partner[i];
           if (own >= 0) kn = alpha * dt / g.len[g.lvl[own]];
+        } else if (kind == BC_CPL_HEAT_CNS || kind == BC_CPL_HEAT_HEAT) {
+          // T_g = 2 T_s - T_b, T_s = (T_other + kappa T_b) / (1 + kappa) (kappa = 1: the mean)
+          const double kap0 = kind == BC_CPL_HEAT_CNS ? gt.bcs[b].v[0] : 1.0;
+          const double kap = kap0 == 0.0 ? 1.0 : kap0;
+          jac = 2.0 * kap / (1.0 + kap) - 1.0;
+          xjac = 2.0 / (1.0 + kap);
+          gi = i;
         } else {
           jac = (kind == BC_EULER_DIRICHLET || kind == BC_HEAT_DIRICHLET) ? -1.0 : 1.0;
         }
@@ -198,6 +208,7 @@ __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double
       const double sgn = c_is_left ? 1.0 : -1.0;
       gc[0] = (wl + wn) * sgn;
       if (own < 0) gc[0] += wl * (-sgn) * jac;
+      if (gi >= 0 && xbar) xbar[gi] = wl * (-sgn) * xjac;  // cotangent of the partner temperature
 #pragma unroll
       for (int v = 0; v < NV; ++v) acc[v] += gc[v];
       return;

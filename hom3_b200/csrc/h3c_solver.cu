@@ -1561,14 +1561,14 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
     Launch La(s, K_OTHER);
     if (s->nd == 2) {
       if (s->desc.physics == H3C_HEAT)
-        k_adj_stage<2, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
+        k_adj_stage<2, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, nullptr, g, gt, s->pc, s->d_sc);
       else
-        k_adj_stage<2, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
+        k_adj_stage<2, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, nullptr, g, gt, s->pc, s->d_sc);
     } else {
       if (s->desc.physics == H3C_HEAT)
-        k_adj_stage<3, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
+        k_adj_stage<3, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, nullptr, g, gt, s->pc, s->d_sc);
       else
-        k_adj_stage<3, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, g, gt, s->pc, s->d_sc);
+        k_adj_stage<3, EULER><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, nullptr, g, gt, s->pc, s->d_sc);
     }
   };
   // ---- backward over segments; all but the last recompute their stage states from the checkpoint ----
@@ -1621,6 +1621,220 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
   cudaMemcpyAsync(s->d_sc, &saved, sizeof(Scalars), cudaMemcpyHostToDevice, s->stream);
   H3C_CUDA(s, cudaStreamSynchronize(s->stream));
   return s->cuda(cudaGetLastError(), "h3c_adjoint");
+}
+
+// ---- adjoint of the coupled conjugate-heat loop ----------------------------
+// lam_f += xbar dT_f/dq at the fluid cell each heat interface ghost reads
+// (T_f = gamma p / rho of the fluid state after its step)
+__global__ void k_cht_heat_to_fluid(const double* __restrict__ xbar, GhostTables gth, const double* __restrict__ qf,
+                                    long long ldf, int ndf, double gammaf, double* __restrict__ lamf) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= gth.ng) return;
+  const int b = gth.bc_apply[i];
+  if (b == 255 || gth.bcs[b].kind != BC_CPL_HEAT_CNS) return;
+  const int P = gth.partner[i];
+  if (P < 0) return;
+  const double xb = xbar[i];
+  const double rho = qf[ndf * ldf + P], rinv = 1.0 / rho;
+  double um2 = 0.0, u[3] = {0, 0, 0};
+  for (int d = 0; d < ndf; ++d) {
+    u[d] = qf[d * ldf + P] * rinv;
+    um2 += u[d] * u[d];
+  }
+  const double gm1 = gammaf - 1.0;
+  const double p = gm1 * (qf[(ndf + 1) * ldf + P] - 0.5 * rho * um2);
+  for (int d = 0; d < ndf; ++d) atomicAdd(lamf + d * ldf + P, xb * (-gammaf * gm1 * u[d] * rinv));
+  atomicAdd(lamf + ndf * ldf + P, xb * gammaf * (0.5 * gm1 * um2 - p * rinv) * rinv);
+  atomicAdd(lamf + (ndf + 1) * ldf + P, xb * gammaf * gm1 * rinv);
+}
+// lam_s += tbar at the solid cell each fluid interface ghost reads
+__global__ void k_cht_fluid_to_heat(const double* __restrict__ tbar, GhostTables gtf, double* __restrict__ lams) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= gtf.ng) return;
+  const int b = gtf.bc_apply[i];
+  if (b == 255 || gtf.bcs[b].kind != BC_CPL_CNS_HEAT) return;
+  const int Q = gtf.partner[i];
+  if (Q < 0) return;
+  atomicAdd(lams + Q, tbar[i]);
+}
+
+static void caller_to_internal(h3c_solver s, const double* src, double* dst) {
+  for (int v = 0; v < s->nv; ++v)
+    cudaMemcpyAsync(s->d_stage + v * s->n_caller, src + v * s->n_caller, sizeof(double) * s->n_caller,
+                    cudaMemcpyDefault, s->stream);
+  k_gather<<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_stage, s->n_caller, dst, s->ld, s->d_dev2caller, s->n_int,
+                                                       s->nv);
+  ++s->launches;
+}
+static void internal_to_caller(h3c_solver s, const double* src, double* dst) {
+  cudaMemsetAsync(s->d_stage, 0, sizeof(double) * s->nv * s->n_caller, s->stream);
+  k_scatter<<<blocks(s->n_int), kBlock, 0, s->stream>>>(src, s->ld, s->d_stage, s->n_caller, s->d_dev2caller, s->n_int,
+                                                        s->nv);
+  ++s->launches;
+  for (int v = 0; v < s->nv; ++v)
+    cudaMemcpyAsync(dst + v * s->n_caller, s->d_stage + v * s->n_caller, sizeof(double) * s->n_caller,
+                    cudaMemcpyDefault, s->stream);
+}
+
+int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps, int64_t every,
+                    const double* dJ_dqN, const double* dJ_dTN, double* dJ_dq0, double* dJ_dT0, double* dts) {
+  if (!cns || !heat || nsteps < 1 || every < 0 || !dJ_dqN || !dJ_dTN || !dJ_dq0 || !dJ_dT0) return H3C_E_INVALID;
+  if (int rc = adjoint_supported(cns, "h3c_cht_adjoint", true)) return rc;
+  if (int rc = adjoint_supported(heat, "h3c_cht_adjoint", true)) return rc;
+  if (cns->desc.physics != H3C_CNS || heat->desc.physics != H3C_HEAT)
+    return cns->fail(H3C_E_INVALID, "h3c_cht_adjoint: expects (cns, heat)");
+  if (cns->stream != heat->stream || cns->partner != heat || heat->partner != cns)
+    return cns->fail(H3C_E_STATE, "h3c_cht_adjoint: solvers are not coupled with each other");
+  if (cns->desc.time_integration != H3C_EULER_FORWARD || heat->desc.time_integration != H3C_EULER_FORWARD)
+    return cns->fail(H3C_E_INVALID, "h3c_cht_adjoint: forward Euler (the coupled loop's scheme) only");
+  if (cns->unfused_dt || heat->unfused_dt) return cns->fail(H3C_E_INVALID, "h3c_cht_adjoint: unsupported condition");
+  if (every == 0 || every > nsteps) every = std::min<int64_t>(nsteps, every == 0 ? 100 : every);
+  const double scaling = Tr0 * cns->Pr0 * cns->Re0;
+  const long long Qf = (long long)cns->nv * cns->ld, Qs = (long long)heat->nv * heat->ld;
+  const long long nck = (nsteps + every - 1) / every;
+  // workspace: checkpoints, stage inputs of one segment (+ the fluid state after it), work and cotangent states,
+  // CNS reverse buffers, per-ghost cross cotangents, dt records
+  const size_t nd = (size_t)Qf * (nck + (every + 1) + 2 + 3 + 1 + cns->nd) + (size_t)Qs * (nck + every + 2 + 2) +
+                    (size_t)heat->ng + (size_t)cns->ng + 2 * (size_t)nsteps + 8;
+  double* ws = nullptr;
+  if (cudaMalloc(&ws, sizeof(double) * nd) != cudaSuccess) {
+    cudaGetLastError();
+    return cns->fail(H3C_E_NOMEM, "h3c_cht_adjoint: %zu bytes of checkpoints do not fit", sizeof(double) * nd);
+  }
+  double* p = ws;
+  auto take = [&](size_t n) { double* r = p; p += n; return r; };
+  double* ckf = take(Qf * nck);
+  double* cks = take(Qs * nck);
+  double* segf = take(Qf * (every + 1));
+  double* segs = take(Qs * every);
+  double* wf = take(2 * Qf);
+  double* wsd = take(2 * Qs);
+  double* lf = take(3 * Qf);
+  double* ls = take(2 * Qs);
+  double* qface = take(Qf);
+  double* sbar = take(cns->nd * Qf);
+  double* xbar = take(std::max<long long>(1, heat->ng));
+  double* tbar = take(std::max<long long>(1, cns->ng));
+  double* dtf = take(nsteps);
+  double* dth = take(nsteps);
+  cudaStream_t st = cns->stream;
+  if (int rc = ensure_stage(cns, cns->n_caller)) { cudaFree(ws); return rc; }
+  if (int rc = ensure_stage(heat, heat->n_caller)) { cudaFree(ws); return rc; }
+  // ---- forward: the coupled loop (coupling::apply, cns step, heat step), checkpoints, dt records ----
+  for (int64_t i = 0; i < nsteps; ++i) {
+    if (i % every == 0) {
+      cudaMemcpyAsync(ckf + Qf * (i / every), cns->d_q[0], sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(cks + Qs * (i / every), heat->d_q[0], sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
+    }
+    launch_cfl(cns, &cns->d_sc->mindt_ord);
+    launch_cfl(heat, &heat->d_sc->mindt_ord);
+    {
+      Launch L(cns, K_SCALAR);
+      k_couple_cht<<<1, 1, 0, st>>>(cns->d_sc, heat->d_sc, scaling);
+    }
+    enqueue_step(cns, true, nullptr, dtf, i);
+    enqueue_step(heat, true, nullptr, dth, i);
+  }
+  Scalars savf, savs;
+  cudaMemcpyAsync(&savf, cns->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&savs, heat->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
+  // ---- terminal cotangents ----
+  double *lfA = lf, *lfB = lf + Qf, *lfT = lf + 2 * Qf, *lsA = ls, *lsB = ls + Qs;
+  cudaMemsetAsync(lf, 0, sizeof(double) * 3 * Qf, st);
+  cudaMemsetAsync(ls, 0, sizeof(double) * 2 * Qs, st);
+  caller_to_internal(cns, dJ_dqN, lfA);
+  caller_to_internal(heat, dJ_dTN, lsA);
+  const Geometry gf = geometry(cns), gs = geometry(heat);
+  const GhostTables gtf = ghosts(cns), gts = ghosts(heat);
+  const unsigned nbf = (unsigned)blocks(cns->n_int), nbs = (unsigned)blocks(heat->n_int);
+  // ---- backward over segments, each recomputed from its checkpoints ----
+  for (long long k = nck - 1; k >= 0; --k) {
+    const long long i0 = k * every, i1 = std::min<long long>(nsteps, i0 + every);
+    double *curf = wf, *curs = wsd;
+    cudaMemcpyAsync(curf, ckf + Qf * k, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(curs, cks + Qs * k, sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
+    for (long long i = i0; i < i1; ++i) {
+      double* sf0 = segf + Qf * (i - i0);
+      double* ss0 = segs + Qs * (i - i0);
+      cudaMemcpyAsync(sf0, curf, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+      cudaMemcpyAsync(ss0, curs, sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
+      double* nxf = (curf == wf) ? wf + Qf : wf;
+      double* nxs = (curs == wsd) ? wsd + Qs : wsd;
+      cns->partner_override = ss0;  // the fluid's wall conditions read the solid before its step
+      double* stf[1] = {sf0};
+      frozen_step(cns, stf, nxf, dtf, i);
+      heat->partner_override = nxf;  // the solid's conditions read the fluid after its step
+      double* sts[1] = {ss0};
+      frozen_step(heat, sts, nxs, dth, i);
+      cns->partner_override = nullptr;
+      heat->partner_override = nullptr;
+      curf = nxf;
+      curs = nxs;
+    }
+    cudaMemcpyAsync(segf + Qf * (i1 - i0), curf, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+    for (long long i = i1 - 1; i >= i0; --i) {
+      double* sf0 = segf + Qf * (i - i0);
+      double* sf1 = segf + Qf * (i - i0 + 1);  // fluid state after step i
+      double* ss0 = segs + Qs * (i - i0);
+      {
+        Launch L(cns, K_SCALAR);
+        k_set_dt_from<<<1, 1, 0, st>>>(cns->d_sc, dtf, i);
+        k_set_dt_from<<<1, 1, 0, st>>>(heat->d_sc, dth, i);
+        ++cns->launches;
+      }
+      // heat step: lam_s^i = (I + dR_s/dT_s)^T lam_s^{i+1}; its interface reads of T_f -> fluid cotangent
+      cudaMemsetAsync(xbar, 0, sizeof(double) * std::max<long long>(1, heat->ng), st);
+      {
+        Launch L(heat, K_OTHER);
+        if (heat->nd == 2)
+          k_adj_stage<2, HEAT><<<nbs, kBlock, 0, st>>>(ss0, lsA, lsB, nullptr, nullptr, 1.0, 1.0, 0.0, 0.0, xbar, gs, gts,
+                                                       heat->pc, heat->d_sc);
+        else
+          k_adj_stage<3, HEAT><<<nbs, kBlock, 0, st>>>(ss0, lsA, lsB, nullptr, nullptr, 1.0, 1.0, 0.0, 0.0, xbar, gs, gts,
+                                                       heat->pc, heat->d_sc);
+      }
+      cudaMemcpyAsync(lfT, lfA, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+      k_cht_heat_to_fluid<<<blocks(std::max<long long>(1, heat->ng)), kBlock, 0, st>>>(xbar, gts, sf1, cns->ld, cns->nd,
+                                                                                        cns->desc.gamma, lfT);
+      ++heat->launches;
+      // fluid step: lam_f^i = (I + dR_f/dq_f)^T lam~_f; its wall reads of T_s -> solid cotangent
+      cudaMemsetAsync(tbar, 0, sizeof(double) * std::max<long long>(1, cns->ng), st);
+      launch_slopes_ptr(cns, sf0);
+      {
+        Launch L(cns, K_OTHER);
+        if (cns->nd == 2) {
+          k_adjc_face<2><<<nbf, kBlock, 0, st>>>(sf0, cns->d_slopes, lfT, 1.0, gf, gtf, cns->pc, cns->d_sc, ss0, qface,
+                                                 sbar, tbar);
+          k_adjc_slopes<2><<<nbf, kBlock, 0, st>>>(sf0, lfT, nullptr, nullptr, 1.0, 0.0, 0.0, gf, gtf, cns->pc, ss0,
+                                                   qface, sbar, tbar, lfB);
+        } else {
+          k_adjc_face<3><<<nbf, kBlock, 0, st>>>(sf0, cns->d_slopes, lfT, 1.0, gf, gtf, cns->pc, cns->d_sc, ss0, qface,
+                                                 sbar, tbar);
+          k_adjc_slopes<3><<<nbf, kBlock, 0, st>>>(sf0, lfT, nullptr, nullptr, 1.0, 0.0, 0.0, gf, gtf, cns->pc, ss0,
+                                                   qface, sbar, tbar, lfB);
+        }
+        ++cns->launches;
+      }
+      k_cht_fluid_to_heat<<<blocks(std::max<long long>(1, cns->ng)), kBlock, 0, st>>>(tbar, gtf, lsB);
+      ++cns->launches;
+      std::swap(lfA, lfB);
+      std::swap(lsA, lsB);
+    }
+  }
+  internal_to_caller(cns, lfA, dJ_dq0);
+  internal_to_caller(heat, lsA, dJ_dT0);
+  if (dts) {
+    cudaMemcpyAsync(dts, dtf, sizeof(double) * nsteps, cudaMemcpyDefault, st);
+    cudaMemcpyAsync(dts + nsteps, dth, sizeof(double) * nsteps, cudaMemcpyDefault, st);
+  }
+  cudaStreamSynchronize(st);
+  // both solvers are left at step N with the scalars of the forward run
+  cudaMemcpyAsync(cns->d_sc, &savf, sizeof(Scalars), cudaMemcpyHostToDevice, st);
+  cudaMemcpyAsync(heat->d_sc, &savs, sizeof(Scalars), cudaMemcpyHostToDevice, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(ws);
+  if (e != cudaSuccess) return cns->cuda(e, "h3c_cht_adjoint");
+  return cns->cuda(cudaGetLastError(), "h3c_cht_adjoint");
 }
 
 int h3c_launches(h3c_solver s, int64_t* n) {

@@ -364,6 +364,19 @@ def cht_solve(Tr0, cns: Solver, heat: Solver, nsteps: int):
     check(lib().h3c_cht_solve(cns.h, heat.h, float(Tr0), int(nsteps)), cns.h)
 
 
+def cht_adjoint(Tr0, cns: Solver, heat: Solver, nsteps: int, dJ_dqN, dJ_dTN, every: int = 0):
+    """Adjoint of nsteps of the coupled loop (h3c_cht_solve) from the current
+    states: returns (dJ/dq0 fluid, dJ/dT0 solid, dts [2][nsteps]) for
+    J = <dJ_dqN, q_N> + <dJ_dTN, T_N>, time steps frozen."""
+    lf = np.ascontiguousarray(dJ_dqN, np.float64)
+    lt = np.ascontiguousarray(dJ_dTN, np.float64)
+    assert lf.shape == (cns.nv, cns.n_cells) and lt.shape == (heat.nv, heat.n_cells)
+    gf, gt, dts = np.empty_like(lf), np.empty_like(lt), np.empty((2, nsteps))
+    check(lib().h3c_cht_adjoint(cns.h, heat.h, float(Tr0), int(nsteps), int(every), _dp(lf), _dp(lt), _dp(gf), _dp(gt),
+                                _dp(dts)), cns.h)
+    return gf, gt, dts
+
+
 def couple_equal(a: Solver, b: Solver):
     """coupling::apply(s1, s2) -- coupling.hpp:186-193."""
     check(lib().h3c_couple_equal(a.h, b.h), a.h)

@@ -269,6 +269,18 @@ int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t ld, int64_
 int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts);
 int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dqN, double* dJ_dq0, double* dts);
 
+/* Discrete adjoint of the coupled conjugate-heat loop (no hom3 counterpart):
+ * nsteps of h3c_cht_solve's loop (forward Euler in both solvers) from the
+ * current states, checkpoints every `every` steps (0: 100), then dJ/dq0 of
+ * the fluid and dJ/dT0 of the solid for J = <dJ_dqN, q_N> + <dJ_dTN, T_N>,
+ * the coupled time steps frozen at the forward values (dts, may be NULL:
+ * [2][nsteps], fluid then solid).  Arrays in each solver's caller numbering,
+ * host or device memory.  The interface conditions are differentiated in both
+ * directions (the fluid wall reads the solid's temperature, the solid ghost
+ * the fluid's). */
+int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps, int64_t every,
+                    const double* dJ_dqN, const double* dJ_dTN, double* dJ_dq0, double* dJ_dT0, double* dts);
+
 /* ---- coupling: coupling.hpp:24-73 ----
  * partner_cells[g - first_ghost] = the partner solver's cell (caller
  * numbering of the partner) that local_bndry_ids (coupling.hpp:24-39) finds

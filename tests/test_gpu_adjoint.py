@@ -236,3 +236,74 @@ def test_cns_adjoint_matches_dual_oracle(name):
 def test_cns_adjoint_matches_finite_differences(name):
     BUILDERS.update(CNS_BUILDERS)
     assert fd_worst(name, 1e-6) <= 1e-6
+
+
+# ---- adjoint of the coupled conjugate-heat loop ----
+def cht_setup(level=6, kappa=10.0):
+    _, (cns, heat) = cases.cht_case(level=level, kappa=kappa, heat_T=1.3)
+    qf, qs = cases.smooth_state(cns), cases.smooth_state(heat)
+    cns.set_state(qf)
+    heat.set_state(qs)
+    gc, gh = cases.gpu_solver_from_oracle(cns), cases.gpu_solver_from_oracle(heat)
+    gc.set_partner(gh, cns.partner_cells())
+    gh.set_partner(gc, heat.partner_cells())
+    return cns, heat, gc, gh, qf, qs
+
+
+def cht_J(gc, gh, qf, qs, dts, lf, ls):
+    gc.set_state(qf, 0)
+    gh.set_state(qs, 0)
+    gc.reset_time()
+    gh.reset_time()
+    for i in range(dts.shape[1]):
+        gc.solve_dt([dts[0, i]])
+        gh.solve_dt([dts[1, i]])
+    return float((gc.state(0) * lf).sum() + (gh.state(0) * ls).sum())
+
+
+@pytest.mark.parametrize("kappa", [0.0, 10.0])
+def test_cht_adjoint_matches_finite_differences(kappa):
+    """The coupled loop (fluid wall reads the solid, solid ghost reads the
+    fluid after its step): fluid and solid directions together, and solid-only
+    directions (the gradient with respect to the solid's initial temperature)."""
+    import hom3_b200 as hb
+    cns, heat, gc, gh, qf, qs = cht_setup(kappa=kappa)
+    fgf, fgs = cns.first_ghost, heat.first_ghost
+    rng = np.random.default_rng(3)
+    lf = np.zeros_like(qf)
+    ls = np.zeros_like(qs)
+    lf[:, :fgf] = rng.standard_normal((qf.shape[0], fgf))
+    ls[:, :fgs] = rng.standard_normal((1, fgs))
+    n = 8
+    gf, gs, dts = hb.cht_adjoint(0.01, gc, gh, n, lf, ls, every=3)
+    assert np.isfinite(gf).all() and np.isfinite(gs).all()
+    worst = 0.0
+    for k in range(16):
+        df = np.zeros_like(qf)
+        ds = np.zeros_like(qs)
+        if k % 2 == 0:
+            df[:, :fgf] = rng.standard_normal((qf.shape[0], fgf))
+        ds[:, :fgs] = rng.standard_normal((1, fgs))
+        eps = 1e-6
+        fd = (cht_J(gc, gh, qf + eps * df, qs + eps * ds, dts, lf, ls)
+              - cht_J(gc, gh, qf - eps * df, qs - eps * ds, dts, lf, ls)) / (2 * eps)
+        ad = (gf * df).sum() + (gs * ds).sum()
+        scale = np.abs(gf * df).sum() + np.abs(gs * ds).sum()
+        worst = max(worst, abs(fd - ad) / scale)
+    assert worst <= 1e-6, worst
+
+
+def test_cht_adjoint_forward_is_the_coupled_loop():
+    import hom3_b200 as hb
+    cns, heat, gc, gh, qf, qs = cht_setup()
+    _, _, gc2, gh2, _, _ = cht_setup()
+    lf = np.zeros_like(qf)
+    ls = np.zeros_like(qs)
+    hb.cht_adjoint(0.01, gc, gh, 5, lf, ls, every=2)
+    for _ in range(5):
+        hb.couple_cht(0.01, gc2, gh2)
+        gc2.solve(1)
+        gh2.solve(1)
+    assert np.array_equal(gc.state(0)[:, :cns.first_ghost], gc2.state(0)[:, :cns.first_ghost])
+    assert np.array_equal(gh.state(0)[:, :heat.first_ghost], gh2.state(0)[:, :heat.first_ghost])
+    assert gc.step() == 5 and gh.step() == 5
