@@ -532,6 +532,7 @@ def run_cht(args, ws, rank, local):
     ms_loop = e0.elapsed_time(e1)
     Ts = heat.state(0)[0, :fgs]
     cells = fgf + fgs
+    adj = cht_adjoint_measure(args, d, make, Tr0) if args.adjoint_steps > 0 else None
     line = {"metric": "cell-updates/s", "value": cells * args.steps * ws / (ms * 1e-3), "unit": "cell-updates/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -542,8 +543,107 @@ def run_cht(args, ws, rank, local):
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "per_solver_loop_value": cells * args.steps / (ms_loop * 1e-3),
             "solid_T_range": [float(Ts.min()), float(Ts.max())], "time": cns.time()}
+    if adj is not None:
+        line["adjoint"] = adj
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def cht_adjoint_measure(args, d, make, Tr0):
+    """Adjoint of the total interface heat flux after N coupled steps with
+    respect to the solid's initial temperature (checkpoints every 100 steps,
+    time steps frozen): time against the forward loop, and central differences
+    of the frozen-dt coupled map in a few random solid directions (seed 2).
+    J = sum over the solid's interface ghosts of (T_b - T_g) = sum 2 (T_b - T_f) / (1 + kappa)."""
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    tf, ts = d["tables_fluid"], d["tables_solid"]
+    fgf, fgs = tf["first_ghost"], ts["first_ghost"]
+    n = min(args.steps, 2000)
+    kappa = float(d["conditions_solid"][3].values[0])
+    ghosts = np.arange(fgs, ts["ncells"])
+    coupled = ts["bc_idx"][fgs:] == 3
+    nb = ts["neighbors"][:, fgs:]
+    bcell = np.where((nb >= 0) & (nb < fgs), nb, -1).max(axis=0)
+    pf = d["partners_solid"]
+    c = 2.0 / (1.0 + kappa)
+
+    def objective(cns, heat):
+        qf, qs = cns.state(0), heat.state(0)
+        rho = qf[2]
+        T = 1.4 * 0.4 * (qf[3] - 0.5 * (qf[0] ** 2 + qf[1] ** 2) / rho) / rho
+        g = ghosts[coupled] - fgs
+        return float((c * (qs[0, bcell[g]] - T[pf[g]])).sum())
+
+    def cotangents(cns):
+        qf = cns.state(0)
+        lf, ls = np.zeros_like(qf), np.zeros((1, ts["ncells"]))
+        g = ghosts[coupled] - fgs
+        np.add.at(ls[0], bcell[g], c)
+        P = pf[g]
+        rho, u, v, E = qf[2, P], qf[0, P] / qf[2, P], qf[1, P] / qf[2, P], qf[3, P]
+        p = 0.4 * (E - 0.5 * rho * (u * u + v * v))
+        np.add.at(lf[0], P, -c * (-1.4 * 0.4 * u / rho))
+        np.add.at(lf[1], P, -c * (-1.4 * 0.4 * v / rho))
+        np.add.at(lf[2], P, -c * 1.4 * (0.5 * 0.4 * (u * u + v * v) - p / rho) / rho)
+        np.add.at(lf[3], P, -c * 1.4 * 0.4 / rho)
+        return lf, ls
+
+    # forward loop time and the final state's cotangents
+    cns, heat = make()
+    stream = torch.cuda.ExternalStream(cns.stream())  # the coupled pair's shared stream
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    hb.cht_solve(Tr0, cns, heat, n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd_ms = e0.elapsed_time(e1)
+    lf, ls = cotangents(cns)
+    J0 = objective(cns, heat)
+    cns, heat = make()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    gf, gs, dts = hb.cht_adjoint(Tr0, cns, heat, n, lf, ls, every=100)
+    adj_s = time.perf_counter() - t0
+    # the same call again with every launch bracketed by events: where the time goes
+    c3, h3 = make()
+    c3.profile(True)
+    h3.profile(True)
+    hb.cht_adjoint(Tr0, c3, h3, n, lf, ls, every=100)
+    torch.cuda.synchronize()
+    kern = {("fluid " + k): v for k, v in c3.profile_read().items()}
+    kern.update({("solid " + k): v for k, v in h3.profile_read().items()})
+    # lf, ls: dJ/dq_N, dJ/dT_N at the final states (J is linear in T, nonlinear in the fluid state)
+    rng = np.random.default_rng(2)
+
+    def J_of(Ts0):
+        c2, h2 = make()
+        h2.set_state(Ts0, 0)
+        h2.reset_time()
+        c2.reset_time()
+        for i in range(n):
+            c2.solve_dt([dts[0, i]])
+            h2.solve_dt([dts[1, i]])
+        return objective(c2, h2)
+
+    worst = 0.0
+    ndir = 4
+    for _ in range(ndir):
+        dT = np.zeros_like(d["q_solid"])
+        dT[0, :fgs] = rng.standard_normal(fgs)
+        eps = 1e-6
+        fd = (J_of(d["q_solid"] + eps * dT) - J_of(d["q_solid"] - eps * dT)) / (2 * eps)
+        ad = float((gs * dT).sum())
+        worst = max(worst, abs(fd - ad) / max(abs(fd), np.abs(gs * dT).sum() * 1e-3))
+    return {"steps": n, "checkpoint_every": 100, "objective": "sum of the interface heat flux at the last step",
+            "J": J0, "forward_ms": fwd_ms, "adjoint_ms": adj_s * 1e3, "ratio": adj_s * 1e3 / fwd_ms,
+            "fd_directions": ndir, "fd_worst_rel": worst,
+            "kernels_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in kern.items()},
+            "what": "h3c_cht_adjoint (forward with checkpoints, coupled recompute, backward; host arrays) / "
+                    "h3c_cht_solve of the same steps"}
 
 
 def measure_adjoint(s, q0, nsteps, stream, fg):

@@ -24,7 +24,10 @@
 
 namespace h3c {
 
-constexpr int kAdjDirs = 8;  // dual directions per pass
+#ifndef H3C_ADJ_DIRS
+#define H3C_ADJ_DIRS 2  // measured fastest on the 512 x 128 fluid: fewer registers spill
+#endif
+constexpr int kAdjDirs = H3C_ADJ_DIRS;  // dual directions per pass
 
 template <int K> __device__ __forceinline__ DN<K> nr_rcp(const DN<K>& a) {
   DN<K> r(nr_rcp(a.v));
