@@ -679,6 +679,18 @@ def measure_adjoint(s, q0, nsteps, stream, fg):
     fwd_ms = ev[0].elapsed_time(ev[1])
     adj_ms = ev[2].elapsed_time(ev[3])
     ak_ms, ak_n = kern.get("adjoint", (0.0, 0))
+    # the same adjoint with the per-cell gather in place of the tile kernel
+    from hom3_b200 import _ffi as F
+    s.set_option(F.OPT_TILE_KERNEL, 0)
+    s.set_state(q0, 0)
+    s.reset_time()
+    torch.cuda.synchronize()
+    s.profile(True)
+    s.adjoint(nsteps, lam, every=0, out=grad)
+    torch.cuda.synchronize()
+    s.profile(False)
+    gk_ms, gk_n = s.profile_read().get("adjoint", (0.0, 0))
+    s.set_option(F.OPT_TILE_KERNEL, 1)
     # algorithmic bytes of one adjoint-stage launch: stage state + cotangent in, cotangent out
     # (+ the extra cotangent of the second launch of a step, counted in the mean) and the tables
     b_launch = fg * (3 * 5 * 8 + 6 * 4 + 1) + 0.5 * fg * 5 * 8
@@ -686,6 +698,8 @@ def measure_adjoint(s, q0, nsteps, stream, fg):
             "what": "h3c_adjoint (forward with checkpoints + backward sweep, device cotangent) / h3c_solve of "
                     "the same steps; the library chose the checkpoint interval",
             "adjoint_kernel_ms": ak_ms / max(ak_n, 1), "adjoint_launches": ak_n,
+            "per_cell_gather_kernel_ms": gk_ms / max(gk_n, 1),
+            "kernels_ms": {k: round(v[0], 3) for k, v in kern.items()},
             "adjoint_kernel_gbs": b_launch / (ak_ms / max(ak_n, 1) * 1e-3) / 1e9 if ak_n else None,
             "grad_finite": bool(torch.isfinite(grad).all().item())}
 

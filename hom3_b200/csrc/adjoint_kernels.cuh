@@ -39,6 +39,14 @@ __device__ __forceinline__ double p_int_d(double s, double M) {
   return (0.25 * ((M + s) * (M + s))) * (2.0 - s * M);
 }
 
+// a[d] for a direction d known only at run time, by selects (no local-memory indexing)
+template <int N> __device__ __forceinline__ double pick(const double* a, int d) {
+  double r = a[0];
+#pragma unroll
+  for (int k = 1; k < N; ++k) r = d == k ? a[k] : r;
+  return r;
+}
+
 // primitive state of one side, all directions (Newton reciprocals as in make_prim)
 template <int ND> struct SideAD {
   double q[ND + 2];
@@ -69,7 +77,7 @@ __device__ __forceinline__ void side_reverse(const SideAD<ND>& S, int d, double 
   double ubar[ND];
 #pragma unroll
   for (int k = 0; k < ND; ++k) ubar[k] = k == d ? Mbar * S.ainv : 0.0;
-  abar -= Mbar * S.M[d] * S.ainv;
+  abar -= Mbar * pick<ND>(S.M, d) * S.ainv;
   const double a2bar = 0.5 * abar * S.ainv;
   pbar += a2bar * gamma * S.rinv;
   double rinvbar = a2bar * gamma * S.p;
@@ -90,7 +98,7 @@ template <int ND>
 __device__ __forceinline__ void ausm_vjp(const SideAD<ND>& SL, const SideAD<ND>& SR, int d, const double* w,
                                          double gamma, double gm1, double* gL, double* gR) {
   constexpr int NV = ND + 2;
-  const double ML = SL.M[d], MR = SR.M[d];
+  const double ML = pick<ND>(SL.M, d), MR = pick<ND>(SR.M, d);
   const double mi = m_int_d(1.0, ML) + m_int_d(-1.0, MR);
   const bool left = mi >= 0.0;
   const SideAD<ND>& Su = left ? SL : SR;
@@ -100,7 +108,7 @@ __device__ __forceinline__ void ausm_vjp(const SideAD<ND>& SL, const SideAD<ND>&
   for (int v = 0; v < NV - 1; ++v) wq += w[v] * Su.q[v];
   wq += w[NV - 1] * (Su.q[NV - 1] + Su.p);
   const double mbar = Su.a * wq;
-  const double pibar = w[d];
+  const double pibar = pick<ND>(w, d);
   const double MLbar = dm_int(1.0, ML) * mbar + dp_int(1.0, ML) * SL.p * pibar;
   const double MRbar = dm_int(-1.0, MR) * mbar + dp_int(-1.0, MR) * SR.p * pibar;
   double pLbar = p_int_d(1.0, ML) * pibar;
@@ -259,6 +267,293 @@ __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double
     if (extra) o += gamma_e * extra[v * ld + c];
     if (extra2) o += gamma_e2 * extra2[v * ld + c];
     gout[v * ld + c] = o;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Euler adjoint stage on the forward's Morton tiles.  The per-cell gather
+// above evaluates the reverse of every face twice, once from each side, and
+// its warps diverge between in-tile, border, ghost and coarse/fine faces.
+// Here every cell publishes its primitive side state and its weighted
+// cotangent k lambda in shared memory, then
+//   (1) every cell reverses its plus faces (one uniform call per direction:
+//       the neighbour comes from shared memory in the tile, else from global
+//       memory or its ghost condition) and, where the right cell is in the
+//       tile and points back (same level), stores that cell's half in the
+//       cell's minus-face slot;
+//   (2) the minus faces left over (tile border, ghost, coarse/fine) are
+//       compacted into a list that the block's threads work through;
+//   (3) every cell sums its plus faces and its minus-face slots in a fixed
+//       order: the result is deterministic.
+// Same result as k_adj_stage<ND, EULER> up to the order of the face sums.
+// Shared memory: side state [ND + 6][kBlock] (q, 1/rho, p, a, 1/a), k lambda
+// [ND + 2][kBlock], minus-face slots [ND][ND + 2][kBlock] of double, plus and
+// minus neighbours [2][ND][kBlock] of int, the work list [ND kBlock] of
+// ushort and the scan's warp totals.
+// ---------------------------------------------------------------------------
+template <int ND> __host__ __device__ constexpr size_t adj_ausm_smem_bytes() {
+  return sizeof(double) * ((ND + 6) + (ND + 2) + ND * (ND + 2)) * kBlock + sizeof(int) * 2 * ND * kBlock +
+         sizeof(unsigned short) * ND * kBlock + sizeof(int) * (kBlock / 32 + 1);
+}
+
+// side state of a cell from its published q, 1/rho, p, a, 1/a (the operations of side_forward)
+template <int ND> __device__ __forceinline__ void side_from_shared(SideAD<ND>& S, const double* ss, int t) {
+  constexpr int NV = ND + 2;
+#pragma unroll
+  for (int v = 0; v < NV; ++v) S.q[v] = ss[v * kBlock + t];
+  S.rinv = ss[NV * kBlock + t];
+  S.p = ss[(NV + 1) * kBlock + t];
+  S.a = ss[(NV + 2) * kBlock + t];
+  S.ainv = ss[(NV + 3) * kBlock + t];
+  S.um2 = 0.0;
+#pragma unroll
+  for (int k = 0; k < ND; ++k) {
+    S.u[k] = S.q[k] * S.rinv;
+    S.um2 = k == 0 ? S.u[k] * S.u[k] : S.um2 + S.u[k] * S.u[k];
+  }
+#pragma unroll
+  for (int k = 0; k < ND; ++k) S.M[k] = S.u[k] * S.ainv;
+}
+
+// Neighbour nb of a face read from global memory: its side state, the
+// weighted cotangent kn lambda of the cell whose residual holds the face on
+// its side (0 for a ghost, the paired cell for a periodic ghost) and the
+// ghost's condition Jacobian dq_ghost / dq_c = jac I (0 for interior cells).
+template <int ND>
+__device__ __forceinline__ void adj_neighbour(int nb, double kn_face, const double* __restrict__ q,
+                                              const double* __restrict__ lam, double alpha, double dt,
+                                              const Geometry& g, const GhostTables& gt, const PhysConst& pc,
+                                              SideAD<ND>& Sn, double* kln, double& jac) {
+  constexpr int NV = ND + 2;
+  const long long ld = g.ld;
+  jac = 0.0;
+  long long own = nb;
+  double kn = kn_face;
+  if (nb >= g.n_int) {
+    const long long i = nb - g.n_int;
+    const int b = gt.bc_apply[i];
+    own = -1;
+    kn = 0.0;
+    if (b != 255) {
+      const int kind = gt.bcs[b].kind;
+      if (kind == BC_PERIODIC) {
+        own = gt.partner[i];
+        if (own >= 0) kn = alpha * dt / g.len[g.lvl[own]];
+      } else {
+        jac = kind == BC_EULER_DIRICHLET ? -1.0 : 1.0;
+      }
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    Sn.q[v] = __ldg(q + v * ld + nb);
+    kln[v] = own >= 0 ? kn * __ldg(lam + v * ld + own) : 0.0;
+  }
+  side_forward<ND>(Sn, pc.gamma, pc.gm1);
+}
+
+#ifndef H3C_ADJT_MINB
+#define H3C_ADJT_MINB 2  // resident blocks per SM the tile adjoint is compiled for
+#endif
+// gout_c = beta lam_c + [VJP of (q -> alpha k R(q)) with cotangent lam]_c + gamma_e extra_c + gamma_e2 extra2_c
+template <int ND, bool HANG>
+__global__ void __launch_bounds__(kBlock, H3C_ADJT_MINB)
+    k_adj_ausm(const double* __restrict__ q, const double* __restrict__ lam, double* __restrict__ gout,
+               const double* __restrict__ extra, const double* __restrict__ extra2, double alpha, double beta,
+               double gamma_e, double gamma_e2, Geometry g, GhostTables gt, PhysConst pc,
+               const Scalars* __restrict__ sc) {
+  constexpr int NV = ND + 2;
+  constexpr int NS = 1 << (ND - 1);
+  constexpr double W = ND == 2 ? 0.5 : 0.25;
+  constexpr int NW = kBlock / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double* ss = reinterpret_cast<double*>(smem_raw);  // [ND + 6][kBlock]
+  double* skl = ss + (ND + 6) * kBlock;              // [NV][kBlock]
+  double* sg = skl + NV * kBlock;                    // [ND][NV][kBlock] minus-face slots
+  int* snp = reinterpret_cast<int*>(sg + ND * NV * kBlock);  // [ND][kBlock]
+  int* snm = snp + ND * kBlock;                               // [ND][kBlock]
+  unsigned short* sitem = reinterpret_cast<unsigned short*>(snm + ND * kBlock);  // [ND kBlock]
+  int* swarp = reinterpret_cast<int*>(sitem + ND * kBlock);                      // [NW + 1]
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const long long ld = g.ld;
+  const long long c0 = (long long)blockIdx.x * kBlock;
+  const long long c = c0 + tid;
+  const long long tile_end = min(c0 + (long long)kBlock, g.n_int);
+  const bool live = c < tile_end;
+  const double dt = sc->dt;
+  auto in_tile = [&](long long n) { return n >= c0 && n < tile_end; };
+
+  // ---- own loads, side state and k lambda -> shared memory ----
+  double hc = 1.0, kc = 0.0;
+  SideAD<ND> Sc;
+  if (live) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Sc.q[v] = __ldg(q + v * ld + c);
+    hc = g.len[g.lvl[c]];
+    kc = alpha * dt / hc;
+    side_forward<ND>(Sc, pc.gamma, pc.gm1);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      ss[v * kBlock + tid] = Sc.q[v];
+      skl[v * kBlock + tid] = kc * __ldg(lam + v * ld + c);
+    }
+    ss[NV * kBlock + tid] = Sc.rinv;
+    ss[(NV + 1) * kBlock + tid] = Sc.p;
+    ss[(NV + 2) * kBlock + tid] = Sc.a;
+    ss[(NV + 3) * kBlock + tid] = Sc.ainv;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      snm[d * kBlock + tid] = __ldg(g.nbr + (2 * d) * ld + c);
+      snp[d * kBlock + tid] = __ldg(g.nbr + (2 * d + 1) * ld + c);
+    }
+  }
+  __syncthreads();
+
+  // ---- (1) plus faces: c is the left cell of F(c, p) ----
+  double acc[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+  if (live) {
+#pragma unroll 1
+    for (int d = 0; d < ND; ++d) {
+      const int p = snp[d * kBlock + tid];
+      double gc[NV], gn[NV], w[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) { gc[v] = 0.0; gn[v] = 0.0; }
+      if (HANG && p < 0) {
+        // c is the coarse cell of a coarse/fine face: its residual takes W times each sub-face
+        const long long k = -p - 2;
+#pragma unroll 1
+        for (int j = 0; j < NS; ++j) {
+          const int f = __ldg(g.sub + j * g.nsub + k);
+          SideAD<ND> Sn;
+          double jac;
+          adj_neighbour<ND>(f, alpha * dt / g.len[g.lvl[f]], q, lam, alpha, dt, g, gt, pc, Sn, w, jac);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) w[v] = w[v] - W * skl[v * kBlock + tid];
+          ausm_vjp<ND>(Sc, Sn, d, w, pc.gamma, pc.gm1, gc, gn);
+        }
+      } else {
+        SideAD<ND> Sn;
+        double jac = 0.0;
+        bool give = false;
+        int t = 0;
+        if (in_tile(p)) {
+          t = (int)(p - c0);
+          side_from_shared<ND>(Sn, ss, t);
+          give = snm[d * kBlock + t] == (int)c;
+          // not pointing back: p is the coarse cell of a coarse/fine face
+          const double f = give ? 1.0 : (g.len[g.lvl[p]] > hc ? W : 1.0);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) w[v] = f * skl[v * kBlock + t];
+        } else {
+          const bool coarser = p < g.n_int && g.len[g.lvl[p]] > hc;
+          const double kp = p < g.n_int ? alpha * dt / g.len[g.lvl[p]] : 0.0;
+          adj_neighbour<ND>(p, coarser ? W * kp : kp, q, lam, alpha, dt, g, gt, pc, Sn, w, jac);
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) w[v] = w[v] - skl[v * kBlock + tid];
+        ausm_vjp<ND>(Sc, Sn, d, w, pc.gamma, pc.gm1, gc, gn);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) gc[v] += jac * gn[v];
+        if (give) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) sg[(d * NV + v) * kBlock + t] = gn[v];
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[v] += gc[v];
+    }
+  }
+
+  // ---- (2) minus faces no in-tile left cell covers -> work list ----
+  int need = 0;
+  if (live) {
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      const int m = snm[d * kBlock + tid];
+      const bool covered = in_tile(m) && snp[d * kBlock + (int)(m - c0)] == (int)c;
+      if (!covered) need |= 1 << d;
+    }
+  }
+  int cnt = __popc(need), incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) swarp[wid] = incl;
+  __syncthreads();
+  if (tid == 0) {
+    int run = 0;
+#pragma unroll
+    for (int k = 0; k < NW; ++k) {
+      const int x = swarp[k];
+      swarp[k] = run;
+      run += x;
+    }
+    swarp[NW] = run;
+  }
+  __syncthreads();
+  {
+    int pos = swarp[wid] + incl - cnt;
+#pragma unroll
+    for (int d = 0; d < ND; ++d)
+      if (need & (1 << d)) sitem[pos++] = (unsigned short)((tid << 2) | d);
+  }
+  const int total = swarp[NW];
+  __syncthreads();
+  for (int k = tid; k < total; k += kBlock) {
+    const int it = sitem[k];
+    const int t = it >> 2, d = it & 3;
+    const long long cc = c0 + t;
+    const int m = snm[d * kBlock + t];
+    const double hx = g.len[g.lvl[cc]];
+    SideAD<ND> Sx;
+    side_from_shared<ND>(Sx, ss, t);
+    double gx[NV], gn[NV], w[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) { gx[v] = 0.0; gn[v] = 0.0; }
+    if (HANG && m < 0) {
+      const long long k2 = -m - 2;
+#pragma unroll 1
+      for (int j = 0; j < NS; ++j) {
+        const int f = __ldg(g.sub + j * g.nsub + k2);
+        SideAD<ND> Sn;
+        double jac;
+        adj_neighbour<ND>(f, alpha * dt / g.len[g.lvl[f]], q, lam, alpha, dt, g, gt, pc, Sn, w, jac);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) w[v] = W * skl[v * kBlock + t] - w[v];
+        ausm_vjp<ND>(Sn, Sx, d, w, pc.gamma, pc.gm1, gn, gx);
+      }
+    } else {
+      const bool coarser = m < g.n_int && g.len[g.lvl[m]] > hx;
+      const double km = m < g.n_int ? alpha * dt / g.len[g.lvl[m]] : 0.0;
+      SideAD<ND> Sn;
+      double jac;
+      adj_neighbour<ND>(m, coarser ? W * km : km, q, lam, alpha, dt, g, gt, pc, Sn, w, jac);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) w[v] = skl[v * kBlock + t] - w[v];
+      ausm_vjp<ND>(Sn, Sx, d, w, pc.gamma, pc.gm1, gn, gx);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) gx[v] += jac * gn[v];
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) sg[(d * NV + v) * kBlock + t] = gx[v];
+  }
+  __syncthreads();
+
+  // ---- (3) sum: plus faces, then the minus-face slots ----
+  if (live) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      double o = beta * __ldg(lam + v * ld + c) + acc[v];
+#pragma unroll
+      for (int d = 0; d < ND; ++d) o += sg[(d * NV + v) * kBlock + tid];
+      if (extra) o += gamma_e * extra[v * ld + c];
+      if (extra2) o += gamma_e2 * extra2[v * ld + c];
+      gout[v * ld + c] = o;
+    }
   }
 }
 

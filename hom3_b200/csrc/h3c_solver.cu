@@ -337,6 +337,20 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
   k_stage<ND, PHYS, FLUX, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
       qin, out, s->d_slopes, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
 }
+// Euler adjoint stage in the tile kernel (one block per Morton tile)
+template <int ND, bool HANG>
+static void adj_ausm_t(h3c_solver s, const double* qin, const double* lamin, double* gout, const double* extra,
+                       const double* extra2, double alpha, double beta, double gam, double gam2) {
+  constexpr size_t smem = adj_ausm_smem_bytes<ND>();
+  static bool attr = false;  // one opt-in per instantiation (dynamic smem above 48 KB)
+  if (!attr) {
+    cudaFuncSetAttribute(k_adj_ausm<ND, HANG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  k_adj_ausm<ND, HANG><<<(unsigned)std::max<long long>(1, s->ntiles), kBlock, smem, s->stream>>>(
+      qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, geometry(s), ghosts(s), s->pc, s->d_sc);
+}
+
 template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG>
 void stage_f(h3c_solver s, const double* qin, double* out, bool fuse) {
   if (fuse) stage_t<ND, PHYS, FLUX, R, MODE, HANG, true>(s, qin, out);
@@ -1559,6 +1573,16 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
       return;
     }
     Launch La(s, K_OTHER);
+    if (s->desc.physics == H3C_EULER && s->tile) {
+      if (s->nd == 2) {
+        if (s->nsub > 0) adj_ausm_t<2, true>(s, qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2);
+        else adj_ausm_t<2, false>(s, qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2);
+      } else {
+        if (s->nsub > 0) adj_ausm_t<3, true>(s, qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2);
+        else adj_ausm_t<3, false>(s, qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2);
+      }
+      return;
+    }
     if (s->nd == 2) {
       if (s->desc.physics == H3C_HEAT)
         k_adj_stage<2, HEAT><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, nullptr, g, gt, s->pc, s->d_sc);

@@ -170,6 +170,49 @@ def test_autograd_function():
     assert np.abs(qn.detach().numpy()[:, :fg] - g3.state(0)[:, :fg]).max() <= 1e-13 * np.abs(q1).max()
 
 
+@pytest.mark.parametrize("name", ["euler2d_fe", "euler2d_rk2", "euler3d_rk2", "euler_dirichlet_rk2",
+                                  "periodic_vortex_rk2", "refined_fe", "refined_rk2"])
+def test_tile_adjoint_matches_per_cell_gather(name):
+    """The Euler adjoint stage on Morton tiles (in-tile faces reversed once,
+    halves handed over through shared memory) against the per-cell gather
+    that reverses every face from both sides: the same sums in another
+    order (the forward's stage kernel follows the option as well)."""
+    from hom3_b200 import _ffi as F
+    o, g, q1, lam = setup(name)
+    fg = o.first_ghost
+    out = {}
+    for tile in (1, 0):
+        g.set_option(F.OPT_TILE_KERNEL, tile)
+        g.set_state(q1, 0)
+        g.reset_time()
+        out[tile] = g.adjoint(NSTEPS, lam, every=4)
+    # the option switches the forward's stage kernel too (same sums, other order)
+    assert np.abs(out[0][1] - out[1][1]).max() <= 1e-13 * out[0][1].max()
+    scale = np.abs(out[0][0][:, :fg]).max()
+    assert np.abs(out[1][0][:, :fg] - out[0][0][:, :fg]).max() <= 1e-12 * scale
+
+
+def test_tile_adjoint_on_a_large_refined_tree():
+    """Many tiles, tile-border, ghost and coarse/fine faces (3D, +2 levels):
+    tile kernel against the per-cell gather after 6 RK2 steps."""
+    from hom3_b200 import _ffi as F
+    _, (o,) = cases.refined_case(level=4, fine=6)
+    q1 = cases.smooth_state(o)
+    o.set_state(q1)
+    g = cases.gpu_solver_from_oracle(o)
+    fg = o.first_ghost
+    lam = np.zeros_like(q1)
+    lam[:, :fg] = np.random.default_rng(3).standard_normal((q1.shape[0], fg))
+    out = {}
+    for tile in (1, 0):
+        g.set_option(F.OPT_TILE_KERNEL, tile)
+        g.set_state(q1, 0)
+        g.reset_time()
+        out[tile] = g.adjoint(6, lam, every=0)[0]
+    scale = np.abs(out[0][:, :fg]).max()
+    assert np.abs(out[1][:, :fg] - out[0][:, :fg]).max() <= 1e-12 * scale
+
+
 def test_unsupported_configurations_are_rejected():
     import hom3_b200 as hb
     _, (o,) = cases.euler_case("sod", nd=2, level=4, flux=h3o.LLF)
