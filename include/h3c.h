@@ -225,7 +225,7 @@ int h3c_status(h3c_solver s, int* flags);
  * 3 first stage / forward Euler, 4 second RK stage, 5 slopes, 7 adjoint stages) and resets. */
 int h3c_launches(h3c_solver s, int64_t* n);
 /* Execution options (no hom3 counterpart; results do not depend on them):
- * H3C_OPT_TILE_KERNEL  Euler stages in the shared-memory tile kernel (default 1)
+ * H3C_OPT_TILE_KERNEL  Euler stages and their adjoint in the shared-memory tile kernels (default 1)
  * H3C_OPT_GRAPHS       replay runs of steps from a captured CUDA graph (default 1) */
 #define H3C_OPT_TILE_KERNEL 1
 #define H3C_OPT_GRAPHS 2
