@@ -13,15 +13,15 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libhom3_b200.so")
 
 # constants of include/h3c.h
 OK, E_INVALID, E_CUDA, E_NONFINITE, E_STATE, E_TIMEOUT, E_NOMEM = 0, -1, -2, -3, -4, -5, -6
-EULER, CNS, HEAT = 0, 1, 2
-FLUX_AUSM, FLUX_LLF = 0, 1
+EULER, CNS, HEAT, ADVECTION = 0, 1, 2, 3
+FLUX_AUSM, FLUX_LLF, FLUX_UPWIND = 0, 1, 2
 EULER_FORWARD, RUNGE_KUTTA_2, SSPRK3 = 0, 1, 2
 RECON_NONE, RECON_MUSCL = 0, 1
 FP64, MIXED = 0, 1
 (BC_EULER_NEUMANN, BC_EULER_DIRICHLET, BC_EULER_VORTEX, BC_CNS_INFLOW, BC_CNS_OUTFLOW,
  BC_CNS_ADIABATIC_NOSLIP, BC_CNS_ADIABATIC_SLIP, BC_CNS_ISOTHERMAL_NOSLIP, BC_HEAT_DIRICHLET,
  BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT,
- BC_PERIODIC) = range(15)
+ BC_PERIODIC, BC_ADV_DIRICHLET, BC_ADV_NEUMANN, BC_ADV_CHARACTERISTIC) = range(18)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
 OPT_TILE_KERNEL, OPT_GRAPHS = 1, 2
 KERNEL_KINDS = ("bc", "cfl", "scalar", "stage1", "stage2", "slopes", "copy", "adjoint")
@@ -70,6 +70,7 @@ SIGNATURES = {
     "h3c_autotune": (_i32, [_vp, _i32, _P(_i32), _P(_dbl)]),
     "h3c_set_state": (_i32, [_vp, _i32, _P(_dbl), _i64]),
     "h3c_get_state": (_i32, [_vp, _i32, _P(_dbl), _i64]),
+    "h3c_set_velocity": (_i32, [_vp, _P(_dbl), _i64]),
     "h3c_state_device": (_i32, [_vp, _i32, _P(_P(_dbl)), _P(_i64)]),
     "h3c_device_order": (_i32, [_vp, _P(_i64)]),
     "h3c_get_stream": (_i32, [_vp, _P(_vp)]),

@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double
                                                       double gamma_e, double gamma_e2, double* __restrict__ xbar,
                                                       Geometry g,
                                                       GhostTables gt, PhysConst pc, const Scalars* __restrict__ sc) {
-  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  constexpr int NV = nvars<ND, PHYS>();
   constexpr int NS = 1 << (ND - 1);
   constexpr double W = ND == 2 ? 0.5 : 0.25;
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -18,14 +18,18 @@ constexpr int kBlock = 256;
 constexpr int kMaxLevels = 32;
 constexpr int kMaxBcs = 64;
 
-enum Physics { EULER = 0, CNS = 1, HEAT = 2 };
-enum Flux { AUSM = 0, LLF = 1 };
+enum Physics { EULER = 0, CNS = 1, HEAT = 2, ADVECTION = 3 };
+enum Flux { AUSM = 0, LLF = 1, UPWIND = 2 };
+// variables per cell: Euler/CNS (rho u_d, rho, rho E); heat T; advection q
+template <int ND, int PHYS> __host__ __device__ constexpr int nvars() {
+  return (PHYS == HEAT || PHYS == ADVECTION) ? 1 : ND + 2;
+}
 enum BcKind {
   BC_EULER_NEUMANN = 0, BC_EULER_DIRICHLET = 1, BC_EULER_VORTEX = 2, BC_CNS_INFLOW = 3,
   BC_CNS_OUTFLOW = 4, BC_CNS_ADIABATIC_NOSLIP = 5, BC_CNS_ADIABATIC_SLIP = 6,
   BC_CNS_ISOTHERMAL_NOSLIP = 7, BC_HEAT_DIRICHLET = 8, BC_HEAT_NEUMANN = 9,
   BC_CPL_EULER_EULER = 10, BC_CPL_CNS_HEAT = 11, BC_CPL_HEAT_CNS = 12, BC_CPL_HEAT_HEAT = 13,
-  BC_PERIODIC = 14
+  BC_PERIODIC = 14, BC_ADV_DIRICHLET = 15, BC_ADV_NEUMANN = 16, BC_ADV_CHARACTERISTIC = 17
 };
 
 // Device-resident step scalars (solver.hpp:406-416) and reduction slots.
@@ -72,6 +76,8 @@ struct Geometry {
   const int* __restrict__ blk_inst;
   const long long* __restrict__ inst_end;
   long long ntiles;
+  // advection velocity u(x_center) of every cell, ghosts included: [nd][ld] (nullptr otherwise)
+  const double* __restrict__ vel;
 };
 
 __device__ __forceinline__ int tile_instance(const Geometry& g, long long tile) {
@@ -315,11 +321,18 @@ __device__ __forceinline__ void viscous(const Prim<R, ND>& L, const Prim<R, ND>&
 
 // ---------------------------------------------------------------------------
 // per-cell time step: euler/physics.hpp:182-196, cns/physics.hpp:167-187,
-// heat/physics.hpp:82-85
+// heat/physics.hpp:82-85, advection/physics.hpp:86-93 (u: the cell's velocity)
 // ---------------------------------------------------------------------------
 template <int ND, int PHYS>
-__device__ __forceinline__ double cell_dt(const double* q, double h, const PhysConst& pc) {
+__device__ __forceinline__ double cell_dt(const double* q, double h, const PhysConst& pc,
+                                          const double* u = nullptr) {
   if (PHYS == HEAT) return pc.cfl * 0.5 * (h * h);
+  if (PHYS == ADVECTION) {
+    double u_max = -1.7976931348623157e308;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) u_max = fmax(u_max, fabs(u[d]));
+    return pc.cfl * h / u_max;
+  }
   Prim<double, ND> P;
 #pragma unroll
   for (int v = 0; v < ND + 2; ++v) P.q[v] = q[v];
@@ -343,7 +356,7 @@ __device__ __forceinline__ double cell_dt(const double* q, double h, const PhysC
 template <int ND, int PHYS>
 __global__ void __launch_bounds__(kBlock) k_cfl(const double* __restrict__ q, Geometry g, PhysConst pc,
                                                 long long* dst) {
-  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  constexpr int NV = nvars<ND, PHYS>();
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int inst = tile_instance(g, blockIdx.x);
   long long o = kOrdMax;
@@ -351,7 +364,12 @@ __global__ void __launch_bounds__(kBlock) k_cfl(const double* __restrict__ q, Ge
     double qc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) qc[v] = __ldg(q + v * g.ld + c);
-    const double dt = cell_dt<ND, PHYS>(qc, g.len[g.lvl[c]], pc);
+    double uc[ND];
+    if (PHYS == ADVECTION) {
+#pragma unroll
+      for (int d = 0; d < ND; ++d) uc[d] = __ldg(g.vel + d * g.ld + c);
+    }
+    const double dt = cell_dt<ND, PHYS>(qc, g.len[g.lvl[c]], pc, uc);
     if (!isnan(dt)) o = dbl_to_ord(dt);
   }
   block_min_atomic(o, per_instance(dst, inst));
@@ -436,7 +454,7 @@ template <int ND, int PHYS>
 __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const double* __restrict__ qlhs,
                                                Geometry g, GhostTables gt, PhysConst pc,
                                                const Scalars* __restrict__ sc, PartnerView pv) {
-  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  constexpr int NV = nvars<ND, PHYS>();
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= gt.ng) return;
   const int b = gt.bc_apply[i];
@@ -488,6 +506,21 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
       for (int v = 0; v < NV; ++v) out[v] = q[v * ld + o];
       break;
     }
+    case BC_ADV_NEUMANN:  // advection/boundary_conditions.hpp:56-63
+      out[0] = qb[0] - gt.dx[i] * B.v[0];
+      break;
+    case BC_ADV_DIRICHLET:  // :29-35
+      out[0] = 2.0 * B.v[0] - qb[0];
+      break;
+    case BC_ADV_CHARACTERISTIC: {  // :79-95
+      // inflow (the boundary cell's velocity along the ghost's direction points into the domain):
+      // dirichlet(q_b, q_b); otherwise neumann(q_b, 0, dx).  Both are q_b.
+      const int pos = gt.pos[i];
+      const double v = g.vel ? g.vel[(pos >> 1) * ld + bc] : 0.0;
+      const bool inflow = (v > 0. && (pos & 1) == 0) || (v < 0. && (pos & 1) == 1);
+      out[0] = inflow ? 2.0 * qb[0] - qb[0] : qb[0] - gt.dx[i] * 0.0;
+      break;
+    }
     case BC_CPL_HEAT_CNS:     // heat/coupling_conditions.hpp:233-246
     case BC_CPL_HEAT_HEAT: {  // :256-269
       if (gt.partner[i] < 0 || pv.q == nullptr) return;
@@ -501,7 +534,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
       break;
     }
     default: {
-      if (PHYS == HEAT) { out[0] = qb[0]; break; }
+      if (NV == 1) { out[0] = qb[0]; break; }
       const double gamma = pc.gamma;
       // pv of the boundary cell: euler/quantities.hpp:173-186
       double bp[ND + 2], gp[ND + 2];
@@ -634,7 +667,7 @@ template <int ND, int PHYS, int FLUX, class R, int MODE, bool HANG, bool FUSE>
 __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin, double* out,
                                                   const double* __restrict__ sl, Geometry g, PhysConst pc,
                                                   const Scalars* __restrict__ sc, long long* dtmin) {
-  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  constexpr int NV = nvars<ND, PHYS>();
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int inst = tile_instance(g, blockIdx.x);
   const bool live = c < instance_end(g, inst);
@@ -650,7 +683,52 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] = 0.0;
 
-    if (PHYS == HEAT) {
+    if (PHYS == ADVECTION) {
+      // advection/physics.hpp:130-153 on the cells' velocities along d: local Lax-Friedrichs,
+      // or hom3's upwind flux u_L q_L, negated when the face velocity (u_L + u_R) / 2 is negative
+      auto adv_flux = [&](double qL, double qR, double uL, double uR) {
+        if (FLUX == LLF) {
+          const double lambda_max = fmax(fabs(uL), fabs(uR));
+          return 0.5 * (qL * uL + qR * uR + lambda_max * (qL - qR));
+        }
+        const double u_srfc = 0.5 * (uL + uR);
+        const double f = uL * qL;
+        return u_srfc < 0 ? f * -1. : f;
+      };
+#pragma unroll
+      for (int d = 0; d < ND; ++d) {
+        const double uc = __ldg(g.vel + d * ld + c);
+        const int m = g.nbr[(2 * d) * ld + c], p = g.nbr[(2 * d + 1) * ld + c];
+        double fm, fp;
+        if (!HANG || m >= 0) {
+          fm = adv_flux(__ldg(qin + m), qc[0], __ldg(g.vel + d * ld + m), uc);
+        } else {
+          const long long k = -m - 2;
+          double ws = 0;
+#pragma unroll
+          for (int j = 0; j < (1 << (ND - 1)); ++j) {
+            const int n = g.sub[j * g.nsub + k];
+            const double f = adv_flux(__ldg(qin + n), qc[0], __ldg(g.vel + d * ld + n), uc);
+            ws = j == 0 ? f : ws + f;
+          }
+          fm = (ND == 2 ? 0.5 : 0.25) * ws;
+        }
+        if (!HANG || p >= 0) {
+          fp = adv_flux(qc[0], __ldg(qin + p), uc, __ldg(g.vel + d * ld + p));
+        } else {
+          const long long k = -p - 2;
+          double ws = 0;
+#pragma unroll
+          for (int j = 0; j < (1 << (ND - 1)); ++j) {
+            const int n = g.sub[j * g.nsub + k];
+            const double f = adv_flux(qc[0], __ldg(qin + n), uc, __ldg(g.vel + d * ld + n));
+            ws = j == 0 ? f : ws + f;
+          }
+          fp = (ND == 2 ? 0.5 : 0.25) * ws;
+        }
+        acc[0] = acc[0] + (fm - fp);
+      }
+    } else if (PHYS == HEAT) {
       // three_point: heat/physics.hpp:113-119, (1/dx)(T_l - T_r)
       const double idx = 1 / dx;
 #pragma unroll
@@ -781,7 +859,12 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
     if (FUSE) {
-      const double cd = cell_dt<ND, PHYS>(o, dx, pc);
+      double uc[ND];
+      if (PHYS == ADVECTION) {
+#pragma unroll
+        for (int d = 0; d < ND; ++d) uc[d] = __ldg(g.vel + d * ld + c);
+      }
+      const double cd = cell_dt<ND, PHYS>(o, dx, pc, uc);
       if (!isnan(cd)) ord = dbl_to_ord(cd);
     }
   }

@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(h3c::kBlock) k_cfl_partials(const double* __re
                                                                const double* __restrict__ len, long long n,
                                                                h3c::PhysConst pc, long long* partials) {
   using namespace h3c;
-  constexpr int NV = PHYS == HEAT ? 1 : ND + 2;
+  constexpr int NV = nvars<ND, PHYS>();
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   long long v = kOrdMax;
   if (c < n) {

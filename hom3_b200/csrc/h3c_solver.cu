@@ -60,6 +60,8 @@ struct h3c_solver_s {
   double* d_gdx = nullptr;
   int* d_gpartner = nullptr;
   double* d_xc = nullptr;
+  double* d_vel = nullptr;  // advection velocity [nd][ld], internal numbering, ghosts included
+  bool vel_set = false;
   int n_bcs = 0;
   std::vector<h3c_bc> bcs;
   std::vector<BcParam> h_bcs;
@@ -150,6 +152,8 @@ void free_grid(h3c_solver s) {
   dfree(s->d_gapply); dfree(s->d_gown); dfree(s->d_gdx); dfree(s->d_gpartner); dfree(s->d_xc);
   dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_q[2]); dfree(s->d_slopes); dfree(s->d_stage);
   dfree(s->d_dev2caller);
+  dfree(s->d_vel);
+  s->vel_set = false;
   dfree(s->d_blk_inst); dfree(s->d_inst_end); dfree(s->d_ginst);
   dfree(s->d_adj);
   s->adj_cap = 0;
@@ -170,6 +174,7 @@ Geometry geometry(const h3c_solver s) {
   g.blk_inst = s->n_inst > 1 ? s->d_blk_inst : nullptr;
   g.inst_end = s->n_inst > 1 ? s->d_inst_end : nullptr;
   g.ntiles = s->ntiles;
+  g.vel = s->d_vel;
   return g;
 }
 
@@ -240,10 +245,12 @@ void launch_bc_ptr(h3c_solver s, double* q, const double* qlhs) {
   if (s->nd == 2) {
     if (s->desc.physics == H3C_EULER) launch_bc_t<2, EULER>(s, q, qlhs);
     else if (s->desc.physics == H3C_CNS) launch_bc_t<2, CNS>(s, q, qlhs);
+    else if (s->desc.physics == H3C_ADVECTION) launch_bc_t<2, ADVECTION>(s, q, qlhs);
     else launch_bc_t<2, HEAT>(s, q, qlhs);
   } else {
     if (s->desc.physics == H3C_EULER) launch_bc_t<3, EULER>(s, q, qlhs);
     else if (s->desc.physics == H3C_CNS) launch_bc_t<3, CNS>(s, q, qlhs);
+    else if (s->desc.physics == H3C_ADVECTION) launch_bc_t<3, ADVECTION>(s, q, qlhs);
     else launch_bc_t<3, HEAT>(s, q, qlhs);
   }
 }
@@ -255,6 +262,7 @@ void launch_cfl_t(h3c_solver s, long long* slot) {
   k_cfl<ND, PHYS><<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_q[0], geometry(s), s->pc, slot);
 }
 void launch_cfl(h3c_solver s, long long* slot) {
+  if (s->desc.physics == H3C_ADVECTION && !s->vel_set) return;  // no velocity yet: no time step
   {
     Launch L(s, K_SCALAR);
     k_reset_slot<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(slot, s->n_inst);
@@ -262,10 +270,12 @@ void launch_cfl(h3c_solver s, long long* slot) {
   if (s->nd == 2) {
     if (s->desc.physics == H3C_EULER) launch_cfl_t<2, EULER>(s, slot);
     else if (s->desc.physics == H3C_CNS) launch_cfl_t<2, CNS>(s, slot);
+    else if (s->desc.physics == H3C_ADVECTION) launch_cfl_t<2, ADVECTION>(s, slot);
     else launch_cfl_t<2, HEAT>(s, slot);
   } else {
     if (s->desc.physics == H3C_EULER) launch_cfl_t<3, EULER>(s, slot);
     else if (s->desc.physics == H3C_CNS) launch_cfl_t<3, CNS>(s, slot);
+    else if (s->desc.physics == H3C_ADVECTION) launch_cfl_t<3, ADVECTION>(s, slot);
     else launch_cfl_t<3, HEAT>(s, slot);
   }
 }
@@ -385,6 +395,10 @@ void stage_nd(h3c_solver s, int mode, const double* qin, double* out, bool fuse)
       if (mixed) stage_m<ND, CNS, AUSM, float>(s, mode, qin, out, fuse);
       else stage_m<ND, CNS, AUSM, double>(s, mode, qin, out, fuse);
       break;
+    case H3C_ADVECTION:
+      if (s->desc.flux == H3C_FLUX_LLF) stage_m<ND, ADVECTION, LLF, double>(s, mode, qin, out, fuse);
+      else stage_m<ND, ADVECTION, UPWIND, double>(s, mode, qin, out, fuse);
+      break;
     default:
       stage_m<ND, HEAT, AUSM, double>(s, mode, qin, out, fuse);
   }
@@ -461,7 +475,7 @@ int h3c_last_error(h3c_solver s, char* buf, size_t n) {
 int h3c_create(const h3c_desc* d, h3c_solver* out) {
   if (!d || !out) { g_last_error = "h3c_create: null argument"; return H3C_E_INVALID; }
   if (d->nd != 2 && d->nd != 3) { g_last_error = "h3c_create: nd must be 2 or 3"; return H3C_E_INVALID; }
-  if (d->physics < 0 || d->physics > 2 || d->flux < 0 || d->flux > 1 || d->time_integration < 0 ||
+  if (d->physics < 0 || d->physics > 3 || d->flux < 0 || d->flux > 2 || d->time_integration < 0 ||
       d->time_integration > 2 || d->precision < 0 || d->precision > 1 || d->reconstruction < 0 ||
       d->reconstruction > 1) {
     g_last_error = "h3c_create: unknown physics / flux / time integration / precision";
@@ -475,10 +489,16 @@ int h3c_create(const h3c_desc* d, h3c_solver* out) {
     g_last_error = "h3c_create: CNS supports the standard flux (AUSM + three-point) only";
     return H3C_E_INVALID;
   }
+  if ((d->physics == H3C_ADVECTION) != (d->flux == H3C_FLUX_UPWIND) &&
+      !(d->physics == H3C_ADVECTION && d->flux == H3C_FLUX_LLF)) {
+    g_last_error = "h3c_create: advection takes the upwind or LLF flux (advection/tags.hpp:18-19); "
+                   "the upwind flux is advection's";
+    return H3C_E_INVALID;
+  }
   auto s = std::make_unique<h3c_solver_s>();
   s->desc = *d;
   s->nd = d->nd;
-  s->nv = d->physics == H3C_HEAT ? 1 : d->nd + 2;
+  s->nv = (d->physics == H3C_HEAT || d->physics == H3C_ADVECTION) ? 1 : d->nd + 2;
   // quantities: euler/quantities.hpp:131-145, cns/quantities.hpp:377-384
   const double gamma = d->gamma, gm1 = gamma - 1.;
   const double T_inf = 1.0 / (1 + 0.5 * gm1 * (d->Minfty * d->Minfty));
@@ -750,7 +770,11 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   for (size_t q = 0; q < ubcs.size(); ++q) {
     BcParam& B = s->h_bcs[q];
     B.kind = ubcs[q].kind;
-    if (B.kind < 0 || B.kind > H3C_BC_PERIODIC) return s->fail(H3C_E_INVALID, "h3c_set_grid: bc kind %d", B.kind);
+    if (B.kind < 0 || B.kind > H3C_BC_ADV_CHARACTERISTIC)
+      return s->fail(H3C_E_INVALID, "h3c_set_grid: bc kind %d", B.kind);
+    const bool adv_kind = B.kind >= H3C_BC_ADV_DIRICHLET;
+    if (adv_kind != (s->desc.physics == H3C_ADVECTION) && B.kind != H3C_BC_PERIODIC)
+      return s->fail(H3C_E_INVALID, "h3c_set_grid: bc kind %d does not belong to this physics", B.kind);
     B.wall = (B.kind == H3C_BC_CNS_ADIABATIC_NOSLIP || B.kind == H3C_BC_CNS_ISOTHERMAL_NOSLIP ||
               B.kind == H3C_BC_CPL_CNS_HEAT);
     for (int j = 0; j < 8; ++j) B.v[j] = ubcs[q].v[j];
@@ -835,6 +859,8 @@ static int ready(h3c_solver s, const char* what) {
     return s->fail(H3C_E_STATE, "%s: coupling conditions without h3c_set_partner", what);
   if (s->needs_periodic && !s->periodic_set)
     return s->fail(H3C_E_STATE, "%s: periodic conditions without h3c_set_periodic", what);
+  if (s->desc.physics == H3C_ADVECTION && !s->vel_set)
+    return s->fail(H3C_E_STATE, "%s: advection without h3c_set_velocity", what);
   return H3C_OK;
 }
 
@@ -863,6 +889,33 @@ int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld) {
   if (which == 0) launch_cfl(s, &s->d_sc->dtmin_ord);
   H3C_CUDA(s, cudaStreamSynchronize(s->stream));
   return s->cuda(cudaGetLastError(), "h3c_set_state");
+}
+
+int h3c_set_velocity(h3c_solver s, const double* u, int64_t ld) {
+  if (!s || !u) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_set_velocity: no grid");
+  if (s->desc.physics != H3C_ADVECTION) return s->fail(H3C_E_INVALID, "h3c_set_velocity: not an advection solver");
+  const long long nc = s->n_caller;
+  if (ld < nc) return s->fail(H3C_E_INVALID, "h3c_set_velocity: ld < n_cells");
+  for (int d = 0; d < s->nd; ++d)
+    for (long long c = 0; c < nc; ++c)
+      if (!std::isfinite(u[d * ld + c])) return s->fail(H3C_E_INVALID, "h3c_set_velocity: non-finite velocity");
+  if (!s->d_vel) H3C_CUDA(s, cudaMalloc(&s->d_vel, sizeof(double) * s->nd * s->ld));
+  H3C_CUDA(s, cudaMemsetAsync(s->d_vel, 0, sizeof(double) * s->nd * s->ld, s->stream));
+  double* tmp = nullptr;
+  H3C_CUDA(s, cudaMalloc(&tmp, sizeof(double) * s->nd * nc));
+  for (int d = 0; d < s->nd; ++d)
+    cudaMemcpyAsync(tmp + d * nc, u + d * ld, sizeof(double) * nc, cudaMemcpyHostToDevice, s->stream);
+  k_gather<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(tmp, nc, s->d_vel, s->ld, s->d_dev2caller, s->n_tot, s->nd);
+  const cudaError_t e = cudaStreamSynchronize(s->stream);
+  cudaFree(tmp);
+  if (e != cudaSuccess) return s->cuda(e, "h3c_set_velocity");
+  s->vel_set = true;
+  drop_graph(s);
+  // the time step depends on the velocity: recompute the next step's dt from the current lhs
+  launch_cfl(s, &s->d_sc->dtmin_ord);
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  return s->cuda(cudaGetLastError(), "h3c_set_velocity");
 }
 
 int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld) {
@@ -1057,6 +1110,8 @@ static int read_scalars(h3c_solver s, Scalars* out) {
 int h3c_min_dt(h3c_solver s, double* dt) {
   if (!s || !dt) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_min_dt: no grid");
+  if (s->desc.physics == H3C_ADVECTION && !s->vel_set)
+    return s->fail(H3C_E_STATE, "h3c_min_dt: advection without h3c_set_velocity");
   launch_cfl(s, &s->d_sc->mindt_ord);
   Scalars sc;
   int rc = read_scalars(s, &sc);

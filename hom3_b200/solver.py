@@ -128,6 +128,18 @@ def heat_neumann(q):
     return Condition(F.BC_HEAT_NEUMANN, [q])
 
 
+def adv_dirichlet(value):
+    return Condition(F.BC_ADV_DIRICHLET, [value])
+
+
+def adv_neumann(flux):
+    return Condition(F.BC_ADV_NEUMANN, [flux])
+
+
+def adv_characteristic():
+    return Condition(F.BC_ADV_CHARACTERISTIC)
+
+
 # ---------------------------------------------------------------------------
 # thin solver over the ABI
 # ---------------------------------------------------------------------------
@@ -146,7 +158,7 @@ class Solver:
             setattr(d, k, float(v))
         self.desc = d
         self.nd, self.physics = nd, physics
-        self.nv = 1 if physics == F.HEAT else nd + 2
+        self.nv = 1 if physics in (F.HEAT, F.ADVECTION) else nd + 2
         h = C.c_void_p()
         check(lib().h3c_create(C.byref(d), C.byref(h)))
         self.h = h
@@ -190,6 +202,13 @@ class Solver:
         q = np.ascontiguousarray(q, np.float64)
         assert q.shape == (self.nv, self.n_cells), q.shape
         self._check(lib().h3c_set_state(self.h, which, _dp(q), self.n_cells))
+
+    def set_velocity(self, u):
+        """Advection velocity u(x_center) of every cell, ghosts included: [nd][n_cells]
+        (Physics::velocity, advection/physics.hpp:116-118)."""
+        u = np.ascontiguousarray(u, np.float64)
+        assert u.shape == (self.nd, self.n_cells), u.shape
+        self._check(lib().h3c_set_velocity(self.h, _dp(u), self.n_cells))
 
     def state(self, which=LHS, out=None) -> np.ndarray:
         if out is None:
@@ -505,11 +524,13 @@ class FvSolver(Solver):
 
     def __init__(self, grid: GridSpec, properties: dict, physics=F.EULER, flux=F.FLUX_AUSM,
                  time_integration=F.EULER_FORWARD, precision=F.FP64):
-        props = {k: v for k, v in properties.items() if k not in ("initialDomain", "initialCondition")}
+        props = {k: v for k, v in properties.items() if k not in ("initialDomain", "initialCondition", "velocity")}
         super().__init__(grid.nd, physics, flux, time_integration, precision, **props)
         self.grid = grid
         self.initial_domain = properties.get("initialDomain", (None, 0))
         self.initial_condition = properties.get("initialCondition")
+        # advection: the "velocity" property, a function of the cell centre (advection/physics.hpp:36-37)
+        self.velocity = properties.get("velocity")
         self.bcs: list = []
         self.tables: Optional[dict] = None
 
@@ -529,6 +550,10 @@ class FvSolver(Solver):
         self.tables = t
         self.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
                       [c for _, c in self.bcs], t["subface_cells"])
+        if self.physics == F.ADVECTION:
+            xc = t["x_center"]
+            self.set_velocity(np.stack([np.asarray(self.velocity(xc[:, c]), np.float64)
+                                        for c in range(t["ncells"])], axis=1))
         q = np.zeros((self.nv, t["ncells"]))
         fg = t["first_ghost"]
         if self.initial_condition is not None:

@@ -42,15 +42,22 @@ extern "C" {
 #define H3C_E_TIMEOUT (-5)   /* a bounded device wait ran out */
 #define H3C_E_NOMEM (-6)     /* device allocation failed */
 
-/* physics: euler/physics.hpp:25, cns/physics.hpp:27, heat/physics.hpp:21 */
+/* physics: euler/physics.hpp:25, cns/physics.hpp:27, heat/physics.hpp:21,
+ * advection/physics.hpp:21-162 (one scalar q carried by a given velocity
+ * field u(x), h3c_set_velocity) */
 #define H3C_EULER 0
 #define H3C_CNS 1
 #define H3C_HEAT 2
+#define H3C_ADVECTION 3
 /* numerical flux tags: euler/tags.hpp:13-16 (AUSM, LLF); cns/tags.hpp:29
  * (standard = AUSM + three-point viscous, selected by H3C_CNS + AUSM);
  * heat/tags.hpp:13 (three_point, the only heat flux). */
 #define H3C_FLUX_AUSM 0
 #define H3C_FLUX_LLF 1
+/* advection/tags.hpp:18-19: local Lax-Friedrichs (H3C_FLUX_LLF) or upwind.
+ * hom3's upwind flux is u_L q_L, negated when the face velocity
+ * (u_L + u_R)/2 is negative (advection/physics.hpp:142-153); reproduced. */
+#define H3C_FLUX_UPWIND 2
 /* time integration tags: solver/fv/tags.hpp:24-25 */
 #define H3C_EULER_FORWARD 0
 #define H3C_RUNGE_KUTTA_2 1
@@ -81,6 +88,9 @@ extern "C" {
  *  CNS_ISOTHERMAL_NOSLIP  v[0] = wall temperature (:200-238)
  *  HEAT_DIRICHLET     v[0] = surface temperature (heat/boundary_conditions.hpp:15-37)
  *  HEAT_NEUMANN       v[0] = surface heat flux (:40-63)
+ *  ADV_DIRICHLET      v[0] = surface value (advection/boundary_conditions.hpp:17-42)
+ *  ADV_NEUMANN        v[0] = surface flux (:45-70)
+ *  ADV_CHARACTERISTIC none (:73-97; both of its branches give the boundary cell's value)
  *  CPL_*              coupling with the partner solver (h3c_set_partner):
  *                     euler/coupling_conditions.hpp:17-35, cns/coupling_conditions.hpp:22-43,
  *                     heat/coupling_conditions.hpp:18-61.  CPL_CNS_HEAT / CPL_HEAT_CNS:
@@ -104,6 +114,9 @@ extern "C" {
 /* EXTENSION (not in hom3): periodic pairing of opposite cube faces; the
  * caller supplies the partner cell of each ghost through h3c_set_periodic. */
 #define H3C_BC_PERIODIC 14
+#define H3C_BC_ADV_DIRICHLET 15
+#define H3C_BC_ADV_NEUMANN 16
+#define H3C_BC_ADV_CHARACTERISTIC 17
 
 typedef struct h3c_solver_s* h3c_solver;
 
@@ -112,7 +125,7 @@ typedef struct h3c_solver_s* h3c_solver;
  *  cns/physics.hpp:57-61; cns/quantities.hpp:23-30; heat/physics.hpp:36-39). */
 typedef struct {
   int nd;               /* 2 or 3 */
-  int physics;          /* H3C_EULER / H3C_CNS / H3C_HEAT */
+  int physics;          /* H3C_EULER / H3C_CNS / H3C_HEAT / H3C_ADVECTION */
   int flux;             /* H3C_FLUX_* */
   int time_integration; /* H3C_EULER_FORWARD / H3C_RUNGE_KUTTA_2 / H3C_SSPRK3 */
   int precision;        /* H3C_FP64 / H3C_MIXED */
@@ -191,6 +204,12 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* grid);
 /* which: 0 = lhs, 1 = rhs.  Host arrays, caller numbering, [nv][ld]. */
 int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld);
 int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld);
+/* Advection velocity of every cell, ghosts included: the physics' velocity
+ * function evaluated at the cell centres (Physics::velocity,
+ * advection/physics.hpp:116-118, which hom3 evaluates at x_center on every
+ * use).  Host array [nd][ld], caller numbering.  Required before an
+ * advection solver steps; the next time step is recomputed from it. */
+int h3c_set_velocity(h3c_solver s, const double* u, int64_t ld);
 /* Device-resident state in the internal (Morton) numbering: pointer, leading
  * dimension and the internal index of every caller cell (perm[caller] = internal). */
 int h3c_state_device(h3c_solver s, int which, double** ptr, int64_t* ld);

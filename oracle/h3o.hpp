@@ -298,8 +298,13 @@ inline std::vector<Sdf> cube_boundaries(int nd, const Tree& t) {
 // Physical parameters: euler/quantities.hpp:23-189, cns/quantities.hpp:23-115,
 // heat/quantities.hpp:13-56
 // ---------------------------------------------------------------------------
-enum PhysicsKind { PHYS_EULER = 0, PHYS_CNS = 1, PHYS_HEAT = 2 };
-enum FluxKind { FLUX_AUSM = 0, FLUX_LLF = 1 };
+enum PhysicsKind { PHYS_EULER = 0, PHYS_CNS = 1, PHYS_HEAT = 2, PHYS_ADVECTION = 3 /* advection/physics.hpp:21-162 */ };
+enum FluxKind { FLUX_AUSM = 0, FLUX_LLF = 1, FLUX_UPWIND = 2 /* advection/tags.hpp:18-19 */ };
+// Advection velocity fields u(x) (the "velocity" property, advection/physics.hpp:36-37)
+enum VelocityKind {
+  VEL_CONSTANT = 0,  // vel = {u_0, u_1, u_2}
+  VEL_ROTATION = 1,  // advection_fv_solver_test.cpp:67-84 (radial_velocity); vel = {u_mag, c_0, c_1}
+};
 enum TimeKind { TI_EULER_FORWARD = 0, TI_RK2 = 1, TI_SSPRK3 = 2 /* EXTENSION: Shu-Osher SSP-RK3 */ };
 enum ReconKind { RECON_NONE = 0, RECON_MUSCL = 1 /* EXTENSION: LSQ + MUSCL + Venkatakrishnan */ };
 
@@ -311,6 +316,8 @@ struct Params {
   double gamma = 1.4, Rspecific = 287.058, T0 = 273.15, rho0 = 1.225, Minfty = 0.1;
   double ReInfty = 100, Pr0 = 0.72, Sutherland0 = 110.4;
   double diffusivity = 1.0, T_ref = 273.15;
+  int vel_kind = VEL_CONSTANT;  // advection velocity field
+  double vel[4] = {0, 0, 0, 0};
   double time_end = 1.0;
   // derived
   double gm1 = 0.4, sOverTref = 0, sOverTrefP1 = 1, Re0 = 1;
@@ -349,6 +356,9 @@ enum BcKind {
   BC_CPL_HEAT_CNS = 12,        // heat/coupling_conditions.hpp:18-38 (heat side)
   BC_CPL_HEAT_HEAT = 13,       // heat/coupling_conditions.hpp:41-61
   BC_PERIODIC = 14,            // EXTENSION (not in hom3): copy of the cell on the opposite face
+  BC_ADV_DIRICHLET = 15,       // advection/boundary_conditions.hpp:17-42 (constant surface value)
+  BC_ADV_NEUMANN = 16,         // :45-70 (constant surface flux)
+  BC_ADV_CHARACTERISTIC = 17,  // :73-97
 };
 
 struct Bc {
@@ -368,6 +378,7 @@ enum IcKind {
   IC_RIEMANN3D_PERTURBED = 5,  // EXTENSION (not in hom3): 3D Riemann + Fourier modes
   IC_VORTEX_PARAM = 6,  // EXTENSION (not in hom3): vortex with centre/strength params
   IC_TAYLOR_GREEN = 7,  // EXTENSION (not in hom3): 3D Taylor-Green vortex
+  IC_DISC = 8,          // advection_fv_solver_test.cpp:100-111: q_in inside a disc, q_out outside
 };
 
 template <class T> struct World;
@@ -393,6 +404,7 @@ template <class T> struct Solver {
   std::vector<Ind> nbr[6];
   std::vector<double> xc[3];
   std::vector<double> len;
+  std::vector<double> vel_[3];  // advection velocity u(x_center) of every cell, ghosts included
   std::vector<SInd> bc_idx;
   std::vector<Ind> node;
   Ind firstGC = INV;
@@ -549,6 +561,35 @@ template <class T> struct Solver {
     return 0.5 * (slope(t, r, v, sdir) + slope(t, l, v, sdir));
   }
   // boundary_info: solver.hpp:298-313
+  // the "velocity" function of the advection physics at x (advection/physics.hpp:36-37, 116-118)
+  void velocity_field(const double* x, double* u) const {
+    for (int d = 0; d < 3; ++d) u[d] = 0;
+    if (P.vel_kind == VEL_CONSTANT) {
+      for (int d = 0; d < nd; ++d) u[d] = P.vel[d];
+      return;
+    }
+    // radial_velocity of advection_fv_solver_test.cpp:67-84 (2D), centre and magnitude as parameters
+    const double u_mag = P.vel[0];
+    const double c0 = P.vel[1], c1 = P.vel[2];
+    const double radius = std::sqrt((x[0] - c0) * (x[0] - c0) + (x[1] - c1) * (x[1] - c1));
+    const double angle = 0.5 * PI - std::acos((x[0] - c0) / radius);
+    u[0] = std::abs(radius * u_mag * std::sin(angle + 0.5 * PI));
+    u[1] = std::abs(radius * u_mag * std::cos(angle + 0.5 * PI));
+    if (x[1] - c1 > 0.) u[0] *= -1;
+    if (x[0] - c0 < 0.) u[1] *= -1;
+  }
+  void compute_velocity() {
+    for (int d = 0; d < 3; ++d) vel_[d].assign(size(), 0.0);
+    if (P.physics != PHYS_ADVECTION) return;
+    for (Ind c = 0; c < size(); ++c) {
+      double x[3] = {0, 0, 0}, u[3];
+      for (int d = 0; d < nd; ++d) x[d] = xc[d][c];
+      velocity_field(x, u);
+      for (int d = 0; d < nd; ++d) vel_[d][c] = u[d];
+    }
+  }
+  double velocity(Ind c, int d) const { return vel_[d][c]; }
+
   Ind boundary_cell(Ind g) const {
     for (int p = 0; p < 2 * nd; ++p)
       if (nbr[p][g] != INV) return nbr[p][g];
@@ -778,6 +819,20 @@ template <class T> struct Solver {
 
   // compute_num_flux dispatch (physics.hpp:175-178, cns 155-161, heat 113-119)
   State face_flux(int t, Ind l, Ind r, int d, double dx, T dt) const {
+    if (P.physics == PHYS_ADVECTION) {
+      State f{};
+      const T qL = q(t, l, 0), qR = q(t, r, 0);
+      const double uL = velocity(l, d), uR = velocity(r, d);
+      if (P.flux == FLUX_LLF) {  // advection/physics.hpp:130-139
+        const double lambda_max = std::max(std::abs(uL), std::abs(uR));
+        f[0] = 0.5 * (qL * uL + qR * uR + lambda_max * (qL - qR));
+      } else {  // upwind: advection/physics.hpp:142-153 (hom3 negates u_L q_L when the face velocity is negative)
+        const double u_srfc = 0.5 * (uL + uR);
+        f[0] = uL * qL;
+        if (u_srfc < 0) f[0] = f[0] * -1.;
+      }
+      return f;
+    }
     if (P.physics == PHYS_HEAT) {
       State f{};
       f[0] = 1 / dx * (q(t, l, 0) - q(t, r, 0));
@@ -829,6 +884,11 @@ template <class T> struct Solver {
     using std::abs;
     const double h = len[c];
     if (P.physics == PHYS_HEAT) return P.cfl * 0.5 * std::pow(h, 2.);
+    if (P.physics == PHYS_ADVECTION) {  // advection/physics.hpp:86-93
+      double u_max = std::numeric_limits<double>::lowest();
+      for (int d = 0; d < nd; ++d) u_max = std::max(u_max, std::abs(velocity(c, d)));
+      return T(P.cfl * h / u_max);
+    }
     const T a_ = a(0, c);
     T S = std::numeric_limits<double>::lowest();
     for (int d = 0; d < nd; ++d) {
@@ -1041,6 +1101,11 @@ template <class T> void Solver<T>::eval_ic(const double* x, ICState& out) const 
     pvars[nd] = inside ? ic[4] : ic[6];
     pvars[nd + 1] = inside ? ic[5] : ic[7];
     out = cv(pvars);
+  } else if (ic_kind == IC_DISC) {
+    // ic = {c_0, c_1, c_2, R, q_in, q_out}: advection_fv_solver_test.cpp:100-111
+    double s2 = 0;
+    for (int d = 0; d < nd; ++d) s2 += (x[d] - ic[d]) * (x[d] - ic[d]);
+    out[0] = std::sqrt(s2) - ic[3] > 0. ? ic[5] : ic[4];
   } else if (ic_kind == IC_TAYLOR_GREEN) {
     // EXTENSION (not in hom3): ic = {U, rho0, p0}; u = U sin x cos y cos z,
     // v = -U cos x sin y cos z, w = 0, p = p0 + rho0 U^2/16 (cos 2x + cos 2y)(cos 2z + 2),
@@ -1198,6 +1263,28 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
         for (int v = 0; v < nv; ++v) q(t, g, v) = q(t, o, v);
         break;
       }
+      case BC_ADV_DIRICHLET:  // advection/boundary_conditions.hpp:29-35; v = {q_srfc}
+        q(t, g, 0) = 2.0 * B.v[0] - q(t, b, 0);
+        break;
+      case BC_ADV_NEUMANN: {  // :56-63; v = {surface flux}, distance of the cell centres
+        double dx2 = 0;
+        for (int d = 0; d < nd; ++d) dx2 += (xc[d][b] - xc[d][g]) * (xc[d][b] - xc[d][g]);
+        q(t, g, 0) = q(t, b, 0) - std::sqrt(dx2) * B.v[0];
+        break;
+      }
+      case BC_ADV_CHARACTERISTIC: {  // :79-95
+        const int pos = opposite_pos[boundary_pos(g)];  // the ghost's position w.r.t. its boundary cell
+        const int dir = pos / 2;
+        const double v = velocity(b, dir);
+        if ((v > 0. && pos % 2 == 0) || (v < 0. && pos % 2 == 1)) {
+          q(t, g, 0) = 2.0 * q(t, b, 0) - q(t, b, 0);  // dirichlet(q_b, q_b)
+        } else {
+          double dx2 = 0;
+          for (int d = 0; d < nd; ++d) dx2 += (xc[d][b] - xc[d][g]) * (xc[d][b] - xc[d][g]);
+          q(t, g, 0) = q(t, b, 0) - std::sqrt(dx2) * 0.0;  // neumann(q_b, 0, dx)
+        }
+        break;
+      }
       case BC_CPL_EULER_EULER: {  // euler/coupling_conditions.hpp:452-460
         const Ind o = partner_cell(g);
         const Solver<T>& os = *w->solvers[B.partner];
@@ -1338,6 +1425,7 @@ template <class T> void Solver<T>::initialize() {
       }
     }
   }
+  compute_velocity();
   // 5) initial condition: cell average by 2^nd Gauss points
   const double gp = 1 / std::sqrt(3);
   for (Ind c = 0; c < firstGC; ++c) {

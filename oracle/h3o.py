@@ -23,16 +23,17 @@ INV = np.iinfo(np.int64).max
 SINV = np.iinfo(np.int32).max
 
 # physics / flux / time integration / bc / ic kinds (oracle/h3o.hpp)
-EULER, CNS, HEAT = 0, 1, 2
-AUSM, LLF = 0, 1
+EULER, CNS, HEAT, ADVECTION = 0, 1, 2, 3
+AUSM, LLF, UPWIND = 0, 1, 2  # UPWIND: advection only
+VEL_CONSTANT, VEL_ROTATION = 0, 1  # advection velocity fields
 EULER_FORWARD, RK2, SSPRK3 = 0, 1, 2  # SSPRK3: EXTENSION (not in hom3)
 RECON_NONE, RECON_MUSCL = 0, 1  # MUSCL: EXTENSION (not in hom3)
 (BC_EULER_NEUMANN, BC_EULER_DIRICHLET, BC_EULER_VORTEX, BC_CNS_INFLOW, BC_CNS_OUTFLOW,
  BC_CNS_ADIABATIC_NOSLIP, BC_CNS_ADIABATIC_SLIP, BC_CNS_ISOTHERMAL_NOSLIP, BC_HEAT_DIRICHLET,
  BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT,
- BC_PERIODIC) = range(15)
+ BC_PERIODIC, BC_ADV_DIRICHLET, BC_ADV_NEUMANN, BC_ADV_CHARACTERISTIC) = range(18)
 (IC_CONSTANT_PV, IC_SHOCK_TUBE, IC_VORTEX, IC_EXPLOSION, IC_CONSTANT_CV,
- IC_RIEMANN3D_PERTURBED, IC_VORTEX_PARAM, IC_TAYLOR_GREEN) = range(8)
+ IC_RIEMANN3D_PERTURBED, IC_VORTEX_PARAM, IC_TAYLOR_GREEN, IC_DISC) = range(9)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
 
 
@@ -49,7 +50,8 @@ class SolverDesc(C.Structure):
         (n, C.c_double) for n in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty",
                                   "ReInfty", "Pr0", "Sutherland0", "diffusivity", "T_ref", "time_end")
     ] + [("domain_kind", C.c_int), ("domain", Sdf), ("ic_kind", C.c_int), ("ic", C.c_double * 80),
-         ("n_bcs", C.c_int), ("bcs", C.POINTER(BcDesc)), ("recon", C.c_int), ("limiter_k", C.c_double)]
+         ("n_bcs", C.c_int), ("bcs", C.POINTER(BcDesc)), ("recon", C.c_int), ("limiter_k", C.c_double),
+         ("vel_kind", C.c_int), ("vel", C.c_double * 4)]
 
 
 class Info(C.Structure):
@@ -102,6 +104,7 @@ def lib():
             "h3o_set_state": (None, [vp, i32, i32, P(dbl)]),
             "h3o_get_tables": (None, [vp, i32, P(i64), P(dbl), P(dbl), P(C.c_int32), P(i64)]),
             "h3o_partner_cells": (i32, [vp, i32, P(i64)]),
+            "h3o_velocity": (None, [vp, i32, P(dbl)]),
             "h3o_nsubfaces": (i64, [vp, i32]),
             "h3o_subfaces": (None, [vp, i32, P(i64)]),
             "h3o_dt": (dbl, [vp, i32]),
@@ -222,6 +225,12 @@ class Solver:
             sub = np.ascontiguousarray(flat.reshape(nsub, ns).T)
         return dict(neighbors=nb, x_center=xc, length=ln, bc_idx=bc, node=node,
                     first_ghost=self.first_ghost, ncells=n, subface_cells=sub)
+
+    def velocity(self):
+        """Advection velocity u(x_center) of every cell, ghosts included: [nd][n_cells]."""
+        out = np.empty((self.w.nd, self.ncells), np.float64)
+        lib().h3o_velocity(self._h, self.idx, _dp(out))
+        return out
 
     def partner_cells(self):
         n = self.ncells - self.first_ghost
@@ -396,9 +405,13 @@ class DualSolver:
 
 
 def _pack_desc(physics=EULER, flux=AUSM, time_integration=EULER_FORWARD, *, bcs=(), domain=None, domain_kind=0,
-               ic_kind=IC_CONSTANT_PV, ic=(), recon=RECON_NONE, limiter_k=1.0, **props):
+               ic_kind=IC_CONSTANT_PV, ic=(), recon=RECON_NONE, limiter_k=1.0, vel_kind=VEL_CONSTANT, vel=(),
+               **props):
     d = SolverDesc()
     d.recon, d.limiter_k = recon, float(limiter_k)
+    d.vel_kind = vel_kind
+    for i, v in enumerate(vel):
+        d.vel[i] = v
     defaults = dict(cfl=0.2, cfl_viscous=0.4, gamma=1.4, Rspecific=287.058, T0=273.15, rho0=1.225, Minfty=0.1,
                     ReInfty=100.0, Pr0=0.72, Sutherland0=110.4, diffusivity=1.0, T_ref=273.15, time_end=1.0)
     defaults.update(props)

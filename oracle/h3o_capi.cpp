@@ -39,6 +39,8 @@ typedef struct {
   const h3o_bc* bcs;
   int recon;         // EXTENSION: 0 none (hom3), 1 MUSCL (LSQ gradients, Venkatakrishnan limiter)
   double limiter_k;  // Venkatakrishnan constant K
+  int vel_kind;      // advection velocity field (VelocityKind)
+  double vel[4];
 } h3o_solver_desc;
 
 static Sdf to_sdf(const h3o_sdf& s) {
@@ -103,8 +105,10 @@ int h3o_add_solver(void* w, const h3o_solver_desc* d) {
   P.time_end = d->time_end;
   P.recon = d->recon;
   P.limiter_k = d->limiter_k;
+  P.vel_kind = d->vel_kind;
+  for (int i = 0; i < 4; ++i) P.vel[i] = d->vel[i];
   P.derive();
-  s->nv = P.physics == PHYS_HEAT ? 1 : ww->nd + 2;
+  s->nv = (P.physics == PHYS_HEAT || P.physics == PHYS_ADVECTION) ? 1 : ww->nd + 2;
   s->domain_kind = d->domain_kind;
   s->domain = to_sdf(d->domain);
   s->ic_kind = d->ic_kind;
@@ -123,6 +127,14 @@ int h3o_add_solver(void* w, const h3o_solver_desc* d) {
 }
 
 static Solver<double>& S(void* w, int s) { return *((W*)w)->solvers[s]; }
+
+// advection velocity of every cell (ghosts included), [nd][n_cells]
+void h3o_velocity(void* w, int s, double* out) {
+  const Solver<double>& so = S(w, s);
+  const int64_t n = so.size();
+  for (int d = 0; d < so.nd; ++d)
+    for (int64_t c = 0; c < n; ++c) out[d * n + c] = so.vel_[d].empty() ? 0.0 : so.vel_[d][c];
+}
 
 int h3o_initialize(void* w, int s) {
   try {

@@ -171,6 +171,31 @@ def euler_euler_case(level=4):
 
 
 # ---------------------------------------------------------------------------
+def advection_case(level=7, flux=h3o.UPWIND, ti=h3o.EULER_FORWARD, bc_kind=None, vel_kind=h3o.VEL_ROTATION,
+                   vel=(0.5, 0.5, 0.5), nd=2, cfl=1.0, fine=None):
+    """advection_fv_solver_test.cpp:53-126: the disc q = 1 (r = 0.08 around (0.25, 0.5)) in q = 0.1,
+    carried by the test's rotating velocity field, characteristic conditions on all faces, upwind flux,
+    forward Euler, CFL 1 (level 7, as in hom3).  bc_kind / vel_kind select other conditions and fields;
+    fine: EXTENSION, refine the r = 0.3 sphere around the centre to that level."""
+    w = h3o.World(nd, [0.0] * nd, [1.0] * nd, level=level)
+    if fine is not None:
+        w.refine_sphere([0.5] * nd, 0.3, fine)
+    g = w.cube_boundaries()
+    if bc_kind is None or bc_kind == h3o.BC_ADV_CHARACTERISTIC:
+        bcs = [h3o.bc(h3o.BC_ADV_CHARACTERISTIC, x) for x in g]
+    elif bc_kind == h3o.BC_PERIODIC:
+        bcs = [h3o.bc(h3o.BC_PERIODIC, x) for x in g]
+    elif bc_kind == h3o.BC_ADV_DIRICHLET:
+        bcs = [h3o.bc(h3o.BC_ADV_DIRICHLET, x, [0.1 + 0.05 * i]) for i, x in enumerate(g)]
+    else:
+        bcs = [h3o.bc(h3o.BC_ADV_NEUMANN, x, [0.02 * (i + 1)]) for i, x in enumerate(g)]
+    centre = [0.25, 0.5, 0.5][:nd] + [0.0] * (3 - nd)
+    s = w.add_solver(h3o.ADVECTION, flux, ti, bcs=bcs, ic_kind=h3o.IC_DISC, ic=centre + [0.08, 1.0, 0.1],
+                     cfl=cfl, time_end=100.0, vel_kind=vel_kind, vel=vel)
+    s.initialize()
+    return w, [s]
+
+
 def gpu_solver_from_oracle(o: "h3o.Solver", precision=0):
     """Hand the oracle's (hom3-numbered) tables and initial state to the C ABI:
     the drop-in path a hom3 Solver would take after Solver::initialize."""
@@ -187,6 +212,8 @@ def gpu_solver_from_oracle(o: "h3o.Solver", precision=0):
                [Condition(k, v) for k, v in info["bcs"]], t["subface_cells"])
     if any(k == h3o.BC_PERIODIC for k, _ in info["bcs"]):
         s.set_periodic(o.partner_cells())
+    if info["physics"] == h3o.ADVECTION:
+        s.set_velocity(o.velocity())
     s.set_state(o.state(0), 0)
     s.reset_time()
     return s

@@ -37,6 +37,14 @@ def test_create_without_gpu_fails_loudly():
         hb.Solver(2)
 
 
+@pytest.mark.parametrize("physics,flux", [(F.ADVECTION, F.FLUX_AUSM), (F.EULER, F.FLUX_UPWIND),
+                                          (F.HEAT, F.FLUX_UPWIND), (F.CNS, F.FLUX_UPWIND)])
+def test_create_rejects_a_flux_of_another_physics(physics, flux):
+    """Checked before any CUDA call: advection takes upwind or LLF, upwind is advection's."""
+    with pytest.raises(hb.H3cError, match="flux"):
+        hb.Solver(2, physics, flux)
+
+
 def _oracle_tables(nd, lo, hi, level, domain=None, dk=0, extra=()):
     w = h3o.World(nd, lo, hi, level=level)
     bcs = [h3o.bc(h3o.BC_EULER_NEUMANN, g) for g in w.cube_boundaries()]

@@ -357,3 +357,64 @@ def test_muscl_graph_replay_matches_single_steps():
         b.solve(1)
     fg = o.first_ghost
     assert np.array_equal(a.state(0)[:, :fg], b.state(0)[:, :fg])
+
+
+# ---- advection (advection/physics.hpp, advection/boundary_conditions.hpp) ----
+def test_advection_hom3_case():
+    """advection_fv_solver_test.cpp:53-126 at its own level 7: the disc in the
+    rotating field, characteristic conditions, upwind flux, forward Euler, CFL 1."""
+    _, (o,) = cases.advection_case(level=7)
+    run_single(o)
+
+
+@pytest.mark.parametrize("bc", [h3o.BC_ADV_DIRICHLET, h3o.BC_ADV_NEUMANN, h3o.BC_PERIODIC])
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2, h3o.SSPRK3])
+@pytest.mark.parametrize("flux", [h3o.LLF, h3o.UPWIND])
+def test_advection_fluxes_and_conditions(flux, ti, bc):
+    _, (o,) = cases.advection_case(level=6, flux=flux, ti=ti, bc_kind=bc, cfl=0.4)
+    run_single(o)
+
+
+def test_advection_3d_uniform_velocity():
+    _, (o,) = cases.advection_case(level=4, nd=3, flux=h3o.LLF, ti=h3o.RK2, vel_kind=h3o.VEL_CONSTANT,
+                                   vel=(0.3, -0.5, 0.7), bc_kind=h3o.BC_ADV_NEUMANN, cfl=0.3)
+    run_single(o)
+
+
+@pytest.mark.parametrize("flux", [h3o.LLF, h3o.UPWIND])
+def test_advection_refined_tree(flux):
+    """EXTENSION: coarse/fine faces (area-weighted sub-face fluxes)."""
+    _, (o,) = cases.advection_case(level=4, fine=6, flux=flux, ti=h3o.RK2, cfl=0.3)
+    run_single(o)
+
+
+def test_advection_graph_replay_and_min_dt():
+    """20 steps replayed from the captured graph, and Solver::min_dt."""
+    _, (o,) = cases.advection_case(level=6, flux=h3o.LLF, ti=h3o.RK2, cfl=0.4)
+    g = cases.gpu_solver_from_oracle(o)
+    assert abs(g.min_dt() - o.min_dt()) <= 1e-15 * o.min_dt()
+    o.solve(20)
+    g.solve(20)
+    check_pair(o, g, TOL_MULTI, "20 graph steps")
+
+
+def test_advection_needs_a_velocity():
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    _, (o,) = cases.advection_case(level=4)
+    info = o.info()
+    s = hb.Solver(2, F.ADVECTION, F.FLUX_UPWIND, F.EULER_FORWARD, cfl=1.0)
+    t = o.tables()
+    from hom3_b200.solver import Condition
+    s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"],
+               [Condition(k, v) for k, v in info["bcs"]])
+    s.set_state(o.state(0), 0)
+    with pytest.raises(hb.H3cError, match="velocity"):
+        s.solve(1)
+    with pytest.raises(hb.H3cError, match="velocity"):
+        s.min_dt()
+    s.set_velocity(o.velocity())
+    s.reset_time()
+    s.solve(2)
+    o.solve(2)
+    check_pair(o, s, TOL_MULTI, "after the velocity")

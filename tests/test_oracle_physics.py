@@ -220,3 +220,98 @@ def test_conductivity_ratio_weights_interface_temperature():
         T = 1.4 * 0.4 * (q[3] - 0.5 * (q[0] ** 2 + q[1] ** 2) / q[2]) / q[2]
         res[kappa] = T.max()
     assert res[50.0] > res[1.0]
+
+
+# ---- advection (advection/physics.hpp, advection/boundary_conditions.hpp) ----
+def _lattice(o):
+    """(i, j) lattice index of every interior cell of a uniform 2D grid."""
+    t = o.tables()
+    fg = o.first_ghost
+    h = t["length"][0]
+    ij = np.floor(t["x_center"][:, :fg] / h).astype(int)
+    return ij, int(round(1 / h))
+
+
+def test_advection_upwind_at_cfl_one_shifts_by_one_cell():
+    """u = (1, 0), CFL 1: dt = h, and the upwind update q - (q - q_left) moves
+    the state exactly one cell per step (to rounding), periodic in x."""
+    _, (o,) = cases.advection_case(level=5, bc_kind=h3o.BC_PERIODIC, vel_kind=h3o.VEL_CONSTANT, vel=(1.0, 0.0))
+    ij, n = _lattice(o)
+    fg = o.first_ghost
+    q0 = np.empty((n, n))
+    q0[ij[0], ij[1]] = o.state(0)[0, :fg]
+    o.solve(7)
+    assert abs(o.dt() - 1.0 / n) <= 1e-15
+    q = np.empty((n, n))
+    q[ij[0], ij[1]] = o.state(0)[0, :fg]
+    assert np.abs(q - np.roll(q0, 7, axis=0)).max() <= 1e-15
+
+
+def test_advection_upwind_reproduces_hom3_sign_for_negative_velocity():
+    """hom3's upwind flux is u_L q_L negated when the face velocity is
+    negative (advection/physics.hpp:142-153), not u_R q_R: with u = (-1, 0)
+    at CFL 1 every face carries +q_L and the state moves one cell in +x."""
+    _, (o,) = cases.advection_case(level=5, bc_kind=h3o.BC_PERIODIC, vel_kind=h3o.VEL_CONSTANT, vel=(-1.0, 0.0))
+    ij, n = _lattice(o)
+    fg = o.first_ghost
+    q0 = np.empty((n, n))
+    q0[ij[0], ij[1]] = o.state(0)[0, :fg]
+    o.solve(1)
+    q = np.empty((n, n))
+    q[ij[0], ij[1]] = o.state(0)[0, :fg]
+    assert np.abs(q - np.roll(q0, 1, axis=0)).max() <= 1e-15
+
+
+@pytest.mark.parametrize("flux", [h3o.LLF, h3o.UPWIND])
+def test_advection_conserves_on_periodic_domain(flux):
+    """Both fluxes are face fluxes F(l, r) shared by the two cells: the sum of
+    q h^2 is conserved on a periodic domain (rotating field, RK2)."""
+    _, (o,) = cases.advection_case(level=5, flux=flux, ti=h3o.RK2, bc_kind=h3o.BC_PERIODIC, cfl=0.4)
+    fg = o.first_ghost
+    h2 = o.tables()["length"][:fg] ** 2
+    m0 = (o.state(0)[0, :fg] * h2).sum()
+    o.solve(20)
+    assert abs((o.state(0)[0, :fg] * h2).sum() - m0) <= 1e-13 * abs(m0)
+
+
+def test_advection_llf_is_bounded_for_a_uniform_velocity():
+    """LLF with a uniform velocity is the monotone upwind scheme: at CFL 0.4 per
+    direction the state stays within the initial bounds."""
+    _, (o,) = cases.advection_case(level=5, flux=h3o.LLF, bc_kind=h3o.BC_PERIODIC, vel_kind=h3o.VEL_CONSTANT,
+                                   vel=(0.6, -0.8), cfl=0.4)
+    fg = o.first_ghost
+    o.solve(30)
+    q = o.state(0)[0, :fg]
+    assert q.min() >= 0.1 - 1e-14 and q.max() <= 1.0 + 1e-14
+
+
+def test_advection_conditions():
+    """Ghost values: Dirichlet 2 v - q_b, Neumann q_b - |x_b - x_g| g, and the
+    characteristic condition, whose inflow and outflow branches both give q_b."""
+    for kind in (h3o.BC_ADV_DIRICHLET, h3o.BC_ADV_NEUMANN, h3o.BC_ADV_CHARACTERISTIC):
+        _, (o,) = cases.advection_case(level=4, bc_kind=kind)
+        t = o.tables()
+        fg = o.first_ghost
+        o.apply_bcs(0)
+        q = o.state(0)[0]
+        info = o.info()
+        for gcell in range(fg, o.ncells):
+            b = next(int(n) for n in t["neighbors"][:, gcell] if 0 <= n < o.ncells)
+            v = info["bcs"][t["bc_idx"][gcell]][1][0]
+            if kind == h3o.BC_ADV_DIRICHLET:
+                want = 2 * v - q[b]
+            elif kind == h3o.BC_ADV_NEUMANN:
+                want = q[b] - np.linalg.norm(t["x_center"][:, b] - t["x_center"][:, gcell]) * v
+            else:
+                want = q[b]
+            assert q[gcell] == want, (kind, gcell)
+
+
+def test_advection_time_step():
+    """compute_dt: CFL h / max_d |u_d(x_c)| (advection/physics.hpp:86-93), min over cells."""
+    _, (o,) = cases.advection_case(level=4, cfl=0.7)
+    t = o.tables()
+    fg = o.first_ghost
+    u = o.velocity()[:, :fg]
+    want = (0.7 * t["length"][:fg] / np.abs(u).max(axis=0)).min()
+    assert abs(o.min_dt() - want) <= 1e-15 * want
