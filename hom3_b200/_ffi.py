@@ -71,6 +71,7 @@ SIGNATURES = {
     "h3c_set_state": (_i32, [_vp, _i32, _P(_dbl), _i64]),
     "h3c_get_state": (_i32, [_vp, _i32, _P(_dbl), _i64]),
     "h3c_set_velocity": (_i32, [_vp, _P(_dbl), _i64]),
+    "h3c_write_vtk": (_i32, [_vp, C.c_char_p, _P(Grid), _P(_i64)]),
     "h3c_state_device": (_i32, [_vp, _i32, _P(_P(_dbl)), _P(_i64)]),
     "h3c_device_order": (_i32, [_vp, _P(_i64)]),
     "h3c_get_stream": (_i32, [_vp, _P(_vp)]),

@@ -10,8 +10,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", f) for f in ("h3c_solver.cu", "h3c_noalloc.cu", "grid_build.cpp")]
-DEPS = SRC + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh"))) + [os.path.join(HERE, "..", "include", "h3c.h")]
+SRC = [os.path.join(HERE, "csrc", f) for f in ("h3c_solver.cu", "h3c_noalloc.cu", "grid_build.cpp", "vtk_writer.cpp")]
+DEPS = SRC + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + glob.glob(os.path.join(HERE, "csrc", "*.hpp"))) \
+    + [os.path.join(HERE, "..", "include", "h3c.h")]
 OUT = os.path.join(HERE, "_lib", "libhom3_b200.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "128,177"]

@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include "vtk_writer.hpp"
+
 #include "../../include/h3c.h"
 #include "fv_kernels.cuh"
 #include "adjoint_kernels.cuh"
@@ -916,6 +918,145 @@ int h3c_set_velocity(h3c_solver s, const double* u, int64_t ld) {
   launch_cfl(s, &s->d_sc->dtmin_ord);
   H3C_CUDA(s, cudaStreamSynchronize(s->stream));
   return s->cuda(cudaGetLastError(), "h3c_set_velocity");
+}
+
+int h3c_write_vtk(h3c_solver s, const char* fname, const h3c_grid* grid, const int64_t* node_ids) {
+  if (!s || !fname || !grid) return H3C_E_INVALID;
+  if (int rc = ready(s, "h3c_write_vtk")) return rc;
+  if (s->n_inst != 1) return s->fail(H3C_E_INVALID, "h3c_write_vtk: single grids only");
+  const long long n = s->n_caller;
+  if (grid->n_cells != n || grid->first_ghost < 0 || grid->first_ghost > n || grid->ld < n || !grid->neighbors ||
+      !grid->x_center || !grid->length || !grid->bc_idx)
+    return s->fail(H3C_E_INVALID, "h3c_write_vtk: the grid is not the one given to h3c_set_grid");
+  const int nd = s->nd, nv = s->nv, phys = s->desc.physics;
+  // write_domain(solver) applies the conditions to lhs first (solver.hpp:328-333)
+  launch_bc(s, 0);
+  std::vector<double> q((size_t)nv * n);
+  if (int rc = h3c_get_state(s, 0, q.data(), n)) return rc;
+  // device columns in the caller's numbering (cell slopes for the vorticity, the advection velocity)
+  auto download = [&](const double* src, int cols, std::vector<double>& out) -> int {
+    double* tmp = nullptr;
+    H3C_CUDA(s, cudaMalloc(&tmp, sizeof(double) * cols * n));
+    k_scatter<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(src, s->ld, tmp, n, s->d_dev2caller, s->n_tot, cols);
+    out.resize((size_t)cols * n);
+    cudaMemcpyAsync(out.data(), tmp, sizeof(double) * cols * n, cudaMemcpyDeviceToHost, s->stream);
+    const cudaError_t e = cudaStreamSynchronize(s->stream);
+    cudaFree(tmp);
+    return s->cuda(e, "h3c_write_vtk");
+  };
+  std::vector<VtkStream> st;
+  auto ints = [&](std::vector<std::string> names, int dims) -> VtkStream& {
+    st.push_back(VtkStream{});
+    st.back().names = std::move(names);
+    st.back().dims = dims;
+    st.back().is_int = true;
+    st.back().ints.assign((size_t)dims * n, INT64_MAX);
+    return st.back();
+  };
+  auto nums = [&](std::vector<std::string> names, int dims) -> VtkStream& {
+    st.push_back(VtkStream{});
+    st.back().names = std::move(names);
+    st.back().dims = dims;
+    st.back().nums.assign((size_t)dims * n, 0.0);
+    return st.back();
+  };
+  // solver.hpp:351-370: cell id, grid node, same-level neighbours, ghost flag, bc index
+  { auto& x = ints({"locallCellIds"}, 1); for (long long c = 0; c < n; ++c) x.ints[c] = c; }
+  { auto& x = ints({"gridNodeIds"}, 1); if (node_ids) for (long long c = 0; c < n; ++c) x.ints[c] = node_ids[c]; }
+  {
+    auto& x = ints({"local_nghbrs"}, 2 * nd);
+    for (int p = 0; p < 2 * nd; ++p)
+      for (long long c = 0; c < n; ++c) {
+        const int64_t v = grid->neighbors[p * grid->ld + c];
+        x.ints[(size_t)p * n + c] = (v >= 0 && v < n) || v <= -2 ? v : INT64_MAX;  // <= -2: sub-face group
+      }
+  }
+  { auto& x = ints({"ghost_cell"}, 1); for (long long c = grid->first_ghost; c < n; ++c) x.ints[c] = 1; }
+  {
+    // SInd bc index; an internal cell's invalid<SInd>() is a valid Ind and is written as is
+    auto& x = ints({"bcIdx"}, 1);
+    for (long long c = 0; c < n; ++c) {
+      const int32_t b = grid->bc_idx[c];
+      x.ints[c] = (b >= 0 && b < grid->n_bcs) ? b : INT32_MAX;
+    }
+  }
+  // conservative variables (V::cv_names: euler/indices.hpp:20-30, heat/indices.hpp:16-22, advection/indices.hpp)
+  {
+    std::vector<std::string> names;
+    if (phys == H3C_HEAT) names = {"T"};
+    else if (phys == H3C_ADVECTION) names = {"q"};
+    else {
+      for (int d = 0; d < nd; ++d) names.push_back("rho_u" + std::to_string(d));
+      names.push_back("rho");
+      names.push_back("rho_E");
+    }
+    auto& x = nums(names, nv);
+    x.nums = q;
+  }
+  // physics_output: euler/physics.hpp:207-226 (+ cns/physics.hpp:193-201), advection/physics.hpp:96-102
+  if (phys == H3C_EULER || phys == H3C_CNS) {
+    const double gamma = s->desc.gamma, gm1 = gamma - 1.0;
+    std::vector<double> a(n), p(n), u((size_t)nd * n), M(n), e(n), T(n);
+    for (long long c = 0; c < n; ++c) {
+      const double rho = q[(size_t)nd * n + c], rhoE = q[(size_t)(nd + 1) * n + c];
+      double um2 = 0;
+      for (int d = 0; d < nd; ++d) {
+        u[(size_t)d * n + c] = q[(size_t)d * n + c] / rho;
+        um2 += u[(size_t)d * n + c] * u[(size_t)d * n + c];
+      }
+      p[c] = gm1 * (rhoE - 0.5 * rho * um2);
+      a[c] = std::sqrt(gamma * p[c] / rho);
+      M[c] = std::sqrt(um2) / a[c];
+      e[c] = p[c] / gm1 / rho;
+      T[c] = gamma * p[c] / rho;
+    }
+    nums({"a"}, 1).nums = a;
+    nums({"p"}, 1).nums = p;
+    nums({"u"}, nd).nums = u;
+    nums({"M"}, 1).nums = M;
+    nums({"e"}, 1).nums = e;
+    nums({"T"}, 1).nums = T;
+    if (phys == H3C_CNS) {
+      std::vector<double> mu(n);
+      for (long long c = 0; c < n; ++c)
+        mu[c] = std::pow(T[c], 1.5) * s->pc.sOverTrefP1 / (T[c] + s->pc.sOverTref);  // cns/quantities.hpp:113-115
+      nums({"mu"}, 1).nums = mu;
+      // vorticity from slope_u (cns/physics.hpp:89-94, 126-138) on the cell slopes of the step
+      launch_slopes_ptr(s, s->d_q[0]);
+      std::vector<double> sl;
+      if (int rc = download(s->d_slopes, nd * nv, sl)) return rc;
+      auto slope = [&](long long c, int v, int sd) { return sl[(size_t)(sd * nv + v) * n + c]; };
+      auto slope_u = [&](long long c, int dir, int sd) {
+        const double rho = q[(size_t)nd * n + c];
+        return (slope(c, dir, sd) * rho - slope(c, nd, sd) * q[(size_t)dir * n + c]) / std::pow(rho, 2.);
+      };
+      const int nw = nd == 2 ? 1 : 3;
+      auto& w = nums({"vorticity"}, nw);
+      for (long long c = 0; c < n; ++c) {
+        if (nd == 2) {
+          w.nums[c] = slope_u(c, 1, 0) - slope_u(c, 0, 1);
+        } else {
+          w.nums[c] = slope_u(c, 2, 1) - slope_u(c, 1, 2);
+          w.nums[(size_t)n + c] = slope_u(c, 0, 2) - slope_u(c, 2, 0);
+          w.nums[(size_t)2 * n + c] = slope_u(c, 1, 0) - slope_u(c, 0, 1);
+        }
+      }
+    }
+  } else if (phys == H3C_ADVECTION) {
+    std::vector<double> vel;
+    if (int rc = download(s->d_vel, nd, vel)) return rc;
+    nums({"u"}, nd).nums = vel;
+  }
+  VtkDomain D;
+  D.path = std::string(fname) + ".vtk";
+  D.nd = nd;
+  D.n_cells = n;
+  D.ld = grid->ld;
+  D.x_center = grid->x_center;
+  D.length = grid->length;
+  std::string err;
+  if (write_vtk_file(D, st, &err)) return s->fail(H3C_E_INVALID, "h3c_write_vtk: %s", err.c_str());
+  return H3C_OK;
 }
 
 int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld) {

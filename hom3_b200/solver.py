@@ -197,6 +197,7 @@ class Solver:
             g.subface_cells = _lp(sub)
         self._check(lib().h3c_set_grid(self.h, C.byref(g)))
         self.n_cells, self.first_ghost = n, int(first_ghost)
+        self._grid = (g, nb, xc, ln, bc, arr)  # the tables h3c_write_vtk is handed again
 
     def set_state(self, q, which=LHS):
         q = np.ascontiguousarray(q, np.float64)
@@ -209,6 +210,16 @@ class Solver:
         u = np.ascontiguousarray(u, np.float64)
         assert u.shape == (self.nd, self.n_cells), u.shape
         self._check(lib().h3c_set_velocity(self.h, _dp(u), self.n_cells))
+
+    def write_vtk(self, fname, node_ids=None):
+        """write_domain(fName, solver) (solver.hpp:336-376): conditions applied to
+        lhs, then fname + ".vtk" in hom3's legacy binary VTK layout."""
+        nid = None
+        if node_ids is not None:
+            nid = np.ascontiguousarray(node_ids, np.int64)
+            assert nid.shape == (self.n_cells,)
+        self._check(lib().h3c_write_vtk(self.h, str(fname).encode(), C.byref(self._grid[0]),
+                                        _lp(nid) if nid is not None else None))
 
     def state(self, which=LHS, out=None) -> np.ndarray:
         if out is None:

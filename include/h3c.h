@@ -204,6 +204,15 @@ int h3c_set_grid(h3c_solver s, const h3c_grid* grid);
 /* which: 0 = lhs, 1 = rhs.  Host arrays, caller numbering, [nv][ld]. */
 int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld);
 int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld);
+/* ---- output: Solver::write_domain (solver.hpp:328-376) ----
+ * Applies the conditions to lhs and writes fname + ".vtk" in hom3's legacy
+ * binary VTK layout (io/vtk.hpp:156-450): the cells in container order as
+ * pixels / voxels, then cell data locallCellIds, gridNodeIds, local_nghbrs_*,
+ * ghost_cell, bcIdx, the conservative variables, and the physics output
+ * (Euler: a, p, u_*, M, e, T; CNS: also mu and vorticity; advection: u_*).
+ * grid: the tables given to h3c_set_grid; node_ids: each cell's grid node
+ * (NULL writes -1).  Host only apart from the state download; single grids. */
+int h3c_write_vtk(h3c_solver s, const char* fname, const h3c_grid* grid, const int64_t* node_ids);
 /* Advection velocity of every cell, ghosts included: the physics' velocity
  * function evaluated at the cell centres (Physics::velocity,
  * advection/physics.hpp:116-118, which hom3 evaluates at x_center on every
