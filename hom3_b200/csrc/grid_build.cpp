@@ -27,27 +27,13 @@
 #include <vector>
 
 #include "../../include/h3c.h"
+#include "grid_build.hpp"
 
 namespace {
 
-std::string g_err;
-
-struct Cell {
-  int level;
-  long long i[3];
-};
-
-struct BuiltGrid {
-  int nd = 2;
-  long long n_int = 0, n_tot = 0, nsub = 0;
-  std::vector<int64_t> nbr;      // [2nd][n_tot]
-  std::vector<double> xc;        // [nd][n_tot]
-  std::vector<double> len;       // [n_tot]
-  std::vector<int32_t> bc;       // [n_tot]
-  std::vector<int64_t> sub;      // [2^(nd-1)][nsub]
-  std::vector<Cell> cells;       // interior + ghost cells (ghost: level/coords of its position)
-  std::vector<h3c_bc> bcs;       // placeholders (conditions are given to h3c_set_grid)
-};
+using gridb::BuiltGrid;
+using gridb::Cell;
+void fail_msg(const char* m) { gridb::set_global_error(m); }
 
 double sdf_eval(int nd, const h3c_sdf& s, const double* x) {
   double r = 0;
@@ -143,8 +129,6 @@ const int kRel[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}
 
 }  // namespace
 
-struct h3c_built_grid_s : BuiltGrid {};
-
 extern "C" {
 
 int h3c_cube_boundaries(const h3c_grid_desc* d, h3c_sdf* out) {
@@ -171,16 +155,16 @@ int h3c_cube_boundaries(const h3c_grid_desc* d, h3c_sdf* out) {
 int h3c_grid_build(const h3c_grid_desc* d, h3c_built_grid* out) {
   if (!d || !out) return H3C_E_INVALID;
   const int nd = d->nd;
-  if (nd != 2 && nd != 3) { g_err = "h3c_grid_build: nd must be 2 or 3"; return H3C_E_INVALID; }
+  if (nd != 2 && nd != 3) { fail_msg("h3c_grid_build: nd must be 2 or 3"); return H3C_E_INVALID; }
   if (d->min_level < 0 || d->n_refine < 0 || d->n_refine > 4 || d->n_bcs < 0 || d->n_bcs > 16) {
-    g_err = "h3c_grid_build: bad level / refine / bc counts";
+    fail_msg("h3c_grid_build: bad level / refine / bc counts");
     return H3C_E_INVALID;
   }
   const Root root = make_root(*d);
   int maxl = d->min_level;
   for (int k = 0; k < d->n_refine; ++k) maxl = std::max(maxl, d->refine_level[k]);
   Levels L;
-  if (!L.init(nd, maxl)) { g_err = "h3c_grid_build: grid too large for dense level maps"; return H3C_E_INVALID; }
+  if (!L.init(nd, maxl)) { fail_msg("h3c_grid_build: grid too large for dense level maps"); return H3C_E_INVALID; }
   // ---- leaves: MinLevel (generation.hpp:355-376), then sphere refinement ----
   std::vector<Cell> leaves;
   {

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "vtk_writer.hpp"
+#include "grid_build.hpp"
 
 #include "../../include/h3c.h"
 #include "fv_kernels.cuh"
@@ -34,6 +35,10 @@ std::string g_last_error;  // errors not tied to a solver (NULL handle)
 
 constexpr long long kForcedNone = std::numeric_limits<long long>::max();
 }  // namespace
+
+namespace gridb {
+void set_global_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace gridb
 
 struct h3c_solver_s {
   h3c_desc desc{};
