@@ -100,6 +100,7 @@ SIGNATURES = {
     "h3c_profile": (_i32, [_vp, _i32]),
     "h3c_profile_read": (_i32, [_vp, _P(_dbl), _P(_i64), _i32]),
     "h3c_grid_build": (_i32, [_P(GridDesc), _P(_vp)]),
+    "h3c_grid_build_device": (_i32, [_P(GridDesc), _P(_vp)]),
     "h3c_grid_view": (_i32, [_vp, _P(Grid)]),
     "h3c_cube_boundaries": (_i32, [_P(GridDesc), _P(Sdf)]),
     "h3c_grid_free": (_i32, [_vp]),

@@ -10,7 +10,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = [os.path.join(HERE, "csrc", f) for f in ("h3c_solver.cu", "h3c_noalloc.cu", "grid_build.cpp", "vtk_writer.cpp")]
+SRC = [os.path.join(HERE, "csrc", f) for f in ("h3c_solver.cu", "h3c_noalloc.cu", "grid_build.cpp", "grid_build_device.cu",
+                                                      "vtk_writer.cpp")]
 DEPS = SRC + sorted(glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + glob.glob(os.path.join(HERE, "csrc", "*.hpp"))) \
     + [os.path.join(HERE, "..", "include", "h3c.h")]
 OUT = os.path.join(HERE, "_lib", "libhom3_b200.so")

@@ -460,10 +460,12 @@ class GridSpec:
         return self.root_length / 2.0 ** level
 
 
-def build_tables(spec: GridSpec, bc_geoms, domain=None, domain_kind=0) -> dict:
-    """Run the library's grid builder and copy its tables out as numpy arrays."""
+def build_tables(spec: GridSpec, bc_geoms, domain=None, domain_kind=0, device=False) -> dict:
+    """Run the library's grid builder -- on the host, or on the GPU with
+    device=True (same tables) -- and copy its tables out as numpy arrays."""
     h = C.c_void_p()
-    check(lib().h3c_grid_build(C.byref(spec.desc(domain, domain_kind, bc_geoms)), C.byref(h)))
+    build = lib().h3c_grid_build_device if device else lib().h3c_grid_build
+    check(build(C.byref(spec.desc(domain, domain_kind, bc_geoms)), C.byref(h)))
     try:
         v = F.Grid()
         check(lib().h3c_grid_view(h, C.byref(v)))

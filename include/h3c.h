@@ -359,6 +359,11 @@ typedef struct {
 
 typedef struct h3c_built_grid_s* h3c_built_grid;
 int h3c_grid_build(const h3c_grid_desc* desc, h3c_built_grid* out);
+/* The same tables built on the GPU (no hom3 counterpart): refinement, 2:1
+ * balance, Morton ranking, neighbour / sub-face search and ghost creation as
+ * data-parallel kernels and scans on the current device, then copied to the
+ * host; bit-identical to h3c_grid_build's.  Free with h3c_grid_free. */
+int h3c_grid_build_device(const h3c_grid_desc* desc, h3c_built_grid* out);
 /* Table views valid until h3c_grid_free; the layout is that of h3c_grid. */
 int h3c_grid_view(h3c_built_grid g, h3c_grid* view);
 /* cube faces of the root cell in hom3's order left,right,bottom,top,front,back;
