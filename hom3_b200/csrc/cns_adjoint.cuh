@@ -192,14 +192,20 @@ __device__ __forceinline__ void adjc_faces(long long c, const double* __restrict
     for (int v = 0; v < NV; ++v) nb[v] = 0.0;
 #pragma unroll
     for (int k = 0; k < ND * NV; ++k) nsb[k] = 0.0;
+    // The neighbour side's derivatives are needed only when the neighbour is a
+    // non-periodic ghost (its state comes from c); an interior or periodic
+    // neighbour takes its own.  Directions in use, in order: own state, [the
+    // neighbour's state,] own transverse slopes[, the neighbour's].
+    const bool all = own == -1;
+    const int ndir = all ? NDIR : NV + NT;
 #pragma unroll 1
-    for (int j0 = 0; j0 < NDIR; j0 += K) {
+    for (int j0 = 0; j0 < ndir; j0 += K) {
       DN<K> aq[NV], bq[NV], as[ND * NV], bs[ND * NV], f[NV];  // a: cell c, b: neighbour
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
         aq[v] = DN<K>(qc[v]);
         bq[v] = DN<K>(qn[v]);
-        const int ja = v - j0, jb = NV + v - j0;
+        const int ja = v - j0, jb = all ? NV + v - j0 : -1;
         if (ja >= 0 && ja < K) aq[v].d[ja] = 1.0;
         if (jb >= 0 && jb < K) bq[v].d[jb] = 1.0;
       }
@@ -211,7 +217,7 @@ __device__ __forceinline__ void adjc_faces(long long c, const double* __restrict
           as[s2 * NV + v] = DN<K>(sl[(s2 * NV + v) * ld + c]);
           bs[s2 * NV + v] = DN<K>(sl[(s2 * NV + v) * ld + n]);
           if (s2 != D) {
-            const int ja = 2 * NV + t - j0, jb = 2 * NV + NT + t - j0;
+            const int ja = (all ? 2 * NV : NV) + t - j0, jb = all ? 2 * NV + NT + t - j0 : -1;
             if (ja >= 0 && ja < K) as[s2 * NV + v].d[ja] = 1.0;
             if (jb >= 0 && jb < K) bs[s2 * NV + v].d[jb] = 1.0;
             ++t;
@@ -222,8 +228,9 @@ __device__ __forceinline__ void adjc_faces(long long c, const double* __restrict
       else cns_face_dual<ND, K, D>(bq, aq, bs, as, len_r, pc, f);
 #pragma unroll
       for (int jj = 0; jj < K; ++jj) {
-        const int j = j0 + jj;
-        if (j >= NDIR) break;
+        const int jl = j0 + jj;
+        if (jl >= ndir) break;
+        const int j = all ? jl : (jl < NV ? jl : jl + NV);  // the direction's index in the full list
         double gj = 0.0;
 #pragma unroll
         for (int v = 0; v < NV; ++v) gj += w[v] * f[v].d[jj];
