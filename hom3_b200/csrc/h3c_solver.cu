@@ -94,6 +94,12 @@ struct h3c_solver_s {
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   const double* graph_q0 = nullptr;  // lhs buffer the capture started from
+  // single steps replayed from captured one-step graphs, one per lhs buffer
+  // (forward Euler alternates the two)
+  cudaGraphExec_t graph1[2] = {nullptr, nullptr};
+  const double* graph1_q0[2] = {nullptr, nullptr};
+  long long graph1_launches = 0;
+  bool plain_done = false;  // a step ran outside capture (kernel attributes are set)
   // coupled conjugate-heat steps (h3c_cht_solve) captured with the heat partner
   cudaGraphExec_t cpl_graph = nullptr;
   h3c_solver cpl_with = nullptr;
@@ -148,6 +154,12 @@ void drop_graph(h3c_solver s) {
   if (s->graph) cudaGraphExecDestroy(s->graph);
   s->graph = nullptr;
   s->graph_steps = 0;
+  for (int k = 0; k < 2; ++k) {
+    if (s->graph1[k]) cudaGraphExecDestroy(s->graph1[k]);
+    s->graph1[k] = nullptr;
+    s->graph1_q0[k] = nullptr;
+  }
+  s->plain_done = false;  // the next capture follows a plain step of the current configuration
   // a coupled graph holds this solver's and its partner's buffers
   drop_cpl_graph(s);
   if (s->partner && s->partner->cpl_with == s) drop_cpl_graph(s->partner);
@@ -1221,6 +1233,52 @@ static bool build_graph(h3c_solver s) {
   return true;
 }
 
+// One step replayed from the one-step graph captured for the current lhs
+// buffer (captured on first use); false when no graph can be had.
+static bool step_graph(h3c_solver s) {
+  int k = -1;
+  for (int j = 0; j < 2 && k < 0; ++j)
+    if (s->graph1[j] && s->graph1_q0[j] == s->d_q[0]) k = j;
+  if (k < 0) {
+    for (int j = 0; j < 2 && k < 0; ++j)
+      if (!s->graph1[j]) k = j;
+    if (k < 0) return false;
+    double* saved[3] = {s->d_q[0], s->d_q[1], s->d_q[2]};
+    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    const long long l0 = s->launches;
+    enqueue_steps(s, 1);
+    const long long per_step = s->launches - l0;
+    s->launches = l0;
+    for (int j = 0; j < 3; ++j) s->d_q[j] = saved[j];  // the capture did not run the step
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (e != cudaSuccess || !g) {
+      cudaGetLastError();
+      if (g) cudaGraphDestroy(g);
+      return false;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&s->graph1[k], g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) {
+      cudaGetLastError();
+      s->graph1[k] = nullptr;
+      return false;
+    }
+    s->graph1_q0[k] = s->d_q[0];
+    s->graph1_launches = per_step;
+  }
+  if (cudaGraphLaunch(s->graph1[k], s->stream) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  s->launches += s->graph1_launches;
+  if (s->desc.time_integration == H3C_EULER_FORWARD) std::swap(s->d_q[0], s->d_q[1]);  // as enqueue_step does
+  return true;
+}
+
 int h3c_solve(h3c_solver s, int64_t nsteps) {
   if (!s || nsteps < 0) return H3C_E_INVALID;
   if (int rc = ready(s, "h3c_solve")) return rc;
@@ -1233,6 +1291,7 @@ int h3c_solve(h3c_solver s, int64_t nsteps) {
     if (!s->graph) {
       const long long l0 = s->launches;
       enqueue_steps(s, 1);  // one plain step first (sets kernel attributes outside capture)
+      s->plain_done = true;
       const long long per_step = s->launches - l0;
       nsteps -= 1;
       if (build_graph(s)) s->graph_launches = per_step * kGraphSteps;
@@ -1243,7 +1302,12 @@ int h3c_solve(h3c_solver s, int64_t nsteps) {
       nsteps -= kGraphSteps;
     }
   }
-  enqueue_steps(s, nsteps);
+  // the remaining single steps from a one-step graph, once a step has run plainly
+  while (graphable && s->plain_done && nsteps > 0 && step_graph(s)) --nsteps;
+  if (nsteps > 0) {
+    enqueue_steps(s, nsteps);
+    s->plain_done = true;
+  }
   return s->cuda(cudaGetLastError(), "h3c_solve");
 }
 

@@ -231,10 +231,11 @@ def test_tile_kernel_matches_per_cell_kernel(ti, flux):
     assert rel_err(a.state(0)[:, :fg], b.state(0)[:, :fg]) <= 1e-13
 
 
-@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2])
+@pytest.mark.parametrize("ti", [h3o.EULER_FORWARD, h3o.RK2, h3o.SSPRK3])
 def test_graph_replay_matches_single_steps(ti):
-    """Runs of steps replay a captured CUDA graph; interleaved odd counts
-    exercise forward Euler's buffer swap against the captured pointers."""
+    """Runs of steps replay a captured CUDA graph and single steps a one-step
+    graph; interleaved odd counts exercise forward Euler's buffer swap against
+    the captured pointers.  Against the same steps launched without graphs."""
     from hom3_b200 import _ffi as F
     _, (o,) = cases.euler_case("sod", nd=3, level=4, ti=ti)
     a = cases.gpu_solver_from_oracle(o)
