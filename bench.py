@@ -146,7 +146,19 @@ def build_workload(args):
     from hom3_b200 import workloads as W
 
     spec = W.riemann3d_spec(args.base_level, args.extra_levels)
-    t = hb.build_tables(spec, spec.cube_boundaries())
+    # the grid tables from the device builder; the host builder's, timed beside, must be identical
+    t0 = time.perf_counter()
+    t = hb.build_tables(spec, spec.cube_boundaries(), device=True)
+    t1 = time.perf_counter()
+    th = hb.build_tables(spec, spec.cube_boundaries())
+    t2 = time.perf_counter()
+    same = all(np.array_equal(t[k], th[k]) for k in ("neighbors", "x_center", "length", "bc_idx")) and (
+        (t["subface_cells"] is None and th["subface_cells"] is None) or
+        np.array_equal(t["subface_cells"], th["subface_cells"]))
+    args.grid_build = {"device_s": round(t1 - t0, 3), "host_s": round(t2 - t1, 3), "identical": bool(same),
+                       "what": "h3c_grid_build_device (kernels + download) vs h3c_grid_build (host), same tables"}
+    if not same:
+        raise RuntimeError("device and host grid builders disagree")
     fg = t["first_ghost"]
     modes = W.fourier_modes()
     q = np.zeros((5, t["ncells"]))
@@ -834,6 +846,7 @@ def main():
     }
     if adj is not None:
         line["adjoint"] = adj
+    line["grid_build"] = getattr(args, "grid_build", None)
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         ups, cells, nst, threads, el = cpu_oracle_run(args)
         line["cpu_baseline"] = {"value": ups, "unit": "cell-updates/s", "cores": threads, "kind": "port",
