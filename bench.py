@@ -476,6 +476,80 @@ def run_vortex(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_advection(args, ws, rank, local):
+    """hom3's advection test (advection_fv_solver_test.cpp:53-126) at a larger
+    size: the disc q = 1 (r = 0.08 around (0.25, 0.5)) in q = 0.1 carried by
+    the test's rotating velocity field on a uniform 2^L x 2^L grid over [0,1]^2,
+    characteristic conditions, forward Euler.  The timed run uses the LLF flux
+    at CFL 0.5; hom3's own upwind flux at CFL 1 (unstable where the face
+    velocity is negative: it negates u_L q_L) is timed beside it."""
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200 import workloads as W
+    from hom3_b200.solver import adv_characteristic
+
+    torch.cuda.set_device(local)
+    level = args.adv_level
+    spec = hb.GridSpec(2, [0.0, 0.0], [1.0, 1.0], level)
+    t = hb.build_tables(spec, spec.cube_boundaries(), device=True)
+    fg, n = t["first_ghost"], t["ncells"]
+    u = W.rotation_velocity(t["x_center"])
+    q0 = np.zeros((1, n))
+    q0[:, :fg] = hb.cell_average(W.disc_ic(), t["x_center"][:, :fg], t["length"][:fg], 2)
+    out = {}
+    for name, flux, cfl in (("llf_fe", F.FLUX_LLF, 0.5), ("hom3_upwind_fe", F.FLUX_UPWIND, 1.0)):
+        s = hb.Solver(2, F.ADVECTION, flux, F.EULER_FORWARD, F.FP64, cfl=cfl, time_end=1e30)
+        s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg, [adv_characteristic()] * 4)
+        s.set_velocity(u)
+        stream = torch.cuda.ExternalStream(s.stream())
+        s.set_state(q0, 0)
+        s.reset_time()
+        s.solve(args.warmup)
+        s.set_state(q0, 0)
+        s.reset_time()
+        torch.cuda.synchronize()
+        l0 = s.launches()
+        with ClockSampler(local) as clk:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            s.solve(args.steps)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+        ms = allreduce_max(ev0.elapsed_time(ev1), ws)
+        launches = s.launches() - l0
+        q = s.state(0)[0, :fg]
+        s.profile(True)
+        s.solve(min(args.steps, 50))
+        torch.cuda.synchronize()
+        s.profile(False)
+        kern = s.profile_read()
+        out[name] = dict(value=fg * args.steps * ws / (ms * 1e-3), ms=ms, launches=int(launches),
+                         q_min=float(q.min()), q_max=float(q.max()), clocks=clk.summary(),
+                         kernels_ms={k: {"total_ms": v[0], "launches": v[1]} for k, v in kern.items()})
+    a = out["llf_fe"]
+    st = a["kernels_ms"].get("stage1", {"total_ms": 0.0, "launches": 0})
+    stage_ms = st["total_ms"] / max(st["launches"], 1)
+    # algorithmic bytes per cell and stage: q read + written (16 B), the cell's velocity (16 B),
+    # 4 int32 neighbours (16 B) and the level byte
+    b_cell = 8 + 8 + 16 + 16 + 1
+    peak, peak_src = peaks()
+    achieved = fg * b_cell / (stage_ms * 1e-3) / 1e9 if stage_ms > 0 else None
+    line = {"metric": "cell-updates/s", "value": a["value"], "unit": "cell-updates/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": a["ms"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"2D advection (hom3's rotating-disc test) on a uniform {2 ** level}^2 grid, "
+                                   "characteristic conditions, LLF flux, forward Euler, CFL 0.5",
+                       "leaf_cells": int(fg), "l2": "working set (state, velocity, tables) exceeds the 126 MB L2"},
+            "roofline": {"bound": "hbm", "kernel": "k_stage (advection)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak if achieved else None,
+                         "algorithmic_bytes_per_cell": b_cell, "avg_launch_ms": stage_ms, "peak_source": peak_src},
+            "gpu_launches": a["launches"], "runs": out, "clocks": a["clocks"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_cht(args, ws, rank, local):
     """Conjugate heat transfer: CNS channel 512 x 128 over a heat-conducting
     solid 512 x 64 in one level-9 root cell, conductivity ratio 10, solid
@@ -727,7 +801,9 @@ def main():
     ap.add_argument("--extra-levels", type=int, default=2)
     ap.add_argument("--cfl", type=float, default=0.4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="riemann3d", choices=["riemann3d", "ensemble", "tgv", "vortex", "cht"])
+    ap.add_argument("--workload", default="riemann3d",
+                    choices=["riemann3d", "ensemble", "tgv", "vortex", "cht", "advection"])
+    ap.add_argument("--adv-level", type=int, default=11)
     ap.add_argument("--vortex-level", type=int, default=8)
     ap.add_argument("--tgv-level", type=int, default=7)
     ap.add_argument("--members", type=int, default=256)
@@ -746,6 +822,9 @@ def main():
         return
     if args.workload == "cht" and args.impl == "ours":
         run_cht(args, ws, rank, local)
+        return
+    if args.workload == "advection" and args.impl == "ours":
+        run_advection(args, ws, rank, local)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)

@@ -185,3 +185,25 @@ def cht_setup(level=9, side=4.0, fluid_rows=128, solid_rows=64, kappa=10.0, seed
     return dict(tables_fluid=tf, tables_solid=ts, conditions_fluid=cf, conditions_solid=cs,
                 partners_fluid=partner_cells(tf, ts), partners_solid=partner_cells(ts, tf), q_fluid=qf, q_solid=qs,
                 props=dict(Minfty=Minfty, ReInfty=ReInfty, Pr0=0.72, cfl=0.4, cfl_viscous=0.4), T_inf=T_inf, h=h)
+
+
+# ---- advection (advection/tests/advection_fv_solver_test.cpp) ----
+def rotation_velocity(x, u_mag=0.5, centre=(0.5, 0.5)):
+    """radial_velocity of advection_fv_solver_test.cpp:67-84 (a rotation about
+    the centre), written as the test writes it, for points x [2][n]."""
+    c0, c1 = centre
+    radius = np.sqrt((x[0] - c0) ** 2 + (x[1] - c1) ** 2)
+    angle = 0.5 * math.pi - np.arccos((x[0] - c0) / radius)
+    v0 = np.abs(radius * u_mag * np.sin(angle + 0.5 * math.pi))
+    v1 = np.abs(radius * u_mag * np.cos(angle + 0.5 * math.pi))
+    v0 = np.where(x[1] - c1 > 0.0, -v0, v0)
+    v1 = np.where(x[0] - c0 < 0.0, -v1, v1)
+    return np.stack([v0, v1])
+
+
+def disc_ic(centre=(0.25, 0.5), radius=0.08, q_in=1.0, q_out=0.1):
+    """constant_ic of advection_fv_solver_test.cpp:100-111: q_in inside the disc, q_out outside."""
+    def f(x):
+        r = np.sqrt((x[0] - centre[0]) ** 2 + (x[1] - centre[1]) ** 2)
+        return np.where(r - radius > 0.0, q_out, q_in)[None, :]
+    return f
