@@ -315,3 +315,17 @@ def test_advection_time_step():
     u = o.velocity()[:, :fg]
     want = (0.7 * t["length"][:fg] / np.abs(u).max(axis=0)).min()
     assert abs(o.min_dt() - want) <= 1e-15 * want
+
+
+def test_advection_bench_inputs_match_the_oracle():
+    """The advection workload's velocity field and initial disc (hom3_b200.workloads)
+    against the oracle's restatement of hom3's test: velocity to rounding of the
+    trigonometric functions, cell averages exactly."""
+    import hom3_b200 as hb
+    from hom3_b200 import workloads as W
+    _, (o,) = cases.advection_case(level=6)
+    t = o.tables()
+    fg = o.first_ghost
+    assert np.abs(W.rotation_velocity(t["x_center"]) - o.velocity()).max() <= 1e-15
+    q = hb.cell_average(W.disc_ic(), t["x_center"][:, :fg], t["length"][:fg], 2)
+    assert np.array_equal(q[0], o.state(0)[0, :fg])
