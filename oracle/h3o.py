@@ -1,7 +1,7 @@
 """ctypes front-end of the CPU oracle (oracle/h3o.hpp).
 
-TEST INFRASTRUCTURE ONLY.  Imported by tests/, by __graft_entry__.smoke() as
-the checker and by the CPU-baseline / reference legs of bench.py.  The shipped
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, by __graft_entry__.smoke() to
+check the GPU's result and by the CPU-baseline / reference legs of bench.py.  The shipped
 library (hom3_b200) never imports it.
 
 Parity status: the grid/neighbour layer is pinned against hom3's golden

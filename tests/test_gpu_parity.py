@@ -3,7 +3,7 @@
 The oracle builds hom3's grid and initial state; its hom3-numbered tables and
 state go through h3c_set_grid / h3c_set_state exactly as a hom3 Solver would
 hand them over, and both sides then step.  Tolerances: FP64 path <= 1e-12
-relative per step, multi-step runs <= 1e-10 (rounding of
+relative per step (the bar this path is held to), multi-step runs <= 1e-10 (rounding of
 FMA-contracted kernels against the oracle's uncontracted arithmetic compounds
 over steps); mixed path (FP32 face fluxes) <= 1e-5 relative per step.
 """

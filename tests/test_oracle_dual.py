@@ -1,5 +1,5 @@
-"""The forward-mode dual-number build of the oracle (Solver<Dual>, the
-checker of the discrete adjoint) against central finite differences of the
+"""The forward-mode dual-number build of the oracle (Solver<Dual>, which the
+GPU's discrete adjoint is compared with) against central finite differences of the
 double build: same values bit for bit, derivatives to second order in the
 finite-difference step.  Time steps are frozen (forced) in both."""
 import numpy as np
