@@ -695,8 +695,30 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
         const double f = uL * qL;
         return u_srfc < 0 ? f * -1. : f;
       };
+      if (!HANG) {
+        // all neighbour indices first, then all neighbour states and velocities: the loads of
+        // every face are in flight together
+        int nm[ND], np_[ND];
+        double uc[ND], qm[ND], qp[ND], um[ND], up[ND];
 #pragma unroll
-      for (int d = 0; d < ND; ++d) {
+        for (int d = 0; d < ND; ++d) {
+          nm[d] = __ldg(g.nbr + (2 * d) * ld + c);
+          np_[d] = __ldg(g.nbr + (2 * d + 1) * ld + c);
+          uc[d] = __ldg(g.vel + d * ld + c);
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d) {
+          qm[d] = __ldg(qin + nm[d]);
+          um[d] = __ldg(g.vel + d * ld + nm[d]);
+          qp[d] = __ldg(qin + np_[d]);
+          up[d] = __ldg(g.vel + d * ld + np_[d]);
+        }
+#pragma unroll
+        for (int d = 0; d < ND; ++d)
+          acc[0] = acc[0] + (adv_flux(qm[d], qc[0], um[d], uc[d]) - adv_flux(qc[0], qp[d], uc[d], up[d]));
+      }
+#pragma unroll
+      for (int d = 0; d < ND && HANG; ++d) {
         const double uc = __ldg(g.vel + d * ld + c);
         const int m = g.nbr[(2 * d) * ld + c], p = g.nbr[(2 * d + 1) * ld + c];
         double fm, fp;
