@@ -477,7 +477,7 @@ def run_vortex(args, ws, rank, local):
 
 
 def run_advection(args, ws, rank, local):
-    """hom3's advection test (advection_fv_solver_test.cpp:53-126) at a larger
+    """hom3's advection test (advection_fv_solver_test.cpp:51-125) at a larger
     size: the disc q = 1 (r = 0.08 around (0.25, 0.5)) in q = 0.1 carried by
     the test's rotating velocity field on a uniform 2^L x 2^L grid over [0,1]^2,
     characteristic conditions, forward Euler.  The timed run uses the LLF flux

@@ -258,7 +258,7 @@ __device__ __forceinline__ void llf(const Prim<R, ND>& L, const Prim<R, ND>& Rt,
   for (int v = 0; v < ND + 2; ++v) f[v] = R(0.5) * ((fl[v] + fr[v]) + dx_dt * (L.q[v] - Rt.q[v]));
 }
 
-// Sutherland's law: cns/quantities.hpp:467-469
+// Sutherland's law: cns/quantities.hpp:113-115
 template <class R> __device__ __forceinline__ R sutherland(R T, R sOverTref, R sOverTrefP1) {
   return (T * sqrt(T)) * sOverTrefP1 / (T + sOverTref);
 }
@@ -321,7 +321,7 @@ __device__ __forceinline__ void viscous(const Prim<R, ND>& L, const Prim<R, ND>&
 
 // ---------------------------------------------------------------------------
 // per-cell time step: euler/physics.hpp:182-196, cns/physics.hpp:167-187,
-// heat/physics.hpp:82-85, advection/physics.hpp:86-93 (u: the cell's velocity)
+// heat/physics.hpp:82-85, advection/physics.hpp:78-87 (u: the cell's velocity)
 // ---------------------------------------------------------------------------
 template <int ND, int PHYS>
 __device__ __forceinline__ double cell_dt(const double* q, double h, const PhysConst& pc,
@@ -406,7 +406,7 @@ __global__ void k_reset_slot(long long* slot, int n_inst) {
 #endif  // H3C_DEVICE_FUNCTIONS_ONLY
 
 // ---------------------------------------------------------------------------
-// isentropic vortex: euler/initial_conditions.hpp:343-368 (2D, hom3's fixed
+// isentropic vortex: euler/initial_conditions.hpp:14-39 (2D, hom3's fixed
 // parameters: beta 5, gamma 1.4, centre (-5,-5), u = v = 1)
 // ---------------------------------------------------------------------------
 __device__ inline void isentropic_vortex(double x0, double x1, double t, double* out) {
@@ -468,17 +468,17 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
   for (int v = 0; v < NV; ++v) qb[v] = q[v * ld + bc];
   double out[NV];
   switch (B.kind) {
-    case BC_EULER_NEUMANN:  // euler/boundary_conditions.hpp:253-264
-    case BC_HEAT_NEUMANN:   // heat/boundary_conditions.hpp:186-194
+    case BC_EULER_NEUMANN:  // euler/boundary_conditions.hpp:17-43
+    case BC_HEAT_NEUMANN:   // heat/boundary_conditions.hpp:40-63
 #pragma unroll
       for (int v = 0; v < NV; ++v) out[v] = qb[v] - gt.dx[i] * B.v[v];
       break;
-    case BC_EULER_DIRICHLET:  // euler/boundary_conditions.hpp:279-288
-    case BC_HEAT_DIRICHLET:   // heat/boundary_conditions.hpp:161-168
+    case BC_EULER_DIRICHLET:  // euler/boundary_conditions.hpp:47-67
+    case BC_HEAT_DIRICHLET:   // heat/boundary_conditions.hpp:15-37
 #pragma unroll
       for (int v = 0; v < NV; ++v) out[v] = 2.0 * B.v[v] - qb[v];
       break;
-    case BC_EULER_VORTEX: {  // euler/boundary_conditions.hpp:304-316
+    case BC_EULER_VORTEX: {  // euler/boundary_conditions.hpp:70-93
       double vg[4] = {0, 0, 0, 0}, vb[4] = {0, 0, 0, 0};
       if (ND == 2) {
         const double t = sc[gt.ginst ? gt.ginst[i] : 0].time;
@@ -492,7 +492,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
       }
       break;
     }
-    case BC_CPL_EULER_EULER: {  // euler/coupling_conditions.hpp:452-460
+    case BC_CPL_EULER_EULER: {  // euler/coupling_conditions.hpp:17-35
       const int o = gt.partner[i];
       if (o < 0 || pv.q == nullptr) return;  // host refuses to launch without partner tables
 #pragma unroll
@@ -506,13 +506,13 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
       for (int v = 0; v < NV; ++v) out[v] = q[v * ld + o];
       break;
     }
-    case BC_ADV_NEUMANN:  // advection/boundary_conditions.hpp:56-63
+    case BC_ADV_NEUMANN:  // advection/boundary_conditions.hpp:50-58
       out[0] = qb[0] - gt.dx[i] * B.v[0];
       break;
-    case BC_ADV_DIRICHLET:  // :29-35
+    case BC_ADV_DIRICHLET:  // :25-32
       out[0] = 2.0 * B.v[0] - qb[0];
       break;
-    case BC_ADV_CHARACTERISTIC: {  // :79-95
+    case BC_ADV_CHARACTERISTIC: {  // :71-91
       // inflow (the boundary cell's velocity along the ghost's direction points into the domain):
       // dirichlet(q_b, q_b); otherwise neumann(q_b, 0, dx).  Both are q_b.
       const int pos = gt.pos[i];
@@ -521,8 +521,8 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
       out[0] = inflow ? 2.0 * qb[0] - qb[0] : qb[0] - gt.dx[i] * 0.0;
       break;
     }
-    case BC_CPL_HEAT_CNS:     // heat/coupling_conditions.hpp:233-246
-    case BC_CPL_HEAT_HEAT: {  // :256-269
+    case BC_CPL_HEAT_CNS:     // heat/coupling_conditions.hpp:24-37
+    case BC_CPL_HEAT_HEAT: {  // :47-60
       if (gt.partner[i] < 0 || pv.q == nullptr) return;
       const double Tother = partner_T(B, pv, gt.partner[i]);
       const double Tthis = qlhs[bc];
@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
           if (d == ndir) gp[d] = 0.0 - bp[d];
       } else if (B.kind == BC_CNS_ISOTHERMAL_NOSLIP || B.kind == BC_CPL_CNS_HEAT) {  // :209-228
         double Ts = B.v[0];
-        if (B.kind == BC_CPL_CNS_HEAT) {  // cns/coupling_conditions.hpp:278-292
+        if (B.kind == BC_CPL_CNS_HEAT) {  // cns/coupling_conditions.hpp:28-42
           if (gt.partner[i] < 0 || pv.q == nullptr) return;
           double ql[ND + 2];
 #pragma unroll
@@ -684,7 +684,7 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
     for (int v = 0; v < NV; ++v) acc[v] = 0.0;
 
     if (PHYS == ADVECTION) {
-      // advection/physics.hpp:130-153 on the cells' velocities along d: local Lax-Friedrichs,
+      // advection/physics.hpp:120-145 on the cells' velocities along d: local Lax-Friedrichs,
       // or hom3's upwind flux u_L q_L, negated when the face velocity (u_L + u_R) / 2 is negative
       auto adv_flux = [&](double qL, double qR, double uL, double uR) {
         if (FLUX == LLF) {

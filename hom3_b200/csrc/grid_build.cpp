@@ -4,7 +4,7 @@
 // (solver.hpp:876-977) without hom3's pointer tree: leaves are addressed by
 // (level, integer coordinates) in dense per-level lookup arrays, neighbours
 // are found by coordinate arithmetic instead of up/down tree walks
-// (implementation.hpp:457-543), and interior cells come out in Morton order,
+// (hierarchical/implementation.hpp:457-543), and interior cells come out in Morton order,
 // which for a MinLevel grid is also hom3's leaf order.  Conventions that must
 // match hom3 to give identical tables:
 //  * cell centres are accumulated from the root centre level by level with
@@ -165,7 +165,7 @@ int h3c_grid_build(const h3c_grid_desc* d, h3c_built_grid* out) {
   for (int k = 0; k < d->n_refine; ++k) maxl = std::max(maxl, d->refine_level[k]);
   Levels L;
   if (!L.init(nd, maxl)) { fail_msg("h3c_grid_build: grid too large for dense level maps"); return H3C_E_INVALID; }
-  // ---- leaves: MinLevel (generation.hpp:355-376), then sphere refinement ----
+  // ---- leaves: MinLevel (grid/generation.hpp:39-60), then sphere refinement ----
   std::vector<Cell> leaves;
   {
     const long long n = 1LL << (nd * d->min_level);

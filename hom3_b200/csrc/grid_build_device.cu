@@ -1,6 +1,6 @@
 // grid_build_device.cu -- the tables of h3c_grid_build (grid_build.cpp)
 // computed on the GPU (no hom3 counterpart: hom3 walks its pointer tree on
-// the host, implementation.hpp:457-543, and creates ghosts cell by cell,
+// the host, hierarchical/implementation.hpp:457-543, and creates ghosts cell by cell,
 // solver.hpp:935-977).
 //
 // The tree lives in dense per-level maps indexed by the Morton code of the

@@ -115,7 +115,7 @@ extern "C" int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t
   if (n_cells < 1 || n_cells > kNoAllocMaxCells || ld < n_cells) return H3C_E_INVALID;
   long long* scratch = nullptr;
   if (int rc = scratch_address(&scratch)) return rc;
-  // physical constants: euler/quantities.hpp:131-145, cns/quantities.hpp:377-384
+  // physical constants: euler/quantities.hpp:131-145, cns/quantities.hpp:28-30, 74-75
   const double gamma = desc->gamma, gm1 = gamma - 1.;
   const double T_inf = 1.0 / (1 + 0.5 * gm1 * (desc->Minfty * desc->Minfty));
   const double rho_inf = std::pow(T_inf, 1. / gm1);

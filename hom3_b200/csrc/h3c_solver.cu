@@ -445,7 +445,7 @@ __global__ void k_force_dt(Scalars* sc, double dt) {
   sc->forced_step = sc->step;
   sc->forced_dt = dt;
 }
-// coupling::apply(Tr0, cns, heat): coupling.hpp:172-183
+// coupling::apply(Tr0, cns, heat): coupling.hpp:52-63
 __global__ void k_couple_cht(Scalars* cns, Scalars* heat, double scaling) {
   const double min_dt_cns = ord_to_dbl(cns->mindt_ord);
   const double min_dt_heat = ord_to_dbl(heat->mindt_ord) / scaling;
@@ -455,7 +455,7 @@ __global__ void k_couple_cht(Scalars* cns, Scalars* heat, double scaling) {
   heat->forced_step = heat->step;
   heat->forced_dt = dt * scaling;
 }
-// coupling::apply(s1, s2): coupling.hpp:186-193
+// coupling::apply(s1, s2): coupling.hpp:66-73
 __global__ void k_couple_equal(Scalars* a, Scalars* b) {
   const double da = ord_to_dbl(a->mindt_ord), db = ord_to_dbl(b->mindt_ord);
   const double dt = (db < da) ? db : da;
@@ -510,7 +510,7 @@ int h3c_create(const h3c_desc* d, h3c_solver* out) {
   }
   if ((d->physics == H3C_ADVECTION) != (d->flux == H3C_FLUX_UPWIND) &&
       !(d->physics == H3C_ADVECTION && d->flux == H3C_FLUX_LLF)) {
-    g_last_error = "h3c_create: advection takes the upwind or LLF flux (advection/tags.hpp:18-19); "
+    g_last_error = "h3c_create: advection takes the upwind or LLF flux (advection/tags.hpp:14-15); "
                    "the upwind flux is advection's";
     return H3C_E_INVALID;
   }
@@ -518,7 +518,7 @@ int h3c_create(const h3c_desc* d, h3c_solver* out) {
   s->desc = *d;
   s->nd = d->nd;
   s->nv = (d->physics == H3C_HEAT || d->physics == H3C_ADVECTION) ? 1 : d->nd + 2;
-  // quantities: euler/quantities.hpp:131-145, cns/quantities.hpp:377-384
+  // quantities: euler/quantities.hpp:131-145, cns/quantities.hpp:28-30, 74-75
   const double gamma = d->gamma, gm1 = gamma - 1.;
   const double T_inf = 1.0 / (1 + 0.5 * gm1 * (d->Minfty * d->Minfty));
   const double rho_inf = std::pow(T_inf, 1. / gm1);
@@ -800,7 +800,7 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
     if (B.kind == H3C_BC_EULER_VORTEX) {
       if (nd != 2 || s->desc.physics == H3C_HEAT)
         return s->fail(H3C_E_INVALID, "h3c_set_grid: the isentropic vortex condition is 2D Euler/CNS only "
-                                      "(euler/initial_conditions.hpp:370-375)");
+                                      "(euler/initial_conditions.hpp:41-46)");
       s->unfused_dt = true;
     }
     if (B.kind >= H3C_BC_CPL_EULER_EULER && B.kind <= H3C_BC_CPL_HEAT_HEAT) s->needs_partner = true;
@@ -1010,7 +1010,7 @@ int h3c_write_vtk(h3c_solver s, const char* fname, const h3c_grid* grid, const i
     auto& x = nums(names, nv);
     x.nums = q;
   }
-  // physics_output: euler/physics.hpp:207-226 (+ cns/physics.hpp:193-201), advection/physics.hpp:96-102
+  // physics_output: euler/physics.hpp:207-226 (+ cns/physics.hpp:193-201), advection/physics.hpp:90-95
   if (phys == H3C_EULER || phys == H3C_CNS) {
     const double gamma = s->desc.gamma, gm1 = gamma - 1.0;
     std::vector<double> a(n), p(n), u((size_t)nd * n), M(n), e(n), T(n);

@@ -2,12 +2,12 @@
 // format: Solver::write_domain (src/solver/fv/solver.hpp:328-376) through
 // io::Vtk<nd, io::format::binary> (src/io/vtk.hpp:156-450).
 //
-// File layout (vtk.hpp:160-167, 226-330): an ASCII header, then POINTS (the
+// File layout (vtk.hpp:177-183, 239-338): an ASCII header, then POINTS (the
 // unique cell vertices sorted by x, then y, then z; 2D points get z = 0),
 // CELLS (2^nd vertex ids per cell, vertex order of child_rel_pos,
 // grid/grid.hpp:41-59), CELL_TYPES (pixel 8 / voxel 11) and CELL_DATA: one
 // SCALARS block per stream component.  Binary values are big-endian float32
-// (Num) and int32 (Ind); an invalid Ind is written as -1 (vtk.hpp:383).
+// (Num) and int32 (Ind); an invalid Ind is written as -1 (vtk.hpp:363, 382-385).
 // Cells are written in container order: internal cells, then ghosts.
 #include <algorithm>
 #include <cmath>
@@ -45,13 +45,13 @@ struct Out {
                                 (unsigned char)u};
     ok = ok && std::fwrite(b, 1, 4, f) == 4;
   }
-  void num(double x) {  // static_cast<float>, byte-swapped (vtk.hpp:384, 410-419)
+  void num(double x) {  // static_cast<float>, byte-swapped (vtk.hpp:364, 375-378, 415-441)
     const float v = (float)x;
     uint32_t u;
     std::memcpy(&u, &v, 4);
     be32(u);
   }
-  void id(int64_t x, int64_t invalid = INT64_MAX) {  // interpret_id (vtk.hpp:383)
+  void id(int64_t x, int64_t invalid = INT64_MAX) {  // interpret_id (vtk.hpp:363, 382-385)
     be32((uint32_t)(int32_t)(x == invalid ? -1 : (int32_t)x));
   }
   void newline() { text("\n"); }
@@ -73,7 +73,7 @@ int write_vtk_file(const VtkDomain& D, const std::vector<VtkStream>& streams, st
         verts[((size_t)c * nvert + v) * 3 + d] = D.x_center[d * D.ld + c] + hh * rel;
       }
   }
-  // unique vertices in the order of vertex_cmp (x major, then y, then z; vtk.hpp:248-265)
+  // unique vertices in the order of vertex_cmp (x major, then y, then z; vtk.hpp:264-294)
   std::vector<int64_t> order((size_t)n * nvert);
   for (size_t i = 0; i < order.size(); ++i) order[i] = (int64_t)i;
   auto key = [&](int64_t i, int d) { return verts[(size_t)i * 3 + d]; };
@@ -103,30 +103,30 @@ int write_vtk_file(const VtkDomain& D, const std::vector<VtkStream>& streams, st
     if (err) *err = "cannot open " + D.path;
     return -1;
   }
-  // header (vtk.hpp:160-167)
+  // header (vtk.hpp:177-183, 407-411)
   o.text("# vtk DataFile Version 2.0\n");
   o.text("HOM3 legacy vtk Output \n");
   o.text("BINARY\n");
   o.text("DATASET UNSTRUCTURED_GRID\n");
-  // points (vtk.hpp:271-279)
+  // points (vtk.hpp:296-304)
   o.text("POINTS " + std::to_string(uniq.size()) + " FLOAT\n");
   for (const int64_t i : uniq) {
     for (int d = 0; d < nd; ++d) o.num(key(i, d));
     if (nd == 2) o.num(0.0);
   }
   o.newline();
-  // cells (vtk.hpp:283-298)
+  // cells (vtk.hpp:306-326)
   o.text("CELLS " + std::to_string(n) + " " + std::to_string(n * (nvert + 1)) + "\n");
   for (int64_t c = 0; c < n; ++c) {
     o.id(nvert);
     for (int v = 0; v < nvert; ++v) o.id(uid[(size_t)c * nvert + v]);
   }
   o.newline();
-  // cell types (vtk.hpp:300-303): pixel 8, voxel 11
+  // cell types (vtk.hpp:328-331): pixel 8, voxel 11
   o.text("CELL_TYPES " + std::to_string(n) + "\n");
   for (int64_t c = 0; c < n; ++c) o.id(nd == 2 ? 8 : 11);
   o.newline();
-  // cell data (vtk.hpp:305-309, 183-218)
+  // cell data (vtk.hpp:333-337, 201-237)
   o.text("CELL_DATA " + std::to_string(n) + "\n");
   for (const VtkStream& s : streams) {
     for (int k = 0; k < s.dims; ++k) {

@@ -206,7 +206,7 @@ class Solver:
 
     def set_velocity(self, u):
         """Advection velocity u(x_center) of every cell, ghosts included: [nd][n_cells]
-        (Physics::velocity, advection/physics.hpp:116-118)."""
+        (Physics::velocity, advection/physics.hpp:104-106)."""
         u = np.ascontiguousarray(u, np.float64)
         assert u.shape == (self.nd, self.n_cells), u.shape
         self._check(lib().h3c_set_velocity(self.h, _dp(u), self.n_cells))
@@ -384,7 +384,7 @@ class Batch(Solver):
 
 
 def couple_cht(Tr0, cns: Solver, heat: Solver):
-    """coupling::apply(Tr0, cns, heat) -- coupling.hpp:167-183."""
+    """coupling::apply(Tr0, cns, heat) -- coupling.hpp:52-63."""
     check(lib().h3c_couple_cht(cns.h, heat.h, float(Tr0)), cns.h)
 
 
@@ -408,7 +408,7 @@ def cht_adjoint(Tr0, cns: Solver, heat: Solver, nsteps: int, dJ_dqN, dJ_dTN, eve
 
 
 def couple_equal(a: Solver, b: Solver):
-    """coupling::apply(s1, s2) -- coupling.hpp:186-193."""
+    """coupling::apply(s1, s2) -- coupling.hpp:66-73."""
     check(lib().h3c_couple_equal(a.h, b.h), a.h)
 
 

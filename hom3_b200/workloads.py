@@ -4,7 +4,7 @@ riemann3d_refined: 3D Euler on a hierarchical Cartesian tree -- base level 6
 (64^3) on the unit cube, refined +2 levels (to level 8) in the sphere of
 radius 0.25 at the centre, 2:1 face balanced.  Initial state: Riemann problem
 split at x = 0.5 (left rho = 1, p = 1; right rho = 0.125, p = 0.1; u = 0) as
-in hom3's shock_tube (euler/initial_conditions.hpp:380-419), with 1%
+in hom3's shock_tube (euler/initial_conditions.hpp:51-90), with 1%
 perturbations of rho and p from 16 Fourier modes (integer wave vectors in
 [1,4]^3, phases U[0, 2pi), numpy PCG64 seed 0).  Zero-gradient outflow
 (Neumann) on all six faces, AUSM flux, RK2.
@@ -71,7 +71,7 @@ def riemann3d_conditions(nd=3):
 # Ensemble of independent 2D isentropic vortices (batched workload).
 # ---------------------------------------------------------------------------
 def vortex_ic(beta, cx, cy, u=1.0, v=1.0, gamma=1.4):
-    """hom3's isentropic vortex (euler/initial_conditions.hpp:343-368) with the
+    """hom3's isentropic vortex (euler/initial_conditions.hpp:14-39) with the
     strength and centre as parameters (hom3 fixes beta = 5, centre (-5, -5))."""
     def f(x):
         dx, dy = x[0] - cx, x[1] - cy
@@ -189,7 +189,7 @@ def cht_setup(level=9, side=4.0, fluid_rows=128, solid_rows=64, kappa=10.0, seed
 
 # ---- advection (advection/tests/advection_fv_solver_test.cpp) ----
 def rotation_velocity(x, u_mag=0.5, centre=(0.5, 0.5)):
-    """radial_velocity of advection_fv_solver_test.cpp:67-84 (a rotation about
+    """radial_velocity of advection_fv_solver_test.cpp:69-85 (a rotation about
     the centre), written as the test writes it, for points x [2][n]."""
     c0, c1 = centre
     radius = np.sqrt((x[0] - c0) ** 2 + (x[1] - c1) ** 2)
@@ -202,7 +202,7 @@ def rotation_velocity(x, u_mag=0.5, centre=(0.5, 0.5)):
 
 
 def disc_ic(centre=(0.25, 0.5), radius=0.08, q_in=1.0, q_out=0.1):
-    """constant_ic of advection_fv_solver_test.cpp:100-111: q_in inside the disc, q_out outside."""
+    """constant_ic of advection_fv_solver_test.cpp:106-115: q_in inside the disc, q_out outside."""
     def f(x):
         r = np.sqrt((x[0] - centre[0]) ** 2 + (x[1] - centre[1]) ** 2)
         return np.where(r - radius > 0.0, q_out, q_in)[None, :]

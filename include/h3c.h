@@ -43,20 +43,20 @@ extern "C" {
 #define H3C_E_NOMEM (-6)     /* device allocation failed */
 
 /* physics: euler/physics.hpp:25, cns/physics.hpp:27, heat/physics.hpp:21,
- * advection/physics.hpp:21-162 (one scalar q carried by a given velocity
+ * advection/physics.hpp:21-149 (one scalar q carried by a given velocity
  * field u(x), h3c_set_velocity) */
 #define H3C_EULER 0
 #define H3C_CNS 1
 #define H3C_HEAT 2
 #define H3C_ADVECTION 3
-/* numerical flux tags: euler/tags.hpp:13-16 (AUSM, LLF); cns/tags.hpp:29
+/* numerical flux tags: euler/tags.hpp:13-16 (AUSM, LLF); cns/tags.hpp:22
  * (standard = AUSM + three-point viscous, selected by H3C_CNS + AUSM);
  * heat/tags.hpp:13 (three_point, the only heat flux). */
 #define H3C_FLUX_AUSM 0
 #define H3C_FLUX_LLF 1
-/* advection/tags.hpp:18-19: local Lax-Friedrichs (H3C_FLUX_LLF) or upwind.
+/* advection/tags.hpp:14-15: local Lax-Friedrichs (H3C_FLUX_LLF) or upwind.
  * hom3's upwind flux is u_L q_L, negated when the face velocity
- * (u_L + u_R)/2 is negative (advection/physics.hpp:142-153); reproduced. */
+ * (u_L + u_R)/2 is negative (advection/physics.hpp:132-145); reproduced. */
 #define H3C_FLUX_UPWIND 2
 /* time integration tags: solver/fv/tags.hpp:24-25 */
 #define H3C_EULER_FORWARD 0
@@ -80,7 +80,7 @@ extern "C" {
  *  EULER_NEUMANN      surface flux per variable (euler/boundary_conditions.hpp:17-43)
  *  EULER_DIRICHLET    surface state per variable (:47-67)
  *  EULER_VORTEX       none; analytic isentropic vortex, overwrites the
- *                     boundary cell too (:71-93, initial_conditions.hpp:343-368)
+ *                     boundary cell too (:71-93, euler/initial_conditions.hpp:14-39)
  *  CNS_INFLOW         surface primitive state (u_0..u_{nd-1}, rho, p); u and
  *                     rho imposed, zero normal pressure gradient (cns/boundary_conditions.hpp:28-65)
  *  CNS_OUTFLOW        same layout, only p is used (:72-105)
@@ -88,9 +88,9 @@ extern "C" {
  *  CNS_ISOTHERMAL_NOSLIP  v[0] = wall temperature (:200-238)
  *  HEAT_DIRICHLET     v[0] = surface temperature (heat/boundary_conditions.hpp:15-37)
  *  HEAT_NEUMANN       v[0] = surface heat flux (:40-63)
- *  ADV_DIRICHLET      v[0] = surface value (advection/boundary_conditions.hpp:17-42)
- *  ADV_NEUMANN        v[0] = surface flux (:45-70)
- *  ADV_CHARACTERISTIC none (:73-97; both of its branches give the boundary cell's value)
+ *  ADV_DIRICHLET      v[0] = surface value (advection/boundary_conditions.hpp:15-37)
+ *  ADV_NEUMANN        v[0] = surface flux (:40-63)
+ *  ADV_CHARACTERISTIC none (:66-94; both of its branches give the boundary cell's value)
  *  CPL_*              coupling with the partner solver (h3c_set_partner):
  *                     euler/coupling_conditions.hpp:17-35, cns/coupling_conditions.hpp:22-43,
  *                     heat/coupling_conditions.hpp:18-61.  CPL_CNS_HEAT / CPL_HEAT_CNS:
@@ -215,7 +215,7 @@ int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld);
 int h3c_write_vtk(h3c_solver s, const char* fname, const h3c_grid* grid, const int64_t* node_ids);
 /* Advection velocity of every cell, ghosts included: the physics' velocity
  * function evaluated at the cell centres (Physics::velocity,
- * advection/physics.hpp:116-118, which hom3 evaluates at x_center on every
+ * advection/physics.hpp:104-106, which hom3 evaluates at x_center on every
  * use).  Host array [nd][ld], caller numbering.  Required before an
  * advection solver steps; the next time step is recomputed from it. */
 int h3c_set_velocity(h3c_solver s, const double* u, int64_t ld);
@@ -315,21 +315,21 @@ int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps,
  * for ghost g, or any negative value for ghosts of non-coupled conditions.
  * Both solvers then share the partner's stream. */
 int h3c_set_partner(h3c_solver s, h3c_solver partner, const int64_t* partner_cells);
-/* coupling::apply(Tr0, cns, heat), coupling.hpp:167-183 */
+/* coupling::apply(Tr0, cns, heat), coupling.hpp:52-63 */
 int h3c_couple_cht(h3c_solver cns, h3c_solver heat, double Tr0);
 /* nsteps of the coupled loop of coupled_cns_heat_test.cpp:235-248 --
  * coupling::apply(Tr0, cns, heat), cns.solve(), heat.solve() per step -- on
  * the solvers' shared stream; runs of steps replay one captured CUDA graph
  * (the same kernels as the three calls per step). */
 int h3c_cht_solve(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps);
-/* coupling::apply(s1, s2), coupling.hpp:186-193 */
+/* coupling::apply(s1, s2), coupling.hpp:66-73 */
 int h3c_couple_equal(h3c_solver a, h3c_solver b);
 /* EXTENSION (not in hom3): partner cells (caller numbering, same solver) for
  * the ghosts of H3C_BC_PERIODIC conditions. */
 int h3c_set_periodic(h3c_solver s, const int64_t* partner_cells);
 
 /* ---- grid builder (the device grid layer): builds hom3-equivalent tables
- * for the MinLevel generator (grid/generation.hpp:355-376) and cube /
+ * for the MinLevel generator (grid/generation.hpp:39-60) and cube /
  * box boundaries (grid/helpers.hpp:112-160, geometry/implicit.hpp:39-205),
  * with leaves in Morton order.  EXTENSION (not in hom3): refinement of the
  * cells that intersect spheres, 2:1 balanced, with coarse/fine faces. ---- */

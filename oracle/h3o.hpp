@@ -105,7 +105,7 @@ struct Tree {
   double rootLength;
   double rootCoords[3] = {0, 0, 0};
   std::vector<Ind> parent, firstChild;
-  std::vector<std::vector<Ind>> node2cell;  // per solver (implementation.hpp:207-218)
+  std::vector<std::vector<Ind>> node2cell;  // per solver (hierarchical/implementation.hpp:207-218)
 
   // RootCell ctor: grid/grid.hpp:108-132 (length starts at machine epsilon)
   Tree(int nd_, const double* xmin, const double* xmax, int maxSolvers) : nd(nd_) {
@@ -124,19 +124,19 @@ struct Tree {
   int npos() const { return 2 * nd; }
   bool is_root(Ind n) const { return parent[n] == INV; }
   bool is_leaf(Ind n) const { return firstChild[n] == INV; }
-  // child(): implementation.hpp:256-259.  For a leaf hom3 adds pos to the
+  // child(): hierarchical/implementation.hpp:256-259.  For a leaf hom3 adds pos to the
   // invalid id (overflow); the intended meaning (no child) is used here.
   Ind child(Ind n, int pos) const { return firstChild[n] == INV ? INV : firstChild[n] + pos; }
-  // position_in_parent: implementation.hpp:271-280
+  // position_in_parent: hierarchical/implementation.hpp:271-280
   int pos_in_parent(Ind n) const { return (int)(n - firstChild[parent[n]]); }
-  // level: implementation.hpp:427-441
+  // level: hierarchical/implementation.hpp:427-441
   int level(Ind n) const {
     int l = 0;
     n = parent[n];
     while (n != INV) { n = parent[n]; ++l; }
     return l;
   }
-  // refine_node: implementation.hpp:320-364 (compact tree -> children appended)
+  // refine_node: hierarchical/implementation.hpp:320-364 (compact tree -> children appended)
   Ind refine(Ind n) {
     const Ind first = size();
     firstChild[n] = first;
@@ -147,7 +147,7 @@ struct Tree {
     }
     return first;
   }
-  // MinLevel::generate_mesh: grid/generation.hpp:361-373.  The node range is
+  // MinLevel::generate_mesh: grid/generation.hpp:45-59.  The node range is
   // fixed at the start of each pass (Range{node_begin, node_end}).
   void min_level(int L) {
     bool done = false;
@@ -159,7 +159,7 @@ struct Tree {
       }
     }
   }
-  // find_samelvl_neighbor: implementation.hpp:457-543
+  // find_samelvl_neighbor: hierarchical/implementation.hpp:457-543
   Ind find_samelvl_neighbor(Ind n, int pos) const {
     if (is_root(n)) return INV;
     std::vector<int> traversed;
@@ -213,7 +213,7 @@ struct Tree {
 
   // EXTENSION (not in hom3): refine leaves whose cell box intersects a sphere
   // until they reach `maxLevel`, then enforce the 2:1 face balance that
-  // find_samelvl_neighbor's documentation requires (implementation.hpp:456).
+  // find_samelvl_neighbor's documentation requires (hierarchical/implementation.hpp:456).
   void refine_sphere(const double* c, double r, int maxLevel);
   void balance_2to1();
 };
@@ -298,12 +298,12 @@ inline std::vector<Sdf> cube_boundaries(int nd, const Tree& t) {
 // Physical parameters: euler/quantities.hpp:23-189, cns/quantities.hpp:23-115,
 // heat/quantities.hpp:13-56
 // ---------------------------------------------------------------------------
-enum PhysicsKind { PHYS_EULER = 0, PHYS_CNS = 1, PHYS_HEAT = 2, PHYS_ADVECTION = 3 /* advection/physics.hpp:21-162 */ };
-enum FluxKind { FLUX_AUSM = 0, FLUX_LLF = 1, FLUX_UPWIND = 2 /* advection/tags.hpp:18-19 */ };
+enum PhysicsKind { PHYS_EULER = 0, PHYS_CNS = 1, PHYS_HEAT = 2, PHYS_ADVECTION = 3 /* advection/physics.hpp:21-149 */ };
+enum FluxKind { FLUX_AUSM = 0, FLUX_LLF = 1, FLUX_UPWIND = 2 /* advection/tags.hpp:14-15 */ };
 // Advection velocity fields u(x) (the "velocity" property, advection/physics.hpp:36-37)
 enum VelocityKind {
   VEL_CONSTANT = 0,  // vel = {u_0, u_1, u_2}
-  VEL_ROTATION = 1,  // advection_fv_solver_test.cpp:67-84 (radial_velocity); vel = {u_mag, c_0, c_1}
+  VEL_ROTATION = 1,  // advection_fv_solver_test.cpp:69-85 (radial_velocity); vel = {u_mag, c_0, c_1}
 };
 enum TimeKind { TI_EULER_FORWARD = 0, TI_RK2 = 1, TI_SSPRK3 = 2 /* EXTENSION: Shu-Osher SSP-RK3 */ };
 enum ReconKind { RECON_NONE = 0, RECON_MUSCL = 1 /* EXTENSION: LSQ + MUSCL + Venkatakrishnan */ };
@@ -324,16 +324,16 @@ struct Params {
   double T_inf = 1, rho_inf = 1, u_inf = 0, p_inf = 1, mu_inf = 1;
   void derive() {
     gm1 = gamma - 1.;
-    T_inf = 1.0 / (1 + 0.5 * gm1 * (Minfty * Minfty));  // quantities.hpp:132-133
+    T_inf = 1.0 / (1 + 0.5 * gm1 * (Minfty * Minfty));  // euler/quantities.hpp:132-133
     rho_inf = std::pow(T_inf, 1. / gm1);               // :136-137
     u_inf = Minfty * std::sqrt(T_inf);                 // :140-141
     p_inf = std::pow(T_inf, gamma / gm1) / gamma;      // :144-145
-    sOverTref = Sutherland0 / T0;                      // cns/quantities.hpp:382
-    sOverTrefP1 = sOverTref + 1.0;                     // :383
-    mu_inf = sutherland(T_inf);                        // :428-429
-    Re0 = ReInfty * mu_inf / (rho_inf * u_inf);        // :384
+    sOverTref = Sutherland0 / T0;                      // cns/quantities.hpp:28
+    sOverTrefP1 = sOverTref + 1.0;                     // :29
+    mu_inf = sutherland(T_inf);                        // :74-75
+    Re0 = ReInfty * mu_inf / (rho_inf * u_inf);        // :30
   }
-  // cns/quantities.hpp:467-469
+  // cns/quantities.hpp:113-115
   double sutherland(double T) const { return std::pow(T, 1.5) * sOverTrefP1 / (T + sOverTref); }
 };
 
@@ -356,9 +356,9 @@ enum BcKind {
   BC_CPL_HEAT_CNS = 12,        // heat/coupling_conditions.hpp:18-38 (heat side)
   BC_CPL_HEAT_HEAT = 13,       // heat/coupling_conditions.hpp:41-61
   BC_PERIODIC = 14,            // EXTENSION (not in hom3): copy of the cell on the opposite face
-  BC_ADV_DIRICHLET = 15,       // advection/boundary_conditions.hpp:17-42 (constant surface value)
-  BC_ADV_NEUMANN = 16,         // :45-70 (constant surface flux)
-  BC_ADV_CHARACTERISTIC = 17,  // :73-97
+  BC_ADV_DIRICHLET = 15,       // advection/boundary_conditions.hpp:15-37 (constant surface value)
+  BC_ADV_NEUMANN = 16,         // :40-63 (constant surface flux)
+  BC_ADV_CHARACTERISTIC = 17,  // :66-94
 };
 
 struct Bc {
@@ -378,7 +378,7 @@ enum IcKind {
   IC_RIEMANN3D_PERTURBED = 5,  // EXTENSION (not in hom3): 3D Riemann + Fourier modes
   IC_VORTEX_PARAM = 6,  // EXTENSION (not in hom3): vortex with centre/strength params
   IC_TAYLOR_GREEN = 7,  // EXTENSION (not in hom3): 3D Taylor-Green vortex
-  IC_DISC = 8,          // advection_fv_solver_test.cpp:100-111: q_in inside a disc, q_out outside
+  IC_DISC = 8,          // advection_fv_solver_test.cpp:106-115: q_in inside a disc, q_out outside
 };
 
 template <class T> struct World;
@@ -452,7 +452,7 @@ template <class T> struct Solver {
   }
   T p(int t, Ind c) const { return P.gm1 * (rho_E(t, c) - 0.5 * rho(t, c) * u_mag2(t, c)); }
   T a(int t, Ind c) const { using std::sqrt; return sqrt(P.gamma * p(t, c) / rho(t, c)); }
-  T Temp(int t, Ind c) const {  // euler T: physics.hpp:144-145; heat T: heat/physics.hpp:51-58
+  T Temp(int t, Ind c) const {  // euler T: euler/physics.hpp:144-145; heat T: heat/physics.hpp:51-58
     if (P.physics == PHYS_HEAT) return q(t, c, 0);
     return P.gamma * p(t, c) / rho(t, c);
   }
@@ -561,14 +561,14 @@ template <class T> struct Solver {
     return 0.5 * (slope(t, r, v, sdir) + slope(t, l, v, sdir));
   }
   // boundary_info: solver.hpp:298-313
-  // the "velocity" function of the advection physics at x (advection/physics.hpp:36-37, 116-118)
+  // the "velocity" function of the advection physics at x (advection/physics.hpp:35-37, 104-106)
   void velocity_field(const double* x, double* u) const {
     for (int d = 0; d < 3; ++d) u[d] = 0;
     if (P.vel_kind == VEL_CONSTANT) {
       for (int d = 0; d < nd; ++d) u[d] = P.vel[d];
       return;
     }
-    // radial_velocity of advection_fv_solver_test.cpp:67-84 (2D), centre and magnitude as parameters
+    // radial_velocity of advection_fv_solver_test.cpp:69-85 (2D), centre and magnitude as parameters
     const double u_mag = P.vel[0];
     const double c0 = P.vel[1], c1 = P.vel[2];
     const double radius = std::sqrt((x[0] - c0) * (x[0] - c0) + (x[1] - c1) * (x[1] - c1));
@@ -817,16 +817,16 @@ template <class T> struct Solver {
     return ausm_w(wl, wr, d);
   }
 
-  // compute_num_flux dispatch (physics.hpp:175-178, cns 155-161, heat 113-119)
+  // compute_num_flux dispatch (euler/physics.hpp:175-178, cns/physics.hpp:155-161, heat/physics.hpp:113-119)
   State face_flux(int t, Ind l, Ind r, int d, double dx, T dt) const {
     if (P.physics == PHYS_ADVECTION) {
       State f{};
       const T qL = q(t, l, 0), qR = q(t, r, 0);
       const double uL = velocity(l, d), uR = velocity(r, d);
-      if (P.flux == FLUX_LLF) {  // advection/physics.hpp:130-139
+      if (P.flux == FLUX_LLF) {  // advection/physics.hpp:120-130
         const double lambda_max = std::max(std::abs(uL), std::abs(uR));
         f[0] = 0.5 * (qL * uL + qR * uR + lambda_max * (qL - qR));
-      } else {  // upwind: advection/physics.hpp:142-153 (hom3 negates u_L q_L when the face velocity is negative)
+      } else {  // upwind: advection/physics.hpp:132-145 (hom3 negates u_L q_L when the face velocity is negative)
         const double u_srfc = 0.5 * (uL + uR);
         f[0] = uL * qL;
         if (u_srfc < 0) f[0] = f[0] * -1.;
@@ -884,7 +884,7 @@ template <class T> struct Solver {
     using std::abs;
     const double h = len[c];
     if (P.physics == PHYS_HEAT) return P.cfl * 0.5 * std::pow(h, 2.);
-    if (P.physics == PHYS_ADVECTION) {  // advection/physics.hpp:86-93
+    if (P.physics == PHYS_ADVECTION) {  // advection/physics.hpp:78-87
       double u_max = std::numeric_limits<double>::lowest();
       for (int d = 0; d < nd; ++d) u_max = std::max(u_max, std::abs(velocity(c, d)));
       return T(P.cfl * h / u_max);
@@ -1029,7 +1029,7 @@ template <class T> struct World {
   int nd = 2;
 };
 
-// isentropic_vortex: euler/initial_conditions.hpp:343-368 (hard-coded
+// isentropic_vortex: euler/initial_conditions.hpp:14-39 (hard-coded
 // beta=5, gamma=1.4, x0=(-5,-5), u=v=1 in hom3).
 template <class T>
 void Solver<T>::isentropic_vortex(const double* x, double t, ICState& out) const {
@@ -1062,7 +1062,7 @@ template <class T> void Solver<T>::eval_ic(const double* x, ICState& out) const 
   } else if (ic_kind == IC_CONSTANT_CV) {
     for (int v = 0; v < nv; ++v) out[v] = ic[v];
   } else if (ic_kind == IC_SHOCK_TUBE) {
-    // ic = {dir, angle, x0, rhoL, umagL, pL, rhoR, umagR, pR}: initial_conditions.hpp:380-419
+    // ic = {dir, angle, x0, rhoL, umagL, pL, rhoR, umagR, pR}: euler/initial_conditions.hpp:51-90
     const int dir = (int)ic[0];
     const double angle = ic[1], x0 = ic[2];
     const double alpha = angle * (2 * PI) / 360;
@@ -1083,7 +1083,7 @@ template <class T> void Solver<T>::eval_ic(const double* x, ICState& out) const 
       for (int d = 0; d < nd; ++d) pvars[d] = uR[d];
       pvars[nd + 1] = ic[8];
     }
-    // shock_tube converts with gamma = 1.4 hard-coded (initial_conditions.hpp:387)
+    // shock_tube converts with gamma = 1.4 hard-coded (euler/initial_conditions.hpp:58)
     ICState c{};
     c[nd] = pvars[nd];
     double vm2 = 0;
@@ -1102,7 +1102,7 @@ template <class T> void Solver<T>::eval_ic(const double* x, ICState& out) const 
     pvars[nd + 1] = inside ? ic[5] : ic[7];
     out = cv(pvars);
   } else if (ic_kind == IC_DISC) {
-    // ic = {c_0, c_1, c_2, R, q_in, q_out}: advection_fv_solver_test.cpp:100-111
+    // ic = {c_0, c_1, c_2, R, q_in, q_out}: advection_fv_solver_test.cpp:106-115
     double s2 = 0;
     for (int d = 0; d < nd; ++d) s2 += (x[d] - ic[d]) * (x[d] - ic[d]);
     out[0] = std::sqrt(s2) - ic[3] > 0. ? ic[5] : ic[4];
@@ -1156,7 +1156,7 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
   for (Ind g = g0; g < g1; ++g) {
     const Ind b = boundary_cell(g);
     switch (B.kind) {
-      case BC_EULER_NEUMANN: {  // euler/boundary_conditions.hpp:253-264
+      case BC_EULER_NEUMANN: {  // euler/boundary_conditions.hpp:17-43
         double dx2 = 0;
         for (int d = 0; d < nd; ++d) dx2 += (xc[d][b] - xc[d][g]) * (xc[d][b] - xc[d][g]);
         const double dx = std::sqrt(dx2);  // cell_dx: solver.hpp:590-592
@@ -1237,10 +1237,10 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
         setQ(t, g, cv(gp));
         break;
       }
-      case BC_HEAT_DIRICHLET:  // heat/boundary_conditions.hpp:161-168; v = {T}
+      case BC_HEAT_DIRICHLET:  // heat/boundary_conditions.hpp:15-37; v = {T}
         q(t, g, 0) = 2.0 * B.v[0] - q(t, b, 0);
         break;
-      case BC_HEAT_NEUMANN: {  // :186-194
+      case BC_HEAT_NEUMANN: {  // :40-63
         double dx2 = 0;
         for (int d = 0; d < nd; ++d) dx2 += (xc[d][b] - xc[d][g]) * (xc[d][b] - xc[d][g]);
         q(t, g, 0) = q(t, b, 0) - std::sqrt(dx2) * B.v[0];
@@ -1263,16 +1263,16 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
         for (int v = 0; v < nv; ++v) q(t, g, v) = q(t, o, v);
         break;
       }
-      case BC_ADV_DIRICHLET:  // advection/boundary_conditions.hpp:29-35; v = {q_srfc}
+      case BC_ADV_DIRICHLET:  // advection/boundary_conditions.hpp:25-32; v = {q_srfc}
         q(t, g, 0) = 2.0 * B.v[0] - q(t, b, 0);
         break;
-      case BC_ADV_NEUMANN: {  // :56-63; v = {surface flux}, distance of the cell centres
+      case BC_ADV_NEUMANN: {  // :50-58; v = {surface flux}, distance of the cell centres
         double dx2 = 0;
         for (int d = 0; d < nd; ++d) dx2 += (xc[d][b] - xc[d][g]) * (xc[d][b] - xc[d][g]);
         q(t, g, 0) = q(t, b, 0) - std::sqrt(dx2) * B.v[0];
         break;
       }
-      case BC_ADV_CHARACTERISTIC: {  // :79-95
+      case BC_ADV_CHARACTERISTIC: {  // :71-91
         const int pos = opposite_pos[boundary_pos(g)];  // the ghost's position w.r.t. its boundary cell
         const int dir = pos / 2;
         const double v = velocity(b, dir);
@@ -1285,7 +1285,7 @@ template <class T> void Solver<T>::apply_bc(int t, int k, Ind g0, Ind g1) {
         }
         break;
       }
-      case BC_CPL_EULER_EULER: {  // euler/coupling_conditions.hpp:452-460
+      case BC_CPL_EULER_EULER: {  // euler/coupling_conditions.hpp:17-35
         const Ind o = partner_cell(g);
         const Solver<T>& os = *w->solvers[B.partner];
         for (int v = 0; v < nv; ++v) q(t, g, v) = os.q(t, o, v);

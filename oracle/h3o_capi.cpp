@@ -200,7 +200,7 @@ void h3o_quantities(void* w, int s, double* out) {
   out[0] = P.T_inf; out[1] = P.rho_inf; out[2] = P.u_inf; out[3] = P.p_inf; out[4] = P.mu_inf;
   out[5] = P.Re0; out[6] = P.gm1; out[7] = P.sOverTref;
 }
-// coupling::apply (CNS-heat): coupling.hpp:167-183
+// coupling::apply (CNS-heat): coupling.hpp:52-63
 void h3o_couple_cht(void* w, int cns, int heat, double Tr0) {
   auto& c = S(w, cns);
   auto& h = S(w, heat);
@@ -211,7 +211,7 @@ void h3o_couple_cht(void* w, int cns, int heat, double Tr0) {
   c.force_dt(dt);
   h.force_dt(dt * scaling);
 }
-// coupling::apply (equal solvers): coupling.hpp:186-193
+// coupling::apply (equal solvers): coupling.hpp:66-73
 void h3o_couple_equal(void* w, int a, int b) {
   const double da = S(w, a).compute_dt(), db = S(w, b).compute_dt();
   const double dt = std::min(da, db);

@@ -73,7 +73,7 @@ CNS_PROPS = dict(gamma=1.4, cfl=0.4, cfl_viscous=0.4, Rspecific=287.058, T0=273.
 
 
 def cns_case(name, level=6, ti=h3o.EULER_FORWARD):
-    """cns_fv_solver_test.cpp:345-536 (level 6 instead of 8 for constant/sod)."""
+    """cns_fv_solver_test.cpp:91-211 (constant_ic, sod_shock_tube_ic; level 6 instead of 8)."""
     if name in ("constant", "sod"):
         w = h3o.World(2, [0, 0], [1, 1], level=level)
         probe = w.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=neumann_cube(w), ic_kind=h3o.IC_CONSTANT_PV,
@@ -92,7 +92,7 @@ def cns_case(name, level=6, ti=h3o.EULER_FORWARD):
         s.initialize()
         return w, [s]
     if name in ("walls", "slip", "isothermal"):
-        # inflow / outflow + Neumann far field (cns_fv_solver_test.cpp:466-536 with the
+        # inflow / outflow + Neumann far field (cns_fv_solver_test.cpp:212-286, flow_past_cube, with the
         # cube replaced by conditions on the cube faces so a small grid has all kinds)
         w0 = h3o.World(2, [0, 0], [1, 1], level=level)
         probe = w0.add_solver(h3o.CNS, h3o.AUSM, ti, bcs=neumann_cube(w0), ic_kind=h3o.IC_CONSTANT_PV,
@@ -114,7 +114,7 @@ def cns_case(name, level=6, ti=h3o.EULER_FORWARD):
 
 
 def heat_case(level=3, ti=h3o.EULER_FORWARD):
-    """heat_fv_solver_test.cpp:621-641 (level 3 instead of 4)."""
+    """heat_fv_solver_test.cpp:81-105 (level 3 instead of 4)."""
     w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=level)
     g = w.cube_boundaries()
     bcs = [h3o.bc(h3o.BC_HEAT_DIRICHLET, g[0], [1.0]), h3o.bc(h3o.BC_HEAT_DIRICHLET, g[1], [1.0])]
@@ -173,7 +173,7 @@ def euler_euler_case(level=4):
 # ---------------------------------------------------------------------------
 def advection_case(level=7, flux=h3o.UPWIND, ti=h3o.EULER_FORWARD, bc_kind=None, vel_kind=h3o.VEL_ROTATION,
                    vel=(0.5, 0.5, 0.5), nd=2, cfl=1.0, fine=None):
-    """advection_fv_solver_test.cpp:53-126: the disc q = 1 (r = 0.08 around (0.25, 0.5)) in q = 0.1,
+    """advection_fv_solver_test.cpp:51-125: the disc q = 1 (r = 0.08 around (0.25, 0.5)) in q = 0.1,
     carried by the test's rotating velocity field, characteristic conditions on all faces, upwind flux,
     forward Euler, CFL 1 (level 7, as in hom3).  bc_kind / vel_kind select other conditions and fields;
     fine: EXTENSION, refine the r = 0.3 sphere around the centre to that level."""

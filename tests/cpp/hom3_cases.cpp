@@ -1,7 +1,7 @@
 // hom3's solver test cases, written against the C++ layer (include/hom3_b200.hpp)
 // the way hom3 writes them against its own Solver
 // (src/solver/fv/euler/tests/euler_fv_solver_test.cpp:85-286,
-//  src/solver/fv/heat/tests/heat_fv_solver_test.cpp:621-641).
+//  src/solver/fv/heat/tests/heat_fv_solver_test.cpp:81-105).
 // hom3's versions only check that the run reaches timeEnd without diverging;
 // these also check the state: a constant state must be preserved exactly and
 // density / pressure / temperature stay positive and finite.
@@ -90,7 +90,7 @@ static int run_cases(int level) {
     const double L[3] = {k == 0 ? 1.0 : 1.0, k == 0 ? 0.75 : -2.0, k == 0 ? 1.0 : 0.4};
     const double R[3] = {k == 0 ? 0.125 : 1.0, k == 0 ? 0.0 : 2.0, k == 0 ? 0.1 : 0.4};
     Solver s{cube3, euler_properties(k == 0 ? 0.2 : 0.15)};
-    s.set_initial_condition([=](const double* x, double* q) {  // ic::shock_tube, initial_conditions.hpp:380-419
+    s.set_initial_condition([=](const double* x, double* q) {  // ic::shock_tube, euler/initial_conditions.hpp:51-90
       const double* S = x[0] < x0 ? L : R;
       const double pv[5] = {S[1], 0.0, 0.0, S[0], S[2]};
       cv(3, pv, q);
@@ -99,7 +99,7 @@ static int run_cases(int level) {
     run_solver(s, 10000);
     report(k == 0 ? "euler_sod_shock_tube_ic" : "euler_problem123_ic", s, physical(s, 3));
   }
-  // explosion_ic (:212-255)
+  // explosion_ic (euler_fv_solver_test.cpp:212-255)
   {
     Solver s{cube3, euler_properties(0.25)};
     s.set_initial_condition([](const double* x, double* q) {
@@ -128,7 +128,7 @@ static int run_cases(int level) {
     run_solver(s, 10000);
     report("euler_isentropic_vortex_ic", s, physical(s, 2));
   }
-  // heat one_dimensional_dirichlet: heat_fv_solver_test.cpp:621-641
+  // heat one_dimensional_dirichlet: heat_fv_solver_test.cpp:81-105
   {
     const Grid g{3, {0, 0, 0}, {1, 1, 1}, level > 4 ? 4 : level};
     Properties p;

@@ -9,7 +9,12 @@ and gtest are absent) and copies out the expected values it asserts:
 * hierarchical_container_test.cpp:134-147 -- same-level neighbours, 3D level 2
 * hierarchical_container_test.cpp:212-274 -- same-level neighbours, 2D level 3
 
-Run once in a checkout that has the hom3 sources:
+It also writes tests/golden/reference_files.json: the line count of every
+source file of hom3 (.hpp, .cpp, .h, CMakeLists.txt), against which
+tests/test_citations.py checks that each file:line citation in this
+repository names lines that exist.
+
+Run once in a checkout that has the hom3 sources (the path is required):
     python tests/golden/make_golden.py /path/to/hom3
 """
 import json
@@ -46,8 +51,23 @@ def parse(src: str):
     return out
 
 
+def file_lengths(root: str):
+    """{path relative to the hom3 checkout: number of lines} of its sources."""
+    out = {}
+    for dp, dn, fn in os.walk(root):
+        dn[:] = sorted(d for d in dn if not d.startswith("."))
+        for f in sorted(fn):
+            if f.endswith((".hpp", ".cpp", ".h")) or f == "CMakeLists.txt":
+                full = os.path.join(dp, f)
+                with open(full, errors="replace") as fh:
+                    out[os.path.relpath(full, root)] = sum(1 for _ in fh)
+    return out
+
+
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py /path/to/hom3")
+    root = sys.argv[1]
     path = os.path.join(root, "src/containers/hierarchical/tests/hierarchical_container_test.cpp")
     with open(path) as f:
         data = parse(f.read())
@@ -56,6 +76,11 @@ def main():
     with open(dst, "w") as f:
         json.dump(data, f, indent=1)
     print("wrote", dst, {k: (len(v) if hasattr(v, "__len__") else v) for k, v in data.items()})
+    lens = file_lengths(root)
+    dst2 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_files.json")
+    with open(dst2, "w") as f:
+        json.dump({"source": "line counts of hom3's source files", "files": lens}, f, indent=0, sort_keys=True)
+    print("wrote", dst2, len(lens), "files")
 
 
 if __name__ == "__main__":

@@ -362,7 +362,7 @@ def test_muscl_graph_replay_matches_single_steps():
 
 # ---- advection (advection/physics.hpp, advection/boundary_conditions.hpp) ----
 def test_advection_hom3_case():
-    """advection_fv_solver_test.cpp:53-126 at its own level 7: the disc in the
+    """advection_fv_solver_test.cpp:51-125 at its own level 7: the disc in the
     rotating field, characteristic conditions, upwind flux, forward Euler, CFL 1."""
     _, (o,) = cases.advection_case(level=7)
     run_single(o)

@@ -18,7 +18,7 @@ def test_constant_state_preserved_exactly():
 
 
 def test_cns_free_stream_preserved():
-    """cns_fv_solver_test.cpp:345-383: free-stream state with Neumann conditions."""
+    """cns_fv_solver_test.cpp:91-141: free-stream state with Neumann conditions."""
     _, (o,) = cases.cns_case("constant", level=4)
     q0 = o.state(0)[:, : o.first_ghost].copy()
     o.solve(10)
@@ -249,7 +249,7 @@ def test_advection_upwind_at_cfl_one_shifts_by_one_cell():
 
 def test_advection_upwind_reproduces_hom3_sign_for_negative_velocity():
     """hom3's upwind flux is u_L q_L negated when the face velocity is
-    negative (advection/physics.hpp:142-153), not u_R q_R: with u = (-1, 0)
+    negative (advection/physics.hpp:132-145), not u_R q_R: with u = (-1, 0)
     at CFL 1 every face carries +q_L and the state moves one cell in +x."""
     _, (o,) = cases.advection_case(level=5, bc_kind=h3o.BC_PERIODIC, vel_kind=h3o.VEL_CONSTANT, vel=(-1.0, 0.0))
     ij, n = _lattice(o)
@@ -308,7 +308,7 @@ def test_advection_conditions():
 
 
 def test_advection_time_step():
-    """compute_dt: CFL h / max_d |u_d(x_c)| (advection/physics.hpp:86-93), min over cells."""
+    """compute_dt: CFL h / max_d |u_d(x_c)| (advection/physics.hpp:78-87), min over cells."""
     _, (o,) = cases.advection_case(level=4, cfl=0.7)
     t = o.tables()
     fg = o.first_ghost
