@@ -926,6 +926,7 @@ def main():
     if adj is not None:
         line["adjoint"] = adj
     line["grid_build"] = getattr(args, "grid_build", None)
+    line["stage_kernel"] = s.kernel_info()
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         ups, cells, nst, threads, el = cpu_oracle_run(args)
         line["cpu_baseline"] = {"value": ups, "unit": "cell-updates/s", "cores": threads, "kind": "port",

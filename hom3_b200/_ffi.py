@@ -23,7 +23,8 @@ FP64, MIXED = 0, 1
  BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT,
  BC_PERIODIC, BC_ADV_DIRICHLET, BC_ADV_NEUMANN, BC_ADV_CHARACTERISTIC) = range(18)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
-OPT_TILE_KERNEL, OPT_GRAPHS = 1, 2
+OPT_TILE_KERNEL, OPT_GRAPHS, OPT_HALO_KERNEL, OPT_PERSISTENT_BLOCKS = 1, 2, 3, 4
+STATUS_DT, STATUS_STATE, STATUS_TIMEOUT = 1, 2, 4
 KERNEL_KINDS = ("bc", "cfl", "scalar", "stage1", "stage2", "slopes", "copy", "adjoint")
 
 
@@ -95,6 +96,7 @@ SIGNATURES = {
     "h3c_adjoint": (_i32, [_vp, _i64, _i64, _P(_dbl), _P(_dbl), _P(_dbl)]),
     "h3c_launches": (_i32, [_vp, _P(_i64)]),
     "h3c_set_option": (_i32, [_vp, _i32, _i32]),
+    "h3c_kernel_info": (_i32, [_vp, _P(_i64), _i32]),
     "h3c_selftest_nr": (_i32, [_P(_dbl), _i64, _P(_dbl), _P(_dbl)]),
     "h3c_min_dt_noalloc": (_i32, [_P(Desc), _vp, _i64, _i64, _vp, _vp, _vp]),
     "h3c_profile": (_i32, [_vp, _i32]),

@@ -38,9 +38,14 @@ struct Scalars {
   long long step, forced_step;
   long long dtmin_ord;  // min of cell dt for the next set_dt (ordered bits)
   long long mindt_ord;  // min of cell dt for h3c_min_dt
-  int status;           // bit0: dt outside [1e-300, 1e300] or non-finite
+  int status;           // kStatus* bits, sticky until h3c_status reads them
   int pad;
 };
+
+// Scalars::status bits
+constexpr int kStatusDt = 1;      // set_dt produced dt outside [1e-300, 1e300] (utilities.hpp:74-76)
+constexpr int kStatusState = 2;   // a cell violates check_variables (euler/physics.hpp:229-239)
+constexpr int kStatusTimeout = 4; // a bounded device wait ran out
 
 // Physical constants of one solver (euler/quantities.hpp, cns/quantities.hpp)
 struct PhysConst {
@@ -140,6 +145,13 @@ __device__ __forceinline__ void block_min_atomic(long long v, long long* dst) {
     }
     if (lane == 0 && v < kOrdMax) atomicMin(dst, v);
   }
+}
+
+// Records in the instance's status that some cell of this warp failed the
+// state check (one atomic per warp that saw one; every lane must call).
+__device__ __forceinline__ void flag_bad_state(bool bad, const Scalars* sc, int inst) {
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0)
+    atomicOr(const_cast<int*>(&sc[inst].status), kStatusState);
 }
 
 // ---------------------------------------------------------------------------
@@ -322,12 +334,21 @@ __device__ __forceinline__ void viscous(const Prim<R, ND>& L, const Prim<R, ND>&
 // ---------------------------------------------------------------------------
 // per-cell time step: euler/physics.hpp:182-196, cns/physics.hpp:167-187,
 // heat/physics.hpp:82-85, advection/physics.hpp:78-87 (u: the cell's velocity)
+// bad (optional): the cell fails hom3's check_variables -- density, energy
+// and pressure positive (euler/physics.hpp:229-239, shared by CNS), T
+// positive (heat/physics.hpp:89-95); for advection only a non-finite value
+// counts, since hom3's own upwind test makes q negative (its flux is
+// reproduced as written).  NaN fails every comparison, so it is bad too.
 // ---------------------------------------------------------------------------
 template <int ND, int PHYS>
 __device__ __forceinline__ double cell_dt(const double* q, double h, const PhysConst& pc,
-                                          const double* u = nullptr) {
-  if (PHYS == HEAT) return pc.cfl * 0.5 * (h * h);
+                                          const double* u = nullptr, bool* bad = nullptr) {
+  if (PHYS == HEAT) {
+    if (bad) *bad = !(q[0] > 0.0);
+    return pc.cfl * 0.5 * (h * h);
+  }
   if (PHYS == ADVECTION) {
+    if (bad) *bad = !isfinite(q[0]);
     double u_max = -1.7976931348623157e308;
 #pragma unroll
     for (int d = 0; d < ND; ++d) u_max = fmax(u_max, fabs(u[d]));
@@ -337,6 +358,7 @@ __device__ __forceinline__ double cell_dt(const double* q, double h, const PhysC
 #pragma unroll
   for (int v = 0; v < ND + 2; ++v) P.q[v] = q[v];
   make_prim<double, ND>(P, pc.gamma, pc.gm1);
+  if (bad) *bad = !(P.q[ND] > 0.0 && P.q[ND + 1] > 0.0 && P.p > 0.0);
   double S = -1.7976931348623157e308;
 #pragma unroll
   for (int d = 0; d < ND; ++d) {
@@ -355,11 +377,12 @@ __device__ __forceinline__ double cell_dt(const double* q, double h, const PhysC
 
 template <int ND, int PHYS>
 __global__ void __launch_bounds__(kBlock) k_cfl(const double* __restrict__ q, Geometry g, PhysConst pc,
-                                                long long* dst) {
+                                                long long* dst, const Scalars* sc) {
   constexpr int NV = nvars<ND, PHYS>();
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int inst = tile_instance(g, blockIdx.x);
   long long o = kOrdMax;
+  bool bad = false;
   if (c < instance_end(g, inst)) {
     double qc[NV];
 #pragma unroll
@@ -369,9 +392,10 @@ __global__ void __launch_bounds__(kBlock) k_cfl(const double* __restrict__ q, Ge
 #pragma unroll
       for (int d = 0; d < ND; ++d) uc[d] = __ldg(g.vel + d * g.ld + c);
     }
-    const double dt = cell_dt<ND, PHYS>(qc, g.len[g.lvl[c]], pc, uc);
+    const double dt = cell_dt<ND, PHYS>(qc, g.len[g.lvl[c]], pc, uc, &bad);
     if (!isnan(dt)) o = dbl_to_ord(dt);
   }
+  flag_bad_state(bad, sc, inst);
   block_min_atomic(o, per_instance(dst, inst));
 }
 
@@ -388,7 +412,7 @@ __global__ void k_set_dt(Scalars* s0, int reset_after, int n_inst) {
     dt = s->tEnd - s->time;
   }
   s->dt = dt;
-  if (!(dt >= 1e-300 && dt <= 1e300)) s->status |= 1;  // utilities.hpp:74-76
+  if (!(dt >= 1e-300 && dt <= 1e300)) s->status |= kStatusDt;  // utilities.hpp:74-76
   if (reset_after) s->dtmin_ord = kOrdMax;
 }
 // advance: solver.hpp:502-505
@@ -672,6 +696,7 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
   const int inst = tile_instance(g, blockIdx.x);
   const bool live = c < instance_end(g, inst);
   long long ord = kOrdMax;
+  bool bad = false;
   if (live) {
     const long long ld = g.ld;
     const double dt = sc[inst].dt;
@@ -886,11 +911,14 @@ __global__ void __launch_bounds__(kBlock) k_stage(const double* __restrict__ qin
 #pragma unroll
         for (int d = 0; d < ND; ++d) uc[d] = __ldg(g.vel + d * ld + c);
       }
-      const double cd = cell_dt<ND, PHYS>(o, dx, pc, uc);
+      const double cd = cell_dt<ND, PHYS>(o, dx, pc, uc, &bad);
       if (!isnan(cd)) ord = dbl_to_ord(cd);
     }
   }
-  if (FUSE) block_min_atomic(ord, per_instance(dtmin, inst));
+  if (FUSE) {
+    flag_bad_state(bad, sc, inst);
+    block_min_atomic(ord, per_instance(dtmin, inst));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1015,6 +1043,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
 
   // ---- phase C: minus faces, residual, update ----
   long long ord = kOrdMax;
+  bool bad = false;
   if (live) {
     double acc[NV];
 #pragma unroll
@@ -1060,11 +1089,14 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
     if (FUSE) {
-      const double cd = cell_dt<ND, EULER>(o, dx, pc);
+      const double cd = cell_dt<ND, EULER>(o, dx, pc, nullptr, &bad);
       if (!isnan(cd)) ord = dbl_to_ord(cd);
     }
   }
-  if (FUSE) block_min_atomic(ord, per_instance(dtmin, inst));
+  if (FUSE) {
+    flag_bad_state(bad, sc, inst);
+    block_min_atomic(ord, per_instance(dtmin, inst));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -1226,6 +1258,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
 
     // ---- minus faces, residual, update ----
     long long ord = kOrdMax;
+  bool bad = false;
     if (live) {
       double acc[NV];
 #pragma unroll
@@ -1278,11 +1311,14 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
 #pragma unroll
       for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
       if (FUSE) {
-        const double cd = cell_dt<ND, EULER>(o, dx, pc);
+        const double cd = cell_dt<ND, EULER>(o, dx, pc, nullptr, &bad);
         if (!isnan(cd)) ord = dbl_to_ord(cd);
       }
     }
-    if (FUSE) block_min_atomic(ord, per_instance(dtmin, inst));
+    if (FUSE) {
+    flag_bad_state(bad, sc, inst);
+    block_min_atomic(ord, per_instance(dtmin, inst));
+  }
     __syncthreads();  // shared memory is rewritten by the next tile
   }
 }

@@ -15,15 +15,29 @@
 // the last call's contents (each call writes every partial it reads, so
 // nothing needs clearing); calls whose kernels overlap on the GPU -- on two
 // streams, or from two host threads -- race on it and must be serialised by
-// the caller.
+// the caller.  Euler, CNS and heat are covered; advection (whose time step
+// needs the per-cell velocity field) is rejected.
+//
+// The first call on a device looks up the array's address.  Under CUDA's
+// default lazy module loading that first call (or the first kernel launch of
+// this library) also loads the library's device code, which reserves device
+// memory for the code and the array; a caller whose pool will own all device
+// memory makes the first call during its own initialisation, before the pool
+// takes the memory (or sets CUDA_MODULE_LOADING=EAGER).  After that, calls
+// reserve nothing.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <mutex>
+#include <string>
 
 #include "../../include/h3c.h"
 #define H3C_DEVICE_FUNCTIONS_ONLY
 #include "fv_kernels.cuh"
+
+namespace gridb {
+void set_global_error(const std::string& msg);  // h3c_last_error(NULL, ...) text
+}
 
 namespace {
 
@@ -110,11 +124,21 @@ int scratch_address(long long** out) {
 extern "C" int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t ld, int64_t n_cells,
                                   const double* length, double* dt_out, void* stream) {
   using namespace h3c;
-  if (!desc || !q || !length || !dt_out) return H3C_E_INVALID;
-  if ((desc->nd != 2 && desc->nd != 3) || desc->physics < 0 || desc->physics > 2) return H3C_E_INVALID;
-  if (n_cells < 1 || n_cells > kNoAllocMaxCells || ld < n_cells) return H3C_E_INVALID;
+  auto fail = [](int code, const std::string& m) {
+    gridb::set_global_error("h3c_min_dt_noalloc: " + m);
+    return code;
+  };
+  if (!desc || !q || !length || !dt_out) return fail(H3C_E_INVALID, "null argument");
+  if (desc->nd != 2 && desc->nd != 3) return fail(H3C_E_INVALID, "nd must be 2 or 3");
+  if (desc->physics < 0 || desc->physics > 2)
+    return fail(H3C_E_INVALID, "physics must be Euler, CNS or heat (advection is not covered)");
+  if (n_cells < 1 || n_cells > kNoAllocMaxCells)
+    return fail(H3C_E_INVALID, "n_cells must be in [1, " + std::to_string(kNoAllocMaxCells) +
+                                   "]: the fixed scratch array holds one partial minimum per 256 cells");
+  if (ld < n_cells) return fail(H3C_E_INVALID, "ld < n_cells");
   long long* scratch = nullptr;
-  if (int rc = scratch_address(&scratch)) return rc;
+  if (int rc = scratch_address(&scratch))
+    return fail(rc, "cudaGetSymbolAddress of the scratch array failed on the current device");
   // physical constants: euler/quantities.hpp:131-145, cns/quantities.hpp:28-30, 74-75
   const double gamma = desc->gamma, gm1 = gamma - 1.;
   const double T_inf = 1.0 / (1 + 0.5 * gm1 * (desc->Minfty * desc->Minfty));
@@ -137,5 +161,6 @@ extern "C" int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t
     else k_cfl_partials<3, HEAT><<<nblocks, kBlock, 0, st>>>(q, ld, length, n_cells, pc, scratch);
   }
   k_cfl_fold<<<1, kBlock, 0, st>>>(scratch, nblocks, dt_out);
-  return cudaGetLastError() == cudaSuccess ? H3C_OK : H3C_E_CUDA;
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? H3C_OK : fail(H3C_E_CUDA, cudaGetErrorString(e));
 }

@@ -16,6 +16,7 @@
 #include <map>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "vtk_writer.hpp"
@@ -27,6 +28,7 @@
 #include "muscl_kernels.cuh"
 #include "muscl_adjoint.cuh"
 #include "cns_adjoint.cuh"
+#include "stage_halo.hpp"
 
 using namespace h3c;
 
@@ -90,6 +92,16 @@ struct h3c_solver_s {
   bool needs_partner = false, needs_periodic = false;  // coupling / periodic conditions present
   bool partner_set = false, periodic_set = false;
   bool tile = true;  // Euler stages use the shared-memory tile kernel
+  // halo-staged Euler/AUSM stage (h3c_stage_halo.cu): tables, launch size
+  bool halo = true;     // option: use it when its tables exist
+  bool halo_ok = false; // tables built for the current grid
+  unsigned short* d_lnb = nullptr;
+  int *d_hids = nullptr, *d_hoff = nullptr, *d_goff = nullptr;
+  unsigned short* d_grp = nullptr;
+  int hmax = 0, halo_bps = 0;
+  size_t halo_smem = 0;
+  double halo_mean = 0;
+  int halo_maxh = 0;
   // CUDA graph of `graph_steps` solver steps, replayed by h3c_solve
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -174,6 +186,8 @@ void free_grid(h3c_solver s) {
   dfree(s->d_vel);
   s->vel_set = false;
   dfree(s->d_blk_inst); dfree(s->d_inst_end); dfree(s->d_ginst);
+  dfree(s->d_lnb); dfree(s->d_hids); dfree(s->d_hoff); dfree(s->d_goff); dfree(s->d_grp);
+  s->halo_ok = false;
   dfree(s->d_adj);
   s->adj_cap = 0;
   s->stage_cap = 0;
@@ -213,6 +227,16 @@ GhostTables ghosts(const h3c_solver s) {
 }
 
 unsigned blocks(long long n) { return (unsigned)std::max<long long>(1, (n + kBlock - 1) / kBlock); }
+
+int num_sms() {
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  return sms;
+}
 
 // kernel kinds reported by h3c_profile_read
 enum { K_BC = 0, K_CFL = 1, K_SCALAR = 2, K_STAGE1 = 3, K_STAGE2 = 4, K_SLOPES = 5, K_COPY = 6, K_OTHER = 7, K_NKINDS = 8 };
@@ -278,7 +302,7 @@ void launch_bc(h3c_solver s, int which) { launch_bc_ptr(s, s->d_q[which], s->d_q
 template <int ND, int PHYS>
 void launch_cfl_t(h3c_solver s, long long* slot) {
   Launch L(s, K_CFL);
-  k_cfl<ND, PHYS><<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_q[0], geometry(s), s->pc, slot);
+  k_cfl<ND, PHYS><<<blocks(s->n_int), kBlock, 0, s->stream>>>(s->d_q[0], geometry(s), s->pc, slot, s->d_sc);
 }
 void launch_cfl(h3c_solver s, long long* slot) {
   if (s->desc.physics == H3C_ADVECTION && !s->vel_set) return;  // no velocity yet: no time step
@@ -336,6 +360,14 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
   if (PHYS == EULER && FLUX == AUSM && s->desc.reconstruction == H3C_RECON_MUSCL) {
     k_stage_muscl<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
         qin, out, s->d_slopes, s->d_xc, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+    return;
+  }
+  if (PHYS == EULER && FLUX == AUSM && s->tile && s->halo && s->halo_ok) {
+    int grid = s->persist_blocks > 0 ? s->persist_blocks : s->halo_bps * num_sms();
+    grid = (int)std::max<long long>(1, std::min<long long>(grid, s->ntiles));
+    HaloGeom hg{s->d_lnb, s->d_hids, s->d_hoff, s->d_grp, s->d_goff, s->hmax};
+    halo_stage(ND, std::is_same<R, float>::value, MODE, HANG, FUSE, qin, out, geometry(s), hg, s->pc, s->d_sc,
+               &s->d_sc->dtmin_ord, &s->d_sc->status, grid, s->halo_smem, s->stream);
     return;
   }
   if (PHYS == EULER && FLUX == AUSM && s->tile) {
@@ -781,6 +813,14 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
     }
     for (long long t = int_start[k] / kBlock; t * kBlock < int_end[k]; ++t) h_blk[t] = k;
   }
+  // ---- tables of the halo-staged Euler/AUSM stage kernel ----
+  HaloHost HH;
+  bool halo_tables = false;
+  if (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM && s->desc.reconstruction != H3C_RECON_MUSCL) {
+    std::vector<long long> tend(s->ntiles);
+    for (long long t = 0; t < s->ntiles; ++t) tend[t] = std::min((t + 1) * kBlock, int_end[h_blk[t]]);
+    halo_tables = halo_build(nd, L, s->ntiles, tend, h_nbr.data(), h_sub.data(), std::max<long long>(nsub, 1), HH);
+  }
   s->bcs = ubcs;
   s->n_bcs = (int)ubcs.size();
   s->h_bcs.assign(std::max<size_t>(1, ubcs.size()), BcParam{});
@@ -854,6 +894,29 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   H3C_CUDA(s, cudaMemcpy(s->d_gown, h_own.data(), ngm, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemcpy(s->d_gdx, h_gdx.data(), sizeof(double) * ngm, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemset(s->d_gpartner, 0xff, sizeof(int) * ngm));
+  if (halo_tables) {
+    const bool mixed = s->desc.precision == H3C_MIXED;
+    const size_t smem = halo_smem_bytes(nd, mixed, HH.hmax);
+    const int bps = halo_prepare(nd, mixed, smem);
+    if (bps > 0) {
+      H3C_CUDA(s, cudaMalloc(&s->d_lnb, sizeof(unsigned short) * HH.lnb.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_hids, sizeof(int) * HH.ids.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_hoff, sizeof(int) * HH.off.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_grp, sizeof(unsigned short) * HH.grp.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_goff, sizeof(int) * HH.goff.size()));
+      H3C_CUDA(s, cudaMemcpy(s->d_lnb, HH.lnb.data(), sizeof(unsigned short) * HH.lnb.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_hids, HH.ids.data(), sizeof(int) * HH.ids.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_hoff, HH.off.data(), sizeof(int) * HH.off.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_grp, HH.grp.data(), sizeof(unsigned short) * HH.grp.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_goff, HH.goff.data(), sizeof(int) * HH.goff.size(), cudaMemcpyHostToDevice));
+      s->hmax = HH.hmax;
+      s->halo_smem = smem;
+      s->halo_bps = bps;
+      s->halo_mean = HH.mean_halo;
+      s->halo_maxh = HH.max_halo;
+      s->halo_ok = true;
+    }
+  }
   H3C_CUDA(s, cudaMemcpy(s->d_bcs, s->h_bcs.data(), sizeof(BcParam) * s->h_bcs.size(), cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemcpy(s->d_dev2caller, dev2caller.data(), sizeof(long long) * n_tot, cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemset(s->d_q[0], 0, sizeof(double) * s->nv * L));
@@ -1317,6 +1380,25 @@ static int read_scalars(h3c_solver s, Scalars* out) {
   return H3C_OK;
 }
 
+// The error the status bits of a step's scalars stand for (hom3 terminates
+// the run instead: solution_diverged, utilities.hpp:74-76, 107-110, and the
+// check_variables asserts, euler/physics.hpp:229-239).  The bits stay set
+// until h3c_status or h3c_reset_time clears them, so every later read of
+// dt / time / step reports the failure too.
+static int status_error(h3c_solver s, const Scalars& sc, int inst = 0) {
+  if (sc.status & kStatusTimeout)
+    return s->fail(H3C_E_TIMEOUT, "instance %d: a bounded device wait for a tile's copies ran out", inst);
+  if (sc.status & kStatusState)
+    return s->fail(H3C_E_NONFINITE,
+                   "instance %d: a cell's density, energy or pressure (temperature for heat) is not positive or not "
+                   "finite (hom3's check_variables); dt = %g at step %lld",
+                   inst, sc.dt, (long long)sc.step);
+  if (sc.status & kStatusDt)
+    return s->fail(H3C_E_NONFINITE, "instance %d: solution diverged: dt = %g is outside [1e-300, 1e300] at step %lld",
+                   inst, sc.dt, (long long)sc.step);
+  return H3C_OK;
+}
+
 int h3c_min_dt(h3c_solver s, double* dt) {
   if (!s || !dt) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_min_dt: no grid");
@@ -1327,7 +1409,7 @@ int h3c_min_dt(h3c_solver s, double* dt) {
   int rc = read_scalars(s, &sc);
   if (rc) return rc;
   *dt = ord_to_dbl(sc.mindt_ord);
-  return H3C_OK;
+  return status_error(s, sc);
 }
 
 int h3c_dt(h3c_solver s, double* dt) {
@@ -1336,7 +1418,7 @@ int h3c_dt(h3c_solver s, double* dt) {
   int rc = read_scalars(s, &sc);
   if (rc) return rc;
   *dt = sc.dt;
-  return H3C_OK;
+  return status_error(s, sc);
 }
 int h3c_time(h3c_solver s, double* t) {
   if (!s || !t) return H3C_E_INVALID;
@@ -1344,7 +1426,7 @@ int h3c_time(h3c_solver s, double* t) {
   int rc = read_scalars(s, &sc);
   if (rc) return rc;
   *t = sc.time;
-  return H3C_OK;
+  return status_error(s, sc);
 }
 int h3c_step(h3c_solver s, int64_t* step) {
   if (!s || !step) return H3C_E_INVALID;
@@ -1352,7 +1434,7 @@ int h3c_step(h3c_solver s, int64_t* step) {
   int rc = read_scalars(s, &sc);
   if (rc) return rc;
   *step = sc.step;
-  return H3C_OK;
+  return status_error(s, sc);
 }
 int h3c_force_dt(h3c_solver s, double dt) {
   if (!s) return H3C_E_INVALID;
@@ -1362,12 +1444,19 @@ int h3c_force_dt(h3c_solver s, double dt) {
 }
 int h3c_status(h3c_solver s, int* flags) {
   if (!s || !flags) return H3C_E_INVALID;
-  Scalars sc;
-  int rc = read_scalars(s, &sc);
-  if (rc) return rc;
-  *flags = sc.status;
-  int zero = 0;
-  H3C_CUDA(s, cudaMemcpy(&s->d_sc->status, &zero, sizeof(int), cudaMemcpyHostToDevice));
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_status: no grid");
+  std::vector<Scalars> h(s->n_inst);
+  H3C_CUDA(s, cudaMemcpyAsync(h.data(), s->d_sc, sizeof(Scalars) * s->n_inst, cudaMemcpyDeviceToHost, s->stream));
+  H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  int f = 0;
+  for (int i = 0; i < s->n_inst; ++i) {
+    f |= h[i].status;
+    if (h[i].status) {
+      const int zero = 0;
+      H3C_CUDA(s, cudaMemcpy(&s->d_sc[i].status, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    }
+  }
+  *flags = f;
   return H3C_OK;
 }
 
@@ -1539,9 +1628,30 @@ int h3c_set_option(h3c_solver s, int option, int value) {
   switch (option) {
     case H3C_OPT_TILE_KERNEL: s->tile = value != 0; break;
     case H3C_OPT_GRAPHS: s->graphs = value != 0; break;
+    case H3C_OPT_HALO_KERNEL: s->halo = value != 0; break;
+    case H3C_OPT_PERSISTENT_BLOCKS:
+      if (value < 0) return s->fail(H3C_E_INVALID, "h3c_set_option: persistent blocks must be >= 0");
+      s->persist_blocks = value;
+      break;
     default: return s->fail(H3C_E_INVALID, "h3c_set_option: unknown option %d", option);
   }
   drop_graph(s);
+  return H3C_OK;
+}
+
+int h3c_kernel_info(h3c_solver s, int64_t* info, int n) {
+  if (!s || !info || n < 0) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_kernel_info: no grid");
+  const bool euler = s->desc.physics == H3C_EULER && s->desc.reconstruction != H3C_RECON_MUSCL;
+  const bool halo = euler && s->desc.flux == H3C_FLUX_AUSM && s->tile && s->halo && s->halo_ok;
+  const int64_t grid = halo ? std::max<long long>(1, std::min<long long>(s->persist_blocks > 0 ? s->persist_blocks
+                                                                         : (long long)s->halo_bps * num_sms(),
+                                                                         s->ntiles))
+                            : (s->persist_blocks > 0 ? std::min<long long>(s->persist_blocks, s->ntiles) : s->ntiles);
+  const int64_t v[8] = {halo ? 2 : (euler && s->tile ? 1 : 0), s->halo_ok ? s->hmax : 0, s->halo_maxh,
+                        (int64_t)std::llround(1000.0 * s->halo_mean), s->halo_bps, grid, (int64_t)s->halo_smem,
+                        s->ntiles};
+  for (int i = 0; i < n && i < 8; ++i) info[i] = v[i];
   return H3C_OK;
 }
 
@@ -1556,6 +1666,8 @@ int h3c_instances(h3c_solver s, double* dt, double* time, int64_t* step) {
     if (time) time[i] = h[i].time;
     if (step) step[i] = h[i].step;
   }
+  for (int i = 0; i < s->n_inst; ++i)
+    if (int rc = status_error(s, h[i], i)) return rc;
   return H3C_OK;
 }
 

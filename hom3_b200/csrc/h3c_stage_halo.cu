@@ -1,0 +1,524 @@
+// h3c_stage_halo.cu -- the Euler/AUSM stage on Morton tiles staged into shared
+// memory by bulk copies, and the host tables it reads.
+//
+// hom3's step evaluates, for every cell, the 2 nd face fluxes of num_flux
+// (src/solver/fv/solver.hpp:440-460) with the AUSM flux
+// (src/solver/fv/euler/physics.hpp:276-325) and applies the explicit update of
+// evolve (solver.hpp:470-494).  Here one block owns a 256-cell tile of the
+// Morton order at a time (persistent blocks take tiles round-robin):
+//
+//  1. copies: one thread issues cp.async.bulk copies of the tile's state
+//     columns, neighbour-slot columns and level bytes into shared memory
+//     (completion counted on an mbarrier); every thread issues 8-byte
+//     cp.async copies of the state of its share of the tile's halo cells
+//     (the cells outside the tile that the tile's faces read, listed at
+//     set-up).  The next tile's copies are issued as soon as the current
+//     tile's copies have been turned into face states, so they are in flight
+//     while the current tile's fluxes are computed.
+//  2. face states: theta = a (rho u, rho, rho E + p), p and the Mach numbers
+//     of every tile and halo cell, computed once into shared memory
+//     (theta_, euler/physics.hpp:315-325).
+//  3. fluxes, direction by direction: each cell evaluates its plus face and
+//     publishes it; a cell takes its minus face from the tile neighbour that
+//     published it (a same-level face, linked both ways), or evaluates it
+//     itself (tile border, coarse/fine face).  Every face flux is the same
+//     F(l, r) evaluation hom3 performs, and each cell sums
+//     F(minus) - F(plus) direction by direction in hom3's order, so results
+//     are bit-identical to the per-cell evaluation.
+//  4. update and the fused CFL minimum of the next step.
+//
+// No branch of a warp reads global memory for a neighbour: the per-lane
+// divergent neighbour loads of the register-tiled kernel (k_stage_ausm) are
+// replaced by the cooperative, coalesced halo copies of step 1.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <thread>
+#include <vector>
+
+#define H3C_DEVICE_FUNCTIONS_ONLY
+#include "fv_kernels.cuh"
+#include "stage_halo.hpp"
+
+namespace h3c {
+
+// ---------------------------------------------------------------------------
+// PTX wrappers: shared-memory mbarrier, 1D bulk copy global -> shared (no
+// multicast), 8-byte asynchronous copies, proxy fences.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// orders this thread's (and, after a barrier, the block's) generic-proxy
+// accesses of shared memory before its following async-proxy (bulk copy) ones
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// A wait for a tile's bulk copies gives up after about two seconds at the
+// B200's clock instead of spinning for ever.
+constexpr long long kWaitCycles = 4000000000LL;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > kWaitCycles) return false;
+  return true;
+}
+
+template <class R, int ND>
+__host__ __device__ constexpr size_t halo_layout_bytes(int hmax) {
+  // mbarrier (16) | landing [nv][S] f64 | face states [2nd+3][S] R |
+  // published plus fluxes [2][nv][256] f64 | neighbour slots [2][2nd][256] u16 | levels [2][256] u8
+  return 16 + 8 * (size_t)(ND + 2) * (kHaloTile + hmax) + sizeof(R) * (size_t)(2 * ND + 3) * (kHaloTile + hmax) +
+         2 * 8 * (size_t)(ND + 2) * kHaloTile + 2 * 2 * (size_t)(2 * ND) * kHaloTile + 2 * (size_t)kHaloTile;
+}
+
+// Face state of a cell from its state q: theta = a (rho u, rho, rho E + p),
+// p and the Mach numbers, the arithmetic of k_stage_ausm's face states.
+template <class R, int ND>
+__device__ __forceinline__ void face_state_of(const double* q, R gamma, R gm1, R* th, R& p, R* M) {
+  Prim<R, ND> P;
+#pragma unroll
+  for (int v = 0; v < ND + 2; ++v) P.q[v] = (R)q[v];
+  make_prim<R, ND>(P, gamma, gm1);
+#pragma unroll
+  for (int v = 0; v < ND + 1; ++v) th[v] = P.q[v] * P.a;
+  th[ND + 1] = (P.q[ND + 1] + P.p) * P.a;
+  p = P.p;
+#pragma unroll
+  for (int d = 0; d < ND; ++d) M[d] = P.M[d];
+}
+
+template <int ND, class R, int MODE, bool HANG, bool FUSE>
+__global__ void __launch_bounds__(kHaloTile, 2)
+    k_stage_halo(const double* __restrict__ qin, double* out, Geometry g, HaloGeom hg, PhysConst pc,
+                 const Scalars* __restrict__ sc, long long* dtmin, int* status) {
+  constexpr int NV = ND + 2, NP = 2 * ND, NS = 1 << (ND - 1), TB = kHaloTile;
+  constexpr int KH = kHaloMaxSlots / kHaloTile;  // halo cells one thread copies, at most
+  constexpr double W = ND == 2 ? 0.5 : 0.25;
+  const int S = TB + hg.hmax;
+  extern __shared__ __align__(128) unsigned char smem[];
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem);
+  double* land = reinterpret_cast<double*>(smem + 16);                                  // [NV][S]
+  R* fs = reinterpret_cast<R*>(land + (size_t)NV * S);                                 // [2ND+3][S]
+  double* fx = reinterpret_cast<double*>(fs + (size_t)(2 * ND + 3) * S);                // [2][NV][TB]
+  unsigned short* ln = reinterpret_cast<unsigned short*>(fx + 2 * NV * TB);              // [2][NP][TB]
+  unsigned char* ll = reinterpret_cast<unsigned char*>(ln + 2 * NP * TB);                // [2][TB]
+  __shared__ double slen[kMaxLevels];
+  const int tid = threadIdx.x;
+  const long long ld = g.ld;
+  const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+
+  long long tile = blockIdx.x;
+  if (tile >= g.ntiles) return;
+  if (tid < kMaxLevels) slen[tid] = g.len[tid];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+
+  // the halo cells of tile t this thread copies; returns the tile's halo size
+  auto fetch_ids = [&](long long t, int* hid) -> int {
+    const int o0 = __ldg(hg.halo_off + t);
+    const int nh = __ldg(hg.halo_off + t + 1) - o0;
+#pragma unroll
+    for (int k = 0; k < KH; ++k) {
+      const int h = tid + k * TB;
+      hid[k] = h < nh ? __ldg(hg.halo_ids + o0 + h) : 0;
+    }
+    return nh;
+  };
+  // the copies of tile t into the landing area and neighbour/level buffer buf
+  auto issue = [&](long long t, int buf, const int* hid, int nh) {
+    if (tid == 0) {
+      const long long c0 = t * TB;
+      const long long te = min(c0 + TB, instance_end(g, tile_instance(g, t)));
+      const unsigned ncp = (unsigned)((te - c0 + 15) & ~15LL);  // whole 16-cell groups: 16-byte multiples
+      fence_proxy_async();
+      mbar_expect_tx(bar, ncp * (8u * NV + 2u * NP + 1u));
+#pragma unroll
+      for (int v = 0; v < NV; ++v) bulk_g2s(land + (size_t)v * S, qin + v * ld + c0, ncp * 8u, bar);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) bulk_g2s(ln + (buf * NP + p) * TB, hg.lnb + p * ld + c0, ncp * 2u, bar);
+      bulk_g2s(ll + buf * TB, g.lvl + c0, ncp, bar);
+    }
+#pragma unroll
+    for (int k = 0; k < KH; ++k) {
+      const int h = tid + k * TB;
+      if (h < nh) {
+        const long long n = hid[k];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) cp_async8(land + (size_t)v * S + TB + h, qin + v * ld + n);
+      }
+    }
+    cp_async_commit();
+  };
+  auto load_fs = [&](int slot, int d, FaceState<R, ND>& F) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) F.th[v] = fs[v * S + slot];
+    F.p = fs[NV * S + slot];
+    F.M = fs[(NV + 1 + d) * S + slot];
+  };
+
+  int hid[KH], hid_n[KH];
+  int nh = fetch_ids(tile, hid);
+  issue(tile, 0, hid, nh);
+
+  for (int it = 0; tile < g.ntiles; tile += gridDim.x, ++it) {
+    const int buf = it & 1;
+    const long long next = tile + gridDim.x;
+    int nh_n = 0;
+    if (next < g.ntiles) nh_n = fetch_ids(next, hid_n);
+    const long long c0 = tile * TB, c = c0 + tid;
+    const int inst = tile_instance(g, tile);
+    const long long te = min(c0 + (long long)TB, instance_end(g, inst));
+    const bool live = c < te;
+    const int gbase = HANG ? __ldg(hg.grp_off + tile) : 0;
+    double qo[NV];
+    if (MODE != 0 && live) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
+    }
+
+    // ---- this tile's copies ----
+    const bool ok = mbar_wait_bounded(bar, (unsigned)(it & 1));
+    cp_async_wait_all();
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) atomicOr(status, 4);
+      return;
+    }
+
+    // ---- face states of the own cell (kept in registers) and the halo cells ----
+    double qc[NV];
+    R thc[NV], pcell = R(0), Mc[ND];
+    if (live) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qc[v] = land[(size_t)v * S + tid];
+      face_state_of<R, ND>(qc, gamma, gm1, thc, pcell, Mc);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) fs[v * S + tid] = thc[v];
+      fs[NV * S + tid] = pcell;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) fs[(NV + 1 + d) * S + tid] = Mc[d];
+    }
+    for (int h = TB + tid; h < TB + nh; h += TB) {
+      double qh[NV];
+      R th[NV], ph, Mh[ND];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qh[v] = land[(size_t)v * S + h];
+      face_state_of<R, ND>(qh, gamma, gm1, th, ph, Mh);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) fs[v * S + h] = th[v];
+      fs[NV * S + h] = ph;
+#pragma unroll
+      for (int d = 0; d < ND; ++d) fs[(NV + 1 + d) * S + h] = Mh[d];
+    }
+    __syncthreads();  // landing area consumed; face states complete
+
+    // ---- the next tile's copies fly while this tile's fluxes are computed ----
+    if (next < g.ntiles) issue(next, buf ^ 1, hid_n, nh_n);
+
+    // ---- fluxes, direction by direction ----
+    const unsigned short* L = ln + buf * NP * TB;
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      double* X = fx + (d & 1) * NV * TB;
+      FaceState<R, ND> Fc;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Fc.th[v] = thc[v];
+      Fc.p = pcell;
+      Fc.M = Mc[d];
+      double fp[NV];
+      if (live) {
+        const int p = L[(2 * d + 1) * TB + tid];
+        if (!HANG || !(p & kGroupBit)) {
+          FaceState<R, ND> Fn;
+          load_fs(p, d, Fn);
+          R f[NV];
+          ausm_face<R, ND>(Fc, Fn, d, f);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
+        } else {
+          const unsigned short* gsl = hg.grp + (size_t)(gbase + (p & ~kGroupBit)) * NS;
+#pragma unroll
+          for (int j = 0; j < NS; ++j) {
+            FaceState<R, ND> Fn;
+            load_fs(__ldg(gsl + j), d, Fn);
+            R f[NV];
+            ausm_face<R, ND>(Fc, Fn, d, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
+          }
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fp[v] = W * fp[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) X[v * TB + tid] = fp[v];
+      }
+      __syncthreads();  // plus fluxes of direction d published
+      if (live) {
+        const int m = L[(2 * d) * TB + tid];
+        double fm[NV];
+        if (m < TB && L[(2 * d + 1) * TB + m] == tid) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = X[v * TB + m];
+        } else if (!HANG || !(m & kGroupBit)) {
+          FaceState<R, ND> Fn;
+          load_fs(m, d, Fn);
+          R f[NV];
+          ausm_face<R, ND>(Fn, Fc, d, f);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
+        } else {
+          const unsigned short* gsl = hg.grp + (size_t)(gbase + (m & ~kGroupBit)) * NS;
+#pragma unroll
+          for (int j = 0; j < NS; ++j) {
+            FaceState<R, ND> Fn;
+            load_fs(__ldg(gsl + j), d, Fn);
+            R f[NV];
+            ausm_face<R, ND>(Fn, Fc, d, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
+          }
+#pragma unroll
+          for (int v = 0; v < NV; ++v) fm[v] = W * fm[v];
+        }
+#pragma unroll
+        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - fp[v]);
+      }
+      // the buffer X is written again two directions later, after the next barrier
+    }
+
+    // ---- update and the next step's CFL minimum ----
+    long long ord = kOrdMax;
+  bool bad = false;
+    if (live) {
+      const double dx = slen[ll[buf * TB + tid]];
+      const double dt = sc[inst].dt;
+      const double k = dt / dx;
+      double o[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], qc[v], k * acc[v]);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
+      if (FUSE) {
+        const double cd = cell_dt<ND, EULER>(o, dx, pc, nullptr, &bad);
+        if (!isnan(cd)) ord = dbl_to_ord(cd);
+      }
+    }
+    if (FUSE) {
+    flag_bad_state(bad, sc, inst);
+    block_min_atomic(ord, per_instance(dtmin, inst));
+  }
+    nh = nh_n;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+bool halo_build(int nd, long long ld, long long ntiles, const std::vector<long long>& tile_end, const int* nbr,
+                const int* sub, long long nsub, HaloHost& H) {
+  const int NP = 2 * nd, NS = 1 << (nd - 1), TB = kHaloTile;
+  H.lnb.assign((size_t)NP * ld, 0);
+  std::vector<std::vector<int>> halo(ntiles);
+  std::vector<std::vector<unsigned short>> grp(ntiles);
+  std::atomic<bool> ok{true};
+  auto work = [&](long long t0, long long t1) {
+    std::vector<int> tmp;
+    for (long long t = t0; t < t1 && ok.load(std::memory_order_relaxed); ++t) {
+      const long long c0 = t * TB, ce = tile_end[t];
+      auto outside = [&](long long v) { return v < c0 || v >= ce; };
+      tmp.clear();
+      for (long long c = c0; c < ce; ++c)
+        for (int p = 0; p < NP; ++p) {
+          const long long v = nbr[p * ld + c];
+          if (v >= 0) {
+            if (outside(v)) tmp.push_back((int)v);
+          } else if (v <= -2) {
+            const long long k = -v - 2;
+            for (int j = 0; j < NS; ++j) {
+              const long long sv = sub[j * nsub + k];
+              if (outside(sv)) tmp.push_back((int)sv);
+            }
+          }
+        }
+      std::sort(tmp.begin(), tmp.end());
+      tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+      if ((int)tmp.size() > kHaloMaxSlots) {
+        ok = false;
+        break;
+      }
+      auto slot = [&](long long v) -> unsigned short {
+        if (!outside(v)) return (unsigned short)(v - c0);
+        return (unsigned short)(TB + (std::lower_bound(tmp.begin(), tmp.end(), (int)v) - tmp.begin()));
+      };
+      std::vector<unsigned short>& G = grp[t];
+      for (long long c = c0; c < ce; ++c)
+        for (int p = 0; p < NP; ++p) {
+          const long long v = nbr[p * ld + c];
+          unsigned short e = 0;
+          if (v >= 0) {
+            e = slot(v);
+          } else if (v <= -2) {
+            const long long k = -v - 2;
+            const size_t gi = G.size() / NS;
+            if (gi >= kGroupBit) {
+              ok = false;
+              break;
+            }
+            e = (unsigned short)(kGroupBit | gi);
+            for (int j = 0; j < NS; ++j) G.push_back(slot(sub[j * nsub + k]));
+          }
+          H.lnb[(size_t)p * ld + c] = e;
+        }
+      halo[t] = tmp;
+    }
+  };
+  const int nthr = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
+  std::vector<std::thread> pool;
+  const long long per = (ntiles + nthr - 1) / nthr;
+  for (int i = 0; i < nthr; ++i) {
+    const long long a = i * per, b = std::min(ntiles, a + per);
+    if (a < b) pool.emplace_back(work, a, b);
+  }
+  for (auto& th : pool) th.join();
+  if (!ok) return false;
+  H.off.assign(ntiles + 1, 0);
+  H.goff.assign(ntiles + 1, 0);
+  size_t nids = 0, ngrp = 0;
+  int mx = 0;
+  for (long long t = 0; t < ntiles; ++t) {
+    nids += halo[t].size();
+    ngrp += grp[t].size() / NS;
+    mx = std::max(mx, (int)halo[t].size());
+    H.off[t + 1] = (int)nids;
+    H.goff[t + 1] = (int)ngrp;
+  }
+  H.ids.resize(std::max<size_t>(nids, 1));
+  H.grp.resize(std::max<size_t>(ngrp * NS, 1));
+  for (long long t = 0; t < ntiles; ++t) {
+    std::copy(halo[t].begin(), halo[t].end(), H.ids.begin() + H.off[t]);
+    std::copy(grp[t].begin(), grp[t].end(), H.grp.begin() + (size_t)H.goff[t] * NS);
+  }
+  H.max_halo = mx;
+  H.mean_halo = ntiles ? (double)nids / ntiles : 0.0;
+  H.hmax = std::max(32, (mx + 31) / 32 * 32);
+  return true;
+}
+
+size_t halo_smem_bytes(int nd, bool mixed, int hmax) {
+  if (nd == 2) return mixed ? halo_layout_bytes<float, 2>(hmax) : halo_layout_bytes<double, 2>(hmax);
+  return mixed ? halo_layout_bytes<float, 3>(hmax) : halo_layout_bytes<double, 3>(hmax);
+}
+
+namespace {
+
+template <int ND, class R, int MODE, bool HANG, bool FUSE>
+int prepare_one(size_t smem) {
+  auto k = k_stage_halo<ND, R, MODE, HANG, FUSE>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kHaloTile, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nb;
+}
+template <int ND, class R, int MODE, bool HANG>
+int prepare_f(size_t smem) {
+  return std::min(prepare_one<ND, R, MODE, HANG, false>(smem), prepare_one<ND, R, MODE, HANG, true>(smem));
+}
+template <int ND, class R, int MODE>
+int prepare_h(size_t smem) {
+  return std::min(prepare_f<ND, R, MODE, false>(smem), prepare_f<ND, R, MODE, true>(smem));
+}
+template <int ND, class R>
+int prepare_m(size_t smem) {
+  return std::min(std::min(prepare_h<ND, R, 0>(smem), prepare_h<ND, R, 2>(smem)),
+                  std::min(prepare_h<ND, R, 3>(smem), prepare_h<ND, R, 4>(smem)));
+}
+
+template <int ND, class R, int MODE, bool HANG, bool FUSE>
+void launch_one(const double* qin, double* out, const Geometry& g, const HaloGeom& h, const PhysConst& pc,
+                const Scalars* sc, long long* dtmin, int* status, int grid, size_t smem, cudaStream_t st) {
+  k_stage_halo<ND, R, MODE, HANG, FUSE><<<grid, kHaloTile, smem, st>>>(qin, out, g, h, pc, sc, dtmin, status);
+}
+template <int ND, class R, int MODE, bool HANG>
+void launch_f(bool fuse, const double* qin, double* out, const Geometry& g, const HaloGeom& h, const PhysConst& pc,
+              const Scalars* sc, long long* dtmin, int* status, int grid, size_t smem, cudaStream_t st) {
+  if (fuse) launch_one<ND, R, MODE, HANG, true>(qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+  else launch_one<ND, R, MODE, HANG, false>(qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+}
+template <int ND, class R, int MODE>
+void launch_h(bool hang, bool fuse, const double* qin, double* out, const Geometry& g, const HaloGeom& h,
+              const PhysConst& pc, const Scalars* sc, long long* dtmin, int* status, int grid, size_t smem,
+              cudaStream_t st) {
+  if (hang) launch_f<ND, R, MODE, true>(fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+  else launch_f<ND, R, MODE, false>(fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+}
+template <int ND, class R>
+void launch_m(int mode, bool hang, bool fuse, const double* qin, double* out, const Geometry& g, const HaloGeom& h,
+              const PhysConst& pc, const Scalars* sc, long long* dtmin, int* status, int grid, size_t smem,
+              cudaStream_t st) {
+  switch (mode) {
+    case 0: launch_h<ND, R, 0>(hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st); break;
+    case 2: launch_h<ND, R, 2>(hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st); break;
+    case 3: launch_h<ND, R, 3>(hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st); break;
+    default: launch_h<ND, R, 4>(hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st); break;
+  }
+}
+
+}  // namespace
+
+int halo_prepare(int nd, bool mixed, size_t smem) {
+  if (nd == 2) return mixed ? prepare_m<2, float>(smem) : prepare_m<2, double>(smem);
+  return mixed ? prepare_m<3, float>(smem) : prepare_m<3, double>(smem);
+}
+
+void halo_stage(int nd, bool mixed, int mode, bool hang, bool fuse, const double* qin, double* out,
+                const Geometry& g, const HaloGeom& h, const PhysConst& pc, const Scalars* sc, long long* dtmin,
+                int* status, int grid, size_t smem, cudaStream_t st) {
+  if (nd == 2) {
+    if (mixed) launch_m<2, float>(mode, hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+    else launch_m<2, double>(mode, hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+  } else {
+    if (mixed) launch_m<3, float>(mode, hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+    else launch_m<3, double>(mode, hang, fuse, qin, out, g, h, pc, sc, dtmin, status, grid, smem, st);
+  }
+}
+
+}  // namespace h3c

@@ -232,6 +232,7 @@ __global__ void __launch_bounds__(kBlock) k_stage_muscl(const double* __restrict
   const int inst = tile_instance(g, blockIdx.x);
   const bool live = c < instance_end(g, inst);
   long long ord = kOrdMax;
+  bool bad = false;
   if (live) {
     const long long ld = g.ld;
     const double dt = sc[inst].dt;
@@ -315,11 +316,14 @@ __global__ void __launch_bounds__(kBlock) k_stage_muscl(const double* __restrict
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
     if (FUSE) {
-      const double cd = cell_dt<ND, EULER>(o, dx, pc);
+      const double cd = cell_dt<ND, EULER>(o, dx, pc, nullptr, &bad);
       if (!isnan(cd)) ord = dbl_to_ord(cd);
     }
   }
-  if (FUSE) block_min_atomic(ord, per_instance(dtmin, inst));
+  if (FUSE) {
+    flag_bad_state(bad, sc, inst);
+    block_min_atomic(ord, per_instance(dtmin, inst));
+  }
 }
 
 }  // namespace h3c

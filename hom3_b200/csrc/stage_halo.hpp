@@ -1,0 +1,72 @@
+// stage_halo.hpp -- host interface of the halo-staged Euler/AUSM stage kernel
+// (h3c_stage_halo.cu), shared with the solver's host code (h3c_solver.cu).
+//
+// The kernel replaces hom3's num_flux + evolve loop (src/solver/fv/
+// solver.hpp:440-460, 470-494) for Euler with the AUSM flux.  It works on
+// 256-cell tiles of the Morton order.  Per tile, set-up time tables list
+//   * the tile's halo: every cell outside the tile that a face of a tile cell
+//     reads (same-level neighbours, ghosts and the fine cells of coarse/fine
+//     sub-face groups), sorted, and
+//   * for every cell and face position the shared-memory slot the face's
+//     neighbour lives in (0..255: a tile cell, 256 + h: halo cell h) or, with
+//     kGroupBit set, the index of the face's sub-face group in the tile's
+//     group list (whose entries are the slots of the group's fine cells).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "fv_kernels.cuh"
+
+namespace h3c {
+
+constexpr int kHaloTile = 256;              // cells per tile = threads per block
+constexpr int kHaloMaxSlots = 1024;         // halo cells a tile may have
+constexpr unsigned short kGroupBit = 0x8000;
+
+// Device tables of the halo-staged kernel.
+struct HaloGeom {
+  const unsigned short* __restrict__ lnb;  // [2nd][ld] neighbour slot (or kGroupBit | group) per cell
+  const int* __restrict__ halo_ids;        // halo cells of all tiles, concatenated
+  const int* __restrict__ halo_off;        // [ntiles + 1] offsets into halo_ids
+  const unsigned short* __restrict__ grp;  // [groups][2^(nd-1)] slots of each group's fine cells
+  const int* __restrict__ grp_off;         // [ntiles + 1] first group of each tile
+  int hmax;                                // halo slots reserved per tile (multiple of 32)
+};
+
+// Host copies of the tables before upload.
+struct HaloHost {
+  std::vector<unsigned short> lnb, grp;
+  std::vector<int> ids, off, goff;
+  int hmax = 0;
+  int max_halo = 0;      // largest halo of any tile
+  double mean_halo = 0;  // halo cells per tile, mean
+};
+
+// Builds the tables from the device-numbered neighbour table nbr [2nd][ld]
+// (>= 0 cell, <= -2 sub-face group -2 - k of sub [2^(nd-1)][nsub]) for the
+// tiles of [0, n_int); tile_end[t] is the end of tile t's cells (tiles never
+// span two batch instances).  Returns false when some tile's halo exceeds
+// kHaloMaxSlots (the tables are then unusable and the caller keeps the
+// per-lane tile kernel).
+bool halo_build(int nd, long long ld, long long ntiles, const std::vector<long long>& tile_end, const int* nbr,
+                const int* sub, long long nsub, HaloHost& H);
+
+// Dynamic shared memory of one block for nd / precision / halo slots.
+size_t halo_smem_bytes(int nd, bool mixed, int hmax);
+
+// Opts every instantiation for nd / precision into `smem` bytes of dynamic
+// shared memory and returns the resident blocks per SM at that size (0 when
+// the kernel cannot be launched with it).  Call outside stream capture.
+int halo_prepare(int nd, bool mixed, size_t smem);
+
+// One stage: out = rk_combine<mode>(out, qin, dt/dx R(qin)) over the tiles,
+// with the fused next-step CFL minimum into dtmin when fuse.  grid blocks
+// take the tiles round-robin.  status receives bit 2 when a bounded wait for
+// a tile's copies runs out.
+void halo_stage(int nd, bool mixed, int mode, bool hang, bool fuse, const double* qin, double* out,
+                const Geometry& g, const HaloGeom& h, const PhysConst& pc, const Scalars* sc, long long* dtmin,
+                int* status, int grid, size_t smem, cudaStream_t st);
+
+}  // namespace h3c

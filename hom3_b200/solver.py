@@ -285,6 +285,18 @@ class Solver:
     def set_option(self, option, value):
         self._check(lib().h3c_set_option(self.h, int(option), int(value)))
 
+    def set_persistent_blocks(self, n):
+        """Blocks of the Euler/AUSM stage launch (0: the library's default)."""
+        self.set_option(F.OPT_PERSISTENT_BLOCKS, n)
+
+    def kernel_info(self) -> dict:
+        """The Euler stage launch in use (h3c_kernel_info)."""
+        v = np.zeros(8, np.int64)
+        self._check(lib().h3c_kernel_info(self.h, _lp(v), 8))
+        return {"halo": int(v[0] == 2), "kernel": ("per_cell", "tile", "halo")[int(v[0])], "halo_slots": int(v[1]),
+                "max_halo": int(v[2]), "mean_halo": v[3] / 1000.0, "blocks_per_sm": int(v[4]), "grid": int(v[5]),
+                "smem_bytes": int(v[6]), "tiles": int(v[7])}
+
     def solve_dt(self, dts):
         """Steps with the given time steps (the frozen-dt forward map)."""
         d = np.ascontiguousarray(dts, np.float64)

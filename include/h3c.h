@@ -241,8 +241,22 @@ int h3c_dt(h3c_solver s, double* dt);
 int h3c_force_dt(h3c_solver s, double dt);
 int h3c_time(h3c_solver s, double* t);
 int h3c_step(h3c_solver s, int64_t* step);
-/* Non-finite / non-positive dt seen by the device since the last call
- * (utilities.hpp:74-76 checks dt in [1e-300, 1e300]); clears the flag. */
+/* Failure detection.  hom3 ends a run when dt leaves [1e-300, 1e300]
+ * (solution_diverged, utilities.hpp:74-76, 107-110) and asserts positive
+ * density, energy and pressure (temperature for heat) in every cell
+ * (check_variables, euler/physics.hpp:229-239, heat/physics.hpp:89-95).
+ * The device records both as status bits of each instance while it steps
+ * (no extra synchronisation: the CFL reduction checks every cell it reads);
+ * h3c_solve stays asynchronous, and the next call that reads the step
+ * scalars -- h3c_dt, h3c_time, h3c_step, h3c_min_dt, h3c_instances --
+ * returns H3C_E_NONFINITE (or H3C_E_TIMEOUT for a device wait that ran out)
+ * with h3c_last_error saying which, after writing the value it read.  The
+ * bits are sticky: h3c_status returns the OR over instances
+ * (H3C_STATUS_DT | H3C_STATUS_STATE | H3C_STATUS_TIMEOUT) and clears them;
+ * h3c_reset_time clears them too. */
+#define H3C_STATUS_DT 1
+#define H3C_STATUS_STATE 2
+#define H3C_STATUS_TIMEOUT 4
 int h3c_status(h3c_solver s, int* flags);
 
 /* ---- instrumentation (no hom3 counterpart: hom3 has no timers) ----
@@ -254,10 +268,23 @@ int h3c_status(h3c_solver s, int* flags);
 int h3c_launches(h3c_solver s, int64_t* n);
 /* Execution options (no hom3 counterpart; results do not depend on them):
  * H3C_OPT_TILE_KERNEL  Euler stages and their adjoint in the shared-memory tile kernels (default 1)
- * H3C_OPT_GRAPHS       replay runs of steps from a captured CUDA graph (default 1) */
+ * H3C_OPT_GRAPHS       replay runs of steps from a captured CUDA graph (default 1)
+ * H3C_OPT_HALO_KERNEL  with the tile kernels on, Euler/AUSM stages stage each tile and its halo
+ *                      into shared memory by bulk copies (default 1; 0: the per-lane tile kernel) */
 #define H3C_OPT_TILE_KERNEL 1
 #define H3C_OPT_GRAPHS 2
+#define H3C_OPT_HALO_KERNEL 3
+/* H3C_OPT_PERSISTENT_BLOCKS  blocks of the Euler/AUSM stage launch, each looping over tiles
+ *                            (0, the default: one block per tile for the per-lane tile kernel,
+ *                            the resident blocks of all SMs for the halo-staged one) */
+#define H3C_OPT_PERSISTENT_BLOCKS 4
 int h3c_set_option(h3c_solver s, int option, int value);
+/* The Euler stage launch in use (no hom3 counterpart): info[0] kernel (0 per
+ * cell, 1 per-lane tile, 2 halo-staged tile), [1] halo slots per tile, [2]
+ * largest tile halo, [3] mean tile halo x 1000, [4] resident blocks per SM
+ * of the halo-staged kernel, [5] blocks launched, [6] its dynamic shared
+ * memory in bytes, [7] 256-cell tiles; the first n entries are written. */
+int h3c_kernel_info(h3c_solver s, int64_t* info, int n);
 /* Self-test of the device reciprocal / reciprocal square root the kernels
  * use in place of division (n <= 2^24 positive inputs, host arrays). */
 int h3c_selftest_nr(const double* x, int64_t n, double* rcp, double* rsqrt);

@@ -212,7 +212,10 @@ inline bool solver_finished(long long maxNoSteps, const Solver& s) {
   return s.time() >= s.final_time() || s.step() >= maxNoSteps;
 }
 inline bool solution_diverged(const Solver& s) {
-  const double dt = s.dt();
+  double dt = 0;
+  const int rc = h3c_dt(s.handle(), &dt);
+  if (rc == H3C_E_NONFINITE) return true;  // dt out of range or a cell failed the state check
+  check(rc, s.handle());
   return dt < 1e-300 || dt > 1e300;
 }
 // run_solver without the VTK output: initialize, step until finished, and
