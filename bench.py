@@ -134,6 +134,16 @@ def allreduce_max(x, ws):
     return float(t.item())
 
 
+def allreduce_sum(xs, ws):
+    if ws == 1:
+        return list(xs)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(list(xs), dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [float(v) for v in t.tolist()]
+
+
 def barrier(ws):
     if ws > 1:
         import torch.distributed as dist
@@ -170,13 +180,12 @@ def build_workload(args):
     return s, t, q, modes
 
 
-def cpu_oracle_run(args, steps_budget_s=15.0, max_steps=None):
-    """The CPU restatement of hom3 (oracle/) on the same workload, OpenMP over
-    all host threads; returns (cell-updates/s, cells, steps, threads, seconds)."""
+def oracle_solver(args, threads):
+    """The CPU restatement of hom3 (oracle/) set up on the default workload:
+    hom3's tree (MinLevel + sphere refinement), conditions and initial state."""
     from oracle import h3o
     from hom3_b200 import workloads as W
 
-    threads = os.cpu_count() or 1
     h3o.set_num_threads(threads)
     w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=args.base_level)
     w.refine_sphere([0.5, 0.5, 0.5], 0.25, args.base_level + args.extra_levels)
@@ -184,9 +193,18 @@ def cpu_oracle_run(args, steps_budget_s=15.0, max_steps=None):
     s = w.add_solver(h3o.EULER, h3o.AUSM, h3o.RK2, bcs=bcs, ic_kind=h3o.IC_RIEMANN3D_PERTURBED,
                      ic=W.riemann3d_oracle_ic(W.fourier_modes()), time_end=1e30, cfl=args.cfl)
     s.initialize()
+    return w, s
+
+
+def cpu_oracle_run(args, steps_budget_s=15.0, max_steps=None, threads=None):
+    """Times the oracle on the default workload: one warm-up step, one step
+    that sizes the sample to about steps_budget_s, then the timed sample.
+    Returns a dict (value in cell-updates/s, cells, steps, threads, seconds)."""
+    threads = threads or os.cpu_count() or 1
+    w, s = oracle_solver(args, threads)
     s.solve(1)  # warm-up step
     t0 = time.perf_counter()
-    s.solve(1)
+    s.solve(1)  # sizes the sample
     one = time.perf_counter() - t0
     n = max(1, min(int(steps_budget_s / max(one, 1e-6)), 50))
     if max_steps is not None:
@@ -194,23 +212,82 @@ def cpu_oracle_run(args, steps_budget_s=15.0, max_steps=None):
     t0 = time.perf_counter()
     s.solve(n)
     el = time.perf_counter() - t0
-    return s.first_ghost * n / el, s.first_ghost, n, threads, el
+    t = s.tables()
+    sub = t["subface_cells"]
+    return {"value": s.first_ghost * n / el, "cells": int(s.first_ghost), "ghosts": int(s.ncells - s.first_ghost),
+            "subface_groups": int(0 if sub is None else sub.shape[1]), "steps": n, "threads": threads,
+            "seconds": el}
+
+
+def parity_record(args, steps=5):
+    """The checker of the timed path: the oracle and the library's FP64 and
+    mixed paths stepped from the oracle's hom3-numbered tables and initial
+    state through the C ABI (the drop-in path), compared after one step and
+    after `steps` steps."""
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200.solver import euler_neumann
+
+    w, o = oracle_solver(args, os.cpu_count() or 1)
+    t = o.tables()
+    fg = o.first_ghost
+
+    def gpu(prec):
+        g = hb.Solver(3, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, prec, cfl=args.cfl, time_end=1e30)
+        g.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg,
+                   [euler_neumann() for _ in range(6)], t["subface_cells"])
+        g.set_state(o.state(0), 0)
+        g.reset_time()
+        return g
+
+    def max_rel(a, b):
+        big = np.abs(b).max()
+        return float(max(np.abs(a[v] - b[v]).max() / max(np.abs(b[v]).max(), 1e-6 * big) for v in range(b.shape[0])))
+
+    def l2_rel(a, b):
+        return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
+
+    g64, gmx = gpu(F.FP64), gpu(F.MIXED)
+    out = {"cells": int(fg), "steps": steps}
+    for g in (g64, gmx):
+        g.solve(1)
+    o.solve(1)
+    qo = o.state(0)[:, :fg]
+    out["fp64_max_rel_after_1"] = max_rel(g64.state(0)[:, :fg], qo)
+    out["dt_rel_after_1"] = abs(g64.dt() - o.dt()) / o.dt()
+    for g in (g64, gmx):
+        g.solve(steps - 1)
+    o.solve(steps - 1)
+    qo = o.state(0)[:, :fg]
+    q64, qmx = g64.state(0)[:, :fg], gmx.state(0)[:, :fg]
+    out[f"fp64_max_rel_after_{steps}"] = max_rel(q64, qo)
+    out[f"fp64_l2_rel_after_{steps}"] = l2_rel(q64, qo)
+    out[f"mixed_l2_rel_after_{steps}"] = l2_rel(qmx, qo)
+    out[f"mixed_max_rel_after_{steps}"] = max_rel(qmx, qo)
+    out["stage_kernel"] = g64.kernel_info()["kernel"]
+    out["what"] = ("oracle (CPU restatement of hom3) vs the library through h3c_set_grid/h3c_set_state with the "
+                   "oracle's tables and state; max_rel: max over variables of max|a-b| / max|b|; l2_rel: "
+                   "||a-b||_2 / ||b||_2 over all variables")
+    return out
 
 
 def run_reference(args, ws, rank):
     if rank != 0:
         return
-    w_cfg = workload_config(args, None)
-    ups, cells, n, threads, el = cpu_oracle_run(args, steps_budget_s=20.0, max_steps=max(args.steps, 1))
+    r = cpu_oracle_run(args, steps_budget_s=20.0, max_steps=max(args.steps, 1))
+    w_cfg = workload_config(args, {"first_ghost": r["cells"], "ncells": r["cells"] + r["ghosts"],
+                                   "subface_groups": r["subface_groups"]})
+    ups, n = r["value"], r["steps"]
     line = {
         "impl": "reference", "metric": "cell-updates/s", "value": ups, "unit": "cell-updates/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / n, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * r["seconds"] / n, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": w_cfg,
-        "cpu_baseline": {"value": ups, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} full RK2 steps of the same {cells}-cell grid (after 2 warm-up steps); "
-                                   "hom3 itself is uncompilable here (Eigen/Boost/MPI absent), so the "
-                                   "reference is the oracle's C++ restatement of hom3, OpenMP"},
+        "cpu_baseline": {"value": ups, "unit": "cell-updates/s", "cores": r["threads"], "kind": "port",
+                         "sample": f"{n} full RK2 steps of the same {r['cells']}-cell grid, timed after two untimed "
+                                   "steps (one warm-up, one that sizes the sample to about 20 s); hom3 itself is "
+                                   "uncompilable here (Eigen/Boost/MPI absent), so the reference is the oracle's "
+                                   "C++ restatement of hom3, OpenMP over all host threads"},
         "e2e": {"value": ups, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -227,14 +304,20 @@ def workload_config(args, t):
         fg = t["first_ghost"]
         cfg["leaf_cells"] = int(fg)
         cfg["ghost_cells"] = int(t["ncells"] - fg)
-        cfg["subface_groups"] = int(0 if t["subface_cells"] is None else t["subface_cells"].shape[1])
+        if "subface_groups" in t:
+            cfg["subface_groups"] = int(t["subface_groups"])
+        else:
+            cfg["subface_groups"] = int(0 if t["subface_cells"] is None else t["subface_cells"].shape[1])
     return cfg
 
 
-def run_ensemble(args, ws, rank, local):
-    """Batched workload: 256 independent 2D isentropic-vortex grids of uneven
-    size (nx, ny in U{32..512}, +1-level patches on 0-30% of each box), one
-    launch per stage over all of them, launch shape from the autotuner."""
+def ensemble_measure(args, ws, local, steps, warmup):
+    """The batched workload: args.members independent 2D isentropic-vortex
+    grids of uneven size (nx, ny in U{32..512}, +1-level patches on 0-30% of
+    each box), one launch per stage over all of them (launch shape from the
+    autotuner), mixed and FP64; the plain FP64 path one grid at a time; the
+    L2 error of the batched runs against the single-instance FP64 runs.
+    Returns a dict (the record the bench line carries)."""
     import concurrent.futures as cf
 
     import torch
@@ -244,8 +327,14 @@ def run_ensemble(args, ws, rank, local):
     from hom3_b200 import workloads as W
     from hom3_b200.solver import euler_neumann
 
+    from hom3_b200 import shard
+
     torch.cuda.set_device(local)
-    ms = W.ensemble_members(args.members)
+    all_ms = W.ensemble_members(args.members)
+    # N ranks split the independent instances (no collective on the data path)
+    rank = int(os.environ.get("RANK", "0"))
+    assign = shard.partition([m["nx"] * m["ny"] for m in all_ms], ws)
+    ms = [all_ms[i] for i in assign[rank]]
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:  # the builder releases the GIL
         tables = list(ex.map(W.ensemble_member_tables, ms))
 
@@ -259,7 +348,8 @@ def run_ensemble(args, ws, rank, local):
     with cf.ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
         states = list(ex.map(ic, zip(ms, tables)))
     q0 = np.concatenate(states, axis=1)
-    cells = sum(t["first_ghost"] for t in tables)
+    local_cells = sum(t["first_ghost"] for t in tables)
+    cells = int(allreduce_sum([local_cells], ws)[0])  # all ranks' instances
     results = {}
     for prec_name in ("mixed", "fp64"):
         prec = F.MIXED if prec_name == "mixed" else F.FP64
@@ -269,19 +359,20 @@ def run_ensemble(args, ws, rank, local):
         b.reset_time()
         choice, _ = b.autotune(10)
         stream = torch.cuda.ExternalStream(b.stream())
-        b.solve(args.warmup)
+        b.solve(warmup)
         torch.cuda.synchronize()
         barrier(ws)
         l0 = b.launches()
         with ClockSampler(local) as clk:
             ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ev0.record(stream)
-            b.solve(args.steps)
+            b.solve(steps)
             ev1.record(stream)
             torch.cuda.synchronize()
         ms_ = allreduce_max(ev0.elapsed_time(ev1), ws)
-        results[prec_name] = dict(value=cells * args.steps * ws / (ms_ * 1e-3), ms=ms_, choice=choice,
-                                  launches=b.launches() - l0, clocks=clk.summary(), state=b.state(0))
+        results[prec_name] = dict(value=cells * steps / (ms_ * 1e-3), ms=ms_, choice=choice,
+                                  launches=b.launches() - l0, clocks=clk.summary(), state=b.state(0),
+                                  kernel=b.kernel_info(), inst=b.instances())
         del b
     # the plain FP64 path without batching: one solver per grid, stepped one after another
     seq = []
@@ -291,37 +382,68 @@ def run_ensemble(args, ws, rank, local):
                     [euler_neumann() for _ in range(4)], t["subface_cells"])
         s1.set_state(q, 0)
         s1.reset_time()
-        s1.solve(args.warmup)
+        s1.solve(warmup)
         seq.append(s1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for s1 in seq:  # each grid finishes before the next starts (dt read-back synchronises)
-        s1.solve(args.steps)
+        s1.solve(steps)
         s1.dt()
     torch.cuda.synchronize()
     seq_s = allreduce_max(time.perf_counter() - t0, ws)
-    seq_value = cells * args.steps * ws / seq_s
+    seq_value = cells * steps / seq_s
+    # accuracy after the same warmup + steps: batched mixed and batched FP64
+    # against the single-instance FP64 runs (relative L2 over all instances)
+    single = np.concatenate([s1.state(0) for s1 in seq], axis=1)
     del seq
-    # accuracy of the mixed path against the FP64 path after the same steps (L2, relative)
     qa, qb = results["mixed"].pop("state"), results["fp64"].pop("state")
-    l2 = float(np.sqrt(((qa - qb) ** 2).sum() / (qb ** 2).sum()))
+    results["fp64_inst"] = results["fp64"].pop("inst")
+    results["mixed"].pop("inst")
+    num_m, num_f, den = allreduce_sum([((qa - single) ** 2).sum(), ((qb - single) ** 2).sum(), (single ** 2).sum()], ws)
+    l2_mixed = float(np.sqrt(num_m / den))
+    l2_fp64 = float(np.sqrt(num_f / den))
+    # per-instance time steps of every rank, gathered in instance order
+    dts = shard.gather(list(zip(*results["fp64_inst"][:2])), assign, rank)
     peak, peak_kind = peaks()
     r = results["mixed"]
+    bytes_cell_step = 2 * 4 * 8 + 3 * 4 * 8 + 2 * (4 * 4 + 1)  # RK2, 2D: states, int32 neighbours, level byte
+    ach = local_cells * bytes_cell_step / (r["ms"] / steps * 1e-3) / 1e9  # this rank's GPU
+    return {
+        "members": args.members, "leaf_cells": int(cells), "steps": steps, "warmup": warmup,
+        "ranks": ws, "instances_per_rank": [len(a) for a in assign],
+        "instance_dt_range": [float(min(d for d, _ in dts)), float(max(d for d, _ in dts))],
+        "batched_mixed_value": r["value"], "batched_fp64_value": results["fp64"]["value"],
+        "plain_fp64_one_grid_at_a_time_value": seq_value,
+        "mixed_over_fp64_batched": r["value"] / results["fp64"]["value"],
+        "batched_fp64_over_one_at_a_time": results["fp64"]["value"] / seq_value,
+        "batched_mixed_over_plain_fp64": r["value"] / seq_value,
+        "l2_rel_batched_mixed_vs_single_fp64": l2_mixed, "l2_rel_batched_fp64_vs_single_fp64": l2_fp64,
+        "autotune_choice": {"mixed": r["choice"], "fp64": results["fp64"]["choice"]},
+        "stage_kernel": {"mixed": r["kernel"], "fp64": results["fp64"]["kernel"]},
+        "gpu_launches_mixed": int(r["launches"]), "clocks": r["clocks"],
+        "roofline": {"bound": "hbm", "peak": peak, "peak_source": peak_kind, "unit": "GB/s", "achieved": ach,
+                     "frac": ach / peak, "what": "whole batched mixed step, algorithmic bytes "
+                                                 f"{bytes_cell_step} B per cell-update"},
+        "what": "batched: one launch per stage over all instances (autotuned launch shape); plain: one solver "
+                "per grid stepped to completion one after another (dt read-back between grids)",
+    }
+
+
+def run_ensemble(args, ws, rank, local):
+    """The batched workload alone, as the bench line (see ensemble_measure)."""
+    e = ensemble_measure(args, ws, local, args.steps, args.warmup)
     line = {
-        "metric": "cell-updates/s", "value": r["value"], "unit": "cell-updates/s", "n_gpus": ws, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32-flux/f64-state", "data": "synthetic",
+        "metric": "cell-updates/s", "value": e["batched_mixed_value"], "unit": "cell-updates/s", "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": e["leaf_cells"] / e["batched_mixed_value"] * 1e3,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32-flux/f64-state",
+        "data": "synthetic",
         "config": {"workload": f"{args.members} independent 2D isentropic vortices (nx, ny in U{{32..512}}, "
                                "+1-level patches on 0-30% of each box, beta in U[1,5]), Neumann outflow, AUSM, RK2, "
-                               "one launch per stage over all instances",
-                   "leaf_cells": int(cells), "autotune_choice": r["choice"], "parallelism": f"replicas x{ws}"},
-        "fp64_value": results["fp64"]["value"], "mixed_over_fp64": r["value"] / results["fp64"]["value"],
-        "plain_fp64_one_grid_at_a_time_value": seq_value, "batched_mixed_over_plain_fp64": r["value"] / seq_value,
-        "l2_rel_mixed_vs_fp64": l2, "gpu_launches": int(r["launches"]), "clocks": r["clocks"],
-        "roofline": {"bound": "hbm", "peak": peak, "peak_source": peak_kind, "unit": "GB/s",
-                     "achieved": cells * (2 * 4 * 8 + 3 * 4 * 8 + 2 * (4 * 4 + 1)) / (r["ms"] / args.steps * 1e-3) / 1e9},
+                               "one launch per stage over all instances of a rank",
+                   "leaf_cells": e["leaf_cells"],
+                   "parallelism": f"instances split over {ws} rank(s), no collective on the data path"},
+        "gpu_launches": e["gpu_launches_mixed"], "clocks": e["clocks"], "roofline": e["roofline"], "batched": e,
     }
-    line["roofline"]["frac"] = line["roofline"]["achieved"] / peak
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -377,8 +499,14 @@ def run_tgv(args, ws, rank, local):
         ms = allreduce_max(ev0.elapsed_time(ev1), ws)
         q = s.state(0)[:, :fg]
         ke = 0.5 * ((q[0] ** 2 + q[1] ** 2 + q[2] ** 2) / q[3]).mean()
+        # per-kernel device time of further steps, every launch bracketed by events
+        s.profile(True)
+        s.solve(min(args.steps, 20))
+        torch.cuda.synchronize()
+        s.profile(False)
+        kern = s.profile_read()
         out[name] = dict(value=fg * args.steps * ws / (ms * 1e-3), ms=ms, ke=float(ke), time=s.time(),
-                         clocks=clk.summary())
+                         clocks=clk.summary(), kernels=kern, stage_kernel=s.kernel_info())
     ke_init = float((0.5 * (q0[0, :fg] ** 2 + q0[1, :fg] ** 2) / q0[3, :fg]).mean())
     line = {"metric": "cell-updates/s", "value": out["fp64"]["value"], "unit": "cell-updates/s", "n_gpus": ws,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["fp64"]["ms"] / args.steps,
@@ -388,7 +516,20 @@ def run_tgv(args, ws, rank, local):
             "mixed_value": out["mixed"]["value"], "mixed_over_fp64": out["mixed"]["value"] / out["fp64"]["value"],
             "ke_fp64": out["fp64"]["ke"], "ke_mixed": out["mixed"]["ke"], "ke_initial": ke_init,
             "ke_rel_diff": abs(out["mixed"]["ke"] - out["fp64"]["ke"]) / out["fp64"]["ke"],
-            "sim_time": out["fp64"]["time"], "clocks": out["fp64"]["clocks"]}
+            "sim_time": out["fp64"]["time"], "clocks": out["fp64"]["clocks"],
+            "stage_kernel": out["fp64"]["stage_kernel"],
+            "kernels_ms": {n: {k: {"total_ms": v[0], "launches": v[1]} for k, v in out[n]["kernels"].items()}
+                           for n in out}}
+    # roofline of the second RK stage: reads lhs and rhs, writes lhs (3 x 5 x 8 B per cell; uniform grid,
+    # no table bytes counted); the CNS stage is FP64-arithmetic heavy, so HBM is a lower bound on its time
+    peak, peak_kind = peaks()
+    st2_ms, st2_n = out["fp64"]["kernels"].get("stage2", (0.0, 0))
+    if st2_n:
+        ach = fg * 3 * 5 * 8 / (st2_ms / st2_n * 1e-3) / 1e9
+        line["roofline"] = {"bound": "hbm", "kernel": "CNS stage (second RK stage)", "achieved": ach, "peak": peak,
+                            "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind,
+                            "algorithmic_bytes_per_launch": fg * 3 * 5 * 8, "avg_launch_ms": st2_ms / st2_n,
+                            "step_frac": fg * 200 / (out["fp64"]["ms"] / args.steps * 1e-3) / 1e9 / peak}
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -732,6 +873,40 @@ def cht_adjoint_measure(args, d, make, Tr0):
                     "h3c_cht_solve of the same steps"}
 
 
+def mixed_record(args, t, q0, ws, local, fp64_value):
+    """The default workload with FP32 face fluxes and FP64 state, update, dt
+    and sums: device-timed cell-updates/s over the same K steps as the FP64
+    line, and its ratio to the FP64 value."""
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200 import workloads as W
+
+    fg = t["first_ghost"]
+    m = hb.Solver(3, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, F.MIXED, cfl=args.cfl, time_end=1e30)
+    m.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg, W.riemann3d_conditions(),
+               t["subface_cells"])
+    m.set_state(q0, 0)
+    m.reset_time()
+    stream = torch.cuda.ExternalStream(m.stream())
+    m.solve(args.warmup)
+    torch.cuda.synchronize()
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        m.solve(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = allreduce_max(ev0.elapsed_time(ev1), ws)
+    v = fg * args.steps * ws / (ms * 1e-3)
+    return {"value": v, "unit": "cell-updates/s", "ms_per_step": ms / args.steps, "mixed_over_fp64": v / fp64_value,
+            "dtype": "f32-flux/f64-state", "stage_kernel": m.kernel_info()["kernel"], "clocks": clk.summary(),
+            "what": "same tree, state, steps and timing as the FP64 line; FP32 face states and fluxes, FP64 "
+                    "state, residual, update and dt"}
+
+
 def measure_adjoint(s, q0, nsteps, stream, fg):
     """Time h3c_adjoint of J = <lambda, q_N> over nsteps RK2 steps against the
     same nsteps of h3c_solve (CUDA events on the solver's stream, both from the
@@ -801,6 +976,9 @@ def main():
     ap.add_argument("--extra-levels", type=int, default=2)
     ap.add_argument("--cfl", type=float, default=0.4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the oracle comparison of the default workload")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision record of the default workload")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble record")
     ap.add_argument("--workload", default="riemann3d",
                     choices=["riemann3d", "ensemble", "tgv", "vortex", "cht", "advection"])
     ap.add_argument("--adv-level", type=int, default=11)
@@ -879,6 +1057,10 @@ def main():
     e2e_s = time.perf_counter() - t0
     e2e_s = allreduce_max(e2e_s, ws)
     e2e = fg * args.steps * ws / e2e_s
+    # ---- the mixed-precision path (FP32 face fluxes, FP64 state) on the same tree ----
+    mixed = None
+    if not args.no_mixed and args.precision == "fp64":
+        mixed = mixed_record(args, t, q0, ws, local, value)
     # ---- discrete adjoint: time of h3c_adjoint (its forward included) over the forward alone ----
     adj = None
     if args.adjoint_steps > 0:
@@ -928,9 +1110,24 @@ def main():
     line["grid_build"] = getattr(args, "grid_build", None)
     line["stage_kernel"] = s.kernel_info()
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
-        ups, cells, nst, threads, el = cpu_oracle_run(args)
-        line["cpu_baseline"] = {"value": ups, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-                                "sample": f"{nst} RK2 steps of the same {cells}-cell workload, {el:.1f} s"}
+        r = cpu_oracle_run(args)
+        r1 = cpu_oracle_run(args, steps_budget_s=8.0, threads=1)
+        line["cpu_baseline"] = {
+            "value": r["value"], "unit": "cell-updates/s", "cores": r["threads"], "kind": "port",
+            "sample": f"{r['steps']} RK2 steps of the same {r['cells']}-cell workload, {r['seconds']:.1f} s, after "
+                      "one warm-up and one sizing step; OpenMP over all host threads",
+            "single_thread": {"value": r1["value"], "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                              "sample": f"{r1['steps']} RK2 steps, {r1['seconds']:.1f} s (hom3's own execution model "
+                                        "is serial)"}}
+    if ws == 1 and rank == 0 and not args.no_parity:
+        line["parity"] = parity_record(args)
+    if mixed is not None:
+        if "parity" in line:
+            mixed["l2_rel_vs_fp64_oracle"] = line["parity"]["mixed_l2_rel_after_5"]
+            mixed["l2_what"] = "after 5 steps from the oracle's state, the parity record's comparison"
+        line["mixed"] = mixed
+    if not args.no_batched:
+        line["batched"] = ensemble_measure(args, ws, local, steps=min(args.steps, 200), warmup=args.warmup)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

@@ -1033,7 +1033,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
           for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fp[v] = W * fp[v];
+        for (int v = 0; v < NV; ++v) fp[v] = __dmul_rn(W, fp[v]);  // rounded: no FMA with the sums below
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) sf[(d * NV + v) * kBlock + tid] = fp[v];
@@ -1077,7 +1077,7 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
           for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fm[v] = W * fm[v];
+        for (int v = 0; v < NV; ++v) fm[v] = __dmul_rn(W, fm[v]);
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);
@@ -1248,7 +1248,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
             for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
           }
 #pragma unroll
-          for (int v = 0; v < NV; ++v) fp[v] = W * fp[v];
+          for (int v = 0; v < NV; ++v) fp[v] = __dmul_rn(W, fp[v]);  // rounded: no FMA with the sums below
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) sf[(d * NV + v) * kBlock + tid] = fp[v];
@@ -1293,7 +1293,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
             for (int v = 0; v < NV; ++v) fm[v] = j == 0 ? (double)f[v] : fm[v] + (double)f[v];
           }
 #pragma unroll
-          for (int v = 0; v < NV; ++v) fm[v] = W * fm[v];
+          for (int v = 0; v < NV; ++v) fm[v] = __dmul_rn(W, fm[v]);
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);

@@ -102,6 +102,14 @@ struct h3c_solver_s {
   size_t halo_smem = 0;
   double halo_mean = 0;
   int halo_maxh = 0;
+  // CNS tile kernel (h3c_stage_cns.cu): its tables reuse d_lnb / d_hids / d_hoff
+  bool cns_ok = false;
+  int* d_h1end = nullptr;
+  unsigned short* d_hnb = nullptr;
+  double* d_gsl = nullptr;  // ghost slopes [nd * nv][ngl]
+  long long ngl = 0;
+  int h1max = 0, cns_bps = 0;
+  size_t cns_smem = 0;
   // CUDA graph of `graph_steps` solver steps, replayed by h3c_solve
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
@@ -187,7 +195,9 @@ void free_grid(h3c_solver s) {
   s->vel_set = false;
   dfree(s->d_blk_inst); dfree(s->d_inst_end); dfree(s->d_ginst);
   dfree(s->d_lnb); dfree(s->d_hids); dfree(s->d_hoff); dfree(s->d_goff); dfree(s->d_grp);
+  dfree(s->d_h1end); dfree(s->d_hnb); dfree(s->d_gsl);
   s->halo_ok = false;
+  s->cns_ok = false;
   dfree(s->d_adj);
   s->adj_cap = 0;
   s->stage_cap = 0;
@@ -360,6 +370,16 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
   if (PHYS == EULER && FLUX == AUSM && s->desc.reconstruction == H3C_RECON_MUSCL) {
     k_stage_muscl<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
         qin, out, s->d_slopes, s->d_xc, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+    return;
+  }
+  if (PHYS == CNS && s->tile && s->halo && s->cns_ok) {
+    int grid = s->persist_blocks > 0 ? s->persist_blocks : s->cns_bps * num_sms();
+    grid = (int)std::max<long long>(1, std::min<long long>(grid, s->ntiles));
+    const CnsHaloGeom ch{HaloGeom{s->d_lnb, s->d_hids, s->d_hoff, s->d_grp, s->d_goff, s->hmax}, s->d_h1end, s->d_hnb,
+                         s->d_gsl, s->ngl, s->h1max};
+    if (s->ng > 0) s->launches++;  // the ghost-slope pass
+    cns_halo_stage(ND, std::is_same<R, float>::value, MODE, FUSE, qin, out, geometry(s), ghosts(s), ch, s->pc,
+                   s->d_sc, &s->d_sc->dtmin_ord, &s->d_sc->status, grid, s->cns_smem, s->stream, s->d_gsl);
     return;
   }
   if (PHYS == EULER && FLUX == AUSM && s->tile && s->halo && s->halo_ok) {
@@ -815,7 +835,13 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   }
   // ---- tables of the halo-staged Euler/AUSM stage kernel ----
   HaloHost HH;
-  bool halo_tables = false;
+  CnsHaloHost CH;
+  bool halo_tables = false, cns_tables = false;
+  if (s->desc.physics == H3C_CNS && ninst == 1 && nsub == 0 && lens.size() == 1) {
+    std::vector<long long> tend(s->ntiles);
+    for (long long t = 0; t < s->ntiles; ++t) tend[t] = std::min((t + 1) * kBlock, n_int);
+    cns_tables = halo_build_cns(nd, L, n_int, s->ntiles, tend, h_nbr.data(), CH);
+  }
   if (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM && s->desc.reconstruction != H3C_RECON_MUSCL) {
     std::vector<long long> tend(s->ntiles);
     for (long long t = 0; t < s->ntiles; ++t) tend[t] = std::min((t + 1) * kBlock, int_end[h_blk[t]]);
@@ -915,6 +941,34 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
       s->halo_mean = HH.mean_halo;
       s->halo_maxh = HH.max_halo;
       s->halo_ok = true;
+    }
+  }
+  if (cns_tables) {
+    const bool mixed = s->desc.precision == H3C_MIXED;
+    const size_t smem = cns_halo_smem_bytes(nd, mixed, CH.base.hmax, CH.h1max);
+    const int bps = smem <= 227 * 1024 ? cns_halo_prepare(nd, mixed, smem) : 0;
+    if (bps > 0) {
+      const HaloHost& B = CH.base;
+      s->ngl = std::max<long long>(1, (ng + 31) / 32 * 32);
+      H3C_CUDA(s, cudaMalloc(&s->d_lnb, sizeof(unsigned short) * B.lnb.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_hids, sizeof(int) * B.ids.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_hoff, sizeof(int) * B.off.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_h1end, sizeof(int) * CH.h1end.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_hnb, sizeof(unsigned short) * CH.hnb.size()));
+      H3C_CUDA(s, cudaMalloc(&s->d_gsl, sizeof(double) * nd * s->nv * s->ngl));
+      H3C_CUDA(s, cudaMemcpy(s->d_lnb, B.lnb.data(), sizeof(unsigned short) * B.lnb.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_hids, B.ids.data(), sizeof(int) * B.ids.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_hoff, B.off.data(), sizeof(int) * B.off.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_h1end, CH.h1end.data(), sizeof(int) * CH.h1end.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemcpy(s->d_hnb, CH.hnb.data(), sizeof(unsigned short) * CH.hnb.size(), cudaMemcpyHostToDevice));
+      H3C_CUDA(s, cudaMemset(s->d_gsl, 0, sizeof(double) * nd * s->nv * s->ngl));
+      s->hmax = B.hmax;
+      s->h1max = CH.h1max;
+      s->cns_smem = smem;
+      s->cns_bps = bps;
+      s->halo_mean = B.mean_halo;
+      s->halo_maxh = B.max_halo;
+      s->cns_ok = true;
     }
   }
   H3C_CUDA(s, cudaMemcpy(s->d_bcs, s->h_bcs.data(), sizeof(BcParam) * s->h_bcs.size(), cudaMemcpyHostToDevice));
@@ -1203,8 +1257,12 @@ int h3c_apply_bcs(h3c_solver s, int which) {
 
 // Solver::solve (solver.hpp:140-145): apply_bcs(lhs), set_dt, evolve, advance.
 // Per-stage preparation of a stage input q: CNS cell slopes or MUSCL gradients.
+static bool cns_tile_active(h3c_solver s) { return s->desc.physics == H3C_CNS && s->tile && s->halo && s->cns_ok; }
+
 static void prepare_stage(h3c_solver s, const double* q, int which) {
-  if (s->desc.physics == H3C_CNS) launch_slopes(s, which);
+  if (s->desc.physics == H3C_CNS) {
+    if (!cns_tile_active(s)) launch_slopes(s, which);  // the tile kernel computes slopes itself
+  }
   else if (s->desc.reconstruction == H3C_RECON_MUSCL) launch_grad(s, q);
 }
 
@@ -1643,14 +1701,16 @@ int h3c_kernel_info(h3c_solver s, int64_t* info, int n) {
   if (!s || !info || n < 0) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_kernel_info: no grid");
   const bool euler = s->desc.physics == H3C_EULER && s->desc.reconstruction != H3C_RECON_MUSCL;
-  const bool halo = euler && s->desc.flux == H3C_FLUX_AUSM && s->tile && s->halo && s->halo_ok;
+  const bool cns = cns_tile_active(s);
+  const bool halo = cns || (euler && s->desc.flux == H3C_FLUX_AUSM && s->tile && s->halo && s->halo_ok);
+  const long long bps = cns ? s->cns_bps : s->halo_bps;
   const int64_t grid = halo ? std::max<long long>(1, std::min<long long>(s->persist_blocks > 0 ? s->persist_blocks
-                                                                         : (long long)s->halo_bps * num_sms(),
+                                                                         : bps * num_sms(),
                                                                          s->ntiles))
                             : (s->persist_blocks > 0 ? std::min<long long>(s->persist_blocks, s->ntiles) : s->ntiles);
-  const int64_t v[8] = {halo ? 2 : (euler && s->tile ? 1 : 0), s->halo_ok ? s->hmax : 0, s->halo_maxh,
-                        (int64_t)std::llround(1000.0 * s->halo_mean), s->halo_bps, grid, (int64_t)s->halo_smem,
-                        s->ntiles};
+  const int64_t v[8] = {halo ? 2 : (euler && s->tile ? 1 : 0), (s->halo_ok || s->cns_ok) ? s->hmax : 0,
+                        s->halo_maxh, (int64_t)std::llround(1000.0 * s->halo_mean), bps, grid,
+                        (int64_t)(cns ? s->cns_smem : s->halo_smem), s->ntiles};
   for (int i = 0; i < n && i < 8; ++i) info[i] = v[i];
   return H3C_OK;
 }

@@ -69,4 +69,39 @@ void halo_stage(int nd, bool mixed, int mode, bool hang, bool fuse, const double
                 const Geometry& g, const HaloGeom& h, const PhysConst& pc, const Scalars* sc, long long* dtmin,
                 int* status, int grid, size_t smem, cudaStream_t st);
 
+// ---------------------------------------------------------------------------
+// CNS (AUSM + three-point viscous flux) on the same tiles (h3c_stage_cns.cu).
+// The viscous flux reads the transverse slopes of both face cells, so the
+// tables add, per tile, a second halo layer: the cells the slopes of the
+// first layer read (the tile's edge-diagonal neighbours, and ghosts next to
+// first-layer boundary cells).  Ghost cells' slopes (a boundary or periodic
+// partner cell's slope, with the walls' sign rule) come from a ghost-only
+// slope pass.  Single-level grids only (hom3's CNS has no coarse/fine faces).
+// ---------------------------------------------------------------------------
+struct CnsHaloGeom {
+  HaloGeom h;                                // lnb, halo ids (layer 1 then layer 2 per tile), offsets, slots
+  const int* __restrict__ h1end;             // [ntiles] end of tile t's layer 1 in halo_ids
+  const unsigned short* __restrict__ hnb;    // [halo_ids entries][2nd] slots of a layer-1 cell's face
+                                             // neighbours (0xffff: that slope is not needed)
+  const double* __restrict__ gsl;            // [nd * nv][ngl] slopes of the ghost cells
+  long long ngl;                             // leading dimension of gsl
+  int h1max;                                 // layer-1 slots reserved per tile (multiple of 32)
+};
+
+struct CnsHaloHost {
+  HaloHost base;                             // lnb, ids, off; grp unused
+  std::vector<int> h1end;
+  std::vector<unsigned short> hnb;
+  int h1max = 0;
+};
+
+bool halo_build_cns(int nd, long long ld, long long n_int, long long ntiles, const std::vector<long long>& tile_end,
+                    const int* nbr, CnsHaloHost& H);
+size_t cns_halo_smem_bytes(int nd, bool mixed, int hmax, int h1max);
+int cns_halo_prepare(int nd, bool mixed, size_t smem);
+// the ghost-slope pass and the stage; h = the grid's (single) cell length
+void cns_halo_stage(int nd, bool mixed, int mode, bool fuse, const double* qin, double* out, const Geometry& g,
+                    const GhostTables& gt, const CnsHaloGeom& h, const PhysConst& pc, const Scalars* sc,
+                    long long* dtmin, int* status, int grid, size_t smem, cudaStream_t st, double* gsl);
+
 }  // namespace h3c

@@ -298,12 +298,18 @@ int h3c_profile_read(h3c_solver s, double* ms, int64_t* count, int nkinds);
  * and would serialise the caller's streams.  Computes the same minimum cell
  * time step as h3c_min_dt (hom3's compute_dt) from caller-owned device
  * buffers: q = interior-cell state [nv][ld], length = their cell lengths,
- * dt_out = one device double; asynchronous on `stream`.  Allocates nothing:
- * its scratch is a fixed 128 KiB array inside the library (held on every GPU
- * that loads it until exit), so n_cells <= 4,194,304; larger sizes return
- * H3C_E_INVALID.  The first call on a device looks up the array's address
- * (make that first call before any stream capture).  Calls share the array:
- * calls that overlap on the GPU race and must be serialised by the caller. */
+ * dt_out = one device double; asynchronous on `stream`.  Euler, CNS and heat
+ * (advection, whose time step needs the velocity field, returns
+ * H3C_E_INVALID).  Allocates nothing: its scratch is a fixed 128 KiB array
+ * inside the library (held on every GPU that loads it until exit), so
+ * n_cells <= 4,194,304; larger sizes return H3C_E_INVALID.  Errors set the
+ * text of h3c_last_error(NULL, ...).  The first call on a device looks up
+ * the array's address (make that first call before any stream capture); with
+ * CUDA's default lazy module loading it also loads the library's device code,
+ * which reserves device memory, so a caller whose pool takes all device
+ * memory makes the first call at its own initialisation, before the pool
+ * does (or sets CUDA_MODULE_LOADING=EAGER).  Calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller. */
 int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t ld, int64_t n_cells,
                        const double* length, double* dt_out, void* stream);
 
