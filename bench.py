@@ -857,7 +857,7 @@ def cht_adjoint_measure(args, d, make, Tr0):
         return objective(c2, h2)
 
     worst = 0.0
-    ndir = 4
+    ndir = 32  # random solid directions (seed 2)
     for _ in range(ndir):
         dT = np.zeros_like(d["q_solid"])
         dT[0, :fgs] = rng.standard_normal(fgs)

@@ -277,46 +277,55 @@ template <class R> __device__ __forceinline__ R sutherland(R T, R sOverTref, R s
 
 // Three-point viscous flux: cns/physics.hpp:305-338 with the surface helpers
 // :221-293 and surface_slope (solver.hpp:656-678).  sl/sr: cell slopes
-// [sd][v] of the left / right cell.
+// [sd][v] of the left / right cell.  hom3 divides by rho_s, rho_s^2, len_r,
+// (T + S) and gm1 Pr0 rho_s face by face; here each divisor's reciprocal is
+// taken once (nr_rcp: hardware estimate + Newton steps, within 2 ulp) and
+// multiplied in, and T^1.5 is T * T * rsqrt(T) -- an arithmetic difference
+// of a few ulp per flux, far inside the parity tolerance.
 template <class R, int ND>
 __device__ __forceinline__ void viscous(const Prim<R, ND>& L, const Prim<R, ND>& Rt, const R* sl,
                                         const R* sr, int d, R len_r, const PhysConst& pc, R* f) {
   constexpr int NV = ND + 2;
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
   const R rho_s = R(0.5) * (L.q[ND] + Rt.q[ND]);
+  const R rinv = nr_rcp(rho_s);
   R rho_u_s[ND], u_s[ND];
   R umag2 = R(0);
 #pragma unroll
   for (int k = 0; k < ND; ++k) {
     rho_u_s[k] = R(0.5) * (L.q[k] + Rt.q[k]);
-    u_s[k] = rho_u_s[k] / rho_s;
+    u_s[k] = rho_u_s[k] * rinv;
     umag2 = k == 0 ? u_s[k] * u_s[k] : umag2 + u_s[k] * u_s[k];
   }
   const R rho_E_s = R(0.5) * (L.q[ND + 1] + Rt.q[ND + 1]);
   const R p_s = gm1 * (rho_E_s - R(0.5) * rho_s * umag2);
+  const R ilen = nr_rcp(len_r);
   auto gs = [&](int v, int sd) -> R {
-    return sd == d ? (Rt.q[v] - L.q[v]) / len_r : R(0.5) * (sr[sd * NV + v] + sl[sd * NV + v]);
+    return sd == d ? (Rt.q[v] - L.q[v]) * ilen : R(0.5) * (sr[sd * NV + v] + sl[sd * NV + v]);
   };
-  const R rs2 = rho_s * rho_s;
+  const R rinv2 = rinv * rinv;
   R gu[ND][ND];  // gu[c][sd] = d u_c / d x_sd at the surface
 #pragma unroll
   for (int c = 0; c < ND; ++c)
 #pragma unroll
-    for (int sd = 0; sd < ND; ++sd) gu[c][sd] = (gs(c, sd) * rho_s - gs(ND, sd) * rho_u_s[c]) / rs2;
+    for (int sd = 0; sd < ND; ++sd) gu[c][sd] = (gs(c, sd) * rho_s - gs(ND, sd) * rho_u_s[c]) * rinv2;
   const R p_avg = R(0.5) * (L.p + Rt.p);
-  const R mu_s = sutherland<R>(gamma * p_avg / rho_s, (R)pc.sOverTref, (R)pc.sOverTrefP1);
+  // Sutherland's law (cns/quantities.hpp:113-115): T^1.5 (1 + S) / (T + S)
+  const R T = gamma * p_avg * rinv;
+  const R mu_s = (T * (T * nr_rsqrt(T))) * (R)pc.sOverTrefP1 * nr_rcp(T + (R)pc.sOverTref);
   R grad_rho_umag2 = gs(ND, d) * umag2;
 #pragma unroll
   for (int k = 0; k < ND; ++k) grad_rho_umag2 = grad_rho_umag2 + rho_s * R(2) * u_s[k] * gu[k][d];
   const R gradP = gm1 * (gs(ND + 1, d) - R(0.5) * grad_rho_umag2);
   const R gradRho = gs(ND, d);
-  const R qf = -mu_s * gamma / (gm1 * (R)pc.Pr0 * rho_s) * (gradP - p_s / rho_s * gradRho);
+  const R cq = gamma / (gm1 * (R)pc.Pr0);  // a kernel constant: hoisted out of the face loops
+  const R qf = -mu_s * cq * rinv * (gradP - p_s * rinv * gradRho);
   // nabla_u(i, j) = gu[j][i]; trace = sum gu[i][i]
   R tr = gu[0][0];
 #pragma unroll
   for (int i = 1; i < ND; ++i) tr = tr + gu[i][i];
-  const R div_u = tr * R(2) / R(3);
-  const R invRe = R(1) / (R)pc.Re0;
+  const R div_u = tr * R(2.0 / 3.0);
+  const R invRe = R(1) / (R)pc.Re0;  // a kernel constant
   R Eacc = R(0);
 #pragma unroll
   for (int k = 0; k < ND; ++k) {
@@ -335,16 +344,17 @@ __device__ __forceinline__ void viscous(const Prim<R, ND>& L, const Prim<R, ND>&
 // per-cell time step: euler/physics.hpp:182-196, cns/physics.hpp:167-187,
 // heat/physics.hpp:82-85, advection/physics.hpp:78-87 (u: the cell's velocity)
 // bad (optional): the cell fails hom3's check_variables -- density, energy
-// and pressure positive (euler/physics.hpp:229-239, shared by CNS), T
-// positive (heat/physics.hpp:89-95); for advection only a non-finite value
-// counts, since hom3's own upwind test makes q negative (its flux is
-// reproduced as written).  NaN fails every comparison, so it is bad too.
+// and pressure positive (euler/physics.hpp:229-239, shared by CNS).  For heat
+// and advection only a non-finite value counts: hom3's own heat test starts
+// from T = 0 (heat/physics.hpp:89-95 asks T > 0, in debug builds only) and
+// its upwind advection test makes q negative (the flux is reproduced as
+// written).  NaN fails every comparison, so it is bad too.
 // ---------------------------------------------------------------------------
 template <int ND, int PHYS>
 __device__ __forceinline__ double cell_dt(const double* q, double h, const PhysConst& pc,
                                           const double* u = nullptr, bool* bad = nullptr) {
   if (PHYS == HEAT) {
-    if (bad) *bad = !(q[0] > 0.0);
+    if (bad) *bad = !isfinite(q[0]);
     return pc.cfl * 0.5 * (h * h);
   }
   if (PHYS == ADVECTION) {

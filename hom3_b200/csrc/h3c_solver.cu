@@ -92,6 +92,8 @@ struct h3c_solver_s {
   bool needs_partner = false, needs_periodic = false;  // coupling / periodic conditions present
   bool partner_set = false, periodic_set = false;
   bool tile = true;  // Euler stages use the shared-memory tile kernel
+  bool cns_adj_dual = false;  // CNS adjoint faces by dual numbers instead of the hand-written reverse
+  int halo_cap = 0;           // cap on the Euler halo entries held in shared memory (0: none)
   // halo-staged Euler/AUSM stage (h3c_stage_halo.cu): tables, launch size
   bool halo = true;     // option: use it when its tables exist
   bool halo_ok = false; // tables built for the current grid
@@ -922,6 +924,9 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   H3C_CUDA(s, cudaMemset(s->d_gpartner, 0xff, sizeof(int) * ngm));
   if (halo_tables) {
     const bool mixed = s->desc.precision == H3C_MIXED;
+    // halo entries kept in shared memory: as many as let 3 blocks share an SM
+    HH.hmax = halo_slots_for(nd, mixed, HH.max_halo, 3);
+    if (s->halo_cap > 0) HH.hmax = std::min(HH.hmax, s->halo_cap);
     const size_t smem = halo_smem_bytes(nd, mixed, HH.hmax);
     const int bps = halo_prepare(nd, mixed, smem);
     if (bps > 0) {
@@ -1446,15 +1451,21 @@ static int read_scalars(h3c_solver s, Scalars* out) {
 static int status_error(h3c_solver s, const Scalars& sc, int inst = 0) {
   if (sc.status & kStatusTimeout)
     return s->fail(H3C_E_TIMEOUT, "instance %d: a bounded device wait for a tile's copies ran out", inst);
-  if (sc.status & kStatusState)
-    return s->fail(H3C_E_NONFINITE,
-                   "instance %d: a cell's density, energy or pressure (temperature for heat) is not positive or not "
-                   "finite (hom3's check_variables); dt = %g at step %lld",
-                   inst, sc.dt, (long long)sc.step);
-  if (sc.status & kStatusDt)
-    return s->fail(H3C_E_NONFINITE, "instance %d: solution diverged: dt = %g is outside [1e-300, 1e300] at step %lld",
-                   inst, sc.dt, (long long)sc.step);
-  return H3C_OK;
+  if (!(sc.status & (kStatusState | kStatusDt))) return H3C_OK;
+  std::string m = "instance " + std::to_string(inst) + ":";
+  char buf[160];
+  if (sc.status & kStatusDt) {
+    std::snprintf(buf, sizeof(buf), " solution diverged: dt = %g is outside [1e-300, 1e300] at step %lld;", sc.dt,
+                  (long long)sc.step);
+    m += buf;
+  }
+  if (sc.status & kStatusState) {
+    std::snprintf(buf, sizeof(buf), " a cell is not finite or (Euler/CNS) has a non-positive density, energy or "
+                                    "pressure (hom3's check_variables) at step %lld;", (long long)sc.step);
+    m += buf;
+  }
+  m.pop_back();
+  return s->fail(H3C_E_NONFINITE, "%s", m.c_str());
 }
 
 int h3c_min_dt(h3c_solver s, double* dt) {
@@ -1687,6 +1698,23 @@ int h3c_set_option(h3c_solver s, int option, int value) {
     case H3C_OPT_TILE_KERNEL: s->tile = value != 0; break;
     case H3C_OPT_GRAPHS: s->graphs = value != 0; break;
     case H3C_OPT_HALO_KERNEL: s->halo = value != 0; break;
+    case H3C_OPT_CNS_ADJOINT_DUAL: s->cns_adj_dual = value != 0; break;
+    case H3C_OPT_HALO_SLOTS: {
+      if (value < 0 || value % 32) return s->fail(H3C_E_INVALID, "h3c_set_option: halo slots must be a multiple of 32");
+      s->halo_cap = value;
+      if (s->halo_ok) {  // the Euler kernel's shared-memory size follows the cap
+        const bool mixed = s->desc.precision == H3C_MIXED;
+        int hm = halo_slots_for(s->nd, mixed, s->halo_maxh, 3);
+        if (value > 0) hm = std::min(hm, value);
+        const size_t smem = halo_smem_bytes(s->nd, mixed, hm);
+        const int bps = halo_prepare(s->nd, mixed, smem);
+        if (bps <= 0) return s->fail(H3C_E_INVALID, "h3c_set_option: %d halo slots do not fit", hm);
+        s->hmax = hm;
+        s->halo_smem = smem;
+        s->halo_bps = bps;
+      }
+      break;
+    }
     case H3C_OPT_PERSISTENT_BLOCKS:
       if (value < 0) return s->fail(H3C_E_INVALID, "h3c_set_option: persistent blocks must be >= 0");
       s->persist_blocks = value;
@@ -1974,13 +2002,13 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
       Launch La(s, K_OTHER);
       const unsigned nb = (unsigned)blocks(s->n_int);
       if (s->nd == 2) {
-        k_adjc_face<2><<<nb, kBlock, 0, s->stream>>>(qin, s->d_slopes, lamin, alpha, g, gt, s->pc, s->d_sc, nullptr,
-                                                     m_qface, m_gbar, nullptr);
+        (s->cns_adj_dual ? k_adjc_face<2, false> : k_adjc_face<2, true>)<<<nb, kBlock, 0, s->stream>>>(
+            qin, s->d_slopes, lamin, alpha, g, gt, s->pc, s->d_sc, nullptr, m_qface, m_gbar, nullptr);
         k_adjc_slopes<2><<<nb, kBlock, 0, s->stream>>>(qin, lamin, extra, extra2, beta, gam, gam2, g, gt, s->pc,
                                                        nullptr, m_qface, m_gbar, nullptr, gout);
       } else {
-        k_adjc_face<3><<<nb, kBlock, 0, s->stream>>>(qin, s->d_slopes, lamin, alpha, g, gt, s->pc, s->d_sc, nullptr,
-                                                     m_qface, m_gbar, nullptr);
+        (s->cns_adj_dual ? k_adjc_face<3, false> : k_adjc_face<3, true>)<<<nb, kBlock, 0, s->stream>>>(
+            qin, s->d_slopes, lamin, alpha, g, gt, s->pc, s->d_sc, nullptr, m_qface, m_gbar, nullptr);
         k_adjc_slopes<3><<<nb, kBlock, 0, s->stream>>>(qin, lamin, extra, extra2, beta, gam, gam2, g, gt, s->pc,
                                                        nullptr, m_qface, m_gbar, nullptr, gout);
       }
@@ -2156,7 +2184,7 @@ int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps,
   // workspace: checkpoints, stage inputs of one segment (+ the fluid state after it), work and cotangent states,
   // CNS reverse buffers, per-ghost cross cotangents, dt records
   const size_t nd = (size_t)Qf * (nck + (every + 1) + 2 + 3 + 1 + cns->nd) + (size_t)Qs * (nck + every + 2 + 2) +
-                    (size_t)heat->ng + (size_t)cns->ng + 2 * (size_t)nsteps + 8;
+                    (size_t)heat->ng + (size_t)cns->ng + 2 * (size_t)nsteps + 2 * (size_t)every + 8;
   double* ws = nullptr;
   if (cudaMalloc(&ws, sizeof(double) * nd) != cudaSuccess) {
     cudaGetLastError();
@@ -2178,23 +2206,67 @@ int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps,
   double* tbar = take(std::max<long long>(1, cns->ng));
   double* dtf = take(nsteps);
   double* dth = take(nsteps);
+  double* sdtf = take(every);  // one segment's time steps (the captured segment graphs read and write these)
+  double* sdth = take(every);
   cudaStream_t st = cns->stream;
+  // Full segments are captured once as CUDA graphs (forward and backward) and
+  // replayed: their buffers are fixed and their time steps go through
+  // sdtf / sdth.  An even segment length returns forward Euler's swapped
+  // state buffers to where the capture started.
+  const bool seg_graphs = cns->graphs && heat->graphs && !cns->prof && !heat->prof && every % 2 == 0;
+  auto capture = [&](auto&& body, cudaGraphExec_t* exec, long long* launches) -> bool {
+    const long long lc = cns->launches, lh = heat->launches;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    double* saved[4] = {cns->d_q[0], cns->d_q[1], heat->d_q[0], heat->d_q[1]};
+    body();
+    cns->d_q[0] = saved[0];  // the capture ran no step
+    cns->d_q[1] = saved[1];
+    heat->d_q[0] = saved[2];
+    heat->d_q[1] = saved[3];
+    *launches = (cns->launches - lc) + (heat->launches - lh);
+    cns->launches = lc;
+    heat->launches = lh;
+    bool ok = cudaStreamEndCapture(st, &g) == cudaSuccess && g && cudaGraphInstantiate(exec, g, 0) == cudaSuccess;
+    if (g) cudaGraphDestroy(g);
+    if (!ok) {
+      cudaGetLastError();
+      *exec = nullptr;
+    }
+    return ok;
+  };
+  cudaGraphExec_t gfwd = nullptr, gbwd = nullptr;
+  long long nl_fwd = 0, nl_bwd = 0;
   if (int rc = ensure_stage(cns, cns->n_caller)) { cudaFree(ws); return rc; }
   if (int rc = ensure_stage(heat, heat->n_caller)) { cudaFree(ws); return rc; }
   // ---- forward: the coupled loop (coupling::apply, cns step, heat step), checkpoints, dt records ----
-  for (int64_t i = 0; i < nsteps; ++i) {
-    if (i % every == 0) {
-      cudaMemcpyAsync(ckf + Qf * (i / every), cns->d_q[0], sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
-      cudaMemcpyAsync(cks + Qs * (i / every), heat->d_q[0], sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
+  auto fwd_seg = [&](long long n) {
+    for (long long j = 0; j < n; ++j) {
+      launch_cfl(cns, &cns->d_sc->mindt_ord);
+      launch_cfl(heat, &heat->d_sc->mindt_ord);
+      {
+        Launch L(cns, K_SCALAR);
+        k_couple_cht<<<1, 1, 0, st>>>(cns->d_sc, heat->d_sc, scaling);
+      }
+      enqueue_step(cns, true, nullptr, sdtf, j);
+      enqueue_step(heat, true, nullptr, sdth, j);
     }
-    launch_cfl(cns, &cns->d_sc->mindt_ord);
-    launch_cfl(heat, &heat->d_sc->mindt_ord);
-    {
-      Launch L(cns, K_SCALAR);
-      k_couple_cht<<<1, 1, 0, st>>>(cns->d_sc, heat->d_sc, scaling);
+  };
+  for (long long k = 0; k < nck; ++k) {
+    const long long i0 = k * every, i1 = std::min<long long>(nsteps, i0 + every);
+    cudaMemcpyAsync(ckf + Qf * k, cns->d_q[0], sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(cks + Qs * k, heat->d_q[0], sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
+    if (seg_graphs && i1 - i0 == every && (gfwd || capture([&] { fwd_seg(every); }, &gfwd, &nl_fwd))) {
+      cudaGraphLaunch(gfwd, st);
+      cns->launches += nl_fwd;
+    } else {
+      fwd_seg(i1 - i0);
     }
-    enqueue_step(cns, true, nullptr, dtf, i);
-    enqueue_step(heat, true, nullptr, dth, i);
+    cudaMemcpyAsync(dtf + i0, sdtf, sizeof(double) * (i1 - i0), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(dth + i0, sdth, sizeof(double) * (i1 - i0), cudaMemcpyDeviceToDevice, st);
   }
   Scalars savf, savs;
   cudaMemcpyAsync(&savf, cns->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, st);
@@ -2208,39 +2280,39 @@ int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps,
   const Geometry gf = geometry(cns), gs = geometry(heat);
   const GhostTables gtf = ghosts(cns), gts = ghosts(heat);
   const unsigned nbf = (unsigned)blocks(cns->n_int), nbs = (unsigned)blocks(heat->n_int);
-  // ---- backward over segments, each recomputed from its checkpoints ----
-  for (long long k = nck - 1; k >= 0; --k) {
-    const long long i0 = k * every, i1 = std::min<long long>(nsteps, i0 + every);
+  // ---- backward over segments, each recomputed from its checkpoint ----
+  // The segment body works on fixed buffers: the checkpoint is copied into
+  // wf / wsd, the segment's time steps into sdtf / sdth, and the cotangents
+  // stay in lf / ls (an even number of swaps per full segment).
+  auto bwd_seg = [&](long long n) {
     double *curf = wf, *curs = wsd;
-    cudaMemcpyAsync(curf, ckf + Qf * k, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
-    cudaMemcpyAsync(curs, cks + Qs * k, sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
-    for (long long i = i0; i < i1; ++i) {
-      double* sf0 = segf + Qf * (i - i0);
-      double* ss0 = segs + Qs * (i - i0);
+    for (long long j = 0; j < n; ++j) {
+      double* sf0 = segf + Qf * j;
+      double* ss0 = segs + Qs * j;
       cudaMemcpyAsync(sf0, curf, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
       cudaMemcpyAsync(ss0, curs, sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
       double* nxf = (curf == wf) ? wf + Qf : wf;
       double* nxs = (curs == wsd) ? wsd + Qs : wsd;
       cns->partner_override = ss0;  // the fluid's wall conditions read the solid before its step
       double* stf[1] = {sf0};
-      frozen_step(cns, stf, nxf, dtf, i);
+      frozen_step(cns, stf, nxf, sdtf, j);
       heat->partner_override = nxf;  // the solid's conditions read the fluid after its step
       double* sts[1] = {ss0};
-      frozen_step(heat, sts, nxs, dth, i);
+      frozen_step(heat, sts, nxs, sdth, j);
       cns->partner_override = nullptr;
       heat->partner_override = nullptr;
       curf = nxf;
       curs = nxs;
     }
-    cudaMemcpyAsync(segf + Qf * (i1 - i0), curf, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
-    for (long long i = i1 - 1; i >= i0; --i) {
-      double* sf0 = segf + Qf * (i - i0);
-      double* sf1 = segf + Qf * (i - i0 + 1);  // fluid state after step i
-      double* ss0 = segs + Qs * (i - i0);
+    cudaMemcpyAsync(segf + Qf * n, curf, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+    for (long long j = n - 1; j >= 0; --j) {
+      double* sf0 = segf + Qf * j;
+      double* sf1 = segf + Qf * (j + 1);  // fluid state after step j
+      double* ss0 = segs + Qs * j;
       {
         Launch L(cns, K_SCALAR);
-        k_set_dt_from<<<1, 1, 0, st>>>(cns->d_sc, dtf, i);
-        k_set_dt_from<<<1, 1, 0, st>>>(heat->d_sc, dth, i);
+        k_set_dt_from<<<1, 1, 0, st>>>(cns->d_sc, sdtf, j);
+        k_set_dt_from<<<1, 1, 0, st>>>(heat->d_sc, sdth, j);
         ++cns->launches;
       }
       // heat step: lam_s^i = (I + dR_s/dT_s)^T lam_s^{i+1}; its interface reads of T_f -> fluid cotangent
@@ -2264,13 +2336,13 @@ int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps,
       {
         Launch L(cns, K_OTHER);
         if (cns->nd == 2) {
-          k_adjc_face<2><<<nbf, kBlock, 0, st>>>(sf0, cns->d_slopes, lfT, 1.0, gf, gtf, cns->pc, cns->d_sc, ss0, qface,
-                                                 sbar, tbar);
+          (cns->cns_adj_dual ? k_adjc_face<2, false> : k_adjc_face<2, true>)<<<nbf, kBlock, 0, st>>>(
+              sf0, cns->d_slopes, lfT, 1.0, gf, gtf, cns->pc, cns->d_sc, ss0, qface, sbar, tbar);
           k_adjc_slopes<2><<<nbf, kBlock, 0, st>>>(sf0, lfT, nullptr, nullptr, 1.0, 0.0, 0.0, gf, gtf, cns->pc, ss0,
                                                    qface, sbar, tbar, lfB);
         } else {
-          k_adjc_face<3><<<nbf, kBlock, 0, st>>>(sf0, cns->d_slopes, lfT, 1.0, gf, gtf, cns->pc, cns->d_sc, ss0, qface,
-                                                 sbar, tbar);
+          (cns->cns_adj_dual ? k_adjc_face<3, false> : k_adjc_face<3, true>)<<<nbf, kBlock, 0, st>>>(
+              sf0, cns->d_slopes, lfT, 1.0, gf, gtf, cns->pc, cns->d_sc, ss0, qface, sbar, tbar);
           k_adjc_slopes<3><<<nbf, kBlock, 0, st>>>(sf0, lfT, nullptr, nullptr, 1.0, 0.0, 0.0, gf, gtf, cns->pc, ss0,
                                                    qface, sbar, tbar, lfB);
         }
@@ -2280,6 +2352,26 @@ int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps,
       ++cns->launches;
       std::swap(lfA, lfB);
       std::swap(lsA, lsB);
+    }
+  };
+  for (long long k = nck - 1; k >= 0; --k) {
+    const long long i0 = k * every, i1 = std::min<long long>(nsteps, i0 + every);
+    cudaMemcpyAsync(wf, ckf + Qf * k, sizeof(double) * Qf, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(wsd, cks + Qs * k, sizeof(double) * Qs, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(sdtf, dtf + i0, sizeof(double) * (i1 - i0), cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(sdth, dth + i0, sizeof(double) * (i1 - i0), cudaMemcpyDeviceToDevice, st);
+    if (seg_graphs && i1 - i0 == every) {
+      double *a0 = lfA, *b0 = lfB, *c0 = lsA, *d0 = lsB;
+      if (!gbwd && !capture([&] { bwd_seg(every); }, &gbwd, &nl_bwd)) {
+        lfA = a0, lfB = b0, lsA = c0, lsB = d0;  // a failed capture ran nothing
+        bwd_seg(every);
+      } else {
+        lfA = a0, lfB = b0, lsA = c0, lsB = d0;  // an even number of swaps: the same buffers
+        cudaGraphLaunch(gbwd, st);
+        cns->launches += nl_bwd;
+      }
+    } else {
+      bwd_seg(i1 - i0);
     }
   }
   internal_to_caller(cns, lfA, dJ_dq0);
@@ -2293,6 +2385,8 @@ int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps,
   cudaMemcpyAsync(cns->d_sc, &savf, sizeof(Scalars), cudaMemcpyHostToDevice, st);
   cudaMemcpyAsync(heat->d_sc, &savs, sizeof(Scalars), cudaMemcpyHostToDevice, st);
   const cudaError_t e = cudaStreamSynchronize(st);
+  if (gfwd) cudaGraphExecDestroy(gfwd);
+  if (gbwd) cudaGraphExecDestroy(gbwd);
   cudaFree(ws);
   if (e != cudaSuccess) return cns->cuda(e, "h3c_cht_adjoint");
   return cns->cuda(cudaGetLastError(), "h3c_cht_adjoint");

@@ -459,7 +459,15 @@ namespace {
 template <int ND, class R, int MODE, bool FUSE>
 int cprep_one(size_t smem) {
   auto k = k_stage_cns_halo<ND, R, MODE, FUSE>;
-  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+  // the opt-in limit (less the kernel's static arrays), not this grid's size: several solvers
+  // share the kernel and its attribute
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa{};
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, k) != cudaSuccess || (size_t)optin < smem + fa.sharedSizeBytes ||
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes) !=
+          cudaSuccess) {
     cudaGetLastError();
     return 0;
   }

@@ -46,10 +46,15 @@ namespace h3c {
 
 template <class R, int ND>
 __host__ __device__ constexpr size_t halo_layout_bytes(int hmax) {
-  // mbarrier (16) | landing [nv][S] f64 | face states [2nd+3][S] R |
-  // published plus fluxes [2][nv][256] f64 | neighbour slots [2][2nd][256] u16 | levels [2][256] u8
-  return 16 + 8 * (size_t)(ND + 2) * (kHaloTile + hmax) + sizeof(R) * (size_t)(2 * ND + 3) * (kHaloTile + hmax) +
-         2 * 8 * (size_t)(ND + 2) * kHaloTile + 2 * 2 * (size_t)(2 * ND) * kHaloTile + 2 * (size_t)kHaloTile;
+  // mbarrier (16) | landing [nv][256 + hmax] f64, later the published plus fluxes [2][nv][256] f64 |
+  // tile face states [nv + 1 + nd][256] R | halo face states [nv + 2][hmax] R |
+  // neighbour slots [2nd][256] u16 | levels [256] u8
+  return 16 +
+         (8 * (size_t)(ND + 2) * (kHaloTile + hmax) > 16 * (size_t)(ND + 2) * kHaloTile
+              ? 8 * (size_t)(ND + 2) * (kHaloTile + hmax)
+              : 16 * (size_t)(ND + 2) * kHaloTile) +
+         sizeof(R) * (size_t)(2 * ND + 3) * kHaloTile + sizeof(R) * (size_t)(ND + 4) * hmax +
+         2 * (size_t)(2 * ND) * kHaloTile + (size_t)kHaloTile;
 }
 
 // Face state of a cell from its state q: theta = a (rho u, rho, rho E + p),
@@ -68,21 +73,30 @@ __device__ __forceinline__ void face_state_of(const double* q, R gamma, R gm1, R
   for (int d = 0; d < ND; ++d) M[d] = P.M[d];
 }
 
+// Halo entries are (cell, direction) pairs: the id word carries the cell in
+// its low 29 bits and the face direction it is read across above them.
+constexpr int kHaloDirShift = 29;
+constexpr int kHaloCellMask = (1 << kHaloDirShift) - 1;
+
 template <int ND, class R, int MODE, bool HANG, bool FUSE>
-__global__ void __launch_bounds__(kHaloTile, 2)
+__global__ void __launch_bounds__(kHaloTile, 3)
     k_stage_halo(const double* __restrict__ qin, double* out, Geometry g, HaloGeom hg, PhysConst pc,
                  const Scalars* __restrict__ sc, long long* dtmin, int* status) {
   constexpr int NV = ND + 2, NP = 2 * ND, NS = 1 << (ND - 1), TB = kHaloTile;
-  constexpr int KH = kHaloMaxSlots / kHaloTile;  // halo cells one thread copies, at most
+  constexpr int KH = kHaloMaxSlots / kHaloTile;  // halo entries one thread copies, at most
+  constexpr int NFT = 2 * ND + 3;                // tile face-state rows: th[nv], p, M[nd]
   constexpr double W = ND == 2 ? 0.5 : 0.25;
-  const int S = TB + hg.hmax;
+  const int HM = hg.hmax;  // halo entries held in shared memory; later ones are read from global memory
+  const int S = TB + HM;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem);
-  double* land = reinterpret_cast<double*>(smem + 16);                                  // [NV][S]
-  R* fs = reinterpret_cast<R*>(land + (size_t)NV * S);                                 // [2ND+3][S]
-  double* fx = reinterpret_cast<double*>(fs + (size_t)(2 * ND + 3) * S);                // [2][NV][TB]
-  unsigned short* ln = reinterpret_cast<unsigned short*>(fx + 2 * NV * TB);              // [2][NP][TB]
-  unsigned char* ll = reinterpret_cast<unsigned char*>(ln + 2 * NP * TB);                // [2][TB]
+  double* land = reinterpret_cast<double*>(smem + 16);  // [NV][S]; after the face states: fluxes [2][NV][TB]
+  const size_t uni = (size_t)NV * S > (size_t)2 * NV * TB ? (size_t)NV * S : (size_t)2 * NV * TB;
+  R* fst = reinterpret_cast<R*>(land + uni);            // [NFT][TB]
+  R* fsh = fst + (size_t)NFT * TB;                      // [NV + 2][HM]
+  unsigned short* ln = reinterpret_cast<unsigned short*>(fsh + (size_t)(NV + 2) * HM);  // [NP][TB]
+  unsigned char* ll = reinterpret_cast<unsigned char*>(ln + NP * TB);                  // [TB]
+  double* fx = land;
   __shared__ double slen[kMaxLevels];
   const int tid = threadIdx.x;
   const long long ld = g.ld;
@@ -97,19 +111,20 @@ __global__ void __launch_bounds__(kHaloTile, 2)
   }
   __syncthreads();
 
-  // the halo cells of tile t this thread copies; returns the tile's halo size
-  auto fetch_ids = [&](long long t, int* hid) -> int {
-    const int o0 = __ldg(hg.halo_off + t);
+  // the halo entries of tile t this thread copies; returns the tile's entry count and its offset
+  auto fetch_ids = [&](long long t, int* hid, int& o0) -> int {
+    o0 = __ldg(hg.halo_off + t);
     const int nh = __ldg(hg.halo_off + t + 1) - o0;
 #pragma unroll
     for (int k = 0; k < KH; ++k) {
       const int h = tid + k * TB;
-      hid[k] = h < nh ? __ldg(hg.halo_ids + o0 + h) : 0;
+      hid[k] = (h < nh && h < HM) ? __ldg(hg.halo_ids + o0 + h) : 0;
     }
     return nh;
   };
-  // the copies of tile t into the landing area and neighbour/level buffer buf
-  auto issue = [&](long long t, int buf, const int* hid, int nh) {
+  // the copies of tile t: its state, neighbour slots and levels by bulk copy,
+  // the state of its first HM halo entries by 8-byte asynchronous copies
+  auto issue = [&](long long t, const int* hid, int nh) {
     if (tid == 0) {
       const long long c0 = t * TB;
       const long long te = min(c0 + TB, instance_end(g, tile_instance(g, t)));
@@ -119,36 +134,30 @@ __global__ void __launch_bounds__(kHaloTile, 2)
 #pragma unroll
       for (int v = 0; v < NV; ++v) bulk_g2s(land + (size_t)v * S, qin + v * ld + c0, ncp * 8u, bar);
 #pragma unroll
-      for (int p = 0; p < NP; ++p) bulk_g2s(ln + (buf * NP + p) * TB, hg.lnb + p * ld + c0, ncp * 2u, bar);
-      bulk_g2s(ll + buf * TB, g.lvl + c0, ncp, bar);
+      for (int p = 0; p < NP; ++p) bulk_g2s(ln + p * TB, hg.lnb + p * ld + c0, ncp * 2u, bar);
+      bulk_g2s(ll, g.lvl + c0, ncp, bar);
     }
 #pragma unroll
     for (int k = 0; k < KH; ++k) {
       const int h = tid + k * TB;
-      if (h < nh) {
-        const long long n = hid[k];
+      if (h < nh && h < HM) {
+        const long long n = hid[k] & kHaloCellMask;
 #pragma unroll
         for (int v = 0; v < NV; ++v) cp_async8(land + (size_t)v * S + TB + h, qin + v * ld + n);
       }
     }
     cp_async_commit();
   };
-  auto load_fs = [&](int slot, int d, FaceState<R, ND>& F) {
-#pragma unroll
-    for (int v = 0; v < NV; ++v) F.th[v] = fs[v * S + slot];
-    F.p = fs[NV * S + slot];
-    F.M = fs[(NV + 1 + d) * S + slot];
-  };
 
   int hid[KH], hid_n[KH];
-  int nh = fetch_ids(tile, hid);
-  issue(tile, 0, hid, nh);
+  int o0 = 0, o0_n = 0;
+  int nh = fetch_ids(tile, hid, o0);
 
   for (int it = 0; tile < g.ntiles; tile += gridDim.x, ++it) {
-    const int buf = it & 1;
+    issue(tile, hid, nh);
     const long long next = tile + gridDim.x;
     int nh_n = 0;
-    if (next < g.ntiles) nh_n = fetch_ids(next, hid_n);
+    if (next < g.ntiles) nh_n = fetch_ids(next, hid_n, o0_n);  // consumed by the next iteration's copies
     const long long c0 = tile * TB, c = c0 + tid;
     const int inst = tile_instance(g, tile);
     const long long te = min(c0 + (long long)TB, instance_end(g, inst));
@@ -164,11 +173,11 @@ __global__ void __launch_bounds__(kHaloTile, 2)
     const bool ok = mbar_wait_bounded(bar, (unsigned)(it & 1));
     cp_async_wait_all();
     if (!__syncthreads_and(ok)) {
-      if (tid == 0) atomicOr(status, 4);
+      if (tid == 0) atomicOr(status, kStatusTimeout);
       return;
     }
 
-    // ---- face states of the own cell (kept in registers) and the halo cells ----
+    // ---- face states: the own cell's (also kept in registers), the halo entries' along their direction ----
     double qc[NV];
     R thc[NV], pcell = R(0), Mc[ND];
     if (live) {
@@ -176,30 +185,52 @@ __global__ void __launch_bounds__(kHaloTile, 2)
       for (int v = 0; v < NV; ++v) qc[v] = land[(size_t)v * S + tid];
       face_state_of<R, ND>(qc, gamma, gm1, thc, pcell, Mc);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) fs[v * S + tid] = thc[v];
-      fs[NV * S + tid] = pcell;
+      for (int v = 0; v < NV; ++v) fst[v * TB + tid] = thc[v];
+      fst[NV * TB + tid] = pcell;
 #pragma unroll
-      for (int d = 0; d < ND; ++d) fs[(NV + 1 + d) * S + tid] = Mc[d];
+      for (int d = 0; d < ND; ++d) fst[(NV + 1 + d) * TB + tid] = Mc[d];
     }
-    for (int h = TB + tid; h < TB + nh; h += TB) {
-      double qh[NV];
-      R th[NV], ph, Mh[ND];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) qh[v] = land[(size_t)v * S + h];
-      face_state_of<R, ND>(qh, gamma, gm1, th, ph, Mh);
+    for (int k = 0; k < KH; ++k) {
+      const int h = tid + k * TB;
+      if (h < nh && h < HM) {
+        double qh[NV];
+        R th[NV], ph, Mh[ND];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) fs[v * S + h] = th[v];
-      fs[NV * S + h] = ph;
+        for (int v = 0; v < NV; ++v) qh[v] = land[(size_t)v * S + TB + h];
+        face_state_of<R, ND>(qh, gamma, gm1, th, ph, Mh);
+        const int dir = hid[k] >> kHaloDirShift;
+        R Md = Mh[0];
 #pragma unroll
-      for (int d = 0; d < ND; ++d) fs[(NV + 1 + d) * S + h] = Mh[d];
+        for (int d = 1; d < ND; ++d) Md = dir == d ? Mh[d] : Md;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fsh[v * HM + h] = th[v];
+        fsh[NV * HM + h] = ph;
+        fsh[(NV + 1) * HM + h] = Md;
+      }
     }
-    __syncthreads();  // landing area consumed; face states complete
+    __syncthreads();  // face states complete; the landing area becomes the flux buffers
 
-    // ---- the next tile's copies fly while this tile's fluxes are computed ----
-    if (next < g.ntiles) issue(next, buf ^ 1, hid_n, nh_n);
+    // the face state of slot s along d: a tile cell, a shared halo entry, or an overflow entry read from global memory
+    auto load_fs = [&](int s, int d, FaceState<R, ND>& F) {
+      if (s < TB) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) F.th[v] = fst[v * TB + s];
+        F.p = fst[NV * TB + s];
+        F.M = fst[(NV + 1 + d) * TB + s];
+      } else if (s - TB < HM) {
+        const int h = s - TB;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) F.th[v] = fsh[v * HM + h];
+        F.p = fsh[NV * HM + h];
+        F.M = fsh[(NV + 1) * HM + h];
+      } else {
+        const int n = __ldg(hg.halo_ids + o0 + (s - TB)) & kHaloCellMask;
+        face_state_global<R, ND>(F, qin, ld, n, d, gamma, gm1);
+      }
+    };
 
     // ---- fluxes, direction by direction ----
-    const unsigned short* L = ln + buf * NP * TB;
     double acc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] = 0.0;
@@ -211,9 +242,9 @@ __global__ void __launch_bounds__(kHaloTile, 2)
       for (int v = 0; v < NV; ++v) Fc.th[v] = thc[v];
       Fc.p = pcell;
       Fc.M = Mc[d];
-      double fp[NV];
       if (live) {
-        const int p = L[(2 * d + 1) * TB + tid];
+        const int p = ln[(2 * d + 1) * TB + tid];
+        double fp[NV];
         if (!HANG || !(p & kGroupBit)) {
           FaceState<R, ND> Fn;
           load_fs(p, d, Fn);
@@ -233,16 +264,16 @@ __global__ void __launch_bounds__(kHaloTile, 2)
             for (int v = 0; v < NV; ++v) fp[v] = j == 0 ? (double)f[v] : fp[v] + (double)f[v];
           }
 #pragma unroll
-          for (int v = 0; v < NV; ++v) fp[v] = __dmul_rn(W, fp[v]);  // rounded: no FMA with the sums below
+          for (int v = 0; v < NV; ++v) fp[v] = __dmul_rn(W, fp[v]);
         }
 #pragma unroll
         for (int v = 0; v < NV; ++v) X[v * TB + tid] = fp[v];
       }
       __syncthreads();  // plus fluxes of direction d published
       if (live) {
-        const int m = L[(2 * d) * TB + tid];
+        const int m = ln[(2 * d) * TB + tid];
         double fm[NV];
-        if (m < TB && L[(2 * d + 1) * TB + m] == tid) {
+        if (m < TB && ln[(2 * d + 1) * TB + m] == tid) {
 #pragma unroll
           for (int v = 0; v < NV; ++v) fm[v] = X[v * TB + m];
         } else if (!HANG || !(m & kGroupBit)) {
@@ -275,9 +306,9 @@ __global__ void __launch_bounds__(kHaloTile, 2)
 
     // ---- update and the next step's CFL minimum ----
     long long ord = kOrdMax;
-  bool bad = false;
+    bool bad = false;
     if (live) {
-      const double dx = slen[ll[buf * TB + tid]];
+      const double dx = slen[ll[tid]];
       const double dt = sc[inst].dt;
       const double k = dt / dx;
       double o[NV];
@@ -291,10 +322,14 @@ __global__ void __launch_bounds__(kHaloTile, 2)
       }
     }
     if (FUSE) {
-    flag_bad_state(bad, sc, inst);
-    block_min_atomic(ord, per_instance(dtmin, inst));
-  }
+      flag_bad_state(bad, sc, inst);
+      block_min_atomic(ord, per_instance(dtmin, inst));
+    }
+    __syncthreads();  // the shared buffers are rewritten by the next tile's copies
     nh = nh_n;
+    o0 = o0_n;
+#pragma unroll
+    for (int k = 0; k < KH; ++k) hid[k] = hid_n[k];
   }
 }
 
@@ -304,12 +339,13 @@ __global__ void __launch_bounds__(kHaloTile, 2)
 bool halo_build(int nd, long long ld, long long ntiles, const std::vector<long long>& tile_end, const int* nbr,
                 const int* sub, long long nsub, HaloHost& H) {
   const int NP = 2 * nd, NS = 1 << (nd - 1), TB = kHaloTile;
+  if (ld >= (1LL << kHaloDirShift)) return false;  // cell ids share their word with the direction
   H.lnb.assign((size_t)NP * ld, 0);
   std::vector<std::vector<int>> halo(ntiles);
   std::vector<std::vector<unsigned short>> grp(ntiles);
   std::atomic<bool> ok{true};
   auto work = [&](long long t0, long long t1) {
-    std::vector<int> tmp;
+    std::vector<long long> tmp;  // (cell << 2) | direction
     for (long long t = t0; t < t1 && ok.load(std::memory_order_relaxed); ++t) {
       const long long c0 = t * TB, ce = tile_end[t];
       auto outside = [&](long long v) { return v < c0 || v >= ce; };
@@ -317,33 +353,35 @@ bool halo_build(int nd, long long ld, long long ntiles, const std::vector<long l
       for (long long c = c0; c < ce; ++c)
         for (int p = 0; p < NP; ++p) {
           const long long v = nbr[p * ld + c];
+          const int dir = p >> 1;
           if (v >= 0) {
-            if (outside(v)) tmp.push_back((int)v);
+            if (outside(v)) tmp.push_back((v << 2) | dir);
           } else if (v <= -2) {
             const long long k = -v - 2;
             for (int j = 0; j < NS; ++j) {
               const long long sv = sub[j * nsub + k];
-              if (outside(sv)) tmp.push_back((int)sv);
+              if (outside(sv)) tmp.push_back((sv << 2) | dir);
             }
           }
         }
       std::sort(tmp.begin(), tmp.end());
       tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
-      if ((int)tmp.size() > kHaloMaxSlots) {
+      if ((long long)tmp.size() + TB >= kGroupBit) {  // slots are 15-bit
         ok = false;
         break;
       }
-      auto slot = [&](long long v) -> unsigned short {
+      auto slot = [&](long long v, int dir) -> unsigned short {
         if (!outside(v)) return (unsigned short)(v - c0);
-        return (unsigned short)(TB + (std::lower_bound(tmp.begin(), tmp.end(), (int)v) - tmp.begin()));
+        return (unsigned short)(TB + (std::lower_bound(tmp.begin(), tmp.end(), (v << 2) | dir) - tmp.begin()));
       };
       std::vector<unsigned short>& G = grp[t];
       for (long long c = c0; c < ce; ++c)
         for (int p = 0; p < NP; ++p) {
           const long long v = nbr[p * ld + c];
+          const int dir = p >> 1;
           unsigned short e = 0;
           if (v >= 0) {
-            e = slot(v);
+            e = slot(v, dir);
           } else if (v <= -2) {
             const long long k = -v - 2;
             const size_t gi = G.size() / NS;
@@ -352,11 +390,13 @@ bool halo_build(int nd, long long ld, long long ntiles, const std::vector<long l
               break;
             }
             e = (unsigned short)(kGroupBit | gi);
-            for (int j = 0; j < NS; ++j) G.push_back(slot(sub[j * nsub + k]));
+            for (int j = 0; j < NS; ++j) G.push_back(slot(sub[j * nsub + k], dir));
           }
           H.lnb[(size_t)p * ld + c] = e;
         }
-      halo[t] = tmp;
+      std::vector<int>& hl = halo[t];
+      hl.resize(tmp.size());
+      for (size_t i = 0; i < tmp.size(); ++i) hl[i] = (int)((tmp[i] >> 2) | ((tmp[i] & 3) << kHaloDirShift));
     }
   };
   const int nthr = std::max(1, std::min<int>((int)std::thread::hardware_concurrency(), 16));
@@ -387,8 +427,16 @@ bool halo_build(int nd, long long ld, long long ntiles, const std::vector<long l
   }
   H.max_halo = mx;
   H.mean_halo = ntiles ? (double)nids / ntiles : 0.0;
-  H.hmax = std::max(32, (mx + 31) / 32 * 32);
+  H.hmax = std::max(32, (mx + 31) / 32 * 32);  // the caller may hold fewer in shared memory (halo_slots_for)
   return true;
+}
+
+int halo_slots_for(int nd, bool mixed, int max_halo, int blocks_per_sm) {
+  // shared memory of an SM (228 KB) less 1 KB reserved per block and the static arrays
+  const size_t budget = (size_t)233472 / blocks_per_sm - 1024 - 512;
+  int hm = std::min(kHaloMaxSlots, std::max(32, (max_halo + 31) / 32 * 32));
+  while (hm > 32 && halo_smem_bytes(nd, mixed, hm) > budget) hm -= 32;
+  return hm;
 }
 
 size_t halo_smem_bytes(int nd, bool mixed, int hmax) {
@@ -401,7 +449,15 @@ namespace {
 template <int ND, class R, int MODE, bool HANG, bool FUSE>
 int prepare_one(size_t smem) {
   auto k = k_stage_halo<ND, R, MODE, HANG, FUSE>;
-  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+  // the opt-in limit (less the kernel's static arrays), not this grid's size: several solvers
+  // share the kernel and its attribute
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa{};
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, k) != cudaSuccess || (size_t)optin < smem + fa.sharedSizeBytes ||
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)fa.sharedSizeBytes) !=
+          cudaSuccess) {
     cudaGetLastError();
     return 0;
   }

@@ -4,8 +4,9 @@
 // The kernel replaces hom3's num_flux + evolve loop (src/solver/fv/
 // solver.hpp:440-460, 470-494) for Euler with the AUSM flux.  It works on
 // 256-cell tiles of the Morton order.  Per tile, set-up time tables list
-//   * the tile's halo: every cell outside the tile that a face of a tile cell
-//     reads (same-level neighbours, ghosts and the fine cells of coarse/fine
+//   * the tile's halo: every (cell, direction) pair such that a face of a
+//     tile cell along that direction reads a cell outside the tile
+//     (same-level neighbours, ghosts and the fine cells of coarse/fine
 //     sub-face groups), sorted, and
 //   * for every cell and face position the shared-memory slot the face's
 //     neighbour lives in (0..255: a tile cell, 256 + h: halo cell h) or, with
@@ -22,7 +23,7 @@
 namespace h3c {
 
 constexpr int kHaloTile = 256;              // cells per tile = threads per block
-constexpr int kHaloMaxSlots = 1024;         // halo cells a tile may have
+constexpr int kHaloMaxSlots = 1024;         // halo entries a tile may hold in shared memory
 constexpr unsigned short kGroupBit = 0x8000;
 
 // Device tables of the halo-staged kernel.
@@ -47,14 +48,18 @@ struct HaloHost {
 // Builds the tables from the device-numbered neighbour table nbr [2nd][ld]
 // (>= 0 cell, <= -2 sub-face group -2 - k of sub [2^(nd-1)][nsub]) for the
 // tiles of [0, n_int); tile_end[t] is the end of tile t's cells (tiles never
-// span two batch instances).  Returns false when some tile's halo exceeds
-// kHaloMaxSlots (the tables are then unusable and the caller keeps the
-// per-lane tile kernel).
+// span two batch instances).  Returns false when a tile's slots overflow 15
+// bits or the cells 29 bits (the caller then keeps the per-lane tile kernel).
+// Halo ids carry the direction in bits 29-30.
 bool halo_build(int nd, long long ld, long long ntiles, const std::vector<long long>& tile_end, const int* nbr,
                 const int* sub, long long nsub, HaloHost& H);
 
 // Dynamic shared memory of one block for nd / precision / halo slots.
 size_t halo_smem_bytes(int nd, bool mixed, int hmax);
+// The halo entries a tile keeps in shared memory so that blocks_per_sm
+// blocks fit on an SM (at most the largest tile halo, rounded up to 32);
+// a tile's entries beyond it are read from global memory where used.
+int halo_slots_for(int nd, bool mixed, int max_halo, int blocks_per_sm);
 
 // Opts every instantiation for nd / precision into `smem` bytes of dynamic
 // shared memory and returns the resident blocks per SM at that size (0 when

@@ -243,8 +243,10 @@ int h3c_time(h3c_solver s, double* t);
 int h3c_step(h3c_solver s, int64_t* step);
 /* Failure detection.  hom3 ends a run when dt leaves [1e-300, 1e300]
  * (solution_diverged, utilities.hpp:74-76, 107-110) and asserts positive
- * density, energy and pressure (temperature for heat) in every cell
- * (check_variables, euler/physics.hpp:229-239, heat/physics.hpp:89-95).
+ * density, energy and pressure in every cell (check_variables,
+ * euler/physics.hpp:229-239; for heat and advection only a non-finite value
+ * counts here, since hom3's own heat and advection tests leave T = 0 and
+ * q < 0 in cells).
  * The device records both as status bits of each instance while it steps
  * (no extra synchronisation: the CFL reduction checks every cell it reads);
  * h3c_solve stays asynchronous, and the next call that reads the step
@@ -278,6 +280,13 @@ int h3c_launches(h3c_solver s, int64_t* n);
  *                            (0, the default: one block per tile for the per-lane tile kernel,
  *                            the resident blocks of all SMs for the halo-staged one) */
 #define H3C_OPT_PERSISTENT_BLOCKS 4
+/* H3C_OPT_CNS_ADJOINT_DUAL  the CNS adjoint's face derivatives by forward-mode dual numbers instead
+ *                           of the hand-written reverse sweep (default 0; kept as a cross-check) */
+#define H3C_OPT_CNS_ADJOINT_DUAL 5
+/* H3C_OPT_HALO_SLOTS  at most this many halo entries per tile in shared memory (a multiple of 32;
+ *                     0, the default: as many as let three blocks share an SM); entries beyond
+ *                     are read from global memory where a face needs them */
+#define H3C_OPT_HALO_SLOTS 6
 int h3c_set_option(h3c_solver s, int option, int value);
 /* The Euler stage launch in use (no hom3 counterpart): info[0] kernel (0 per
  * cell, 1 per-lane tile, 2 halo-staged tile), [1] halo slots per tile, [2]

@@ -350,3 +350,40 @@ def test_cht_adjoint_forward_is_the_coupled_loop():
     assert np.array_equal(gc.state(0)[:, :cns.first_ghost], gc2.state(0)[:, :cns.first_ghost])
     assert np.array_equal(gh.state(0)[:, :heat.first_ghost], gh2.state(0)[:, :heat.first_ghost])
     assert gc.step() == 5 and gh.step() == 5
+
+
+@pytest.mark.parametrize("name", sorted(CNS_BUILDERS))
+def test_cns_adjoint_reverse_equals_dual_evaluation(name):
+    """The hand-written reverse of the CNS face flux (AUSM + viscous, one
+    forward and one reverse sweep per face) against the forward-mode dual
+    evaluation of the same flux it replaced: the same derivatives to rounding."""
+    from hom3_b200 import _ffi as F
+    BUILDERS.update(CNS_BUILDERS)
+    o, g, q1, lam = setup(name)
+    fg = o.first_ghost
+    grad_rev, dts = g.adjoint(NSTEPS, lam, every=5)
+    g.set_state(q1, 0)
+    g.reset_time()
+    g.set_option(F.OPT_CNS_ADJOINT_DUAL, 1)
+    grad_dual, dts2 = g.adjoint(NSTEPS, lam, every=5)
+    assert np.array_equal(dts, dts2)
+    scale = np.abs(grad_dual[:, :fg]).max()
+    assert np.max(np.abs(grad_rev[:, :fg] - grad_dual[:, :fg])) <= 1e-12 * scale
+
+
+def test_cht_adjoint_reverse_equals_dual_evaluation():
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    cns, heat, gc, gh, qf, qs = cht_setup()
+    rng = np.random.default_rng(7)
+    lf = np.zeros_like(qf)
+    ls = np.zeros_like(qs)
+    lf[:, :cns.first_ghost] = rng.standard_normal((qf.shape[0], cns.first_ghost))
+    ls[:, :heat.first_ghost] = rng.standard_normal((1, heat.first_ghost))
+    gf1, gs1, dts1 = hb.cht_adjoint(0.01, gc, gh, 6, lf, ls, every=4)
+    _, _, gc2, gh2, _, _ = cht_setup()
+    gc2.set_option(F.OPT_CNS_ADJOINT_DUAL, 1)
+    gf2, gs2, dts2 = hb.cht_adjoint(0.01, gc2, gh2, 6, lf, ls, every=4)
+    assert np.array_equal(dts1, dts2)
+    assert np.max(np.abs(gf1 - gf2)) <= 1e-12 * np.abs(gf2).max()
+    assert np.max(np.abs(gs1 - gs2)) <= 1e-12 * np.abs(gs2).max()
