@@ -177,6 +177,8 @@ def build_workload(args):
     s = hb.Solver(3, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, prec, cfl=args.cfl, time_end=1e30)
     s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg, W.riemann3d_conditions(),
                t["subface_cells"])
+    if getattr(args, "euler_kernel", None) is not None:
+        s.set_option(F.OPT_EULER_KERNEL, args.euler_kernel)
     return s, t, q, modes
 
 
@@ -484,6 +486,8 @@ def run_tgv(args, ws, rank, local):
         s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg,
                    [Condition(F.BC_PERIODIC) for _ in range(6)])
         s.set_periodic(partners)
+        if args.halo_kernel is not None:
+            s.set_option(F.OPT_HALO_KERNEL, args.halo_kernel)
         s.set_state(q0, 0)
         s.reset_time()
         stream = torch.cuda.ExternalStream(s.stream())
@@ -979,6 +983,10 @@ def main():
     ap.add_argument("--no-parity", action="store_true", help="skip the oracle comparison of the default workload")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision record of the default workload")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble record")
+    ap.add_argument("--halo-kernel", type=int, default=None,
+                    help="1: stage tiles into shared memory (the library's default), 0: the kernels without it")
+    ap.add_argument("--euler-kernel", type=int, default=None,
+                    help="Euler stage kernel: 0 halo-staged tile, 1 per-lane tile, 2 per cell (default: the library's)")
     ap.add_argument("--workload", default="riemann3d",
                     choices=["riemann3d", "ensemble", "tgv", "vortex", "cht", "advection"])
     ap.add_argument("--adv-level", type=int, default=11)

@@ -24,7 +24,7 @@ FP64, MIXED = 0, 1
  BC_PERIODIC, BC_ADV_DIRICHLET, BC_ADV_NEUMANN, BC_ADV_CHARACTERISTIC) = range(18)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
 (OPT_TILE_KERNEL, OPT_GRAPHS, OPT_HALO_KERNEL, OPT_PERSISTENT_BLOCKS, OPT_CNS_ADJOINT_DUAL,
- OPT_HALO_SLOTS) = 1, 2, 3, 4, 5, 6
+ OPT_HALO_SLOTS, OPT_EULER_KERNEL) = 1, 2, 3, 4, 5, 6, 7
 STATUS_DT, STATUS_STATE, STATUS_TIMEOUT = 1, 2, 4
 KERNEL_KINDS = ("bc", "cfl", "scalar", "stage1", "stage2", "slopes", "copy", "adjoint")
 

@@ -147,6 +147,27 @@ __device__ __forceinline__ void block_min_atomic(long long v, long long* dst) {
   }
 }
 
+// The same minimum without a block barrier, for kernels that have none: each
+// warp folds its minimum into a shared slot; the last warp of the block to
+// arrive (a shared counter) makes the one global atomicMin.  slot and cnt
+// must hold kOrdMax and 0 before the first warp arrives (set at the kernel's
+// start, before a barrier).  Every warp of the block must call it once.
+__device__ __forceinline__ void block_min_atomic_nobar(long long v, long long* dst, long long* slot, unsigned* cnt) {
+  for (int o = 16; o > 0; o >>= 1) {
+    long long w = __shfl_down_sync(0xffffffffu, v, o);
+    v = w < v ? w : v;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(slot, v);
+    __threadfence_block();
+    if (atomicAdd(cnt, 1u) == (blockDim.x >> 5) - 1) {
+      __threadfence_block();
+      const long long m = *(volatile long long*)slot;
+      if (m < kOrdMax) atomicMin(dst, m);
+    }
+  }
+}
+
 // Records in the instance's status that some cell of this warp failed the
 // state check (one atomic per warp that saw one; every lane must call).
 __device__ __forceinline__ void flag_bad_state(bool bad, const Scalars* sc, int inst) {
@@ -375,7 +396,8 @@ __device__ __forceinline__ double cell_dt(const double* q, double h, const PhysC
     const double cand = fabs(P.u[d]) + P.a;
     S = (S < cand) ? cand : S;
   }
-  const double dt_inv = pc.cfl * h / S;
+  // cfl h / S with S's reciprocal by nr_rcp (within 2 ulp of the division)
+  const double dt_inv = PHYS == CNS ? pc.cfl * h / S : (pc.cfl * h) * nr_rcp(S);
   if (PHYS != CNS) return dt_inv;
   const double T = pc.gamma * P.p / P.q[ND];
   const double S_coeff = sutherland<double>(T, pc.sOverTref, pc.sOverTrefP1) / (P.q[ND] * h);
@@ -1330,6 +1352,169 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
     block_min_atomic(ord, per_instance(dtmin, inst));
   }
     __syncthreads();  // shared memory is rewritten by the next tile
+  }
+}
+
+// ---------------------------------------------------------------------------
+// AUSM stage, one thread per cell without shared memory: every face of the
+// cell is evaluated by the cell itself (each interior face twice, once from
+// each side, as hom3's num_flux does: solver.hpp:446-453), the neighbours'
+// face states recomputed from their state.  No barrier and no divergence
+// between border and interior cells: a warp's lanes all run the same code.
+// The face flux is the tile kernels' F(l, r) (face_state_global +
+// ausm_face), summed per direction in hom3's order.
+// ---------------------------------------------------------------------------
+#ifndef H3C_CELL_MINB
+#define H3C_CELL_MINB 3  // blocks per SM the per-cell AUSM kernel is register-budgeted for
+#endif
+template <int ND, class R, int MODE, bool HANG, bool FUSE>
+__global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const double* __restrict__ qin, double* out,
+                                                                          Geometry g, PhysConst pc,
+                                                                          const Scalars* __restrict__ sc,
+                                                                          long long* dtmin) {
+  constexpr int NV = ND + 2, NS = 1 << (ND - 1);
+  constexpr double W = ND == 2 ? 0.5 : 0.25;
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int inst = tile_instance(g, blockIdx.x);
+  const bool live = c < instance_end(g, inst);
+  const long long ld = g.ld;
+  const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+  __shared__ long long min_slot;
+  __shared__ unsigned min_cnt;
+  if (FUSE) {
+    if (threadIdx.x == 0) {
+      min_slot = kOrdMax;
+      min_cnt = 0;
+    }
+    __syncthreads();  // every warp is at the start: the only barrier
+  }
+  long long ord = kOrdMax;
+  bool bad = false;
+  if (live) {
+    double qc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
+    int nb[2 * ND];
+#pragma unroll
+    for (int p = 0; p < 2 * ND; ++p) nb[p] = __ldg(g.nbr + p * ld + c);
+    const double dx = g.len[g.lvl[c]];
+    // the cell's own face state
+    Prim<R, ND> Pc;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) Pc.q[v] = (R)qc[v];
+    make_prim<R, ND>(Pc, gamma, gm1);
+    R thc[NV];
+#pragma unroll
+    for (int v = 0; v < ND + 1; ++v) thc[v] = Pc.q[v] * Pc.a;
+    thc[ND + 1] = (Pc.q[ND + 1] + Pc.p) * Pc.a;
+    // the state of both neighbours along d, loaded together, then their face states along d
+    auto neighbour_fs = [&](int n, int d, FaceState<R, ND>& F, const double* qn) {
+      Prim<R, ND> P;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) P.q[v] = (R)qn[v];
+      make_prim<R, ND>(P, gamma, gm1);
+#pragma unroll
+      for (int v = 0; v < ND + 1; ++v) F.th[v] = P.q[v] * P.a;
+      F.th[ND + 1] = (P.q[ND + 1] + P.p) * P.a;
+      F.p = P.p;
+      F.M = P.M[d];
+    };
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+    // the two neighbours' states along a direction, loaded one direction ahead
+    // of the arithmetic so that their latency overlaps the previous direction
+    double qm[NV], qp[NV];
+    auto load_pair = [&](int d, double* am, double* ap) {
+      const int m = nb[2 * d], p = nb[2 * d + 1];
+      if (!HANG || (m >= 0 && p >= 0)) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          am[v] = __ldg(qin + v * ld + m);
+          ap[v] = __ldg(qin + v * ld + p);
+        }
+      }
+    };
+    load_pair(0, qm, qp);
+#pragma unroll
+    for (int d = 0; d < ND; ++d) {
+      double qm_n[NV], qp_n[NV];
+      if (d + 1 < ND) load_pair(d + 1 < ND ? d + 1 : d, qm_n, qp_n);
+      FaceState<R, ND> Fc;
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Fc.th[v] = thc[v];
+      Fc.p = Pc.p;
+      Fc.M = Pc.M[d];
+      const int m = nb[2 * d], p = nb[2 * d + 1];
+      double fm[NV], fp[NV];
+      if (!HANG || (m >= 0 && p >= 0)) {
+        FaceState<R, ND> Fm, Fp;
+        neighbour_fs(m, d, Fm, qm);
+        neighbour_fs(p, d, Fp, qp);
+        R f[NV];
+        ausm_face<R, ND>(Fm, Fc, d, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
+        ausm_face<R, ND>(Fc, Fp, d, f);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
+      } else {
+        // coarse/fine faces: W times the sum over the group's fine cells
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+          const int n = side == 0 ? m : p;
+          double* fo = side == 0 ? fm : fp;
+          const int cnt = n >= 0 ? 1 : NS;
+          const long long k = -(long long)n - 2;
+#pragma unroll 1
+          for (int j = 0; j < cnt; ++j) {
+            const int nn = n >= 0 ? n : __ldg(g.sub + j * g.nsub + k);
+            double qn[NV];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) qn[v] = __ldg(qin + v * ld + nn);
+            FaceState<R, ND> Fn;
+            neighbour_fs(nn, d, Fn, qn);
+            R f[NV];
+            if (side == 0) ausm_face<R, ND>(Fn, Fc, d, f);
+            else ausm_face<R, ND>(Fc, Fn, d, f);
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fo[v] = j == 0 ? (double)f[v] : fo[v] + (double)f[v];
+          }
+          if (n < 0) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) fo[v] = __dmul_rn(W, fo[v]);
+          }
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - fp[v]);
+      if (d + 1 < ND) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          qm[v] = qm_n[v];
+          qp[v] = qp_n[v];
+        }
+      }
+    }
+    const double k = sc[inst].dt * nr_rcp(dx);
+    double qo[NV];  // the start state of the in-place stages, read only now (fewer live registers)
+    if (MODE != 0) {
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
+    }
+    double o[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], qc[v], k * acc[v]);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
+    if (FUSE) {
+      const double cd = cell_dt<ND, EULER>(o, dx, pc, nullptr, &bad);
+      if (!isnan(cd)) ord = dbl_to_ord(cd);
+    }
+  }
+  if (FUSE) {
+    flag_bad_state(bad, sc, inst);
+    block_min_atomic_nobar(ord, per_instance(dtmin, inst), &min_slot, &min_cnt);
   }
 }
 

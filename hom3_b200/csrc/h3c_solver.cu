@@ -36,6 +36,12 @@ namespace {
 std::string g_last_error;  // errors not tied to a solver (NULL handle)
 
 constexpr long long kForcedNone = std::numeric_limits<long long>::max();
+
+// An instantiated graph of solver steps and the lhs buffer its capture started from.
+struct StepGraph {
+  cudaGraphExec_t exec = nullptr;
+  const double* q0 = nullptr;
+};
 }  // namespace
 
 namespace gridb {
@@ -94,6 +100,7 @@ struct h3c_solver_s {
   bool tile = true;  // Euler stages use the shared-memory tile kernel
   bool cns_adj_dual = false;  // CNS adjoint faces by dual numbers instead of the hand-written reverse
   int halo_cap = 0;           // cap on the Euler halo entries held in shared memory (0: none)
+  int euler_kernel = 2;       // Euler/AUSM stage: 0 halo-staged tile, 1 per-lane tile, 2 per cell
   // halo-staged Euler/AUSM stage (h3c_stage_halo.cu): tables, launch size
   bool halo = true;     // option: use it when its tables exist
   bool halo_ok = false; // tables built for the current grid
@@ -112,15 +119,11 @@ struct h3c_solver_s {
   long long ngl = 0;
   int h1max = 0, cns_bps = 0;
   size_t cns_smem = 0;
-  // CUDA graph of `graph_steps` solver steps, replayed by h3c_solve
-  cudaGraphExec_t graph = nullptr;
-  int graph_steps = 0;
-  const double* graph_q0 = nullptr;  // lhs buffer the capture started from
-  // single steps replayed from captured one-step graphs, one per lhs buffer
-  // (forward Euler alternates the two)
-  cudaGraphExec_t graph1[2] = {nullptr, nullptr};
-  const double* graph1_q0[2] = {nullptr, nullptr};
-  long long graph1_launches = 0;
+  // Captured step graphs replayed by h3c_solve: runs of kGraphSteps steps
+  // (graph8) and single steps (graph1), one of each per lhs buffer the
+  // capture started from (forward Euler alternates the two buffers).
+  StepGraph graph8[2], graph1[2];
+  long long graph_per_step = 0;  // kernel launches one captured step holds
   bool plain_done = false;  // a step ran outside capture (kernel attributes are set)
   // coupled conjugate-heat steps (h3c_cht_solve) captured with the heat partner
   cudaGraphExec_t cpl_graph = nullptr;
@@ -173,14 +176,11 @@ void drop_cpl_graph(h3c_solver s) {
 }
 
 void drop_graph(h3c_solver s) {
-  if (s->graph) cudaGraphExecDestroy(s->graph);
-  s->graph = nullptr;
-  s->graph_steps = 0;
-  for (int k = 0; k < 2; ++k) {
-    if (s->graph1[k]) cudaGraphExecDestroy(s->graph1[k]);
-    s->graph1[k] = nullptr;
-    s->graph1_q0[k] = nullptr;
-  }
+  for (int k = 0; k < 2; ++k)
+    for (StepGraph* g : {&s->graph8[k], &s->graph1[k]}) {
+      if (g->exec) cudaGraphExecDestroy(g->exec);
+      *g = StepGraph{};
+    }
   s->plain_done = false;  // the next capture follows a plain step of the current configuration
   // a coupled graph holds this solver's and its partner's buffers
   drop_cpl_graph(s);
@@ -384,7 +384,12 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
                    s->d_sc, &s->d_sc->dtmin_ord, &s->d_sc->status, grid, s->cns_smem, s->stream, s->d_gsl);
     return;
   }
-  if (PHYS == EULER && FLUX == AUSM && s->tile && s->halo && s->halo_ok) {
+  if (PHYS == EULER && FLUX == AUSM && s->tile && s->euler_kernel == 2) {  // the per-cell AUSM kernel
+    k_stage_ausm_cell<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
+        qin, out, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+    return;
+  }
+  if (PHYS == EULER && FLUX == AUSM && s->tile && s->halo && s->halo_ok && s->euler_kernel == 0) {
     int grid = s->persist_blocks > 0 ? s->persist_blocks : s->halo_bps * num_sms();
     grid = (int)std::max<long long>(1, std::min<long long>(grid, s->ntiles));
     HaloGeom hg{s->d_lnb, s->d_hids, s->d_hoff, s->d_grp, s->d_goff, s->hmax};
@@ -1329,107 +1334,92 @@ static void enqueue_steps(h3c_solver s, int64_t nsteps) {
 // state pointers to where the capture started.
 constexpr int kGraphSteps = 8;
 
-static bool build_graph(h3c_solver s) {
-  drop_graph(s);
-  cudaGraph_t g = nullptr;
+// Captures `n` steps starting from the current lhs buffer into `slot`
+// (capturing runs nothing: the state and the buffer pointers stay as they
+// were); false when the stream cannot be captured.
+static bool capture_steps(h3c_solver s, int n, StepGraph* slot) {
+  double* saved[3] = {s->d_q[0], s->d_q[1], s->d_q[2]};
   if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
   const long long l0 = s->launches;
-  enqueue_steps(s, kGraphSteps);
+  enqueue_steps(s, n);
+  const long long per_step = (s->launches - l0) / n;
+  s->launches = l0;
+  for (int j = 0; j < 3; ++j) s->d_q[j] = saved[j];
+  cudaGraph_t g = nullptr;
   const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
   if (e != cudaSuccess || !g) {
     cudaGetLastError();
-    s->launches = l0;
     if (g) cudaGraphDestroy(g);
     return false;
   }
-  const cudaError_t ei = cudaGraphInstantiate(&s->graph, g, 0);
+  const cudaError_t ei = cudaGraphInstantiate(&slot->exec, g, 0);
   cudaGraphDestroy(g);
-  s->launches = l0;
   if (ei != cudaSuccess) {
     cudaGetLastError();
-    s->graph = nullptr;
+    *slot = StepGraph{};
     return false;
   }
-  s->graph_steps = kGraphSteps;
-  s->graph_launches = 0;
-  s->graph_q0 = s->d_q[0];
+  slot->q0 = s->d_q[0];
+  s->graph_per_step = per_step;
   return true;
 }
 
-// One step replayed from the one-step graph captured for the current lhs
-// buffer (captured on first use); false when no graph can be had.
-static bool step_graph(h3c_solver s) {
-  int k = -1;
-  for (int j = 0; j < 2 && k < 0; ++j)
-    if (s->graph1[j] && s->graph1_q0[j] == s->d_q[0]) k = j;
-  if (k < 0) {
-    for (int j = 0; j < 2 && k < 0; ++j)
-      if (!s->graph1[j]) k = j;
-    if (k < 0) return false;
-    double* saved[3] = {s->d_q[0], s->d_q[1], s->d_q[2]};
-    if (cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-      cudaGetLastError();
-      return false;
-    }
-    const long long l0 = s->launches;
-    enqueue_steps(s, 1);
-    const long long per_step = s->launches - l0;
-    s->launches = l0;
-    for (int j = 0; j < 3; ++j) s->d_q[j] = saved[j];  // the capture did not run the step
-    cudaGraph_t g = nullptr;
-    const cudaError_t e = cudaStreamEndCapture(s->stream, &g);
-    if (e != cudaSuccess || !g) {
-      cudaGetLastError();
-      if (g) cudaGraphDestroy(g);
-      return false;
-    }
-    const cudaError_t ei = cudaGraphInstantiate(&s->graph1[k], g, 0);
-    cudaGraphDestroy(g);
-    if (ei != cudaSuccess) {
-      cudaGetLastError();
-      s->graph1[k] = nullptr;
-      return false;
-    }
-    s->graph1_q0[k] = s->d_q[0];
-    s->graph1_launches = per_step;
+// The graph of `n` steps for the current lhs buffer, captured on first use.
+static StepGraph* graph_for(h3c_solver s, StepGraph* slots, int n) {
+  for (int j = 0; j < 2; ++j)
+    if (slots[j].exec && slots[j].q0 == s->d_q[0]) return &slots[j];
+  for (int j = 0; j < 2; ++j)
+    if (!slots[j].exec) return capture_steps(s, n, &slots[j]) ? &slots[j] : nullptr;
+  return nullptr;
+}
+
+// Captures every step graph a later h3c_solve can replay, for both lhs
+// buffers where forward Euler alternates them, so that no capture or
+// instantiation falls inside a later run of steps whatever its length.
+static void capture_all(h3c_solver s) {
+  const bool fe = s->desc.time_integration == H3C_EULER_FORWARD;
+  for (int side = 0; side < (fe ? 2 : 1); ++side) {
+    if (side) std::swap(s->d_q[0], s->d_q[1]);
+    graph_for(s, s->graph8, kGraphSteps);
+    graph_for(s, s->graph1, 1);
+    if (side) std::swap(s->d_q[0], s->d_q[1]);
   }
-  if (cudaGraphLaunch(s->graph1[k], s->stream) != cudaSuccess) {
+}
+
+static bool launch_graph(h3c_solver s, const StepGraph* g, int n) {
+  if (cudaGraphLaunch(g->exec, s->stream) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  s->launches += s->graph1_launches;
-  if (s->desc.time_integration == H3C_EULER_FORWARD) std::swap(s->d_q[0], s->d_q[1]);  // as enqueue_step does
+  s->launches += s->graph_per_step * n;
+  // as enqueue_step does; kGraphSteps is even, so only single steps swap
+  if (s->desc.time_integration == H3C_EULER_FORWARD && (n & 1)) std::swap(s->d_q[0], s->d_q[1]);
   return true;
 }
 
 int h3c_solve(h3c_solver s, int64_t nsteps) {
   if (!s || nsteps < 0) return H3C_E_INVALID;
   if (int rc = ready(s, "h3c_solve")) return rc;
-  // Runs of steps replay a captured graph (no per-launch host cost); coupled
-  // solvers read their partner's current buffers and profiling brackets
-  // every launch, so those take the plain path.
+  // Steps replay captured graphs (no per-launch host cost) once one step has
+  // run plainly (kernel attributes are set outside capture); coupled solvers
+  // read their partner's current buffers and profiling brackets every
+  // launch, so those take the plain path.
   const bool graphable = s->graphs && !s->prof && s->partner == nullptr;
-  if (graphable && nsteps >= kGraphSteps) {
-    if (s->graph && s->graph_q0 != s->d_q[0]) drop_graph(s);  // forward Euler swapped buffers since
-    if (!s->graph) {
-      const long long l0 = s->launches;
-      enqueue_steps(s, 1);  // one plain step first (sets kernel attributes outside capture)
-      s->plain_done = true;
-      const long long per_step = s->launches - l0;
-      nsteps -= 1;
-      if (build_graph(s)) s->graph_launches = per_step * kGraphSteps;
-    }
-    while (s->graph && nsteps >= kGraphSteps) {
-      H3C_CUDA(s, cudaGraphLaunch(s->graph, s->stream));
-      s->launches += s->graph_launches;
-      nsteps -= kGraphSteps;
-    }
+  if (graphable && !s->plain_done && nsteps > 0) {
+    enqueue_steps(s, 1);
+    s->plain_done = true;
+    --nsteps;
   }
-  // the remaining single steps from a one-step graph, once a step has run plainly
-  while (graphable && s->plain_done && nsteps > 0 && step_graph(s)) --nsteps;
+  if (graphable && s->plain_done) {
+    capture_all(s);
+    for (StepGraph* g; nsteps >= kGraphSteps && (g = graph_for(s, s->graph8, kGraphSteps)) &&
+                       launch_graph(s, g, kGraphSteps);)
+      nsteps -= kGraphSteps;
+    for (StepGraph* g; nsteps > 0 && (g = graph_for(s, s->graph1, 1)) && launch_graph(s, g, 1);) --nsteps;
+  }
   if (nsteps > 0) {
     enqueue_steps(s, nsteps);
     s->plain_done = true;
@@ -1698,6 +1688,10 @@ int h3c_set_option(h3c_solver s, int option, int value) {
     case H3C_OPT_TILE_KERNEL: s->tile = value != 0; break;
     case H3C_OPT_GRAPHS: s->graphs = value != 0; break;
     case H3C_OPT_HALO_KERNEL: s->halo = value != 0; break;
+    case H3C_OPT_EULER_KERNEL:
+      if (value < 0 || value > 2) return s->fail(H3C_E_INVALID, "h3c_set_option: Euler kernel must be 0, 1 or 2");
+      s->euler_kernel = value;
+      break;
     case H3C_OPT_CNS_ADJOINT_DUAL: s->cns_adj_dual = value != 0; break;
     case H3C_OPT_HALO_SLOTS: {
       if (value < 0 || value % 32) return s->fail(H3C_E_INVALID, "h3c_set_option: halo slots must be a multiple of 32");
@@ -1736,7 +1730,9 @@ int h3c_kernel_info(h3c_solver s, int64_t* info, int n) {
                                                                          : bps * num_sms(),
                                                                          s->ntiles))
                             : (s->persist_blocks > 0 ? std::min<long long>(s->persist_blocks, s->ntiles) : s->ntiles);
-  const int64_t v[8] = {halo ? 2 : (euler && s->tile ? 1 : 0), (s->halo_ok || s->cns_ok) ? s->hmax : 0,
+  const bool cellk = euler && s->desc.flux == H3C_FLUX_AUSM && s->tile && s->euler_kernel == 2;
+  const bool halo_used = halo && (cns || s->euler_kernel == 0);
+  const int64_t v[8] = {cellk ? 3 : halo_used ? 2 : (euler && s->tile ? 1 : 0), (s->halo_ok || s->cns_ok) ? s->hmax : 0,
                         s->halo_maxh, (int64_t)std::llround(1000.0 * s->halo_mean), bps, grid,
                         (int64_t)(cns ? s->cns_smem : s->halo_smem), s->ntiles};
   for (int i = 0; i < n && i < 8; ++i) info[i] = v[i];
@@ -1759,15 +1755,40 @@ int h3c_instances(h3c_solver s, double* dt, double* time, int64_t* step) {
   return H3C_OK;
 }
 
-// Times `nsteps` steps for each launch configuration (stage kernel variant x
-// persistent grid size) from the same saved state and keeps the fastest.
+// Launch configurations h3c_autotune chooses from; the index is the choice
+// it returns.  persist: blocks per SM of a persistent grid (0: the kernel's
+// default grid).
+struct TuneCand {
+  bool tile;
+  int euler_kernel;
+  int persist;
+};
+constexpr TuneCand kTune[] = {
+    {true, 1, 0}, {true, 1, 1}, {true, 1, 2}, {true, 1, 3}, {true, 1, 4},  // per-lane tile (CNS: its tile kernel)
+    {false, 2, 0},                                                          // generic per-cell kernels
+    {true, 2, 0},                                                           // per-cell AUSM kernel
+    {true, 0, 1}, {true, 0, 2}, {true, 0, 3},                               // halo-staged tile kernel
+};
+constexpr int kTuneN = sizeof(kTune) / sizeof(kTune[0]);
+
+// Whether candidate i launches a kernel of its own for this solver (the
+// others would repeat a configuration already timed).
+static bool tune_applies(h3c_solver s, int i) {
+  const TuneCand& c = kTune[i];
+  if (!c.tile) return true;
+  const bool euler_ausm = s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM &&
+                          s->desc.reconstruction != H3C_RECON_MUSCL;
+  if (euler_ausm) return c.euler_kernel != 0 || (s->halo && s->halo_ok);
+  if (s->desc.physics == H3C_CNS && s->halo && s->cns_ok) return c.euler_kernel == 1;
+  return i == 0;  // one tile configuration where the options change nothing else
+}
+
+// Times `nsteps` steps for each launch configuration that applies (stage
+// kernel x persistent grid size) from the same saved state and keeps the fastest.
 int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_out) {
   if (!s || nsteps < 1) return H3C_E_INVALID;
   if (int rc = ready(s, "h3c_autotune")) return rc;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int cand_persist[5] = {0, sms, 2 * sms, 3 * sms, 4 * sms};
+  const int sms = num_sms();
   const size_t qbytes = sizeof(double) * s->nv * s->ld;
   double* save = nullptr;
   Scalars* save_sc = nullptr;
@@ -1785,6 +1806,12 @@ int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_out) {
     cudaMemcpyAsync(q1, save + s->nv * s->ld, qbytes, cudaMemcpyDeviceToDevice, s->stream);
     cudaMemcpyAsync(s->d_sc, save_sc, sizeof(Scalars) * s->n_inst, cudaMemcpyDeviceToDevice, s->stream);
   };
+  auto apply = [&](int i) {
+    s->tile = kTune[i].tile;
+    s->euler_kernel = kTune[i].euler_kernel;
+    s->persist_blocks = kTune[i].persist * sms;
+    drop_graph(s);
+  };
   cudaEvent_t a, b;
   cudaEventCreate(&a);
   cudaEventCreate(&b);
@@ -1792,29 +1819,25 @@ int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_out) {
   double best_ms = 1e300;
   const bool prof = s->prof;
   s->prof = false;
-  for (int tile = 1; tile >= 0; --tile) {
-    for (int k = 0; k < 5; ++k) {
-      const int idx = (1 - tile) * 5 + k;
-      if (!tile && k > 0) continue;  // the per-cell kernel has no persistent variant
-      restore();
-      s->tile = tile != 0;
-      s->persist_blocks = cand_persist[k];
-      drop_graph(s);
-      h3c_solve(s, 1);  // warm-up (kernel attributes, graph capture below)
-      cudaEventRecord(a, s->stream);
-      h3c_solve(s, nsteps);
-      cudaEventRecord(b, s->stream);
-      cudaEventSynchronize(b);
-      float ms = 0;
-      cudaEventElapsedTime(&ms, a, b);
-      if (ms < best_ms) { best_ms = ms; best = idx; }
+  for (int i = 0; i < kTuneN; ++i) {
+    if (!tune_applies(s, i)) continue;
+    restore();
+    apply(i);
+    h3c_solve(s, 2);  // warm-up: a plain step (kernel attributes), then the graph captures
+    cudaEventRecord(a, s->stream);
+    h3c_solve(s, nsteps);
+    cudaEventRecord(b, s->stream);
+    cudaEventSynchronize(b);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, a, b);
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = i;
     }
   }
   s->prof = prof;
   restore();
-  s->tile = best < 5;
-  s->persist_blocks = best < 5 ? cand_persist[best] : 0;
-  drop_graph(s);
+  apply(best);
   cudaStreamSynchronize(s->stream);
   cudaEventDestroy(a);
   cudaEventDestroy(b);

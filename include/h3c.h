@@ -192,10 +192,14 @@ int h3c_last_error(h3c_solver s, char* buf, size_t n);
 int h3c_set_grids(h3c_solver s, int n, const h3c_grid* grids);
 /* per-instance dt, time and step (arrays of n; any may be NULL) */
 int h3c_instances(h3c_solver s, double* dt, double* time, int64_t* step);
-/* Times nsteps steps for each launch configuration -- stage kernel variant
- * (shared-memory tile or per cell) x persistent grid size (one block per tile,
- * or 1-4 blocks per SM) -- from the same saved state, restores the state and
- * keeps the fastest; returns its index and its time per step (ms). */
+/* Times nsteps steps for each launch configuration that applies to the
+ * solver, from the same saved state, restores the state and keeps the
+ * fastest (sets H3C_OPT_TILE_KERNEL, H3C_OPT_EULER_KERNEL and
+ * H3C_OPT_PERSISTENT_BLOCKS); returns its index and its time per step (ms).
+ * Index: 0-4 the per-lane tile kernel (CNS: the CNS tile kernel) with its
+ * default grid or 1-4 persistent blocks per SM; 5 the generic per-cell
+ * kernels; 6 the per-cell AUSM kernel; 7-9 the halo-staged tile kernel with
+ * 1-3 persistent blocks per SM. */
 int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_per_step);
 
 /* ---- data: the tables create_local_cells/create_ghost_cells build
@@ -271,8 +275,9 @@ int h3c_launches(h3c_solver s, int64_t* n);
 /* Execution options (no hom3 counterpart; results do not depend on them):
  * H3C_OPT_TILE_KERNEL  Euler stages and their adjoint in the shared-memory tile kernels (default 1)
  * H3C_OPT_GRAPHS       replay runs of steps from a captured CUDA graph (default 1)
- * H3C_OPT_HALO_KERNEL  with the tile kernels on, Euler/AUSM stages stage each tile and its halo
- *                      into shared memory by bulk copies (default 1; 0: the per-lane tile kernel) */
+ * H3C_OPT_HALO_KERNEL  the halo-staged tile kernels (each tile and its halo copied into shared
+ *                      memory by bulk copies) may be used: the CNS stage and H3C_OPT_EULER_KERNEL 0
+ *                      (default 1; 0: CNS steps in the per-cell kernel, Euler kernel 0 in the per-lane one) */
 #define H3C_OPT_TILE_KERNEL 1
 #define H3C_OPT_GRAPHS 2
 #define H3C_OPT_HALO_KERNEL 3
@@ -287,9 +292,13 @@ int h3c_launches(h3c_solver s, int64_t* n);
  *                     0, the default: as many as let three blocks share an SM); entries beyond
  *                     are read from global memory where a face needs them */
 #define H3C_OPT_HALO_SLOTS 6
+/* H3C_OPT_EULER_KERNEL  the Euler/AUSM stage kernel (with the tile kernels on): 0 the halo-staged
+ *                       tile kernel when its tables exist, 1 the per-lane tile kernel, 2 (the
+ *                       default) one thread per cell without shared memory, faces from both sides */
+#define H3C_OPT_EULER_KERNEL 7
 int h3c_set_option(h3c_solver s, int option, int value);
 /* The Euler stage launch in use (no hom3 counterpart): info[0] kernel (0 per
- * cell, 1 per-lane tile, 2 halo-staged tile), [1] halo slots per tile, [2]
+ * cell, 1 per-lane tile, 2 halo-staged tile, 3 the per-cell AUSM kernel), [1] halo slots per tile, [2]
  * largest tile halo, [3] mean tile halo x 1000, [4] resident blocks per SM
  * of the halo-staged kernel, [5] blocks launched, [6] its dynamic shared
  * memory in bytes, [7] 256-cell tiles; the first n entries are written. */

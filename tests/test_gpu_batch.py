@@ -72,3 +72,30 @@ def test_autotune_keeps_the_state():
     ta, tb = a.instances()[1], b.instances()[1]
     assert np.allclose(ta, tb, rtol=1e-12, atol=0)
     assert np.array_equal(a.instances()[2], b.instances()[2])
+
+
+KERNEL_OF_CHOICE = ["tile"] * 5 + ["per_cell", "cell", "halo", "halo", "halo"]
+
+
+def test_autotune_single_tree_sets_the_chosen_kernel():
+    """On one refined tree every Euler/AUSM configuration applies; the chosen
+    one is the kernel in use afterwards and the state is the untuned one's."""
+    import torch
+    import cases
+    from oracle import h3o
+    _, (o,) = cases.refined_case(ti=h3o.RK2, level=3, fine=5)
+    a = cases.gpu_solver_from_oracle(o, 0)
+    b = cases.gpu_solver_from_oracle(o, 0)
+    choice, ms_step = a.autotune(3)
+    assert 0 <= choice < 10 and ms_step > 0
+    info = a.kernel_info()
+    assert info["kernel"] == KERNEL_OF_CHOICE[choice], (choice, info)
+    if choice >= 7:
+        sms = torch.cuda.get_device_properties(0).multi_processor_count
+        assert info["grid"] == min(info["tiles"], (choice - 6) * sms)
+    a.solve(4)
+    b.solve(4)
+    fg = o.first_ghost
+    qa, qb = a.state(0)[:, :fg], b.state(0)[:, :fg]
+    assert np.max(np.abs(qa - qb)) <= 1e-12 * np.max(np.abs(qb))
+    assert a.step() == b.step() == 4

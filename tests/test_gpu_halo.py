@@ -1,10 +1,11 @@
-"""The halo-staged Euler/AUSM stage kernel (tile + halo copied into shared
-memory by bulk copies) against the per-lane tile kernel and the oracle.
+"""The Euler/AUSM stage kernels against one another and the oracle: the
+halo-staged tile kernel (tile + halo copied into shared memory by bulk
+copies), the per-lane tile kernel and the per-cell kernel (the default).
 
 Both kernels evaluate the same face fluxes F(l, r) from the same face states
 and sum them in hom3's order; the compiler may still fuse a product into a
 sum (FMA) at different places in the two kernels, so their states agree to a
-few ulps, step after step (FP64: 1e-13 relative; FP32 face fluxes: 1e-6), on
+few ulps, step after step (FP64: 1e-13 relative; FP32 face fluxes: 1e-5), on
 every grid kind the stage meets: uniform and refined trees (coarse/fine
 sub-face groups inside a tile and in its halo), periodic partners, partial
 last tiles, batches of grids, every time integration and both precisions,
@@ -21,13 +22,15 @@ pytestmark = pytest.mark.gpu
 
 
 def _pair(o, precision=0):
+    """(halo-staged kernel, per-lane tile kernel) solvers from the oracle's state."""
     a = cases.gpu_solver_from_oracle(o, precision)
     b = cases.gpu_solver_from_oracle(o, precision)
-    b.set_option(F.OPT_HALO_KERNEL, 0)
+    a.set_option(F.OPT_EULER_KERNEL, 0)
+    b.set_option(F.OPT_EULER_KERNEL, 1)
     return a, b
 
 
-TOL = {0: 1e-13, 1: 1e-6}  # FP64, mixed
+TOL = {0: 1e-13, 1: 1e-5}  # FP64, mixed (FP32 face fluxes)
 
 
 def _same(a, b, fg, what, precision=0):
@@ -84,6 +87,7 @@ def test_halo_kernel_partial_last_tile_against_oracle():
     o.initialize()
     assert o.first_ghost % 256 != 0
     g = cases.gpu_solver_from_oracle(o)
+    g.set_option(F.OPT_EULER_KERNEL, 0)
     assert g.kernel_info()["halo"] == 1
     o.solve(1)
     g.solve(1)
@@ -95,22 +99,25 @@ def test_halo_kernel_partial_last_tile_against_oracle():
     assert rel_err(g.state(0)[:, :fg], o.state(0)[:, :fg]) <= 1e-10
 
 
+@pytest.mark.parametrize("kernel", [0, 2])
 @pytest.mark.parametrize("precision", [F.FP64, F.MIXED])
-def test_halo_kernel_batches(precision):
+def test_halo_and_per_cell_kernels_batches(precision, kernel):
+    """Batches of grids in the halo-staged (0) and per-cell (2) kernels
+    against the per-lane tile kernel."""
     from test_gpu_batch import members
     from hom3_b200.solver import euler_neumann
     ms, tables, states = members(7)
     conds = [[euler_neumann() for _ in range(4)] for _ in tables]
 
-    def make(halo):
+    def make(k):
         b = hb.Batch(2, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, precision, cfl=0.4, time_end=1e9)
         b.set_grids(tables, conds)
         b.set_state(np.concatenate(states, axis=1), 0)
         b.reset_time()
-        b.set_option(F.OPT_HALO_KERNEL, halo)
+        b.set_option(F.OPT_EULER_KERNEL, k)
         return b
 
-    a, b = make(1), make(0)
+    a, b = make(kernel), make(1)
     a.solve(6)
     b.solve(6)
     from test_gpu_parity import rel_err
@@ -131,3 +138,30 @@ def test_halo_entries_beyond_shared_memory_read_from_global(slots):
     a.solve(4)
     b.solve(4)
     _same(a, b, o.first_ghost, f"{slots} slots")
+
+
+@pytest.mark.parametrize("case", ["refined_rk2", "refined_fe_mixed", "explosion_rk3", "periodic_vortex"])
+def test_per_cell_ausm_kernel(case):
+    """The per-cell AUSM kernel (each face from both sides, no shared memory)
+    against the per-lane tile kernel and the oracle."""
+    precision = 1 if case.endswith("mixed") else 0
+    if case.startswith("refined"):
+        _, (o,) = cases.refined_case(ti=h3o.RK2 if "rk2" in case else h3o.EULER_FORWARD, level=3, fine=5)
+    elif case == "explosion_rk3":
+        _, (o,) = cases.euler_case("explosion", nd=3, level=4, ti=h3o.SSPRK3)
+    else:
+        _, (o,) = cases.periodic_vortex_case(level=6, ti=h3o.RK2)
+    a, b = _pair(o, precision)
+    a.set_option(F.OPT_EULER_KERNEL, 2)  # the default
+    assert a.kernel_info()["kernel"] == "cell"
+    fg = o.first_ghost
+    o.solve(1)
+    a.solve(1)
+    b.solve(1)
+    _same(a, b, fg, "1 step", precision)
+    if precision == 0:
+        from test_gpu_parity import rel_err
+        assert rel_err(a.state(0)[:, :fg], o.state(0)[:, :fg]) <= 1e-12
+    a.solve(5)
+    b.solve(5)
+    _same(a, b, fg, "6 steps", precision)

@@ -62,7 +62,7 @@ def test_headline_tree_fp64_and_mixed_against_oracle(headline):
     vol = o.tables()["length"][:fg] ** 3
     g = cases.gpu_solver_from_oracle(o, 0)
     m = cases.gpu_solver_from_oracle(o, 1)
-    assert g.kernel_info()["kernel"] == "halo"
+    assert g.kernel_info()["kernel"] == "cell"
     assert abs(g.dt() - o.dt()) <= 1e-12 * o.dt()
     t0 = totals(o.state(0)[:, :fg], vol)
     o.solve(1)
@@ -87,14 +87,17 @@ def test_headline_tree_fp64_and_mixed_against_oracle(headline):
     assert g.status() == 0 and m.status() == 0
 
 
-def test_headline_tree_per_lane_kernel_agrees(headline):
-    """The per-lane tile kernel on the same tree agrees with the halo kernel to rounding."""
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_headline_tree_other_stage_kernels_agree(headline, kernel):
+    """The halo-staged (0) and per-lane (1) tile kernels on the same tree agree
+    with the default per-cell kernel to rounding."""
     from hom3_b200 import _ffi as F
     _, o = headline
     fg = o.first_ghost
     a = cases.gpu_solver_from_oracle(o, 0)
     b = cases.gpu_solver_from_oracle(o, 0)
-    b.set_option(F.OPT_HALO_KERNEL, 0)
+    b.set_option(F.OPT_EULER_KERNEL, kernel)
+    assert b.kernel_info()["kernel"] == ("halo", "tile")[kernel]
     a.solve(2)
     b.solve(2)
     assert rel_err(a.state(0)[:, :fg], b.state(0)[:, :fg]) <= 1e-13
