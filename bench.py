@@ -893,6 +893,12 @@ def mixed_record(args, t, q0, ws, local, fp64_value):
                t["subface_cells"])
     m.set_state(q0, 0)
     m.reset_time()
+    tune = None
+    if args.euler_kernel is not None:
+        m.set_option(F.OPT_EULER_KERNEL, args.euler_kernel)
+    elif not args.no_autotune:
+        choice, _ = m.autotune(10)
+        tune = {"choice": choice, "kernel": m.kernel_info()["kernel"]}
     stream = torch.cuda.ExternalStream(m.stream())
     m.solve(args.warmup)
     torch.cuda.synchronize()
@@ -906,7 +912,8 @@ def mixed_record(args, t, q0, ws, local, fp64_value):
     ms = allreduce_max(ev0.elapsed_time(ev1), ws)
     v = fg * args.steps * ws / (ms * 1e-3)
     return {"value": v, "unit": "cell-updates/s", "ms_per_step": ms / args.steps, "mixed_over_fp64": v / fp64_value,
-            "dtype": "f32-flux/f64-state", "stage_kernel": m.kernel_info()["kernel"], "clocks": clk.summary(),
+            "dtype": "f32-flux/f64-state", "stage_kernel": m.kernel_info()["kernel"], "autotune": tune,
+            "clocks": clk.summary(),
             "what": "same tree, state, steps and timing as the FP64 line; FP32 face states and fluxes, FP64 "
                     "state, residual, update and dt"}
 
@@ -985,6 +992,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble record")
     ap.add_argument("--halo-kernel", type=int, default=None,
                     help="1: stage tiles into shared memory (the library's default), 0: the kernels without it")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the library's default Euler stage launch instead of h3c_autotune's choice")
     ap.add_argument("--euler-kernel", type=int, default=None,
                     help="Euler stage kernel: 0 halo-staged tile, 1 per-lane tile, 2 per cell (default: the library's)")
     ap.add_argument("--workload", default="riemann3d",
@@ -1025,6 +1034,11 @@ def main():
     # ---- device-resident timing ('value') ----
     s.set_state(q0, 0)
     s.reset_time()
+    tune = None
+    if args.euler_kernel is None and not args.no_autotune:
+        # the stage kernel and launch shape for this GPU, timed from the initial state (which it restores)
+        choice, tune_ms = s.autotune(10)
+        tune = {"choice": choice, "ms_per_step": tune_ms, "kernel": s.kernel_info()["kernel"]}
     with ClockSampler(local) as clk:
         s.solve(args.warmup)
         torch.cuda.synchronize()
@@ -1117,6 +1131,7 @@ def main():
         line["adjoint"] = adj
     line["grid_build"] = getattr(args, "grid_build", None)
     line["stage_kernel"] = s.kernel_info()
+    line["autotune"] = tune
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         r = cpu_oracle_run(args)
         r1 = cpu_oracle_run(args, steps_budget_s=8.0, threads=1)

@@ -1374,15 +1374,20 @@ __global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const
                                                                           long long* dtmin) {
   constexpr int NV = ND + 2, NS = 1 << (ND - 1);
   constexpr double W = ND == 2 ? 0.5 : 0.25;
-  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int tid = threadIdx.x;
+  const long long c = (long long)blockIdx.x * blockDim.x + tid;
   const int inst = tile_instance(g, blockIdx.x);
   const bool live = c < instance_end(g, inst);
   const long long ld = g.ld;
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+  // The cell's own face state (theta, p, Mach number along each direction),
+  // kept in the thread's column of shared memory rather than in registers
+  // across the direction loop: at three blocks per SM the loop spills otherwise.
+  __shared__ R own[NV + 1 + ND][kBlock];
   __shared__ long long min_slot;
   __shared__ unsigned min_cnt;
   if (FUSE) {
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
       min_slot = kOrdMax;
       min_cnt = 0;
     }
@@ -1391,24 +1396,19 @@ __global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const
   long long ord = kOrdMax;
   bool bad = false;
   if (live) {
-    double qc[NV];
+    {
+      Prim<R, ND> P;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
-    int nb[2 * ND];
+      for (int v = 0; v < NV; ++v) P.q[v] = (R)__ldg(qin + v * ld + c);
+      make_prim<R, ND>(P, gamma, gm1);
 #pragma unroll
-    for (int p = 0; p < 2 * ND; ++p) nb[p] = __ldg(g.nbr + p * ld + c);
-    const double dx = g.len[g.lvl[c]];
-    // the cell's own face state
-    Prim<R, ND> Pc;
+      for (int v = 0; v < ND + 1; ++v) own[v][tid] = P.q[v] * P.a;
+      own[ND + 1][tid] = (P.q[ND + 1] + P.p) * P.a;
+      own[NV][tid] = P.p;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) Pc.q[v] = (R)qc[v];
-    make_prim<R, ND>(Pc, gamma, gm1);
-    R thc[NV];
-#pragma unroll
-    for (int v = 0; v < ND + 1; ++v) thc[v] = Pc.q[v] * Pc.a;
-    thc[ND + 1] = (Pc.q[ND + 1] + Pc.p) * Pc.a;
-    // the state of both neighbours along d, loaded together, then their face states along d
-    auto neighbour_fs = [&](int n, int d, FaceState<R, ND>& F, const double* qn) {
+      for (int d = 0; d < ND; ++d) own[NV + 1 + d][tid] = P.M[d];
+    }
+    auto neighbour_fs = [&](int d, FaceState<R, ND>& F, const double* qn) {
       Prim<R, ND> P;
 #pragma unroll
       for (int v = 0; v < NV; ++v) P.q[v] = (R)qn[v];
@@ -1422,35 +1422,26 @@ __global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const
     double acc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] = 0.0;
-    // the two neighbours' states along a direction, loaded one direction ahead
-    // of the arithmetic so that their latency overlaps the previous direction
-    double qm[NV], qp[NV];
-    auto load_pair = [&](int d, double* am, double* ap) {
-      const int m = nb[2 * d], p = nb[2 * d + 1];
-      if (!HANG || (m >= 0 && p >= 0)) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          am[v] = __ldg(qin + v * ld + m);
-          ap[v] = __ldg(qin + v * ld + p);
-        }
-      }
-    };
-    load_pair(0, qm, qp);
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
-      double qm_n[NV], qp_n[NV];
-      if (d + 1 < ND) load_pair(d + 1 < ND ? d + 1 : d, qm_n, qp_n);
+      const int m = __ldg(g.nbr + 2 * d * ld + c), p = __ldg(g.nbr + (2 * d + 1) * ld + c);
       FaceState<R, ND> Fc;
 #pragma unroll
-      for (int v = 0; v < NV; ++v) Fc.th[v] = thc[v];
-      Fc.p = Pc.p;
-      Fc.M = Pc.M[d];
-      const int m = nb[2 * d], p = nb[2 * d + 1];
+      for (int v = 0; v < NV; ++v) Fc.th[v] = own[v][tid];
+      Fc.p = own[NV][tid];
+      Fc.M = own[NV + 1 + d][tid];
       double fm[NV], fp[NV];
       if (!HANG || (m >= 0 && p >= 0)) {
+        // both neighbours' states along d, loaded together
+        double qm[NV], qp[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          qm[v] = __ldg(qin + v * ld + m);
+          qp[v] = __ldg(qin + v * ld + p);
+        }
         FaceState<R, ND> Fm, Fp;
-        neighbour_fs(m, d, Fm, qm);
-        neighbour_fs(p, d, Fp, qp);
+        neighbour_fs(d, Fm, qm);
+        neighbour_fs(d, Fp, qp);
         R f[NV];
         ausm_face<R, ND>(Fm, Fc, d, f);
 #pragma unroll
@@ -1473,7 +1464,7 @@ __global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const
 #pragma unroll
             for (int v = 0; v < NV; ++v) qn[v] = __ldg(qin + v * ld + nn);
             FaceState<R, ND> Fn;
-            neighbour_fs(nn, d, Fn, qn);
+            neighbour_fs(d, Fn, qn);
             R f[NV];
             if (side == 0) ausm_face<R, ND>(Fn, Fc, d, f);
             else ausm_face<R, ND>(Fc, Fn, d, f);
@@ -1488,16 +1479,12 @@ __global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - fp[v]);
-      if (d + 1 < ND) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          qm[v] = qm_n[v];
-          qp[v] = qp_n[v];
-        }
-      }
     }
+    const double dx = g.len[g.lvl[c]];
     const double k = sc[inst].dt * nr_rcp(dx);
-    double qo[NV];  // the start state of the in-place stages, read only now (fewer live registers)
+    double qc[NV], qo[NV];  // the stage input and the in-place stages' start state, read only now
+#pragma unroll
+    for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
     if (MODE != 0) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];

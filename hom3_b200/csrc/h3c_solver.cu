@@ -29,6 +29,7 @@
 #include "muscl_adjoint.cuh"
 #include "cns_adjoint.cuh"
 #include "stage_halo.hpp"
+#include "stage_warp.hpp"
 
 using namespace h3c;
 
@@ -100,7 +101,8 @@ struct h3c_solver_s {
   bool tile = true;  // Euler stages use the shared-memory tile kernel
   bool cns_adj_dual = false;  // CNS adjoint faces by dual numbers instead of the hand-written reverse
   int halo_cap = 0;           // cap on the Euler halo entries held in shared memory (0: none)
-  int euler_kernel = 2;       // Euler/AUSM stage: 0 halo-staged tile, 1 per-lane tile, 2 per cell
+  int euler_kernel = 1;       // Euler/AUSM stage: 0 halo-staged tile, 1 per-lane tile, 2 per cell, 3 warp-tiled
+  int warp_bps = 0;           // resident blocks per SM of the warp-tiled kernel (0: unavailable)
   // halo-staged Euler/AUSM stage (h3c_stage_halo.cu): tables, launch size
   bool halo = true;     // option: use it when its tables exist
   bool halo_ok = false; // tables built for the current grid
@@ -384,7 +386,12 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
                    s->d_sc, &s->d_sc->dtmin_ord, &s->d_sc->status, grid, s->cns_smem, s->stream, s->d_gsl);
     return;
   }
-  if (PHYS == EULER && FLUX == AUSM && s->tile && s->euler_kernel == 2) {  // the per-cell AUSM kernel
+  if (PHYS == EULER && FLUX == AUSM && s->tile && s->euler_kernel == 3 && s->warp_bps > 0) {
+    warp_stage(ND, std::is_same<R, float>::value, MODE, HANG, FUSE, qin, out, geometry(s), s->pc, s->d_sc,
+               &s->d_sc->dtmin_ord, s->stream);
+    return;
+  }
+  if (PHYS == EULER && FLUX == AUSM && s->tile && s->euler_kernel >= 2) {  // the per-cell AUSM kernel
     k_stage_ausm_cell<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
         qin, out, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
     return;
@@ -953,6 +960,8 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
       s->halo_ok = true;
     }
   }
+  if (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM && s->desc.reconstruction != H3C_RECON_MUSCL)
+    s->warp_bps = warp_prepare(nd, s->desc.precision == H3C_MIXED);
   if (cns_tables) {
     const bool mixed = s->desc.precision == H3C_MIXED;
     const size_t smem = cns_halo_smem_bytes(nd, mixed, CH.base.hmax, CH.h1max);
@@ -1027,8 +1036,8 @@ int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld) {
   if (ld < nc) return s->fail(H3C_E_INVALID, "h3c_set_state: ld < n_cells");
   int rc = ensure_stage(s, nc);
   if (rc) return rc;
-  for (int v = 0; v < s->nv; ++v)
-    H3C_CUDA(s, cudaMemcpyAsync(s->d_stage + v * nc, q + v * ld, sizeof(double) * nc, cudaMemcpyHostToDevice,
+  for (int v = 0; v < s->nv; ++v)  // q in host or device memory (unified addressing)
+    H3C_CUDA(s, cudaMemcpyAsync(s->d_stage + v * nc, q + v * ld, sizeof(double) * nc, cudaMemcpyDefault,
                                 s->stream));
   k_gather<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_stage, nc, s->d_q[which], s->ld, s->d_dev2caller,
                                                        s->n_tot, s->nv);
@@ -1212,8 +1221,8 @@ int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld) {
   if (rc) return rc;
   k_scatter<<<blocks(s->n_tot), kBlock, 0, s->stream>>>(s->d_q[which], s->ld, s->d_stage, nc, s->d_dev2caller,
                                                         s->n_tot, s->nv);
-  for (int v = 0; v < s->nv; ++v)
-    H3C_CUDA(s, cudaMemcpyAsync(q + v * ld, s->d_stage + v * nc, sizeof(double) * nc, cudaMemcpyDeviceToHost,
+  for (int v = 0; v < s->nv; ++v)  // q in host or device memory (unified addressing)
+    H3C_CUDA(s, cudaMemcpyAsync(q + v * ld, s->d_stage + v * nc, sizeof(double) * nc, cudaMemcpyDefault,
                                 s->stream));
   H3C_CUDA(s, cudaStreamSynchronize(s->stream));
   return s->cuda(cudaGetLastError(), "h3c_get_state");
@@ -1689,7 +1698,7 @@ int h3c_set_option(h3c_solver s, int option, int value) {
     case H3C_OPT_GRAPHS: s->graphs = value != 0; break;
     case H3C_OPT_HALO_KERNEL: s->halo = value != 0; break;
     case H3C_OPT_EULER_KERNEL:
-      if (value < 0 || value > 2) return s->fail(H3C_E_INVALID, "h3c_set_option: Euler kernel must be 0, 1 or 2");
+      if (value < 0 || value > 3) return s->fail(H3C_E_INVALID, "h3c_set_option: Euler kernel must be 0, 1, 2 or 3");
       s->euler_kernel = value;
       break;
     case H3C_OPT_CNS_ADJOINT_DUAL: s->cns_adj_dual = value != 0; break;
@@ -1730,9 +1739,12 @@ int h3c_kernel_info(h3c_solver s, int64_t* info, int n) {
                                                                          : bps * num_sms(),
                                                                          s->ntiles))
                             : (s->persist_blocks > 0 ? std::min<long long>(s->persist_blocks, s->ntiles) : s->ntiles);
-  const bool cellk = euler && s->desc.flux == H3C_FLUX_AUSM && s->tile && s->euler_kernel == 2;
+  const bool ausm_tile = euler && s->desc.flux == H3C_FLUX_AUSM && s->tile;
+  const bool warpk = ausm_tile && s->euler_kernel == 3 && s->warp_bps > 0;
+  const bool cellk = ausm_tile && s->euler_kernel >= 2 && !warpk;
   const bool halo_used = halo && (cns || s->euler_kernel == 0);
-  const int64_t v[8] = {cellk ? 3 : halo_used ? 2 : (euler && s->tile ? 1 : 0), (s->halo_ok || s->cns_ok) ? s->hmax : 0,
+  const int64_t v[8] = {warpk ? 4 : cellk ? 3 : halo_used ? 2 : (euler && s->tile ? 1 : 0),
+                        (s->halo_ok || s->cns_ok) ? s->hmax : 0,
                         s->halo_maxh, (int64_t)std::llround(1000.0 * s->halo_mean), bps, grid,
                         (int64_t)(cns ? s->cns_smem : s->halo_smem), s->ntiles};
   for (int i = 0; i < n && i < 8; ++i) info[i] = v[i];
@@ -1768,6 +1780,7 @@ constexpr TuneCand kTune[] = {
     {false, 2, 0},                                                          // generic per-cell kernels
     {true, 2, 0},                                                           // per-cell AUSM kernel
     {true, 0, 1}, {true, 0, 2}, {true, 0, 3},                               // halo-staged tile kernel
+    {true, 3, 0},                                                           // warp-tiled kernel
 };
 constexpr int kTuneN = sizeof(kTune) / sizeof(kTune[0]);
 
@@ -1778,7 +1791,7 @@ static bool tune_applies(h3c_solver s, int i) {
   if (!c.tile) return true;
   const bool euler_ausm = s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM &&
                           s->desc.reconstruction != H3C_RECON_MUSCL;
-  if (euler_ausm) return c.euler_kernel != 0 || (s->halo && s->halo_ok);
+  if (euler_ausm) return (c.euler_kernel != 0 || (s->halo && s->halo_ok)) && (c.euler_kernel != 3 || s->warp_bps > 0);
   if (s->desc.physics == H3C_CNS && s->halo && s->cns_ok) return c.euler_kernel == 1;
   return i == 0;  // one tile configuration where the options change nothing else
 }

@@ -200,6 +200,14 @@ class Solver:
         self._grid = (g, nb, xc, ln, bc, arr)  # the tables h3c_write_vtk is handed again
 
     def set_state(self, q, which=LHS):
+        """q: [nv][n_cells] float64, a numpy array or a CUDA tensor (copied device to device)."""
+        if hasattr(q, "is_cuda") and q.is_cuda:
+            import torch
+            t = q.contiguous()
+            assert t.dtype == torch.float64 and tuple(t.shape) == (self.nv, self.n_cells), (t.dtype, t.shape)
+            self._check(lib().h3c_set_state(self.h, which, C.cast(t.data_ptr(), C.POINTER(C.c_double)),
+                                            self.n_cells))
+            return
         q = np.ascontiguousarray(q, np.float64)
         assert q.shape == (self.nv, self.n_cells), q.shape
         self._check(lib().h3c_set_state(self.h, which, _dp(q), self.n_cells))
@@ -221,7 +229,15 @@ class Solver:
         self._check(lib().h3c_write_vtk(self.h, str(fname).encode(), C.byref(self._grid[0]),
                                         _lp(nid) if nid is not None else None))
 
-    def state(self, which=LHS, out=None) -> np.ndarray:
+    def state(self, which=LHS, out=None):
+        """The state [nv][n_cells] in caller numbering: a new numpy array, or
+        written into `out` (a numpy array or a contiguous float64 CUDA tensor)."""
+        if out is not None and hasattr(out, "is_cuda") and out.is_cuda:
+            import torch
+            assert out.dtype == torch.float64 and tuple(out.shape) == (self.nv, self.n_cells) and out.is_contiguous()
+            self._check(lib().h3c_get_state(self.h, which, C.cast(out.data_ptr(), C.POINTER(C.c_double)),
+                                            self.n_cells))
+            return out
         if out is None:
             out = np.empty((self.nv, self.n_cells), np.float64)
         assert out.shape == (self.nv, self.n_cells) and out.dtype == np.float64 and out.flags.c_contiguous
@@ -289,11 +305,18 @@ class Solver:
         """Blocks of the Euler/AUSM stage launch (0: the library's default)."""
         self.set_option(F.OPT_PERSISTENT_BLOCKS, n)
 
+    def autotune(self, nsteps=20):
+        """Times every applicable stage launch configuration from the current
+        state and keeps the fastest (h3c_autotune): (choice, ms per step)."""
+        ch, ms = C.c_int(), C.c_double()
+        self._check(lib().h3c_autotune(self.h, nsteps, C.byref(ch), C.byref(ms)))
+        return ch.value, ms.value
+
     def kernel_info(self) -> dict:
         """The Euler stage launch in use (h3c_kernel_info)."""
         v = np.zeros(8, np.int64)
         self._check(lib().h3c_kernel_info(self.h, _lp(v), 8))
-        return {"halo": int(v[0] == 2), "kernel": ("per_cell", "tile", "halo", "cell")[int(v[0])], "halo_slots": int(v[1]),
+        return {"halo": int(v[0] == 2), "kernel": ("per_cell", "tile", "halo", "cell", "warp")[int(v[0])], "halo_slots": int(v[1]),
                 "max_halo": int(v[2]), "mean_halo": v[3] / 1000.0, "blocks_per_sm": int(v[4]), "grid": int(v[5]),
                 "smem_bytes": int(v[6]), "tiles": int(v[7])}
 
@@ -389,10 +412,6 @@ class Batch(Solver):
         self._check(lib().h3c_instances(self.h, _dp(dt), _dp(tm), _lp(st)))
         return dt, tm, st
 
-    def autotune(self, nsteps=20):
-        ch, ms = C.c_int(), C.c_double()
-        self._check(lib().h3c_autotune(self.h, nsteps, C.byref(ch), C.byref(ms)))
-        return ch.value, ms.value
 
 
 def couple_cht(Tr0, cns: Solver, heat: Solver):

@@ -199,13 +199,13 @@ int h3c_instances(h3c_solver s, double* dt, double* time, int64_t* step);
  * Index: 0-4 the per-lane tile kernel (CNS: the CNS tile kernel) with its
  * default grid or 1-4 persistent blocks per SM; 5 the generic per-cell
  * kernels; 6 the per-cell AUSM kernel; 7-9 the halo-staged tile kernel with
- * 1-3 persistent blocks per SM. */
+ * 1-3 persistent blocks per SM; 10 the warp-tiled kernel. */
 int h3c_autotune(h3c_solver s, int nsteps, int* choice, double* ms_per_step);
 
 /* ---- data: the tables create_local_cells/create_ghost_cells build
  * (solver.hpp:876-977) and the state columns lhs/rhs (container.hpp:59-60) ---- */
 int h3c_set_grid(h3c_solver s, const h3c_grid* grid);
-/* which: 0 = lhs, 1 = rhs.  Host arrays, caller numbering, [nv][ld]. */
+/* which: 0 = lhs, 1 = rhs.  Arrays in host or device memory, caller numbering, [nv][ld]. */
 int h3c_set_state(h3c_solver s, int which, const double* q, int64_t ld);
 int h3c_get_state(h3c_solver s, int which, double* q, int64_t ld);
 /* ---- output: Solver::write_domain (solver.hpp:328-376) ----
@@ -293,12 +293,14 @@ int h3c_launches(h3c_solver s, int64_t* n);
  *                     are read from global memory where a face needs them */
 #define H3C_OPT_HALO_SLOTS 6
 /* H3C_OPT_EULER_KERNEL  the Euler/AUSM stage kernel (with the tile kernels on): 0 the halo-staged
- *                       tile kernel when its tables exist, 1 the per-lane tile kernel, 2 (the
- *                       default) one thread per cell without shared memory, faces from both sides */
+ *                       tile kernel when its tables exist, 1 (the default) the per-lane tile kernel,
+ *                       2 one thread per cell, faces from both sides, 3 one warp per 32 Morton cells
+ *                       (each face state once per warp, each face between two of its cells once) */
 #define H3C_OPT_EULER_KERNEL 7
 int h3c_set_option(h3c_solver s, int option, int value);
 /* The Euler stage launch in use (no hom3 counterpart): info[0] kernel (0 per
- * cell, 1 per-lane tile, 2 halo-staged tile, 3 the per-cell AUSM kernel), [1] halo slots per tile, [2]
+ * cell, 1 per-lane tile, 2 halo-staged tile, 3 the per-cell AUSM kernel, 4 the warp-tiled AUSM
+ * kernel), [1] halo slots per tile, [2]
  * largest tile halo, [3] mean tile halo x 1000, [4] resident blocks per SM
  * of the halo-staged kernel, [5] blocks launched, [6] its dynamic shared
  * memory in bytes, [7] 256-cell tiles; the first n entries are written. */

@@ -387,3 +387,34 @@ def test_cht_adjoint_reverse_equals_dual_evaluation():
     assert np.array_equal(dts1, dts2)
     assert np.max(np.abs(gf1 - gf2)) <= 1e-12 * np.abs(gf2).max()
     assert np.max(np.abs(gs1 - gs2)) <= 1e-12 * np.abs(gs2).max()
+
+
+def test_autograd_function_cuda_tensors_stay_on_device():
+    """With CUDA tensors the state, output, cotangent and gradient move device
+    to device; the results are the host path's."""
+    import torch
+    from hom3_b200.autograd import solve
+    o, g, q1, lam = setup("euler2d_rk2")
+    q0 = torch.tensor(q1, device="cuda", requires_grad=True)
+    qn = solve(q0, g, NSTEPS, every=4)
+    assert qn.is_cuda
+    loss = (qn * torch.from_numpy(lam).cuda()).sum()
+    loss.backward()
+    assert q0.grad.is_cuda
+    _, g2, _, _ = setup("euler2d_rk2")
+    grad, _ = g2.adjoint(NSTEPS, lam, every=4)
+    assert np.array_equal(q0.grad.cpu().numpy(), grad)
+    _, g3, _, _ = setup("euler2d_rk2")
+    g3.solve(NSTEPS)
+    assert np.array_equal(qn.detach().cpu().numpy(), g3.state(0))
+
+
+def test_state_round_trip_through_device_memory():
+    import torch
+    o, g, q1, _ = setup("euler2d_rk2")
+    t = torch.tensor(q1, device="cuda")
+    g.set_state(t, 0)
+    back = torch.empty_like(t)
+    g.state(0, out=back)
+    assert torch.equal(back, t)
+    assert np.array_equal(g.state(0), q1)

@@ -1,6 +1,7 @@
 """The Euler/AUSM stage kernels against one another and the oracle: the
 halo-staged tile kernel (tile + halo copied into shared memory by bulk
-copies), the per-lane tile kernel and the per-cell kernel (the default).
+copies), the per-lane tile kernel (the default), the per-cell kernel and the
+warp-tiled kernel.
 
 Both kernels evaluate the same face fluxes F(l, r) from the same face states
 and sum them in hom3's order; the compiler may still fuse a product into a
@@ -78,17 +79,20 @@ def test_halo_kernel_uniform_and_periodic(nd, level):
     _same(a, b, o.first_ghost, "4 steps")
 
 
-def test_halo_kernel_partial_last_tile_against_oracle():
-    """A tree whose interior cell count is not a multiple of the tile size."""
+@pytest.mark.parametrize("kernel", [0, 3])
+def test_partial_last_tile_and_warp_against_oracle(kernel):
+    """A tree whose interior cell count is not a multiple of the tile size
+    (256) nor of the warp size (32): the last warp's missing cells include
+    ghost indices that must not be taken for cells of the warp."""
     w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=3)
     w.refine_sphere([0.3, 0.6, 0.5], 0.2, 5)
     o = w.add_solver(h3o.EULER, h3o.AUSM, h3o.RK2, bcs=cases.neumann_cube(w), ic_kind=h3o.IC_SHOCK_TUBE,
                      ic=[0, 0, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1], time_end=1.0, cfl=0.4)
     o.initialize()
-    assert o.first_ghost % 256 != 0
+    assert o.first_ghost % 32 != 0
     g = cases.gpu_solver_from_oracle(o)
-    g.set_option(F.OPT_EULER_KERNEL, 0)
-    assert g.kernel_info()["halo"] == 1
+    g.set_option(F.OPT_EULER_KERNEL, kernel)
+    assert g.kernel_info()["kernel"] == ("halo", "tile", "cell", "warp")[kernel]
     o.solve(1)
     g.solve(1)
     fg = o.first_ghost
@@ -99,11 +103,12 @@ def test_halo_kernel_partial_last_tile_against_oracle():
     assert rel_err(g.state(0)[:, :fg], o.state(0)[:, :fg]) <= 1e-10
 
 
-@pytest.mark.parametrize("kernel", [0, 2])
+@pytest.mark.parametrize("kernel", [0, 2, 3])
 @pytest.mark.parametrize("precision", [F.FP64, F.MIXED])
-def test_halo_and_per_cell_kernels_batches(precision, kernel):
-    """Batches of grids in the halo-staged (0) and per-cell (2) kernels
-    against the per-lane tile kernel."""
+def test_stage_kernels_batches(precision, kernel):
+    """Batches of grids (a warp's cells never span two grids) in the
+    halo-staged (0), per-cell (2) and warp-tiled (3) kernels against the
+    per-lane tile kernel."""
     from test_gpu_batch import members
     from hom3_b200.solver import euler_neumann
     ms, tables, states = members(7)
@@ -140,10 +145,12 @@ def test_halo_entries_beyond_shared_memory_read_from_global(slots):
     _same(a, b, o.first_ghost, f"{slots} slots")
 
 
+@pytest.mark.parametrize("kernel", [2, 3])
 @pytest.mark.parametrize("case", ["refined_rk2", "refined_fe_mixed", "explosion_rk3", "periodic_vortex"])
-def test_per_cell_ausm_kernel(case):
-    """The per-cell AUSM kernel (each face from both sides, no shared memory)
-    against the per-lane tile kernel and the oracle."""
+def test_per_cell_and_warp_ausm_kernels(case, kernel):
+    """The per-cell AUSM kernel (2: each face from both sides, no shared
+    memory) and the warp-tiled one (3: face states once per warp, each face
+    inside a warp once) against the per-lane tile kernel and the oracle."""
     precision = 1 if case.endswith("mixed") else 0
     if case.startswith("refined"):
         _, (o,) = cases.refined_case(ti=h3o.RK2 if "rk2" in case else h3o.EULER_FORWARD, level=3, fine=5)
@@ -152,8 +159,8 @@ def test_per_cell_ausm_kernel(case):
     else:
         _, (o,) = cases.periodic_vortex_case(level=6, ti=h3o.RK2)
     a, b = _pair(o, precision)
-    a.set_option(F.OPT_EULER_KERNEL, 2)  # the default
-    assert a.kernel_info()["kernel"] == "cell"
+    a.set_option(F.OPT_EULER_KERNEL, kernel)
+    assert a.kernel_info()["kernel"] == {2: "cell", 3: "warp"}[kernel]
     fg = o.first_ghost
     o.solve(1)
     a.solve(1)

@@ -62,7 +62,7 @@ def test_headline_tree_fp64_and_mixed_against_oracle(headline):
     vol = o.tables()["length"][:fg] ** 3
     g = cases.gpu_solver_from_oracle(o, 0)
     m = cases.gpu_solver_from_oracle(o, 1)
-    assert g.kernel_info()["kernel"] == "cell"
+    assert g.kernel_info()["kernel"] == "tile"
     assert abs(g.dt() - o.dt()) <= 1e-12 * o.dt()
     t0 = totals(o.state(0)[:, :fg], vol)
     o.solve(1)
@@ -87,17 +87,18 @@ def test_headline_tree_fp64_and_mixed_against_oracle(headline):
     assert g.status() == 0 and m.status() == 0
 
 
-@pytest.mark.parametrize("kernel", [0, 1])
+@pytest.mark.parametrize("kernel", [0, 2, 3])
 def test_headline_tree_other_stage_kernels_agree(headline, kernel):
-    """The halo-staged (0) and per-lane (1) tile kernels on the same tree agree
-    with the default per-cell kernel to rounding."""
+    """The halo-staged tile kernel (0), the per-cell kernel (2) and the
+    warp-tiled kernel (3) on the same tree agree with the default per-lane
+    tile kernel to rounding."""
     from hom3_b200 import _ffi as F
     _, o = headline
     fg = o.first_ghost
     a = cases.gpu_solver_from_oracle(o, 0)
     b = cases.gpu_solver_from_oracle(o, 0)
     b.set_option(F.OPT_EULER_KERNEL, kernel)
-    assert b.kernel_info()["kernel"] == ("halo", "tile")[kernel]
+    assert b.kernel_info()["kernel"] == ("halo", "tile", "cell", "warp")[kernel]
     a.solve(2)
     b.solve(2)
     assert rel_err(a.state(0)[:, :fg], b.state(0)[:, :fg]) <= 1e-13
