@@ -66,38 +66,64 @@ __global__ void __launch_bounds__(kBlock) k_ghost_slopes(const double* __restric
   }
 }
 
+// The slopes a face reads: the transverse slopes of momentum and density
+// (cns/physics.hpp:305-338 reads no energy slope), [sd][v] for v <= nd.
+template <int ND> constexpr int kCnsSlopeVars = ND + 1;
+
+// Shared memory of one block.  In FP64 the copies land in the primitive
+// rows themselves (the tile and first-layer cells' states are the first nv
+// rows of the primitives) and only the second layer has a landing area of
+// its own; in FP32 (R = float) the FP64 states land in a separate area.
+//   mbarrier (16) | [FP32: landing [nv][S] f64] | primitives [nv + nd + 2][S1] R |
+//   [FP64: second-layer landing [nv][S - S1] f64] | slopes [nd (nd + 1)][S1] R |
+//   plus fluxes [nv][256] f64 | neighbour slots [2][2nd][256] u16
+template <class R, int ND>
+__host__ __device__ constexpr bool cns_land_in_prims() {
+  return sizeof(R) == sizeof(double);
+}
 template <class R, int ND>
 __host__ __device__ constexpr size_t cns_layout_bytes(int hmax, int h1max) {
-  // mbarrier (16) | landing [nv][S] f64 | primitives [nv + nd + 2][S1] R | slopes [nd nv][S1] R |
-  // published plus fluxes [2][nv][256] f64 | neighbour slots [2][2nd][256] u16
-  return 16 + 8 * (size_t)(ND + 2) * (kHaloTile + hmax) +
-         sizeof(R) * (size_t)(2 * ND + 4 + ND * (ND + 2)) * (kHaloTile + h1max) + 2 * 8 * (size_t)(ND + 2) * kHaloTile +
+  return 16 + (cns_land_in_prims<R, ND>() ? 8 * (size_t)(ND + 2) * (hmax - h1max) : 8 * (size_t)(ND + 2) * (kHaloTile + hmax)) +
+         sizeof(R) * (size_t)(2 * ND + 4 + ND * kCnsSlopeVars<ND>) * (kHaloTile + h1max) + 8 * (size_t)(ND + 2) * kHaloTile +
          2 * 2 * (size_t)(2 * ND) * kHaloTile;
 }
 
+#ifndef H3C_CNS_MINB
+#define H3C_CNS_MINB 2  // blocks per SM the CNS tile kernel is register-budgeted for
+#endif
+
 template <int ND, class R, int MODE, bool FUSE>
-__global__ void __launch_bounds__(kHaloTile, 1)
+__global__ void __launch_bounds__(kHaloTile, H3C_CNS_MINB)
     k_stage_cns_halo(const double* __restrict__ qin, double* out, Geometry g, CnsHaloGeom ch, PhysConst pc,
                      const Scalars* __restrict__ sc, long long* dtmin, int* status) {
   constexpr int NV = ND + 2, NP = 2 * ND, TB = kHaloTile;
   constexpr int NPR = NV + ND + 2;  // q[nv], M[nd], p, a
-  constexpr int NSL = ND * NV;      // slopes [sd][v]
+  constexpr int SV = kCnsSlopeVars<ND>;
+  constexpr int NSL = ND * SV;      // slopes [sd][v], v <= nd
   constexpr int KH = kHaloMaxSlots / kHaloTile;
+  constexpr bool LIP = cns_land_in_prims<R, ND>();
   const HaloGeom& hg = ch.h;
-  const int S = TB + hg.hmax, S1 = TB + ch.h1max;
+  const int S = TB + hg.hmax, S1 = TB + ch.h1max, S2 = S - S1;
   extern __shared__ __align__(128) unsigned char smem[];
   unsigned long long* bar = reinterpret_cast<unsigned long long*>(smem);
-  double* land = reinterpret_cast<double*>(smem + 16);                           // [NV][S]
-  R* pr = reinterpret_cast<R*>(land + (size_t)NV * S);                          // [NPR][S1]
-  R* sl = pr + (size_t)NPR * S1;                                                 // [NSL][S1]
-  double* fx = reinterpret_cast<double*>(sl + (size_t)NSL * S1);                  // [2][NV][TB]
-  unsigned short* ln = reinterpret_cast<unsigned short*>(fx + 2 * NV * TB);       // [2][NP][TB]
+  double* land = reinterpret_cast<double*>(smem + 16);                           // FP32: [NV][S]
+  R* pr = reinterpret_cast<R*>(land + (LIP ? 0 : (size_t)NV * S));              // [NPR][S1]
+  double* land2 = reinterpret_cast<double*>(pr + (size_t)NPR * S1);             // FP64: [NV][S2]
+  R* sl = reinterpret_cast<R*>(land2 + (LIP ? (size_t)NV * S2 : 0));             // [NSL][S1]
+  double* fx = reinterpret_cast<double*>(sl + (size_t)NSL * S1);                  // [NV][TB]
+  unsigned short* ln = reinterpret_cast<unsigned short*>(fx + NV * TB);           // [2][NP][TB]
   const int tid = threadIdx.x;
   const long long ld = g.ld;
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
   const double h = g.len[0];  // single-level grid
   const double h2 = 2. * h;
   const R hr = (R)h;
+
+  // where the state of slot s (tile, first or second layer) lands
+  auto qslot = [&](int v, int s) -> double* {
+    if (LIP) return s < S1 ? reinterpret_cast<double*>(pr) + (size_t)v * S1 + s : land2 + (size_t)v * S2 + (s - S1);
+    return land + (size_t)v * S + s;
+  };
 
   long long tile = blockIdx.x;
   if (tile >= g.ntiles) return;
@@ -127,7 +153,7 @@ __global__ void __launch_bounds__(kHaloTile, 1)
       fence_proxy_async();
       mbar_expect_tx(bar, ncp * (8u * NV + 2u * NP));
 #pragma unroll
-      for (int v = 0; v < NV; ++v) bulk_g2s(land + (size_t)v * S, qin + v * ld + c0, ncp * 8u, bar);
+      for (int v = 0; v < NV; ++v) bulk_g2s(qslot(v, 0), qin + v * ld + c0, ncp * 8u, bar);
 #pragma unroll
       for (int p = 0; p < NP; ++p) bulk_g2s(ln + (buf * NP + p) * TB, hg.lnb + p * ld + c0, ncp * 2u, bar);
     }
@@ -137,18 +163,22 @@ __global__ void __launch_bounds__(kHaloTile, 1)
       if (hh < nh) {
         const long long n = hid[k];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) cp_async8(land + (size_t)v * S + TB + hh, qin + v * ld + n);
+        for (int v = 0; v < NV; ++v) cp_async8(qslot(v, TB + hh), qin + v * ld + n);
       }
     }
     cp_async_commit();
   };
-  // primitive variables of a state (make_prim, euler/physics.hpp:83-125) into slot s
-  auto store_prim = [&](const double* q, int s, Prim<R, ND>& P) {
+  // primitive variables of a state (make_prim, euler/physics.hpp:83-125) into slot s;
+  // in FP64 the state rows already hold q
+  auto store_prim = [&](const double* q, int s) {
+    Prim<R, ND> P;
 #pragma unroll
     for (int v = 0; v < NV; ++v) P.q[v] = (R)q[v];
     make_prim<R, ND>(P, gamma, gm1);
+    if (!LIP) {
 #pragma unroll
-    for (int v = 0; v < NV; ++v) pr[v * S1 + s] = P.q[v];
+      for (int v = 0; v < NV; ++v) pr[v * S1 + s] = P.q[v];
+    }
 #pragma unroll
     for (int d = 0; d < ND; ++d) pr[(NV + d) * S1 + s] = P.M[d];
     pr[(NV + ND) * S1 + s] = P.p;
@@ -164,13 +194,19 @@ __global__ void __launch_bounds__(kHaloTile, 1)
     P.p = pr[(NV + ND) * S1 + s];
     P.a = pr[(NV + ND + 1) * S1 + s];
   };
-  // the transverse slopes (sd != d, v <= nd) the viscous flux of direction d reads
+  // the transverse slopes (sd != d, v <= nd) the viscous flux of direction d
+  // reads, in the [sd][v] layout (v < nv) the viscous flux indexes
   auto load_slopes = [&](int s, int d, R* out_) {
 #pragma unroll
     for (int sd = 0; sd < ND; ++sd)
 #pragma unroll
       for (int v = 0; v < NV; ++v)
-        out_[sd * NV + v] = (sd != d && v <= ND) ? sl[(sd * NV + v) * S1 + s] : R(0);
+        out_[sd * NV + v] = (sd != d && v < SV) ? sl[(sd * SV + v) * S1 + s] : R(0);
+  };
+  // central slopes of slot s from its face-neighbour slots m, p along sd
+  auto store_slopes = [&](int s, int sd, int m, int p) {
+#pragma unroll
+    for (int v = 0; v < SV; ++v) sl[(sd * SV + v) * S1 + s] = (R)((*qslot(v, p) - *qslot(v, m)) / h2);
   };
   // the face flux F(l, r): AUSM + three-point viscous (cns/physics.hpp:155-161)
   auto face = [&](const Prim<R, ND>& L, const Prim<R, ND>& Rt, const R* sL, const R* sR, int d, R* f) {
@@ -181,33 +217,18 @@ __global__ void __launch_bounds__(kHaloTile, 1)
     for (int v = 0; v < NV; ++v) f[v] = f[v] + fv[v];
   };
 
-  int hid[KH], hid_n[KH];
+  int hid[KH];
   int o0, nh1;
   int nh = fetch_ids(tile, hid, o0, nh1);
   issue(tile, 0, hid, nh);
 
   for (int it = 0; tile < g.ntiles; tile += gridDim.x, ++it) {
-    const int buf = it & 1;
+    const int buf = LIP ? 0 : (it & 1);
     const long long next = tile + gridDim.x;
-    int nh_n = 0, o0_n = 0, nh1_n = 0;
-    if (next < g.ntiles) nh_n = fetch_ids(next, hid_n, o0_n, nh1_n);
-    // face-neighbour slots of the layer-1 cells this thread handles
-    unsigned short hn[KH][NP];
-#pragma unroll
-    for (int k = 0; k < KH; ++k) {
-      const int hh = tid + k * TB;
-#pragma unroll
-      for (int p = 0; p < NP; ++p) hn[k][p] = hh < nh1 ? __ldg(ch.hnb + (size_t)(o0 + hh) * NP + p) : 0xffff;
-    }
     const long long c0 = tile * TB, c = c0 + tid;
     const int inst = tile_instance(g, tile);
     const long long te = min(c0 + (long long)TB, instance_end(g, inst));
     const bool live = c < te;
-    double qo[NV];
-    if (MODE != 0 && live) {
-#pragma unroll
-      for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
-    }
 
     const bool ok = mbar_wait_bounded(bar, (unsigned)(it & 1));
     cp_async_wait_all();
@@ -218,19 +239,13 @@ __global__ void __launch_bounds__(kHaloTile, 1)
 
     // ---- primitives and slopes of the own cell and the layer-1 cells ----
     const unsigned short* L = ln + buf * NP * TB;
-    double qc[NV];
-    Prim<R, ND> Pc;
     if (live) {
+      double qc[NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) qc[v] = land[(size_t)v * S + tid];
-      store_prim(qc, tid, Pc);
+      for (int v = 0; v < NV; ++v) qc[v] = *qslot(v, tid);
+      store_prim(qc, tid);
 #pragma unroll
-      for (int sd = 0; sd < ND; ++sd) {
-        const int m = L[(2 * sd) * TB + tid], p = L[(2 * sd + 1) * TB + tid];
-#pragma unroll
-        for (int v = 0; v < NV; ++v)
-          sl[(sd * NV + v) * S1 + tid] = (R)((land[(size_t)v * S + p] - land[(size_t)v * S + m]) / h2);
-      }
+      for (int sd = 0; sd < ND; ++sd) store_slopes(tid, sd, L[(2 * sd) * TB + tid], L[(2 * sd + 1) * TB + tid]);
     }
 #pragma unroll
     for (int k = 0; k < KH; ++k) {
@@ -239,29 +254,34 @@ __global__ void __launch_bounds__(kHaloTile, 1)
         const int s = TB + hh;
         double qh[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) qh[v] = land[(size_t)v * S + s];
-        Prim<R, ND> P;
-        store_prim(qh, s, P);
+        for (int v = 0; v < NV; ++v) qh[v] = *qslot(v, s);
+        store_prim(qh, s);
         const long long n = hid[k];
         if (n >= g.n_int) {  // a ghost: the ghost-slope pass
 #pragma unroll
-          for (int j = 0; j < NSL; ++j) sl[j * S1 + s] = (R)__ldg(ch.gsl + j * ch.ngl + (n - g.n_int));
+          for (int sd = 0; sd < ND; ++sd)
+#pragma unroll
+            for (int v = 0; v < SV; ++v)
+              sl[(sd * SV + v) * S1 + s] = (R)__ldg(ch.gsl + (sd * NV + v) * ch.ngl + (n - g.n_int));
         } else {
 #pragma unroll
           for (int sd = 0; sd < ND; ++sd) {
-            const int m = hn[k][2 * sd], p = hn[k][2 * sd + 1];
-            if (m != 0xffff) {
-#pragma unroll
-              for (int v = 0; v < NV; ++v)
-                sl[(sd * NV + v) * S1 + s] = (R)((land[(size_t)v * S + p] - land[(size_t)v * S + m]) / h2);
-            }
+            const unsigned short m = __ldg(ch.hnb + (size_t)(o0 + hh) * NP + 2 * sd);
+            const unsigned short p = __ldg(ch.hnb + (size_t)(o0 + hh) * NP + 2 * sd + 1);
+            if (m != 0xffff) store_slopes(s, sd, m, p);
           }
         }
       }
     }
-    __syncthreads();  // landing area consumed; primitives and slopes complete
+    __syncthreads();  // primitives and slopes complete
 
-    if (next < g.ntiles) issue(next, buf ^ 1, hid_n, nh_n);
+    int hid_n[KH], o0_n = 0, nh1_n = 0, nh_n = 0;
+    if (!LIP) {  // FP32: the next tile lands in its own area while this one's fluxes run
+      if (next < g.ntiles) {
+        nh_n = fetch_ids(next, hid_n, o0_n, nh1_n);
+        issue(next, buf ^ 1, hid_n, nh_n);
+      }
+    }
 
     // ---- fluxes, direction by direction ----
     double acc[NV];
@@ -269,31 +289,32 @@ __global__ void __launch_bounds__(kHaloTile, 1)
     for (int v = 0; v < NV; ++v) acc[v] = 0.0;
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
-      double* X = fx + (d & 1) * NV * TB;
-      R slc[NSL];
       if (live) {
-        load_slopes(tid, d, slc);
+        Prim<R, ND> Pc, Pn;
+        load_prim_s(tid, d, Pc);
         const int p = L[(2 * d + 1) * TB + tid];
-        Prim<R, ND> Pn;
         load_prim_s(p, d, Pn);
-        R sn[NSL];
+        R slc[ND * NV], sn[ND * NV];
+        load_slopes(tid, d, slc);
         load_slopes(p, d, sn);
         R f[NV];
         face(Pc, Pn, slc, sn, d, f);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) X[v * TB + tid] = (double)f[v];
+        for (int v = 0; v < NV; ++v) fx[v * TB + tid] = (double)f[v];
       }
-      __syncthreads();
+      __syncthreads();  // this direction's plus faces are published
       if (live) {
         const int m = L[(2 * d) * TB + tid];
         double fm[NV];
         if (m < TB && L[(2 * d + 1) * TB + m] == tid) {
 #pragma unroll
-          for (int v = 0; v < NV; ++v) fm[v] = X[v * TB + m];
+          for (int v = 0; v < NV; ++v) fm[v] = fx[v * TB + m];
         } else {
-          Prim<R, ND> Pn;
+          Prim<R, ND> Pc, Pn;
+          load_prim_s(tid, d, Pc);
           load_prim_s(m, d, Pn);
-          R sn[NSL];
+          R slc[ND * NV], sn[ND * NV];
+          load_slopes(tid, d, slc);
           load_slopes(m, d, sn);
           R f[NV];
           face(Pn, Pc, sn, slc, d, f);
@@ -302,8 +323,9 @@ __global__ void __launch_bounds__(kHaloTile, 1)
         }
         // the own plus flux as published (a rounded value: no FMA with this sum, as in the per-cell kernel)
 #pragma unroll
-        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - X[v * TB + tid]);
+        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - fx[v * TB + tid]);
       }
+      __syncthreads();  // the next direction rewrites the plus faces
     }
 
     // ---- update and the next step's CFL minimum ----
@@ -312,6 +334,13 @@ __global__ void __launch_bounds__(kHaloTile, 1)
     if (live) {
       const double dt = sc[inst].dt;
       const double k = dt / h;
+      double qc[NV], qo[NV];  // FP32: the landing area already holds the next tile
+#pragma unroll
+      for (int v = 0; v < NV; ++v) qc[v] = LIP ? *qslot(v, tid) : __ldg(qin + v * ld + c);
+      if (MODE != 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
+      }
       double o[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], qc[v], k * acc[v]);
@@ -326,11 +355,19 @@ __global__ void __launch_bounds__(kHaloTile, 1)
       flag_bad_state(bad, sc, inst);
       block_min_atomic(ord, per_instance(dtmin, inst));
     }
-    nh = nh_n;
-    o0 = o0_n;
-    nh1 = nh1_n;
+    if (LIP) {  // FP64: the next tile lands where this one's primitives were
+      __syncthreads();
+      if (next < g.ntiles) {
+        nh = fetch_ids(next, hid, o0, nh1);
+        issue(next, 0, hid, nh);
+      }
+    } else {
+      nh = nh_n;
+      o0 = o0_n;
+      nh1 = nh1_n;
 #pragma unroll
-    for (int k = 0; k < KH; ++k) hid[k] = hid_n[k];
+      for (int k = 0; k < KH; ++k) hid[k] = hid_n[k];
+    }
   }
 }
 

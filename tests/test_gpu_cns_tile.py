@@ -61,14 +61,17 @@ def test_cns_tile_equals_per_cell_2d_conditions(name):
         _same(a, b, o.first_ghost, f"{name}: {n} steps")
 
 
+@pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("grid", [1, 5, 0])
-def test_cns_tile_any_persistent_grid(grid):
+def test_cns_tile_any_persistent_grid(grid, precision):
+    """Blocks looping over several tiles: each tile's copies land while (FP32)
+    or after (FP64) the previous tile's fluxes run."""
     _, (o,) = cases.tgv_case(level=4, ti=h3o.RK2)
-    a, b = _pair(o)
+    a, b = _pair(o, precision)
     a.set_persistent_blocks(grid)
     a.solve(3)
     b.solve(3)
-    _same(a, b, o.first_ghost, f"grid {grid}")
+    _same(a, b, o.first_ghost, f"grid {grid}", precision)
 
 
 def test_cns_tile_against_oracle_tgv():
