@@ -534,8 +534,114 @@ def run_tgv(args, ws, rank, local):
                             "unit": "GB/s", "frac": ach / peak, "peak_source": peak_kind,
                             "algorithmic_bytes_per_launch": fg * 3 * 5 * 8, "avg_launch_ms": st2_ms / st2_n,
                             "step_frac": fg * 200 / (out["fp64"]["ms"] / args.steps * 1e-3) / 1e9 / peak}
+    if args.tgv_end > 0 and ws == 1:
+        line["long_run"] = tgv_long_record(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def tgv_long_record(args):
+    """The Taylor-Green vortex as its configuration specifies it: the oracle's
+    tree, conditions and cell-averaged initial state handed to the library
+    through the C ABI (FP64 and mixed), the kinetic-energy dissipation rate
+    -dKE/dt of the first `tgv_oracle_steps` steps against the FP64 oracle,
+    then both GPU paths to `tgv_end` convective time units (t U / L with
+    U = 0.1, L = 1: 10 units = 100 time units) with KE sampled along the way."""
+    import torch
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200.solver import Condition
+    from oracle import h3o
+
+    h3o.set_num_threads(os.cpu_count() or 1)
+    t0 = time.perf_counter()
+    w = h3o.World(3, [0, 0, 0], [2 * math.pi] * 3, level=args.tgv_level)
+    bcs = [h3o.bc(h3o.BC_PERIODIC, g) for g in w.cube_boundaries()]
+    o = w.add_solver(h3o.CNS, h3o.AUSM, h3o.RK2, bcs=bcs, ic_kind=h3o.IC_TAYLOR_GREEN, ic=[0.1, 1.0, 1 / 1.4],
+                     Minfty=0.1, ReInfty=1600.0, Pr0=0.71, cfl=0.5, cfl_viscous=0.4, time_end=1e30, gamma=1.4,
+                     Rspecific=287.058, T0=273.15, rho0=1.225, Sutherland0=110.4)
+    o.initialize()
+    setup_s = time.perf_counter() - t0
+    info, tab = o.info(), o.tables()
+    fg = o.first_ghost
+    props = {k: info[k] for k in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty", "ReInfty",
+                                  "Pr0", "Sutherland0", "time_end")}
+
+    def gpu(prec):
+        g = hb.Solver(3, info["physics"], info["flux"], info["ti"], prec, **props)
+        g.set_grid(tab["neighbors"], tab["x_center"], tab["length"], tab["bc_idx"], fg,
+                   [Condition(k, v) for k, v in info["bcs"]], tab["subface_cells"])
+        g.set_periodic(o.partner_cells())
+        g.set_state(o.state(0), 0)
+        g.reset_time()
+        return g
+
+    def ke(q):
+        q = q[:, :fg]
+        return float((0.5 * (q[0] ** 2 + q[1] ** 2 + q[2] ** 2) / q[3]).mean())
+
+    g64, gmx = gpu(F.FP64), gpu(F.MIXED)
+    # ---- the first steps against the oracle ----
+    k = args.tgv_oracle_steps
+    series = {"oracle": [(0.0, ke(o.state(0)))], "fp64": [(0.0, ke(g64.state(0)))], "mixed": [(0.0, ke(gmx.state(0)))]}
+    t1 = time.perf_counter()
+    for _ in range(k):
+        o.solve(1)
+        series["oracle"].append((o.time(), ke(o.state(0))))
+    oracle_s = time.perf_counter() - t1
+    for name, g in (("fp64", g64), ("mixed", gmx)):
+        for _ in range(k):
+            g.solve(1)
+            series[name].append((g.time(), ke(g.state(0))))
+
+    def rates(ser):
+        return [-(b[1] - a[1]) / (b[0] - a[0]) for a, b in zip(ser[:-1], ser[1:])]
+
+    eps = {n: rates(v) for n, v in series.items()}
+    rec = {"cells": int(fg), "oracle_steps": k, "oracle_setup_s": setup_s, "oracle_s": oracle_s,
+           "oracle_threads": os.cpu_count() or 1}
+    if k > 0:
+        scale = max(abs(e) for e in eps["oracle"])
+        rec["eps_oracle"] = eps["oracle"]
+        rec["eps_rel_diff_fp64_vs_oracle"] = max(abs(a - b) for a, b in zip(eps["fp64"], eps["oracle"])) / scale
+        rec["eps_rel_diff_mixed_vs_oracle"] = max(abs(a - b) for a, b in zip(eps["mixed"], eps["oracle"])) / scale
+        qo = o.state(0)[:, :fg]
+        rec["state_max_rel_fp64_vs_oracle"] = float(np.abs(g64.state(0)[:, :fg] - qo).max() / np.abs(qo).max())
+        rec["state_l2_rel_mixed_vs_oracle"] = float(np.sqrt(((gmx.state(0)[:, :fg] - qo) ** 2).sum() / (qo ** 2).sum()))
+    del o, w
+    # ---- both GPU paths on to the end time, KE sampled every `every` steps ----
+    t_end = args.tgv_end / 0.1
+    every = 50
+    for name, g in (("fp64", g64), ("mixed", gmx)):
+        ser = [series[name][-1]]
+        stream = torch.cuda.ExternalStream(g.stream())
+        steps, dev_ms = 0, 0.0
+        while g.time() < t_end:
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            g.solve(every)
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            dev_ms += ev0.elapsed_time(ev1)
+            steps += every
+            ser.append((g.time(), ke(g.state(0))))
+        e = rates(ser)
+        i = int(np.argmax(e)) if e else 0
+        rec[name] = {"steps": steps + k, "time": g.time(), "convective_time": g.time() * 0.1,
+                     "device_ms": dev_ms, "value": fg * steps / (dev_ms * 1e-3) if dev_ms else None,
+                     "ke_end": ser[-1][1], "ke_start": series[name][0][1],
+                     "eps_peak": e[i] if e else None,
+                     "eps_peak_convective_time": 0.5 * (ser[i][0] + ser[i + 1][0]) * 0.1 if e else None,
+                     "samples": [(round(a * 0.1, 4), b) for a, b in ser[:: max(1, len(ser) // 40)]]}
+        series[name + "_long"] = ser
+    a, b = rates(series["fp64_long"]), rates(series["mixed_long"])
+    m = min(len(a), len(b))
+    if m:
+        rec["eps_rel_diff_mixed_vs_fp64"] = max(abs(x - y) for x, y in zip(a[:m], b[:m])) / max(abs(x) for x in a[:m])
+    rec["what"] = ("KE = mean of rho |u|^2 / 2 over the cells; eps = -dKE/dt between samples (every step against "
+                   "the oracle, every 50 steps to the end); tables and initial state are the oracle's")
+    return rec
 
 
 def run_vortex(args, ws, rank, local):
@@ -1001,6 +1107,10 @@ def main():
     ap.add_argument("--adv-level", type=int, default=11)
     ap.add_argument("--vortex-level", type=int, default=8)
     ap.add_argument("--tgv-level", type=int, default=7)
+    ap.add_argument("--tgv-end", type=float, default=0.0,
+                    help="TGV: also run from the oracle's state to this convective time (0: timing only)")
+    ap.add_argument("--tgv-oracle-steps", type=int, default=3,
+                    help="TGV long run: steps compared with the FP64 oracle before the GPU-only run")
     ap.add_argument("--members", type=int, default=256)
     ap.add_argument("--adjoint-steps", type=int, default=50)
     args = ap.parse_args()
