@@ -644,6 +644,66 @@ def tgv_long_record(args):
     return rec
 
 
+def run_decomposed(args, ws, rank, local):
+    """The default workload's one grid split over the ranks (hom3_b200/domain.py):
+    each rank steps one Morton-range subdomain; before every stage the ranks
+    exchange the cells their faces read (NCCL send/recv of device buffers),
+    and before every step they take the minimum time step (NCCL all-reduce).
+    Strong scaling: the total work is the one grid whatever N.  Device time
+    with CUDA events on each rank's stream, max over ranks."""
+    import torch
+    import torch.distributed as dist
+
+    import hom3_b200 as hb
+    from hom3_b200 import _ffi as F
+    from hom3_b200 import domain
+    from hom3_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    spec = W.riemann3d_spec(args.base_level, args.extra_levels)
+    t = hb.build_tables(spec, spec.cube_boundaries())
+    fg = t["first_ghost"]
+    q = np.zeros((5, t["ncells"]))
+    q[:, :fg] = hb.cell_average(W.riemann3d_ic(W.fourier_modes()), t["x_center"][:, :fg], t["length"][:fg], 3)
+    prec = F.MIXED if args.precision == "mixed" else F.FP64
+
+    def make():
+        return hb.Solver(3, F.EULER, F.FLUX_AUSM, F.RUNGE_KUTTA_2, prec, cfl=args.cfl, time_end=1e30)
+
+    group = dist.group.WORLD if ws > 1 else None
+    if ws == 1:  # one rank: a process group of one, so the same exchange code runs
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ.setdefault("MASTER_PORT", "29533")
+        dist.init_process_group("gloo", rank=0, world_size=1)
+    d = domain.DomainSolver(t, 3, make, W.riemann3d_conditions(), rank, ws, group)
+    d.set_state(q)
+    stream = torch.cuda.ExternalStream(d.s.stream())
+    d.solve(args.warmup)
+    torch.cuda.synchronize()
+    barrier(ws)
+    with ClockSampler(local) as clk:
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        d.solve(args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = allreduce_max(ev0.elapsed_time(ev1), ws)
+    halo = d.sub.halo.size
+    line = {"metric": "cell-updates/s", "value": fg * args.steps / (ms * 1e-3), "unit": "cell-updates/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f64" if prec == F.FP64 else "f32-flux/f64-state", "data": "synthetic",
+            "config": dict(workload_config(args, t), parallelism=f"domain decomposition x{ws}"),
+            "cells_per_rank": int(d.sub.cells.size), "exchange_ghosts_rank0": int(halo),
+            "clocks": clk.summary(),
+            "what": "one grid split along the Morton order; per stage an exchange of the cells each "
+                    "subdomain's faces read, per step an all-reduce of the minimum time step"}
+    if ws == 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def run_vortex(args, ws, rank, local):
     """2D Euler isentropic vortex on a uniform 256^2 grid over [0, 10]^2,
     periodic, beta 5, centre (5, 5), free stream rho = u = v = p = 1, CFL 0.5:
@@ -1098,6 +1158,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-ensemble record")
     ap.add_argument("--halo-kernel", type=int, default=None,
                     help="1: stage tiles into shared memory (the library's default), 0: the kernels without it")
+    ap.add_argument("--decompose", action="store_true",
+                    help="split the default workload's one grid over the N ranks (strong scaling) "
+                         "instead of running N replicas")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the library's default Euler stage launch instead of h3c_autotune's choice")
     ap.add_argument("--euler-kernel", type=int, default=None,
@@ -1118,6 +1181,9 @@ def main():
     ws, rank, local = dist_setup()
     if args.workload == "ensemble" and args.impl == "ours":
         run_ensemble(args, ws, rank, local)
+        return
+    if args.decompose and args.impl == "ours":
+        run_decomposed(args, ws, rank, local)
         return
     if args.workload == "tgv" and args.impl == "ours":
         run_tgv(args, ws, rank, local)

@@ -21,7 +21,7 @@ FP64, MIXED = 0, 1
 (BC_EULER_NEUMANN, BC_EULER_DIRICHLET, BC_EULER_VORTEX, BC_CNS_INFLOW, BC_CNS_OUTFLOW,
  BC_CNS_ADIABATIC_NOSLIP, BC_CNS_ADIABATIC_SLIP, BC_CNS_ISOTHERMAL_NOSLIP, BC_HEAT_DIRICHLET,
  BC_HEAT_NEUMANN, BC_CPL_EULER_EULER, BC_CPL_CNS_HEAT, BC_CPL_HEAT_CNS, BC_CPL_HEAT_HEAT,
- BC_PERIODIC, BC_ADV_DIRICHLET, BC_ADV_NEUMANN, BC_ADV_CHARACTERISTIC) = range(18)
+ BC_PERIODIC, BC_ADV_DIRICHLET, BC_ADV_NEUMANN, BC_ADV_CHARACTERISTIC, BC_EXCHANGE) = range(19)
 SDF_NONE, SDF_EDGE, SDF_SQUARE, SDF_SPHERE = range(4)
 (OPT_TILE_KERNEL, OPT_GRAPHS, OPT_HALO_KERNEL, OPT_PERSISTENT_BLOCKS, OPT_CNS_ADJOINT_DUAL,
  OPT_HALO_SLOTS, OPT_EULER_KERNEL) = 1, 2, 3, 4, 5, 6, 7
@@ -79,6 +79,10 @@ SIGNATURES = {
     "h3c_get_stream": (_i32, [_vp, _P(_vp)]),
     "h3c_sizes": (_i32, [_vp, _P(_i64), _P(_i64), _P(_i32)]),
     "h3c_solve": (_i32, [_vp, _i64]),
+    "h3c_stages": (_i32, [_vp, _P(_i32)]),
+    "h3c_solve_stage": (_i32, [_vp, _i32]),
+    "h3c_stage_input": (_i32, [_vp, _i32, _P(_P(_dbl))]),
+    "h3c_dtmin_device": (_i32, [_vp, _P(_P(_i64))]),
     "h3c_reset_time": (_i32, [_vp]),
     "h3c_apply_bcs": (_i32, [_vp, _i32]),
     "h3c_min_dt": (_i32, [_vp, _P(_dbl)]),

@@ -29,7 +29,7 @@ enum BcKind {
   BC_CNS_OUTFLOW = 4, BC_CNS_ADIABATIC_NOSLIP = 5, BC_CNS_ADIABATIC_SLIP = 6,
   BC_CNS_ISOTHERMAL_NOSLIP = 7, BC_HEAT_DIRICHLET = 8, BC_HEAT_NEUMANN = 9,
   BC_CPL_EULER_EULER = 10, BC_CPL_CNS_HEAT = 11, BC_CPL_HEAT_CNS = 12, BC_CPL_HEAT_HEAT = 13,
-  BC_PERIODIC = 14, BC_ADV_DIRICHLET = 15, BC_ADV_NEUMANN = 16, BC_ADV_CHARACTERISTIC = 17
+  BC_PERIODIC = 14, BC_ADV_DIRICHLET = 15, BC_ADV_NEUMANN = 16, BC_ADV_CHARACTERISTIC = 17, BC_EXCHANGE = 18
 };
 
 // Device-resident step scalars (solver.hpp:406-416) and reduction slots.
@@ -516,6 +516,7 @@ __global__ void __launch_bounds__(kBlock) k_bc(double* __restrict__ q, const dou
   const int b = gt.bc_apply[i];
   if (b == 255) return;
   const BcParam& B = gt.bcs[b];
+  if (B.kind == BC_EXCHANGE) return;  // written by the caller (another solver's cells)
   const long long gcell = g.n_int + i;
   const int bc = gt.bndry[i];
   const long long ld = g.ld;

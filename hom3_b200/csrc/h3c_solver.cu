@@ -127,6 +127,7 @@ struct h3c_solver_s {
   StepGraph graph8[2], graph1[2];
   long long graph_per_step = 0;  // kernel launches one captured step holds
   bool plain_done = false;  // a step ran outside capture (kernel attributes are set)
+  int stage_next = 0;       // the next part of a step run by parts (h3c_solve_stage); 0 between steps
   // coupled conjugate-heat steps (h3c_cht_solve) captured with the heat partner
   cudaGraphExec_t cpl_graph = nullptr;
   h3c_solver cpl_with = nullptr;
@@ -191,6 +192,7 @@ void drop_graph(h3c_solver s) {
 
 void free_grid(h3c_solver s) {
   drop_graph(s);
+  s->stage_next = 0;
   dfree(s->d_nbr); dfree(s->d_lvl); dfree(s->d_sub); dfree(s->d_gbndry); dfree(s->d_gpos);
   dfree(s->d_gapply); dfree(s->d_gown); dfree(s->d_gdx); dfree(s->d_gpartner); dfree(s->d_xc);
   dfree(s->d_bcs); dfree(s->d_q[0]); dfree(s->d_q[1]); dfree(s->d_q[2]); dfree(s->d_slopes); dfree(s->d_stage);
@@ -869,10 +871,10 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   for (size_t q = 0; q < ubcs.size(); ++q) {
     BcParam& B = s->h_bcs[q];
     B.kind = ubcs[q].kind;
-    if (B.kind < 0 || B.kind > H3C_BC_ADV_CHARACTERISTIC)
+    if (B.kind < 0 || B.kind > H3C_BC_EXCHANGE)
       return s->fail(H3C_E_INVALID, "h3c_set_grid: bc kind %d", B.kind);
-    const bool adv_kind = B.kind >= H3C_BC_ADV_DIRICHLET;
-    if (adv_kind != (s->desc.physics == H3C_ADVECTION) && B.kind != H3C_BC_PERIODIC)
+    const bool adv_kind = B.kind >= H3C_BC_ADV_DIRICHLET && B.kind <= H3C_BC_ADV_CHARACTERISTIC;
+    if (adv_kind != (s->desc.physics == H3C_ADVECTION) && B.kind != H3C_BC_PERIODIC && B.kind != H3C_BC_EXCHANGE)
       return s->fail(H3C_E_INVALID, "h3c_set_grid: bc kind %d does not belong to this physics", B.kind);
     B.wall = (B.kind == H3C_BC_CNS_ADIABATIC_NOSLIP || B.kind == H3C_BC_CNS_ISOTHERMAL_NOSLIP ||
               B.kind == H3C_BC_CPL_CNS_HEAT);
@@ -888,6 +890,11 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   }
   if (ninst > 1 && (s->needs_partner || s->needs_periodic))
     return s->fail(H3C_E_INVALID, "h3c_set_grids: coupling and periodic conditions need a single grid");
+  for (const BcParam& B : s->h_bcs)
+    if (B.kind == H3C_BC_EXCHANGE &&
+        (s->desc.physics == H3C_CNS || s->desc.reconstruction == H3C_RECON_MUSCL))
+      return s->fail(H3C_E_INVALID, "h3c_set_grid: exchange ghosts need a first-order flux without cell slopes "
+                                    "(not CNS, not MUSCL): their slopes would be the neighbouring subdomain's");
   s->dev2caller = dev2caller;
   s->caller2dev = caller2dev;
   s->partner = nullptr;
@@ -1261,6 +1268,7 @@ int h3c_reset_time(h3c_solver s) {
   if (!s) return H3C_E_INVALID;
   if (s->ng < 0) return H3C_E_INVALID;
   if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_reset_time: no grid");
+  s->stage_next = 0;  // a step run by parts starts over
   k_init_time<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, s->desc.time_end, s->n_inst);
   launch_cfl(s, &s->d_sc->dtmin_ord);
   k_set_dt<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, 0, s->n_inst);
@@ -1288,50 +1296,69 @@ static void prepare_stage(h3c_solver s, const double* q, int which) {
 // One solver step (solver.hpp:140-145) on the solver's buffers.  keep (may be
 // null) receives copies of the ghost-filled stage inputs in consecutive
 // nv * ld slots; dts (may be null) records the step's dt at index i.
-static void enqueue_step(h3c_solver s, bool fuse, double* keep, double* dts, long long i) {
+// Stages per step of the time integration.
+static int stage_count(const h3c_solver s) {
+  const int ti = s->desc.time_integration;
+  return ti == H3C_EULER_FORWARD ? 1 : ti == H3C_RUNGE_KUTTA_2 ? 2 : 3;
+}
+
+// Part k of one step (k = 0 .. stage_count - 1, in order): k = 0 applies the
+// conditions to lhs and sets the step's dt; k > 0 applies the conditions to
+// its stage input; every part then runs its stage; the last part advances
+// time and step.  keep (optional) receives each stage's input; dts (optional)
+// records the step's dt at index i.
+static void enqueue_stage(h3c_solver s, int k, bool fuse, double* keep, double* dts, long long i) {
   const size_t Qb = sizeof(double) * s->nv * s->ld;
   const long long Q = s->nv * s->ld;
-  launch_bc(s, 0);
-  if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
-  {
-    Launch L(s, K_SCALAR);
-    k_set_dt<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, 1, s->n_inst);
-  }
-  if (dts) {
-    Launch L(s, K_SCALAR);
-    k_record_dt<<<1, 1, 0, s->stream>>>(s->d_sc, dts, i);
-  }
-  if (keep) cudaMemcpyAsync(keep, s->d_q[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
-  prepare_stage(s, s->d_q[0], 0);
   const int ti = s->desc.time_integration;
-  if (ti == H3C_EULER_FORWARD) {
-    // evolve(euler_forward): solver.hpp:470-479 (rhs = lhs + R; lhs = rhs as a buffer swap)
-    launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
-    std::swap(s->d_q[0], s->d_q[1]);
-  } else if (ti == H3C_RUNGE_KUTTA_2) {
-    // evolve(runge_kutta_2): solver.hpp:483-494
-    launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
+  const int last = stage_count(s) - 1;
+  if (k == 0) {
+    launch_bc(s, 0);
+    if (!fuse) launch_cfl(s, &s->d_sc->dtmin_ord);
+    {
+      Launch L(s, K_SCALAR);
+      k_set_dt<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, 1, s->n_inst);
+    }
+    if (dts) {
+      Launch L(s, K_SCALAR);
+      k_record_dt<<<1, 1, 0, s->stream>>>(s->d_sc, dts, i);
+    }
+    if (keep) cudaMemcpyAsync(keep, s->d_q[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
+    prepare_stage(s, s->d_q[0], 0);
+    if (ti == H3C_EULER_FORWARD) {
+      // evolve(euler_forward): solver.hpp:470-479 (rhs = lhs + R; lhs = rhs as a buffer swap)
+      launch_stage(s, 0, s->d_q[0], s->d_q[1], fuse);
+      std::swap(s->d_q[0], s->d_q[1]);
+    } else {
+      // evolve(runge_kutta_2): solver.hpp:483-494, and the first SSP-RK3 stage
+      launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
+    }
+  } else if (k == 1) {
     launch_bc(s, 1);
     if (keep) cudaMemcpyAsync(keep + Q, s->d_q[1], Qb, cudaMemcpyDeviceToDevice, s->stream);
-    prepare_stage(s, s->d_q[1], 1);
-    launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
+    if (ti == H3C_RUNGE_KUTTA_2) {
+      prepare_stage(s, s->d_q[1], 1);
+      launch_stage(s, 2, s->d_q[1], s->d_q[0], fuse);
+    } else {
+      // EXTENSION: SSP-RK3, conditions before every stage
+      cudaMemcpyAsync(s->d_q[2], s->d_q[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
+      prepare_stage(s, s->d_q[1], 1);
+      launch_stage(s, 3, s->d_q[1], s->d_q[2], false);
+    }
   } else {
-    // EXTENSION: SSP-RK3, conditions before every stage
-    launch_stage(s, 0, s->d_q[0], s->d_q[1], false);
-    launch_bc(s, 1);
-    if (keep) cudaMemcpyAsync(keep + Q, s->d_q[1], Qb, cudaMemcpyDeviceToDevice, s->stream);
-    cudaMemcpyAsync(s->d_q[2], s->d_q[0], Qb, cudaMemcpyDeviceToDevice, s->stream);
-    prepare_stage(s, s->d_q[1], 1);
-    launch_stage(s, 3, s->d_q[1], s->d_q[2], false);
     launch_bc(s, 2);
     if (keep) cudaMemcpyAsync(keep + 2 * Q, s->d_q[2], Qb, cudaMemcpyDeviceToDevice, s->stream);
     prepare_stage(s, s->d_q[2], 2);
     launch_stage(s, 4, s->d_q[2], s->d_q[0], fuse);
   }
-  {
+  if (k == last) {
     Launch L(s, K_SCALAR);
     k_advance<<<blocks(s->n_inst), kBlock, 0, s->stream>>>(s->d_sc, s->n_inst);
   }
+}
+
+static void enqueue_step(h3c_solver s, bool fuse, double* keep, double* dts, long long i) {
+  for (int k = 0; k < stage_count(s); ++k) enqueue_stage(s, k, fuse, keep, dts, i);
 }
 
 static void enqueue_steps(h3c_solver s, int64_t nsteps) {
@@ -1412,6 +1439,8 @@ static bool launch_graph(h3c_solver s, const StepGraph* g, int n) {
 int h3c_solve(h3c_solver s, int64_t nsteps) {
   if (!s || nsteps < 0) return H3C_E_INVALID;
   if (int rc = ready(s, "h3c_solve")) return rc;
+  if (s->stage_next != 0)
+    return s->fail(H3C_E_STATE, "h3c_solve: a step run by parts is at part %d (h3c_solve_stage)", s->stage_next);
   // Steps replay captured graphs (no per-launch host cost) once one step has
   // run plainly (kernel attributes are set outside capture); coupled solvers
   // read their partner's current buffers and profiling brackets every
@@ -1434,6 +1463,37 @@ int h3c_solve(h3c_solver s, int64_t nsteps) {
     s->plain_done = true;
   }
   return s->cuda(cudaGetLastError(), "h3c_solve");
+}
+
+int h3c_stages(h3c_solver s, int* n) {
+  if (!s || !n) return H3C_E_INVALID;
+  *n = stage_count(s);
+  return H3C_OK;
+}
+
+int h3c_solve_stage(h3c_solver s, int k) {
+  if (!s) return H3C_E_INVALID;
+  if (int rc = ready(s, "h3c_solve_stage")) return rc;
+  if (k != s->stage_next)
+    return s->fail(H3C_E_STATE, "h3c_solve_stage: part %d requested, part %d is next", k, s->stage_next);
+  enqueue_stage(s, k, !s->unfused_dt, nullptr, nullptr, 0);
+  s->stage_next = k + 1 == stage_count(s) ? 0 : k + 1;
+  return s->cuda(cudaGetLastError(), "h3c_solve_stage");
+}
+
+int h3c_stage_input(h3c_solver s, int k, double** ptr) {
+  if (!s || !ptr || k < 0 || k >= stage_count(s)) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_stage_input: no grid");
+  *ptr = s->d_q[k];  // lhs, rhs, third buffer: the inputs of parts 0, 1, 2
+  return H3C_OK;
+}
+
+int h3c_dtmin_device(h3c_solver s, int64_t** ptr) {
+  if (!s || !ptr) return H3C_E_INVALID;
+  if (!s->has_grid) return s->fail(H3C_E_STATE, "h3c_dtmin_device: no grid");
+  static_assert(sizeof(long long) == sizeof(int64_t), "ordered bits");
+  *ptr = reinterpret_cast<int64_t*>(&s->d_sc->dtmin_ord);
+  return H3C_OK;
 }
 
 static int read_scalars(h3c_solver s, Scalars* out) {

@@ -43,6 +43,19 @@ def _lp(a):
 # ---------------------------------------------------------------------------
 # geometry (geometry/implicit.hpp:39-205) and conditions
 # ---------------------------------------------------------------------------
+class _DeviceArray:
+    """A device pointer presented through __cuda_array_interface__ (torch.as_tensor makes a view of it)."""
+
+    def __init__(self, ptr, shape, typestr):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 3, "strides": None}
+
+
+def _device_view(ptr, shape, typestr):
+    import torch
+    return torch.as_tensor(_DeviceArray(ptr, shape, typestr), device="cuda")
+
+
 def _sdf(kind, p, inverted=False) -> F.Sdf:
     s = F.Sdf()
     s.kind = kind
@@ -304,6 +317,31 @@ class Solver:
     def set_persistent_blocks(self, n):
         """Blocks of the Euler/AUSM stage launch (0: the library's default)."""
         self.set_option(F.OPT_PERSISTENT_BLOCKS, n)
+
+    # ---- stepping by parts (one grid split over several solvers) ----
+    def stages(self) -> int:
+        """Stages per step (h3c_stages)."""
+        v = C.c_int()
+        self._check(lib().h3c_stages(self.h, C.byref(v)))
+        return v.value
+
+    def solve_stage(self, k):
+        """Part k of one step (h3c_solve_stage)."""
+        self._check(lib().h3c_solve_stage(self.h, k))
+
+    def stage_input(self, k):
+        """Part k's input state as a float64 CUDA tensor view [nv][ld] in the
+        internal numbering (h3c_stage_input)."""
+        p = C.POINTER(C.c_double)()
+        self._check(lib().h3c_stage_input(self.h, k, C.byref(p)))
+        _, ld = self.device_state(0)
+        return _device_view(C.cast(p, C.c_void_p).value, (self.nv, ld), "<f8")
+
+    def dtmin_device(self):
+        """The device int64 part 0 takes the step's dt from (h3c_dtmin_device), as a 1-element CUDA tensor view."""
+        p = C.POINTER(C.c_int64)()
+        self._check(lib().h3c_dtmin_device(self.h, C.byref(p)))
+        return _device_view(C.cast(p, C.c_void_p).value, (1,), "<i8")
 
     def autotune(self, nsteps=20):
         """Times every applicable stage launch configuration from the current

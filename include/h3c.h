@@ -117,6 +117,11 @@ extern "C" {
 #define H3C_BC_ADV_DIRICHLET 15
 #define H3C_BC_ADV_NEUMANN 16
 #define H3C_BC_ADV_CHARACTERISTIC 17
+/* EXTENSION (not in hom3, which has no domain decomposition): the ghost is a
+ * cell of a neighbouring subdomain (another solver holding another part of
+ * the same grid); the library leaves its state as the caller writes it
+ * between the parts of a step (h3c_solve_stage).  Any physics. */
+#define H3C_BC_EXCHANGE 18
 
 typedef struct h3c_solver_s* h3c_solver;
 
@@ -264,6 +269,26 @@ int h3c_step(h3c_solver s, int64_t* step);
 #define H3C_STATUS_STATE 2
 #define H3C_STATUS_TIMEOUT 4
 int h3c_status(h3c_solver s, int* flags);
+
+/* ---- stepping by parts (no hom3 counterpart: hom3 has no domain decomposition) ----
+ * One grid split over several solvers (subdomains, one per GPU) needs, before
+ * every stage, the neighbouring subdomains' cells in its H3C_BC_EXCHANGE
+ * ghosts, and one time step for all.  h3c_stages: stages per step (forward
+ * Euler 1, RK2 2, SSP-RK3 3).  h3c_solve_stage(s, k), k = 0 .. stages - 1 in
+ * order, is part k of one h3c_solve step: part 0 applies the conditions to
+ * lhs and sets the step's dt from the minimum cell time step; part k > 0
+ * applies the conditions to its input; each part then runs its stage; the
+ * last part also advances time and step.  h3c_stage_input(s, k, &p): device
+ * pointer (internal numbering, [nv][ld], see h3c_device_order) of part k's
+ * input state, into whose exchange ghosts the caller writes before part k.
+ * h3c_dtmin_device(s, &p): the device int64 from which part 0 takes the
+ * step's dt (the minimum cell time step of lhs as ordered bits: integer
+ * order is time-step order); the caller replaces it by the minimum over the
+ * subdomains before part 0.  h3c_solve refuses to run between parts. */
+int h3c_stages(h3c_solver s, int* n);
+int h3c_solve_stage(h3c_solver s, int k);
+int h3c_stage_input(h3c_solver s, int k, double** ptr);
+int h3c_dtmin_device(h3c_solver s, int64_t** ptr);
 
 /* ---- instrumentation (no hom3 counterpart: hom3 has no timers) ----
  * h3c_launches: kernels this solver has launched since creation.
