@@ -22,6 +22,8 @@
 #include "vtk_writer.hpp"
 #include "grid_build.hpp"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/h3c.h"
 #include "fv_kernels.cuh"
 #include "adjoint_kernels.cuh"
@@ -37,6 +39,12 @@ namespace {
 std::string g_last_error;  // errors not tied to a solver (NULL handle)
 
 constexpr long long kForcedNone = std::numeric_limits<long long>::max();
+
+// An NVTX range over a host call (visible to nsys / ncu range filters; a no-op without a tool attached).
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+};
 
 // An instantiated graph of solver steps and the lhs buffer its capture started from.
 struct StepGraph {
@@ -721,8 +729,36 @@ static int prepare_instance(h3c_solver s, int k, const h3c_grid* gr, InstanceTab
   return H3C_OK;
 }
 
+// Every index the stage, condition and CFL kernels read through, checked on
+// the device after upload (the tables are renumbered on the host, so this
+// checks that step): neighbour entries of interior cells are cells or
+// sub-face groups, group members and ghosts' boundary cells are cells, level
+// bytes index the length table, halo-list entries are cells.  bad[0] counts
+// violations; the kernels never index through an unchecked table.
+__global__ void k_check_tables(const int* __restrict__ nbr, const int* __restrict__ sub,
+                               const int* __restrict__ gbndry, const unsigned char* __restrict__ lvl,
+                               const int* __restrict__ hids, long long nhids, long long n_int, long long n_tot,
+                               long long ld, long long nsub, int np, int nsubc, long long ng, int nlev,
+                               unsigned long long* bad) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long b = 0;
+  if (i < n_int) {
+    for (int p = 0; p < np; ++p) {
+      const long long v = nbr[p * ld + i];
+      b += !((v >= 0 && v < n_tot) || (v <= -2 && -v - 2 < nsub));
+    }
+    b += lvl[i] >= nlev;
+  }
+  if (i < nsub)
+    for (int j = 0; j < nsubc; ++j) b += !(sub[j * nsub + i] >= 0 && sub[j * nsub + i] < n_tot);
+  if (i < ng) b += !(gbndry[i] >= 0 && gbndry[i] < n_int);
+  if (i < nhids) b += !(hids[i] >= 0 && hids[i] < n_tot);
+  if (b) atomicAdd(bad, b);
+}
+
 static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   if (!s || !grids || ninst < 1) return H3C_E_INVALID;
+  Range r("h3c_set_grid");
   const int nd = s->nd, np = 2 * nd, nsubc = 1 << (nd - 1);
   if (ninst > 1 && s->desc.physics == H3C_CNS)
     return s->fail(H3C_E_INVALID, "h3c_set_grids: batches of CNS grids are not supported");
@@ -1003,6 +1039,22 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   H3C_CUDA(s, cudaMemset(s->d_q[1], 0, sizeof(double) * s->nv * L));
   if (s->d_q[2]) H3C_CUDA(s, cudaMemset(s->d_q[2], 0, sizeof(double) * s->nv * L));
   if (s->d_slopes) H3C_CUDA(s, cudaMemset(s->d_slopes, 0, sizeof(double) * nd * s->nv * L));
+  {
+    unsigned long long* d_bad = nullptr;
+    H3C_CUDA(s, cudaMalloc(&d_bad, sizeof(unsigned long long)));
+    cudaMemset(d_bad, 0, sizeof(unsigned long long));
+    const long long nh = (s->halo_ok || s->cns_ok) && s->d_hids ? HH.ids.size() + CH.base.ids.size() : 0;
+    const long long span = std::max({n_int, nsub, ng, nh, 1LL});
+    k_check_tables<<<blocks(span), kBlock, 0, s->stream>>>(s->d_nbr, s->d_sub, s->d_gbndry, s->d_lvl, s->d_hids, nh,
+                                                           n_int, n_tot, L, nsub, np, nsubc, ng, s->nlev, d_bad);
+    unsigned long long bad = 0;
+    const cudaError_t e = cudaMemcpyAsync(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s->stream);
+    const cudaError_t e2 = cudaStreamSynchronize(s->stream);
+    cudaFree(d_bad);
+    H3C_CUDA(s, e);
+    H3C_CUDA(s, e2);
+    if (bad) return s->fail(H3C_E_INVALID, "h3c_set_grid: %llu device table entries out of range", bad);
+  }
   k_init_time<<<blocks(ninst), kBlock, 0, s->stream>>>(s->d_sc, s->desc.time_end, ninst);
   H3C_CUDA(s, cudaGetLastError());
   s->has_grid = true;
@@ -1438,6 +1490,7 @@ static bool launch_graph(h3c_solver s, const StepGraph* g, int n) {
 
 int h3c_solve(h3c_solver s, int64_t nsteps) {
   if (!s || nsteps < 0) return H3C_E_INVALID;
+  Range r("h3c_solve");
   if (int rc = ready(s, "h3c_solve")) return rc;
   if (s->stage_next != 0)
     return s->fail(H3C_E_STATE, "h3c_solve: a step run by parts is at part %d (h3c_solve_stage)", s->stage_next);
@@ -1473,6 +1526,8 @@ int h3c_stages(h3c_solver s, int* n) {
 
 int h3c_solve_stage(h3c_solver s, int k) {
   if (!s) return H3C_E_INVALID;
+  static const char* names[3] = {"h3c_solve_stage 0", "h3c_solve_stage 1", "h3c_solve_stage 2"};
+  Range r(names[k >= 0 && k < 3 ? k : 0]);
   if (int rc = ready(s, "h3c_solve_stage")) return rc;
   if (k != s->stage_next)
     return s->fail(H3C_E_STATE, "h3c_solve_stage: part %d requested, part %d is next", k, s->stage_next);
@@ -1672,6 +1727,7 @@ static void enqueue_cht(h3c_solver cns, h3c_solver heat, double scaling, int64_t
 }
 
 int h3c_cht_solve(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps) {
+  Range r("h3c_cht_solve");
   if (!cns || !heat || nsteps < 0) return H3C_E_INVALID;
   if (int rc = ready(cns, "h3c_cht_solve")) return rc;
   if (int rc = ready(heat, "h3c_cht_solve")) return rc;
@@ -1988,6 +2044,7 @@ static void frozen_step(h3c_solver s, double* const* st, double* out, const doub
 }
 
 int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts) {
+  Range r("h3c_solve_dt");
   if (!s || nsteps < 0 || (nsteps > 0 && !dts)) return H3C_E_INVALID;
   if (int rc = ready(s, "h3c_solve_dt")) return rc;
   if (s->n_inst != 1) return s->fail(H3C_E_INVALID, "h3c_solve_dt: single grids only");
@@ -2016,6 +2073,7 @@ int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts) {
 // stores the stage states of the last segment as it goes, so that segment
 // (all of them when every >= nsteps) needs no recomputation.
 int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dqN, double* dJ_dq0, double* dts_out) {
+  Range r("h3c_adjoint");
   if (!s || nsteps < 1 || every < 0 || !dJ_dqN || !dJ_dq0) return H3C_E_INVALID;
   if (int rc = adjoint_supported(s, "h3c_adjoint")) return rc;
   const long long L = s->ld, nv = s->nv, Q = nv * L;
@@ -2263,6 +2321,7 @@ static void internal_to_caller(h3c_solver s, const double* src, double* dst) {
 
 int h3c_cht_adjoint(h3c_solver cns, h3c_solver heat, double Tr0, int64_t nsteps, int64_t every,
                     const double* dJ_dqN, const double* dJ_dTN, double* dJ_dq0, double* dJ_dT0, double* dts) {
+  Range r("h3c_cht_adjoint");
   if (!cns || !heat || nsteps < 1 || every < 0 || !dJ_dqN || !dJ_dTN || !dJ_dq0 || !dJ_dT0) return H3C_E_INVALID;
   if (int rc = adjoint_supported(cns, "h3c_cht_adjoint", true)) return rc;
   if (int rc = adjoint_supported(heat, "h3c_cht_adjoint", true)) return rc;

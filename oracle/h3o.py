@@ -18,7 +18,8 @@ import subprocess
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "_build", "libh3o.so")
+# H3O_LIB names another build of the same sources (the sanitizer test loads one built with ASan/UBSan)
+_LIB_PATH = os.environ.get("H3O_LIB") or os.path.join(_HERE, "_build", "libh3o.so")
 INV = np.iinfo(np.int64).max
 SINV = np.iinfo(np.int32).max
 
