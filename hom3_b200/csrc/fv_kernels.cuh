@@ -1423,63 +1423,75 @@ __global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const
     double acc[NV];
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+    // Directions whose faces are all plain run in the unrolled loop; a
+    // direction with a coarse/fine group on either side is deferred to a
+    // second, rolled loop after it, so that the group path's registers are
+    // not live across the common path (which would spill it).
+    unsigned deferred = 0;
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       const int m = __ldg(g.nbr + 2 * d * ld + c), p = __ldg(g.nbr + (2 * d + 1) * ld + c);
+      if (HANG && (m < 0 || p < 0)) {
+        deferred |= 1u << d;
+        continue;
+      }
       FaceState<R, ND> Fc;
 #pragma unroll
       for (int v = 0; v < NV; ++v) Fc.th[v] = own[v][tid];
       Fc.p = own[NV][tid];
       Fc.M = own[NV + 1 + d][tid];
-      double fm[NV], fp[NV];
-      if (!HANG || (m >= 0 && p >= 0)) {
-        // both neighbours' states along d, loaded together
-        double qm[NV], qp[NV];
+      // both neighbours' states along d, loaded together
+      double qm[NV], qp[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          qm[v] = __ldg(qin + v * ld + m);
-          qp[v] = __ldg(qin + v * ld + p);
-        }
-        FaceState<R, ND> Fm, Fp;
-        neighbour_fs(d, Fm, qm);
-        neighbour_fs(d, Fp, qp);
-        R f[NV];
-        ausm_face<R, ND>(Fm, Fc, d, f);
+      for (int v = 0; v < NV; ++v) {
+        qm[v] = __ldg(qin + v * ld + m);
+        qp[v] = __ldg(qin + v * ld + p);
+      }
+      FaceState<R, ND> Fm, Fp;
+      neighbour_fs(d, Fm, qm);
+      neighbour_fs(d, Fp, qp);
+      R f[NV];
+      double fm[NV];
+      ausm_face<R, ND>(Fm, Fc, d, f);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
-        ausm_face<R, ND>(Fc, Fp, d, f);
+      for (int v = 0; v < NV; ++v) fm[v] = (double)f[v];
+      ausm_face<R, ND>(Fc, Fp, d, f);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) fp[v] = (double)f[v];
-      } else {
-        // coarse/fine faces: W times the sum over the group's fine cells
+      for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - (double)f[v]);
+    }
+    if (HANG && deferred) {
+      // coarse/fine faces: W times the sum over the group's fine cells
+#pragma unroll 1
+      for (int d = 0; d < ND; ++d) {
+        if (!((deferred >> d) & 1u)) continue;
+        FaceState<R, ND> Fc;
 #pragma unroll
+        for (int v = 0; v < NV; ++v) Fc.th[v] = own[v][tid];
+        Fc.p = own[NV][tid];
+        Fc.M = own[NV + 1 + d][tid];
+        double fo[2][NV];
+#pragma unroll 1
         for (int side = 0; side < 2; ++side) {
-          const int n = side == 0 ? m : p;
-          double* fo = side == 0 ? fm : fp;
+          const int n = __ldg(g.nbr + (2 * d + side) * ld + c);
           const int cnt = n >= 0 ? 1 : NS;
-          const long long k = -(long long)n - 2;
+          const long long kk = -(long long)n - 2;
+          double sum[NV];
 #pragma unroll 1
           for (int j = 0; j < cnt; ++j) {
-            const int nn = n >= 0 ? n : __ldg(g.sub + j * g.nsub + k);
-            double qn[NV];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) qn[v] = __ldg(qin + v * ld + nn);
             FaceState<R, ND> Fn;
-            neighbour_fs(d, Fn, qn);
+            face_state_global<R, ND>(Fn, qin, ld, n >= 0 ? n : __ldg(g.sub + j * g.nsub + kk), d, gamma, gm1);
             R f[NV];
             if (side == 0) ausm_face<R, ND>(Fn, Fc, d, f);
             else ausm_face<R, ND>(Fc, Fn, d, f);
 #pragma unroll
-            for (int v = 0; v < NV; ++v) fo[v] = j == 0 ? (double)f[v] : fo[v] + (double)f[v];
+            for (int v = 0; v < NV; ++v) sum[v] = j == 0 ? (double)f[v] : sum[v] + (double)f[v];
           }
-          if (n < 0) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) fo[v] = __dmul_rn(W, fo[v]);
-          }
+          for (int v = 0; v < NV; ++v) fo[side][v] = n < 0 ? __dmul_rn(W, sum[v]) : sum[v];
         }
-      }
 #pragma unroll
-      for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - fp[v]);
+        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fo[0][v] - fo[1][v]);
+      }
     }
     const double dx = g.len[g.lvl[c]];
     const double k = sc[inst].dt * nr_rcp(dx);
