@@ -733,11 +733,13 @@ static int prepare_instance(h3c_solver s, int k, const h3c_grid* gr, InstanceTab
 // the device after upload (the tables are renumbered on the host, so this
 // checks that step): neighbour entries of interior cells are cells or
 // sub-face groups, group members and ghosts' boundary cells are cells, level
-// bytes index the length table, halo-list entries are cells.  bad[0] counts
-// violations; the kernels never index through an unchecked table.
+// bytes index the length table, halo-list entries (their cell bits,
+// hid_mask) are cells.  bad[0] counts violations; the kernels never index
+// through an unchecked table.
 __global__ void k_check_tables(const int* __restrict__ nbr, const int* __restrict__ sub,
                                const int* __restrict__ gbndry, const unsigned char* __restrict__ lvl,
-                               const int* __restrict__ hids, long long nhids, long long n_int, long long n_tot,
+                               const int* __restrict__ hids, int hid_mask, long long nhids, long long n_int,
+                               long long n_tot,
                                long long ld, long long nsub, int np, int nsubc, long long ng, int nlev,
                                unsigned long long* bad) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -752,7 +754,10 @@ __global__ void k_check_tables(const int* __restrict__ nbr, const int* __restric
   if (i < nsub)
     for (int j = 0; j < nsubc; ++j) b += !(sub[j * nsub + i] >= 0 && sub[j * nsub + i] < n_tot);
   if (i < ng) b += !(gbndry[i] >= 0 && gbndry[i] < n_int);
-  if (i < nhids) b += !(hids[i] >= 0 && hids[i] < n_tot);
+  if (i < nhids) {
+    const int h = hids[i] & hid_mask;
+    b += !(hids[i] >= 0 && h < n_tot);
+  }
   if (b) atomicAdd(bad, b);
 }
 
@@ -1045,8 +1050,10 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
     cudaMemset(d_bad, 0, sizeof(unsigned long long));
     const long long nh = (s->halo_ok || s->cns_ok) && s->d_hids ? HH.ids.size() + CH.base.ids.size() : 0;
     const long long span = std::max({n_int, nsub, ng, nh, 1LL});
-    k_check_tables<<<blocks(span), kBlock, 0, s->stream>>>(s->d_nbr, s->d_sub, s->d_gbndry, s->d_lvl, s->d_hids, nh,
-                                                           n_int, n_tot, L, nsub, np, nsubc, ng, s->nlev, d_bad);
+    const int hid_mask = s->halo_ok ? kHaloCellMask : -1;  // Euler entries carry a direction
+    k_check_tables<<<blocks(span), kBlock, 0, s->stream>>>(s->d_nbr, s->d_sub, s->d_gbndry, s->d_lvl, s->d_hids,
+                                                           hid_mask, nh, n_int, n_tot, L, nsub, np, nsubc, ng,
+                                                           s->nlev, d_bad);
     unsigned long long bad = 0;
     const cudaError_t e = cudaMemcpyAsync(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s->stream);
     const cudaError_t e2 = cudaStreamSynchronize(s->stream);

@@ -73,11 +73,6 @@ __device__ __forceinline__ void face_state_of(const double* q, R gamma, R gm1, R
   for (int d = 0; d < ND; ++d) M[d] = P.M[d];
 }
 
-// Halo entries are (cell, direction) pairs: the id word carries the cell in
-// its low 29 bits and the face direction it is read across above them.
-constexpr int kHaloDirShift = 29;
-constexpr int kHaloCellMask = (1 << kHaloDirShift) - 1;
-
 template <int ND, class R, int MODE, bool HANG, bool FUSE>
 __global__ void __launch_bounds__(kHaloTile, 3)
     k_stage_halo(const double* __restrict__ qin, double* out, Geometry g, HaloGeom hg, PhysConst pc,

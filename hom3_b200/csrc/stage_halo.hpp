@@ -25,6 +25,11 @@ namespace h3c {
 constexpr int kHaloTile = 256;              // cells per tile = threads per block
 constexpr int kHaloMaxSlots = 1024;         // halo entries a tile may hold in shared memory
 constexpr unsigned short kGroupBit = 0x8000;
+// Euler halo entries are (cell, direction) pairs: the id word carries the
+// cell in its low 29 bits and the face direction it is read across above
+// them (the CNS tables list plain cell ids).
+constexpr int kHaloDirShift = 29;
+constexpr int kHaloCellMask = (1 << kHaloDirShift) - 1;
 
 // Device tables of the halo-staged kernel.
 struct HaloGeom {
