@@ -731,20 +731,21 @@ static int prepare_instance(h3c_solver s, int k, const h3c_grid* gr, InstanceTab
 
 // Every index the stage, condition and CFL kernels read through, checked on
 // the device after upload (the tables are renumbered on the host, so this
-// checks that step): neighbour entries of interior cells are cells or
+// checks that step): neighbour entries of interior cells (not the padding
+// between the instances of a batch, dev2caller < 0) are cells or
 // sub-face groups, group members and ghosts' boundary cells are cells, level
 // bytes index the length table, halo-list entries (their cell bits,
 // hid_mask) are cells.  bad[0] counts violations; the kernels never index
 // through an unchecked table.
 __global__ void k_check_tables(const int* __restrict__ nbr, const int* __restrict__ sub,
                                const int* __restrict__ gbndry, const unsigned char* __restrict__ lvl,
-                               const int* __restrict__ hids, int hid_mask, long long nhids, long long n_int,
-                               long long n_tot,
+                               const int* __restrict__ hids, int hid_mask, long long nhids,
+                               const long long* __restrict__ dev2caller, long long n_int, long long n_tot,
                                long long ld, long long nsub, int np, int nsubc, long long ng, int nlev,
                                unsigned long long* bad) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned long long b = 0;
-  if (i < n_int) {
+  if (i < n_int && dev2caller[i] >= 0) {
     for (int p = 0; p < np; ++p) {
       const long long v = nbr[p * ld + i];
       b += !((v >= 0 && v < n_tot) || (v <= -2 && -v - 2 < nsub));
@@ -1052,7 +1053,8 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
     const long long span = std::max({n_int, nsub, ng, nh, 1LL});
     const int hid_mask = s->halo_ok ? kHaloCellMask : -1;  // Euler entries carry a direction
     k_check_tables<<<blocks(span), kBlock, 0, s->stream>>>(s->d_nbr, s->d_sub, s->d_gbndry, s->d_lvl, s->d_hids,
-                                                           hid_mask, nh, n_int, n_tot, L, nsub, np, nsubc, ng,
+                                                           hid_mask, nh, s->d_dev2caller, n_int, n_tot, L, nsub,
+                                                           np, nsubc, ng,
                                                            s->nlev, d_bad);
     unsigned long long bad = 0;
     const cudaError_t e = cudaMemcpyAsync(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost, s->stream);
