@@ -326,6 +326,8 @@ class DomainSolver:
             exchange(self.s.stage_input(k), self.part.send, self.part.recv, self.group)
 
     def _dt_min(self):
+        if self.world == 1:  # one subdomain: its own minimum is the grid's
+            return
         torch = self.torch
         with torch.cuda.stream(self.part.stream):
             min_all(self.s.dtmin_device(), self.group)
