@@ -90,7 +90,7 @@ def test_autotune_single_tree_sets_the_chosen_kernel():
     assert 0 <= choice < len(KERNEL_OF_CHOICE) and ms_step > 0
     info = a.kernel_info()
     assert info["kernel"] == KERNEL_OF_CHOICE[choice], (choice, info)
-    if choice >= 7:
+    if 7 <= choice <= 9:  # the halo-staged kernel at 1-3 persistent blocks per SM
         sms = torch.cuda.get_device_properties(0).multi_processor_count
         assert info["grid"] == min(info["tiles"], (choice - 6) * sms)
     a.solve(4)
@@ -99,3 +99,21 @@ def test_autotune_single_tree_sets_the_chosen_kernel():
     qa, qb = a.state(0)[:, :fg], b.state(0)[:, :fg]
     assert np.max(np.abs(qa - qb)) <= 1e-12 * np.max(np.abs(qb))
     assert a.step() == b.step() == 4
+
+
+def test_autotune_cns_times_the_tile_kernel_grids_and_the_per_cell_kernel():
+    """For CNS the candidates are the tile kernel's grid sizes (0-4) and the
+    per-cell kernels (5); the state after tuning is the untuned one's."""
+    import cases
+    from oracle import h3o
+    _, (o,) = cases.tgv_case(level=4, ti=h3o.RK2)
+    a = cases.gpu_solver_from_oracle(o, 0)
+    b = cases.gpu_solver_from_oracle(o, 0)
+    choice, ms_step = a.autotune(3)
+    assert 0 <= choice <= 5 and ms_step > 0
+    assert a.kernel_info()["kernel"] == ("per_cell" if choice == 5 else "halo")
+    a.solve(3)
+    b.solve(3)
+    fg = o.first_ghost
+    qa, qb = a.state(0)[:, :fg], b.state(0)[:, :fg]
+    assert np.max(np.abs(qa - qb)) <= 1e-12 * np.max(np.abs(qb))

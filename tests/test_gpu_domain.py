@@ -80,6 +80,12 @@ def test_split_with_every_euler_stage_kernel(kernel):
     _compare(o, 0, 2, (1, 3), kernel)
 
 
+def test_split_heat():
+    """hom3's heat test grid (Dirichlet and Neumann walls) in three parts."""
+    _, (o,) = cases.heat_case(level=4, ti=h3o.RK2)
+    _compare(o, 0, 3, (1, 3))
+
+
 def test_split_mixed_precision():
     _, (o,) = cases.refined_case(ti=h3o.RK2, level=3, fine=5)
     _compare(o, 1, 3, (1, 3))
