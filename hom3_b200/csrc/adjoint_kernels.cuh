@@ -131,11 +131,54 @@ __device__ __forceinline__ void ausm_vjp(const SideAD<ND>& SL, const SideAD<ND>&
   side_reverse<ND>(SR, d, gamma, gm1, MRbar, aRbar, pRbar, gR);
 }
 
+// gL += w^T dF/dq_L, gR += w^T dF/dq_R for the local Lax-Friedrichs flux
+// F = 1/2 (f(q_L) + f(q_R) + dx/dt (q_L - q_R)) along d (euler/physics.hpp:
+// 98-113, 262-267).  The physical flux f is differentiated exactly; the
+// dissipation term's cotangent wdiss = 1/2 sum over the two residuals of
+// (dx/dt of the cell that evaluated the face) x (its part of w) is passed in,
+// since each cell evaluates its faces with its own length.
+template <int ND>
+__device__ __forceinline__ void euler_flux_vjp(const SideAD<ND>& S, int d, const double* w, double gm1, double gamma,
+                                               double* g) {
+  // f_k = m_d u_k + p [k == d], f_rho = m_d, f_E = u_d (E + p)
+  const double ud = pick<ND>(S.u, d);
+  const double H = (S.q[ND + 1] + S.p) * S.rinv;
+  const double wd = pick<ND>(w, d);
+  double wu = 0.0;  // sum_k w_k u_k
+#pragma unroll
+  for (int k = 0; k < ND; ++k) wu += w[k] * S.u[k];
+  const double wpm = wd + w[ND + 1] * ud;  // cotangent of p through f_d and f_E
+#pragma unroll
+  for (int j = 0; j < ND; ++j) {
+    double gj = ud * w[j] - gm1 * S.u[j] * wpm;  // u_d w_j + dp/dm_j (w_d + w_E u_d)
+    if (j == d) gj += wu + w[ND] + w[ND + 1] * H;
+    g[j] += gj;
+  }
+  g[ND] += -ud * wu + 0.5 * gm1 * S.um2 * wpm - w[ND + 1] * ud * H;
+  g[ND + 1] += gm1 * wd + gamma * ud * w[ND + 1];
+}
+
+template <int ND>
+__device__ __forceinline__ void llf_vjp(const SideAD<ND>& SL, const SideAD<ND>& SR, int d, const double* w,
+                                        const double* wdiss, double gamma, double gm1, double* gL, double* gR) {
+  constexpr int NV = ND + 2;
+  double hw[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) hw[v] = 0.5 * w[v];
+  euler_flux_vjp<ND>(SL, d, hw, gm1, gamma, gL);
+  euler_flux_vjp<ND>(SR, d, hw, gm1, gamma, gR);
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    gL[v] += wdiss[v];
+    gR[v] -= wdiss[v];
+  }
+}
+
 // Per-cell adjoint of one stage:
 //   gout_c = beta lam_c + [VJP of (q -> alpha k R(q)) with cotangent lam]_c
 //            + gamma_e extra_c + gamma_e2 extra2_c
 // q is the stage input with its ghosts filled by the conditions.
-template <int ND, int PHYS>
+template <int ND, int PHYS, int FLUX = AUSM>
 __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double* __restrict__ q, const double* __restrict__ lam,
                                                       double* __restrict__ gout, const double* __restrict__ extra,
                                                       const double* __restrict__ extra2, double alpha, double beta,
@@ -225,8 +268,23 @@ __global__ void __launch_bounds__(kBlock, H3C_ADJ_MINB) k_adj_stage(const double
 #pragma unroll
     for (int v = 0; v < NV; ++v) Sn.q[v] = q[v * ld + nb_cell];
     side_forward<ND>(Sn, pc.gamma, pc.gm1);
-    if (c_is_left) ausm_vjp<ND>(Sc, Sn, d, w, pc.gamma, pc.gm1, gc, gn);
-    else ausm_vjp<ND>(Sn, Sc, d, w, pc.gamma, pc.gm1, gn, gc);
+    if (FLUX == LLF) {
+      // c's residual evaluates the face with dx_c / dt, the neighbour's with its own length
+      const double cdx = hc / dt, ndx = own >= 0 ? g.len[g.lvl[own]] / dt : 0.0;
+      double wdiss[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double wc = c_is_left ? -kc_face * lc[v] : kc_face * lc[v];
+        const double wn = c_is_left ? kn * ln[v] : -kn * ln[v];
+        wdiss[v] = 0.5 * (cdx * wc + ndx * wn);
+      }
+      if (c_is_left) llf_vjp<ND>(Sc, Sn, d, w, wdiss, pc.gamma, pc.gm1, gc, gn);
+      else llf_vjp<ND>(Sn, Sc, d, w, wdiss, pc.gamma, pc.gm1, gn, gc);
+    } else if (c_is_left) {
+      ausm_vjp<ND>(Sc, Sn, d, w, pc.gamma, pc.gm1, gc, gn);
+    } else {
+      ausm_vjp<ND>(Sn, Sc, d, w, pc.gamma, pc.gm1, gn, gc);
+    }
 #pragma unroll
     for (int v = 0; v < NV; ++v) acc[v] += gc[v] + jac * gn[v];
   };

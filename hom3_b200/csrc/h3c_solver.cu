@@ -1991,8 +1991,8 @@ static int adjoint_supported(h3c_solver s, const char* what, bool coupled = fals
   if (int rc = ready(s, what)) return rc;
   if (s->n_inst != 1) return s->fail(H3C_E_INVALID, "%s: single grids only", what);
   const bool ok_phys = ((s->desc.physics == H3C_EULER || s->desc.physics == H3C_CNS) && s->desc.flux == H3C_FLUX_AUSM) ||
-                       s->desc.physics == H3C_HEAT;
-  if (!ok_phys) return s->fail(H3C_E_INVALID, "%s: Euler and CNS with AUSM, and heat only", what);
+                       (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_LLF) || s->desc.physics == H3C_HEAT;
+  if (!ok_phys) return s->fail(H3C_E_INVALID, "%s: Euler (AUSM, LLF), CNS (AUSM) and heat only", what);
   if (s->desc.physics == H3C_CNS && s->nsub > 0)
     return s->fail(H3C_E_INVALID, "%s: CNS on coarse/fine faces has no adjoint", what);
   if (s->ghost_unapplied) return s->fail(H3C_E_INVALID, "%s: a ghost cell gets no condition", what);
@@ -2201,6 +2201,13 @@ int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dq
       return;
     }
     Launch La(s, K_OTHER);
+    if (s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_LLF) {  // the per-cell gather
+      if (s->nd == 2)
+        k_adj_stage<2, EULER, LLF><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, nullptr, g, gt, s->pc, s->d_sc);
+      else
+        k_adj_stage<3, EULER, LLF><<<blocks(s->n_int), kBlock, 0, s->stream>>>(qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2, nullptr, g, gt, s->pc, s->d_sc);
+      return;
+    }
     if (s->desc.physics == H3C_EULER && s->tile) {
       if (s->nd == 2) {
         if (s->nsub > 0) adj_ausm_t<2, true>(s, qin, lamin, gout, extra, extra2, alpha, beta, gam, gam2);

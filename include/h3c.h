@@ -370,8 +370,9 @@ int h3c_min_dt_noalloc(const h3c_desc* desc, const double* q, int64_t ld, int64_
  * host or device memory; ghost entries of dJ_dqN are ignored, of dJ_dq0 zero.
  * The last segment's stage states are kept from the forward run; the other
  * segments are recomputed from their checkpoints.  The workspace stays
- * allocated for the next call.  Euler with the AUSM flux and heat;
- * Neumann / Dirichlet / periodic conditions. */
+ * allocated for the next call.  Euler with the AUSM (and MUSCL) or LLF flux,
+ * CNS, and heat; Neumann / Dirichlet / periodic conditions (CNS also its wall,
+ * inflow and outflow conditions). */
 int h3c_solve_dt(h3c_solver s, int64_t nsteps, const double* dts);
 int h3c_adjoint(h3c_solver s, int64_t nsteps, int64_t every, const double* dJ_dqN, double* dJ_dq0, double* dts);
 

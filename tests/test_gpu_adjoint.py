@@ -26,8 +26,29 @@ BUILDERS = {
     "periodic_vortex_rk2": lambda: cases.periodic_vortex_case(level=5),
     "refined_fe": lambda: cases.refined_case(ti=h3o.EULER_FORWARD),
     "refined_rk2": lambda: cases.refined_case(ti=h3o.RK2),
+    "euler2d_llf_rk2": lambda: cases.euler_case("sod", nd=2, level=5, ti=h3o.RK2, flux=h3o.LLF),
+    "euler3d_llf_fe": lambda: cases.euler_case("sod", nd=3, level=3, ti=h3o.EULER_FORWARD, flux=h3o.LLF),
+    "refined_llf_rk2": lambda: _refined_llf(),
 }
+
+
+def _refined_llf():
+    """The refined tree of cases.refined_case with the LLF flux: its faces are
+    evaluated with the evaluating cell's own length, so a coarse/fine face
+    enters the coarse and the fine residual with different dissipation."""
+    w = h3o.World(3, [0, 0, 0], [1, 1, 1], level=2)
+    w.refine_sphere([0.5, 0.5, 0.5], 0.3, 4)
+    s = w.add_solver(h3o.EULER, h3o.LLF, h3o.RK2, bcs=cases.neumann_cube(w), ic_kind=h3o.IC_SHOCK_TUBE,
+                     ic=[0, 0, 0.5, 1.0, 0.0, 1.0, 0.125, 0.0, 0.1], time_end=1.0, cfl=0.4)
+    s.initialize()
+    return w, [s]
 NSTEPS = 12
+
+
+def nsteps(name):
+    """Steps of a case: hom3's LLF flux (dissipation dx/dt, euler/physics.hpp:262-267) is unstable in 2D and 3D
+    (each face relaxes the cell half-way to its neighbour), so its cases stop before the growth shows."""
+    return (2 if "refined" in name else 4) if "llf" in name else NSTEPS
 
 
 def setup(name, seed=0):
@@ -52,11 +73,12 @@ def frozen_J(g, q, dts, lam):
 def test_adjoint_matches_dual_oracle(name):
     o, g, q1, lam = setup(name)
     fg = o.first_ghost
-    grad, dts = g.adjoint(NSTEPS, lam, every=5)
+    n = nsteps(name)
+    grad, dts = g.adjoint(n, lam, every=min(5, n - 1))
     assert np.isfinite(grad).all()
     assert np.all(grad[:, fg:] == 0.0)
     # the forward of the adjoint took the solver's own CFL steps
-    for i in range(NSTEPS):
+    for i in range(n):
         o.solve(1)
         assert abs(dts[i] - o.dt()) <= 1e-12 * o.dt(), (i, dts[i], o.dt())
     rng = np.random.default_rng(11)
@@ -79,7 +101,8 @@ def fd_worst(name, eps, ndir=32):
     GPU frozen-dt map over ndir random directions dq."""
     o, g, q1, lam = setup(name, seed=2)
     fg = o.first_ghost
-    grad, dts = g.adjoint(NSTEPS, lam, every=4)
+    grad, dts = g.adjoint(nsteps(name), lam, every=min(4, nsteps(name) - 1))
+    assert np.isfinite(grad).all()
     rng = np.random.default_rng(2)
     worst = 0.0
     for _ in range(ndir):
@@ -88,11 +111,15 @@ def fd_worst(name, eps, ndir=32):
         fd = (frozen_J(g, q1 + eps * dq, dts, lam) - frozen_J(g, q1 - eps * dq, dts, lam)) / (2 * eps)
         ad = (grad * dq).sum()
         scale = np.abs(grad * dq).sum()
-        worst = max(worst, abs(fd - ad) / scale)
+        gap = abs(fd - ad) / scale
+        worst = gap if not np.isfinite(gap) else max(worst, gap)  # a NaN gap must not compare away
+        if not np.isfinite(worst):
+            break
     return worst
 
 
-@pytest.mark.parametrize("name", ["euler2d_rk2", "heat3d_fe", "periodic_vortex_rk2", "refined_rk2"])
+@pytest.mark.parametrize("name", ["euler2d_rk2", "heat3d_fe", "periodic_vortex_rk2", "refined_rk2", "euler2d_llf_rk2",
+                                  "refined_llf_rk2"])
 def test_adjoint_matches_finite_differences(name):
     """32 random directions, central differences of the GPU frozen-dt map."""
     assert fd_worst(name, 1e-6) <= 1e-6
@@ -215,7 +242,7 @@ def test_tile_adjoint_on_a_large_refined_tree():
 
 def test_unsupported_configurations_are_rejected():
     import hom3_b200 as hb
-    _, (o,) = cases.euler_case("sod", nd=2, level=4, flux=h3o.LLF)
+    _, (o,) = cases.advection_case(level=4)
     g = cases.gpu_solver_from_oracle(o)
     with pytest.raises(hb.H3cError):
         g.adjoint(2, np.zeros((o.nv, o.ncells)))
