@@ -150,6 +150,11 @@ def barrier(ws):
         dist.barrier()
 
 
+def hb_fma_rates():
+    from hom3_b200.solver import fma_rates
+    return fma_rates()
+
+
 def build_workload(args):
     import hom3_b200 as hb
     from hom3_b200 import _ffi as F
@@ -1308,6 +1313,10 @@ def main():
     line["grid_build"] = getattr(args, "grid_build", None)
     line["stage_kernel"] = s.kernel_info()
     line["autotune"] = tune
+    r64, r32 = hb_fma_rates()
+    line["fma_rates"] = {"fp64_tflops": 2 * r64 / 1e12, "fp32_tflops": 2 * r32 / 1e12,
+                         "what": "h3c_fma_rates: register-only FMA chains on this GPU (1 FMA = 2 flops); the FP64 "
+                                 "rate bounds the stage kernels' face arithmetic"}
     if ws == 1 and rank == 0 and not args.no_cpu_baseline:
         r = cpu_oracle_run(args)
         r1 = cpu_oracle_run(args, steps_budget_s=8.0, threads=1)

@@ -80,6 +80,7 @@ SIGNATURES = {
     "h3c_sizes": (_i32, [_vp, _P(_i64), _P(_i64), _P(_i32)]),
     "h3c_solve": (_i32, [_vp, _i64]),
     "h3c_stages": (_i32, [_vp, _P(_i32)]),
+    "h3c_fma_rates": (_i32, [_P(_dbl), _P(_dbl)]),
     "h3c_solve_stage": (_i32, [_vp, _i32]),
     "h3c_stage_input": (_i32, [_vp, _i32, _P(_P(_dbl))]),
     "h3c_dtmin_device": (_i32, [_vp, _P(_P(_i64))]),

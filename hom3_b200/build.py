@@ -17,7 +17,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 SRC = [os.path.join(CSRC, f) for f in ("h3c_solver.cu", "h3c_stage_halo.cu", "h3c_stage_cns.cu", "h3c_stage_warp.cu",
-                                       "h3c_noalloc.cu", "grid_build.cpp", "grid_build_device.cu", "vtk_writer.cpp")]
+                                       "h3c_rates.cu", "h3c_noalloc.cu", "grid_build.cpp", "grid_build_device.cu",
+                                       "vtk_writer.cpp")]
 OBJ_DIR = os.path.join(HERE, "_build")
 OUT = os.path.join(HERE, "_lib", "libhom3_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

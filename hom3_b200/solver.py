@@ -43,6 +43,13 @@ def _lp(a):
 # ---------------------------------------------------------------------------
 # geometry (geometry/implicit.hpp:39-205) and conditions
 # ---------------------------------------------------------------------------
+def fma_rates():
+    """(FP64, FP32) fused multiply-adds per second of the current device (h3c_fma_rates)."""
+    a, b = C.c_double(), C.c_double()
+    check(lib().h3c_fma_rates(C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
 class _DeviceArray:
     """A device pointer presented through __cuda_array_interface__ (torch.as_tensor makes a view of it)."""
 

@@ -290,6 +290,13 @@ int h3c_solve_stage(h3c_solver s, int k);
 int h3c_stage_input(h3c_solver s, int k, double** ptr);
 int h3c_dtmin_device(h3c_solver s, int64_t** ptr);
 
+/* Fused multiply-add issue rates of the current device (no hom3 counterpart):
+ * long register-only FMA chains, timed with CUDA events; FP64 and FP32 FMAs
+ * per second (one FMA = two flops).  The roofline of an arithmetic-bound
+ * stage kernel is set by the FP64 rate, which the copy and GEMM peaks do not
+ * give.  Allocates and frees a few bytes of device memory. */
+int h3c_fma_rates(double* fp64_per_s, double* fp32_per_s);
+
 /* ---- instrumentation (no hom3 counterpart: hom3 has no timers) ----
  * h3c_launches: kernels this solver has launched since creation.
  * h3c_profile(s, 1): bracket every subsequent launch with CUDA events on the
