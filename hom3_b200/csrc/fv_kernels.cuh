@@ -1207,7 +1207,6 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
     // ---- own loads first: state, neighbours, level ----
     double qc[NV];
     int nbp[ND], nbm[ND];
-    double dx = 1.0;
     if (live) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) qc[v] = __ldg(qin + v * ld + c);
@@ -1216,7 +1215,6 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
         nbm[d] = __ldg(g.nbr + (2 * d) * ld + c);
         nbp[d] = __ldg(g.nbr + (2 * d + 1) * ld + c);
       }
-      dx = g.len[g.lvl[c]];
     }
     // ---- face state of the cell -> shared memory ----
     if (live) {
@@ -1336,15 +1334,18 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
 #pragma unroll
         for (int v = 0; v < NV; ++v) qo[v] = out[v * ld + c];
       }
+      // the cell's own state and length read again (L1/L2) rather than held
+      // in registers across the face loops: fewer spills at 64 registers
       const double dt = sc[inst].dt;
-      const double k = dt / dx;
+      const double dxc = g.len[g.lvl[c]];
+      const double k = dt / dxc;
       double o[NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], qc[v], k * acc[v]);
+      for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], __ldg(qin + v * ld + c), k * acc[v]);
 #pragma unroll
       for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
       if (FUSE) {
-        const double cd = cell_dt<ND, EULER>(o, dx, pc, nullptr, &bad);
+        const double cd = cell_dt<ND, EULER>(o, dxc, pc, nullptr, &bad);
         if (!isnan(cd)) ord = dbl_to_ord(cd);
       }
     }
