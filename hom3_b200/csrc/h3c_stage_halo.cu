@@ -173,9 +173,11 @@ __global__ void __launch_bounds__(kHaloTile, 3)
     }
 
     // ---- face states: the own cell's (also kept in registers), the halo entries' along their direction ----
-    double qc[NV];
+    // (the cell's own state is read again from global memory at the update,
+    // not held in registers across the face loops)
     R thc[NV], pcell = R(0), Mc[ND];
     if (live) {
+      double qc[NV];
 #pragma unroll
       for (int v = 0; v < NV; ++v) qc[v] = land[(size_t)v * S + tid];
       face_state_of<R, ND>(qc, gamma, gm1, thc, pcell, Mc);
@@ -308,7 +310,7 @@ __global__ void __launch_bounds__(kHaloTile, 3)
       const double k = dt / dx;
       double o[NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], qc[v], k * acc[v]);
+      for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], __ldg(qin + v * ld + c), k * acc[v]);
 #pragma unroll
       for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
       if (FUSE) {

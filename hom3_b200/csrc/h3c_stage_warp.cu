@@ -116,16 +116,15 @@ __global__ void __launch_bounds__(kBlock, H3C_WARP_MINB)
   auto in_warp = [&](int n) { return n >= w0 && n < wend; };
 
   // ---- 1. own state and face state ----
-  double qc[NV];
+  // (the own state is read again at the update rather than held in registers
+  // across the face lists)
   int nb[2 * ND];
-#pragma unroll
-  for (int v = 0; v < NV; ++v) qc[v] = live ? __ldg(qin + v * ld + c) : 1.0;
 #pragma unroll
   for (int p = 0; p < 2 * ND; ++p) nb[p] = live ? __ldg(g.nbr + p * ld + c) : -1;
   if (live) {
     Prim<R, ND> P;
 #pragma unroll
-    for (int v = 0; v < NV; ++v) P.q[v] = (R)qc[v];
+    for (int v = 0; v < NV; ++v) P.q[v] = (R)__ldg(qin + v * ld + c);
     make_prim<R, ND>(P, gamma, gm1);
 #pragma unroll
     for (int v = 0; v < ND + 1; ++v) S.own[v][lane] = P.q[v] * P.a;
@@ -315,7 +314,7 @@ __global__ void __launch_bounds__(kBlock, H3C_WARP_MINB)
     }
     double o[NV];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], qc[v], k * acc[v]);
+    for (int v = 0; v < NV; ++v) o[v] = rk_combine<MODE>(MODE == 0 ? 0.0 : qo[v], __ldg(qin + v * ld + c), k * acc[v]);
 #pragma unroll
     for (int v = 0; v < NV; ++v) out[v * ld + c] = o[v];
     if (FUSE) {
