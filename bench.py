@@ -1169,7 +1169,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the library's default Euler stage launch instead of h3c_autotune's choice")
     ap.add_argument("--euler-kernel", type=int, default=None,
-                    help="Euler stage kernel: 0 halo-staged tile, 1 per-lane tile, 2 per cell (default: the library's)")
+                    help="Euler stage kernel: 0 halo-staged tile, 1 per-lane tile, 2 per cell, 3 warp-tiled, 4 per-lane tile "
+                         "of 512 cells (default: the autotuner's choice)")
     ap.add_argument("--workload", default="riemann3d",
                     choices=["riemann3d", "ensemble", "tgv", "vortex", "cht", "advection"])
     ap.add_argument("--adv-level", type=int, default=11)

@@ -147,6 +147,27 @@ __device__ __forceinline__ void block_min_atomic(long long v, long long* dst) {
   }
 }
 
+// block_min_atomic for a block of TB threads (TB / 32 <= 32 warps).
+template <int TB>
+__device__ __forceinline__ void block_min_atomic_tb(long long v, long long* dst) {
+  __shared__ long long red[TB / 32];
+  for (int o = 16; o > 0; o >>= 1) {
+    long long w = __shfl_down_sync(0xffffffffu, v, o);
+    v = w < v ? w : v;
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < TB / 32 ? red[lane] : kOrdMax;
+    for (int o = 16; o > 0; o >>= 1) {
+      long long w = __shfl_down_sync(0xffffffffu, v, o);
+      v = w < v ? w : v;
+    }
+    if (lane == 0 && v < kOrdMax) atomicMin(dst, v);
+  }
+}
+
 // The same minimum without a block barrier, for kernels that have none: each
 // warp folds its minimum into a shared slot; the last warp of the block to
 // arrive (a shared counter) makes the one global atomicMin.  slot and cnt
@@ -1141,9 +1162,9 @@ __global__ void __launch_bounds__(kBlock, 3) k_stage_tile(const double* __restri
 // Shared memory: face state [2ND+4][kBlock] of R, plus-face flux
 // [ND][ND+2][kBlock] of double, plus neighbours [ND][kBlock] of int.
 // ---------------------------------------------------------------------------
-template <class R, int ND>
+template <class R, int ND, int TB = kBlock>
 __host__ __device__ constexpr size_t ausm_smem_bytes() {
-  return sizeof(R) * (2 * ND + 3) * kBlock + sizeof(double) * ND * (ND + 2) * kBlock + sizeof(int) * ND * kBlock;
+  return sizeof(R) * (2 * ND + 3) * TB + sizeof(double) * ND * (ND + 2) * TB + sizeof(int) * ND * TB;
 }
 
 template <class R, int ND> struct FaceState {
@@ -1181,27 +1202,30 @@ __device__ __forceinline__ void face_state_global(FaceState<R, ND>& F, const dou
 #endif
 // Persistent: block b processes tiles b, b + gridDim.x, ... (the grid size is
 // a launch choice the batch autotuner makes; one block per tile by default).
-template <int ND, class R, int MODE, bool HANG, bool FUSE>
-__global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const double* __restrict__ qin, double* out,
-                                                                      Geometry g, PhysConst pc,
-                                                                      const Scalars* __restrict__ sc,
-                                                                      long long* dtmin) {
+// TB: cells per tile = threads per block.  kBlock (256: an 8x8x4 Morton brick
+// in 3D), or 512 (8x8x8) for one grid: g.ntiles then counts 512-cell tiles,
+// and the same 32 warps per SM come as two blocks instead of four.
+template <int ND, class R, int MODE, bool HANG, bool FUSE, int TB = kBlock>
+__global__ void __launch_bounds__(TB, H3C_AUSM_MINB * kBlock / TB) k_stage_ausm(const double* __restrict__ qin,
+                                                                              double* out, Geometry g, PhysConst pc,
+                                                                              const Scalars* __restrict__ sc,
+                                                                              long long* dtmin) {
   constexpr int NV = ND + 2;
   constexpr int NS = 1 << (ND - 1);
   constexpr double W = ND == 2 ? 0.5 : 0.25;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  R* sfs = reinterpret_cast<R*>(smem_raw);                                   // [NV + 1 + ND][kBlock]
-  double* sf = reinterpret_cast<double*>(smem_raw + sizeof(R) * (2 * ND + 3) * kBlock);  // [ND][NV][kBlock]
-  int* snp = reinterpret_cast<int*>(sf + ND * NV * kBlock);                  // [ND][kBlock]
+  R* sfs = reinterpret_cast<R*>(smem_raw);                                   // [NV + 1 + ND][TB]
+  double* sf = reinterpret_cast<double*>(smem_raw + sizeof(R) * (2 * ND + 3) * TB);  // [ND][NV][TB]
+  int* snp = reinterpret_cast<int*>(sf + ND * NV * TB);                  // [ND][TB]
   const int tid = threadIdx.x;
   const long long ld = g.ld;
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
 
   for (long long tile = blockIdx.x; tile < g.ntiles; tile += gridDim.x) {
-    const long long c0 = tile * kBlock;
+    const long long c0 = tile * TB;
     const long long c = c0 + tid;
     const int inst = tile_instance(g, tile);
-    const long long tile_end = min(c0 + (long long)kBlock, instance_end(g, inst));
+    const long long tile_end = min(c0 + (long long)TB, instance_end(g, inst));
     const bool live = c < tile_end;
 
     // ---- own loads first: state, neighbours, level ----
@@ -1223,13 +1247,13 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
       for (int v = 0; v < NV; ++v) Pc.q[v] = (R)qc[v];
       make_prim<R, ND>(Pc, gamma, gm1);
 #pragma unroll
-      for (int v = 0; v < ND + 1; ++v) sfs[v * kBlock + tid] = Pc.q[v] * Pc.a;
-      sfs[(ND + 1) * kBlock + tid] = (Pc.q[ND + 1] + Pc.p) * Pc.a;
-      sfs[NV * kBlock + tid] = Pc.p;
+      for (int v = 0; v < ND + 1; ++v) sfs[v * TB + tid] = Pc.q[v] * Pc.a;
+      sfs[(ND + 1) * TB + tid] = (Pc.q[ND + 1] + Pc.p) * Pc.a;
+      sfs[NV * TB + tid] = Pc.p;
 #pragma unroll
-      for (int d = 0; d < ND; ++d) sfs[(NV + 1 + d) * kBlock + tid] = Pc.M[d];
+      for (int d = 0; d < ND; ++d) sfs[(NV + 1 + d) * TB + tid] = Pc.M[d];
 #pragma unroll
-      for (int d = 0; d < ND; ++d) snp[d * kBlock + tid] = nbp[d];
+      for (int d = 0; d < ND; ++d) snp[d * TB + tid] = nbp[d];
     }
     __syncthreads();
 
@@ -1238,18 +1262,18 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
       if (in_tile(n)) {
         const int t = (int)(n - c0);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + t];
-        F.p = sfs[NV * kBlock + t];
-        F.M = sfs[(NV + 1 + d) * kBlock + t];
+        for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * TB + t];
+        F.p = sfs[NV * TB + t];
+        F.M = sfs[(NV + 1 + d) * TB + t];
       } else {
         face_state_global<R, ND>(F, qin, ld, (int)n, d, gamma, gm1);
       }
     };
     auto own = [&](int d, FaceState<R, ND>& F) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * kBlock + tid];
-      F.p = sfs[NV * kBlock + tid];
-      F.M = sfs[(NV + 1 + d) * kBlock + tid];
+      for (int v = 0; v < NV; ++v) F.th[v] = sfs[v * TB + tid];
+      F.p = sfs[NV * TB + tid];
+      F.M = sfs[(NV + 1 + d) * TB + tid];
     };
 
     // ---- plus faces ----
@@ -1282,7 +1306,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
           for (int v = 0; v < NV; ++v) fp[v] = __dmul_rn(W, fp[v]);  // rounded: no FMA with the sums below
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sf[(d * NV + v) * kBlock + tid] = fp[v];
+        for (int v = 0; v < NV; ++v) sf[(d * NV + v) * TB + tid] = fp[v];
       }
     }
     __syncthreads();
@@ -1298,10 +1322,10 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
       for (int d = 0; d < ND; ++d) {
         const int m = nbm[d];
         double fm[NV];
-        if (in_tile(m) && snp[d * kBlock + (int)(m - c0)] == (int)c) {
+        if (in_tile(m) && snp[d * TB + (int)(m - c0)] == (int)c) {
           const int t = (int)(m - c0);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) fm[v] = sf[(d * NV + v) * kBlock + t];
+          for (int v = 0; v < NV; ++v) fm[v] = sf[(d * NV + v) * TB + t];
         } else if (!HANG || m >= 0) {
           FaceState<R, ND> Fc, Fn;
           own(d, Fc);
@@ -1327,7 +1351,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
           for (int v = 0; v < NV; ++v) fm[v] = __dmul_rn(W, fm[v]);
         }
 #pragma unroll
-        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * kBlock + tid]);
+        for (int v = 0; v < NV; ++v) acc[v] = acc[v] + (fm[v] - sf[(d * NV + v) * TB + tid]);
       }
       double qo[NV];
       if (MODE != 0) {
@@ -1351,7 +1375,7 @@ __global__ void __launch_bounds__(kBlock, H3C_AUSM_MINB) k_stage_ausm(const doub
     }
     if (FUSE) {
     flag_bad_state(bad, sc, inst);
-    block_min_atomic(ord, per_instance(dtmin, inst));
+    block_min_atomic_tb<TB>(ord, per_instance(dtmin, inst));
   }
     __syncthreads();  // shared memory is rewritten by the next tile
   }

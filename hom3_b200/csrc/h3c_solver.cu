@@ -109,7 +109,8 @@ struct h3c_solver_s {
   bool tile = true;  // Euler stages use the shared-memory tile kernel
   bool cns_adj_dual = false;  // CNS adjoint faces by dual numbers instead of the hand-written reverse
   int halo_cap = 0;           // cap on the Euler halo entries held in shared memory (0: none)
-  int euler_kernel = 1;       // Euler/AUSM stage: 0 halo-staged tile, 1 per-lane tile, 2 per cell, 3 warp-tiled
+  int euler_kernel = 1;       // Euler/AUSM stage: 0 halo-staged tile, 1 per-lane tile, 2 per cell, 3 warp-tiled,
+                              // 4 per-lane tile of 512 cells (3D, one grid)
   int warp_bps = 0;           // resident blocks per SM of the warp-tiled kernel (0: unavailable)
   // halo-staged Euler/AUSM stage (h3c_stage_halo.cu): tables, launch size
   bool halo = true;     // option: use it when its tables exist
@@ -401,7 +402,7 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
                &s->d_sc->dtmin_ord, s->stream);
     return;
   }
-  if (PHYS == EULER && FLUX == AUSM && s->tile && s->euler_kernel >= 2) {  // the per-cell AUSM kernel
+  if (PHYS == EULER && FLUX == AUSM && s->tile && (s->euler_kernel == 2 || s->euler_kernel == 3)) {  // per cell
     k_stage_ausm_cell<ND, R, MODE, HANG, FUSE><<<blocks(s->n_int), kBlock, 0, s->stream>>>(
         qin, out, geometry(s), s->pc, s->d_sc, &s->d_sc->dtmin_ord);
     return;
@@ -413,6 +414,25 @@ void stage_t(h3c_solver s, const double* qin, double* out) {
     halo_stage(ND, std::is_same<R, float>::value, MODE, HANG, FUSE, qin, out, geometry(s), hg, s->pc, s->d_sc,
                &s->d_sc->dtmin_ord, &s->d_sc->status, grid, s->halo_smem, s->stream);
     return;
+  }
+  if constexpr (ND == 3) {
+    if (PHYS == EULER && FLUX == AUSM && s->tile && s->euler_kernel == 4 && s->n_inst == 1) {
+      // 512-cell tiles (8x8x8 Morton bricks), two blocks of 512 threads per SM
+      constexpr int TB = 512;
+      constexpr size_t smem = ausm_smem_bytes<R, ND, TB>();
+      static bool attr = false;  // one opt-in per instantiation (dynamic smem above 48 KB)
+      if (!attr) {
+        cudaFuncSetAttribute(k_stage_ausm<ND, R, MODE, HANG, FUSE, TB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        attr = true;
+      }
+      Geometry g = geometry(s);
+      g.ntiles = (s->n_int + TB - 1) / TB;
+      const long long grid = s->persist_blocks > 0 ? std::min<long long>(s->persist_blocks, g.ntiles) : g.ntiles;
+      k_stage_ausm<ND, R, MODE, HANG, FUSE, TB><<<(unsigned)std::max<long long>(1, grid), TB, smem, s->stream>>>(
+          qin, out, g, s->pc, s->d_sc, &s->d_sc->dtmin_ord);
+      return;
+    }
   }
   if (PHYS == EULER && FLUX == AUSM && s->tile) {
     constexpr size_t smem = ausm_smem_bytes<R, ND>();
@@ -1823,7 +1843,8 @@ int h3c_set_option(h3c_solver s, int option, int value) {
     case H3C_OPT_GRAPHS: s->graphs = value != 0; break;
     case H3C_OPT_HALO_KERNEL: s->halo = value != 0; break;
     case H3C_OPT_EULER_KERNEL:
-      if (value < 0 || value > 3) return s->fail(H3C_E_INVALID, "h3c_set_option: Euler kernel must be 0, 1, 2 or 3");
+      if (value < 0 || value > 4)
+        return s->fail(H3C_E_INVALID, "h3c_set_option: Euler kernel must be 0, 1, 2, 3 or 4");
       s->euler_kernel = value;
       break;
     case H3C_OPT_CNS_ADJOINT_DUAL: s->cns_adj_dual = value != 0; break;
@@ -1865,10 +1886,11 @@ int h3c_kernel_info(h3c_solver s, int64_t* info, int n) {
                                                                          s->ntiles))
                             : (s->persist_blocks > 0 ? std::min<long long>(s->persist_blocks, s->ntiles) : s->ntiles);
   const bool ausm_tile = euler && s->desc.flux == H3C_FLUX_AUSM && s->tile;
+  const bool tile512 = ausm_tile && s->euler_kernel == 4 && s->nd == 3 && s->n_inst == 1;
   const bool warpk = ausm_tile && s->euler_kernel == 3 && s->warp_bps > 0;
-  const bool cellk = ausm_tile && s->euler_kernel >= 2 && !warpk;
+  const bool cellk = ausm_tile && (s->euler_kernel == 2 || s->euler_kernel == 3) && !warpk;
   const bool halo_used = halo && (cns || s->euler_kernel == 0);
-  const int64_t v[8] = {warpk ? 4 : cellk ? 3 : halo_used ? 2 : (euler && s->tile ? 1 : 0),
+  const int64_t v[8] = {tile512 ? 5 : warpk ? 4 : cellk ? 3 : halo_used ? 2 : (euler && s->tile ? 1 : 0),
                         (s->halo_ok || s->cns_ok) ? s->hmax : 0,
                         s->halo_maxh, (int64_t)std::llround(1000.0 * s->halo_mean), bps, grid,
                         (int64_t)(cns ? s->cns_smem : s->halo_smem), s->ntiles};
@@ -1906,6 +1928,7 @@ constexpr TuneCand kTune[] = {
     {true, 2, 0},                                                           // per-cell AUSM kernel
     {true, 0, 1}, {true, 0, 2}, {true, 0, 3},                               // halo-staged tile kernel
     {true, 3, 0},                                                           // warp-tiled kernel
+    {true, 4, 0},                                                           // per-lane tile of 512 cells
 };
 constexpr int kTuneN = sizeof(kTune) / sizeof(kTune[0]);
 
@@ -1916,7 +1939,9 @@ static bool tune_applies(h3c_solver s, int i) {
   if (!c.tile) return true;
   const bool euler_ausm = s->desc.physics == H3C_EULER && s->desc.flux == H3C_FLUX_AUSM &&
                           s->desc.reconstruction != H3C_RECON_MUSCL;
-  if (euler_ausm) return (c.euler_kernel != 0 || (s->halo && s->halo_ok)) && (c.euler_kernel != 3 || s->warp_bps > 0);
+  if (euler_ausm)
+    return (c.euler_kernel != 0 || (s->halo && s->halo_ok)) && (c.euler_kernel != 3 || s->warp_bps > 0) &&
+           (c.euler_kernel != 4 || (s->nd == 3 && s->n_inst == 1));
   if (s->desc.physics == H3C_CNS && s->halo && s->cns_ok) return c.euler_kernel == 1;
   return i == 0;  // one tile configuration where the options change nothing else
 }

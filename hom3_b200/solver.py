@@ -361,7 +361,7 @@ class Solver:
         """The Euler stage launch in use (h3c_kernel_info)."""
         v = np.zeros(8, np.int64)
         self._check(lib().h3c_kernel_info(self.h, _lp(v), 8))
-        return {"halo": int(v[0] == 2), "kernel": ("per_cell", "tile", "halo", "cell", "warp")[int(v[0])], "halo_slots": int(v[1]),
+        return {"halo": int(v[0] == 2), "kernel": ("per_cell", "tile", "halo", "cell", "warp", "tile512")[int(v[0])], "halo_slots": int(v[1]),
                 "max_halo": int(v[2]), "mean_halo": v[3] / 1000.0, "blocks_per_sm": int(v[4]), "grid": int(v[5]),
                 "smem_bytes": int(v[6]), "tiles": int(v[7])}
 

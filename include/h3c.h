@@ -327,12 +327,14 @@ int h3c_launches(h3c_solver s, int64_t* n);
 /* H3C_OPT_EULER_KERNEL  the Euler/AUSM stage kernel (with the tile kernels on): 0 the halo-staged
  *                       tile kernel when its tables exist, 1 (the default) the per-lane tile kernel,
  *                       2 one thread per cell, faces from both sides, 3 one warp per 32 Morton cells
- *                       (each face state once per warp, each face between two of its cells once) */
+ *                       (each face state once per warp, each face between two of its cells once),
+ *                       4 the per-lane tile kernel on 512-cell tiles (8x8x8 Morton bricks, 512-thread
+ *                       blocks; 3D single grids, otherwise kernel 1) */
 #define H3C_OPT_EULER_KERNEL 7
 int h3c_set_option(h3c_solver s, int option, int value);
 /* The Euler stage launch in use (no hom3 counterpart): info[0] kernel (0 per
  * cell, 1 per-lane tile, 2 halo-staged tile, 3 the per-cell AUSM kernel, 4 the warp-tiled AUSM
- * kernel), [1] halo slots per tile, [2]
+ * kernel, 5 the per-lane tile kernel on 512-cell tiles), [1] halo slots per tile, [2]
  * largest tile halo, [3] mean tile halo x 1000, [4] resident blocks per SM
  * of the halo-staged kernel, [5] blocks launched, [6] its dynamic shared
  * memory in bytes, [7] 256-cell tiles; the first n entries are written. */

@@ -74,7 +74,7 @@ def test_autotune_keeps_the_state():
     assert np.array_equal(a.instances()[2], b.instances()[2])
 
 
-KERNEL_OF_CHOICE = ["tile"] * 5 + ["per_cell", "cell", "halo", "halo", "halo", "warp"]
+KERNEL_OF_CHOICE = ["tile"] * 5 + ["per_cell", "cell", "halo", "halo", "halo", "warp", "tile512"]
 
 
 def test_autotune_single_tree_sets_the_chosen_kernel():

@@ -74,7 +74,7 @@ def test_split_refined_tree_equals_one_grid(ti, parts):
     _compare(o, 0, parts, (1, 2, 4))
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4])
 def test_split_with_every_euler_stage_kernel(kernel):
     _, (o,) = cases.refined_case(ti=h3o.RK2, level=3, fine=5)
     _compare(o, 0, 2, (1, 3), kernel)

@@ -79,7 +79,7 @@ def test_halo_kernel_uniform_and_periodic(nd, level):
     _same(a, b, o.first_ghost, "4 steps")
 
 
-@pytest.mark.parametrize("kernel", [0, 3])
+@pytest.mark.parametrize("kernel", [0, 3, 4])
 def test_partial_last_tile_and_warp_against_oracle(kernel):
     """A tree whose interior cell count is not a multiple of the tile size
     (256) nor of the warp size (32): the last warp's missing cells include
@@ -92,7 +92,7 @@ def test_partial_last_tile_and_warp_against_oracle(kernel):
     assert o.first_ghost % 32 != 0
     g = cases.gpu_solver_from_oracle(o)
     g.set_option(F.OPT_EULER_KERNEL, kernel)
-    assert g.kernel_info()["kernel"] == ("halo", "tile", "cell", "warp")[kernel]
+    assert g.kernel_info()["kernel"] == ("halo", "tile", "cell", "warp", "tile512")[kernel]
     o.solve(1)
     g.solve(1)
     fg = o.first_ghost
@@ -103,7 +103,7 @@ def test_partial_last_tile_and_warp_against_oracle(kernel):
     assert rel_err(g.state(0)[:, :fg], o.state(0)[:, :fg]) <= 1e-10
 
 
-@pytest.mark.parametrize("kernel", [0, 2, 3])
+@pytest.mark.parametrize("kernel", [0, 2, 3, 4])
 @pytest.mark.parametrize("precision", [F.FP64, F.MIXED])
 def test_stage_kernels_batches(precision, kernel):
     """Batches of grids (a warp's cells never span two grids) in the
@@ -145,12 +145,14 @@ def test_halo_entries_beyond_shared_memory_read_from_global(slots):
     _same(a, b, o.first_ghost, f"{slots} slots")
 
 
-@pytest.mark.parametrize("kernel", [2, 3])
+@pytest.mark.parametrize("kernel", [2, 3, 4])
 @pytest.mark.parametrize("case", ["refined_rk2", "refined_fe_mixed", "explosion_rk3", "periodic_vortex"])
 def test_per_cell_and_warp_ausm_kernels(case, kernel):
     """The per-cell AUSM kernel (2: each face from both sides, no shared
-    memory) and the warp-tiled one (3: face states once per warp, each face
-    inside a warp once) against the per-lane tile kernel and the oracle."""
+    memory), the warp-tiled one (3: face states once per warp, each face
+    inside a warp once) and the per-lane kernel on 512-cell tiles (4; 3D
+    grids, the 256-cell tiles in 2D) against the per-lane tile kernel and the
+    oracle."""
     precision = 1 if case.endswith("mixed") else 0
     if case.startswith("refined"):
         _, (o,) = cases.refined_case(ti=h3o.RK2 if "rk2" in case else h3o.EULER_FORWARD, level=3, fine=5)
@@ -160,7 +162,8 @@ def test_per_cell_and_warp_ausm_kernels(case, kernel):
         _, (o,) = cases.periodic_vortex_case(level=6, ti=h3o.RK2)
     a, b = _pair(o, precision)
     a.set_option(F.OPT_EULER_KERNEL, kernel)
-    assert a.kernel_info()["kernel"] == {2: "cell", 3: "warp"}[kernel]
+    want = {2: "cell", 3: "warp", 4: "tile512" if case != "periodic_vortex" else "tile"}[kernel]
+    assert a.kernel_info()["kernel"] == want
     fg = o.first_ghost
     o.solve(1)
     a.solve(1)

@@ -87,18 +87,18 @@ def test_headline_tree_fp64_and_mixed_against_oracle(headline):
     assert g.status() == 0 and m.status() == 0
 
 
-@pytest.mark.parametrize("kernel", [0, 2, 3])
+@pytest.mark.parametrize("kernel", [0, 2, 3, 4])
 def test_headline_tree_other_stage_kernels_agree(headline, kernel):
-    """The halo-staged tile kernel (0), the per-cell kernel (2) and the
-    warp-tiled kernel (3) on the same tree agree with the default per-lane
-    tile kernel to rounding."""
+    """The halo-staged tile kernel (0), the per-cell kernel (2), the
+    warp-tiled kernel (3) and the per-lane kernel on 512-cell tiles (4) on the
+    same tree agree with the default per-lane tile kernel to rounding."""
     from hom3_b200 import _ffi as F
     _, o = headline
     fg = o.first_ghost
     a = cases.gpu_solver_from_oracle(o, 0)
     b = cases.gpu_solver_from_oracle(o, 0)
     b.set_option(F.OPT_EULER_KERNEL, kernel)
-    assert b.kernel_info()["kernel"] == ("halo", "tile", "cell", "warp")[kernel]
+    assert b.kernel_info()["kernel"] == ("halo", "tile", "cell", "warp", "tile512")[kernel]
     a.solve(2)
     b.solve(2)
     assert rel_err(a.state(0)[:, :fg], b.state(0)[:, :fg]) <= 1e-13
