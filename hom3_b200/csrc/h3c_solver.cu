@@ -102,6 +102,7 @@ struct h3c_solver_s {
   long long* d_dev2caller = nullptr;
   std::vector<long long> dev2caller, caller2dev;
   Scalars* d_sc = nullptr;
+  Scalars* h_sc = nullptr;  // pinned host copy of instance 0's scalars (the per-step dt read-back)
   bool unfused_dt = false;  // a condition rewrites interior cells (vortex)
   bool ghost_unapplied = false;  // some ghost gets no condition (hom3's find_if segments)
   bool needs_partner = false, needs_periodic = false;  // coupling / periodic conditions present
@@ -636,6 +637,11 @@ int h3c_create(const h3c_desc* d, h3c_solver* out) {
     g_last_error = std::string("h3c_create: cudaMalloc: ") + cudaGetErrorString(e);
     return H3C_E_NOMEM;
   }
+  // a direct DMA target for the step scalars (a pageable one is staged by the driver)
+  if (cudaMallocHost(&s->h_sc, sizeof(Scalars)) != cudaSuccess) {
+    cudaGetLastError();
+    s->h_sc = nullptr;
+  }
   k_init_time<<<1, 1, 0, s->stream>>>(s->d_sc, d->time_end, 1);
   *out = s.release();
   return H3C_OK;
@@ -646,6 +652,7 @@ int h3c_destroy(h3c_solver s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   free_grid(s);
   dfree(s->d_sc);
+  if (s->h_sc) cudaFreeHost(s->h_sc);
   for (auto& r : s->prof_rec) { cudaEventDestroy(r.second.first); cudaEventDestroy(r.second.second); }
   for (auto e : s->ev_pool) cudaEventDestroy(e);
   if (s->stream && s->own_stream) cudaStreamDestroy(s->stream);
@@ -1581,8 +1588,10 @@ int h3c_dtmin_device(h3c_solver s, int64_t** ptr) {
 }
 
 static int read_scalars(h3c_solver s, Scalars* out) {
-  H3C_CUDA(s, cudaMemcpyAsync(out, s->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
+  Scalars* dst = s->h_sc ? s->h_sc : out;
+  H3C_CUDA(s, cudaMemcpyAsync(dst, s->d_sc, sizeof(Scalars), cudaMemcpyDeviceToHost, s->stream));
   H3C_CUDA(s, cudaStreamSynchronize(s->stream));
+  if (dst != out) *out = *dst;
   return H3C_OK;
 }
 
