@@ -224,6 +224,16 @@ __device__ __forceinline__ double nr_rsqrt(double x) {
 __device__ __forceinline__ float nr_rcp(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ float nr_rsqrt(float x) { return rsqrtf(x); }
 
+// Moves cell c's row of a [nv][ld] state towards L2 (a hint: no register is
+// taken and nothing waits on it).  The in-place stages read their start
+// state only at the update, after the face loops; issued at the start, the
+// prefetch overlaps that read's DRAM latency with the face work.
+template <int NV>
+__device__ __forceinline__ void prefetch_row_l2(const double* q, long long ld, long long c) {
+#pragma unroll
+  for (int v = 0; v < NV; ++v) asm volatile("prefetch.global.L2 [%0];" ::"l"(q + v * ld + c));
+}
+
 // ---------------------------------------------------------------------------
 // primitive variables: euler/physics.hpp:83-125.  u = rho u / rho,
 // p = (gamma - 1)(rho E - rho |u|^2 / 2), a = sqrt(gamma p / rho), and the
@@ -1227,6 +1237,7 @@ __global__ void __launch_bounds__(TB, H3C_AUSM_MINB * kBlock / TB) k_stage_ausm(
     const int inst = tile_instance(g, tile);
     const long long tile_end = min(c0 + (long long)TB, instance_end(g, inst));
     const bool live = c < tile_end;
+    if (MODE != 0 && live) prefetch_row_l2<NV>(out, ld, c);  // the in-place start state, read at the update
 
     // ---- own loads first: state, neighbours, level ----
     double qc[NV];
@@ -1406,6 +1417,7 @@ __global__ void __launch_bounds__(kBlock, H3C_CELL_MINB) k_stage_ausm_cell(const
   const bool live = c < instance_end(g, inst);
   const long long ld = g.ld;
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
+  if (MODE != 0 && live) prefetch_row_l2<NV>(out, ld, c);  // the in-place start state, read at the update
   // The cell's own face state (theta, p, Mach number along each direction),
   // kept in the thread's column of shared memory rather than in registers
   // across the direction loop: at three blocks per SM the loop spills otherwise.

@@ -229,6 +229,7 @@ __global__ void __launch_bounds__(kHaloTile, H3C_CNS_MINB)
     const int inst = tile_instance(g, tile);
     const long long te = min(c0 + (long long)TB, instance_end(g, inst));
     const bool live = c < te;
+    if (MODE != 0 && live) prefetch_row_l2<NV>(out, ld, c);  // the in-place start state, read at the update
 
     const bool ok = mbar_wait_bounded(bar, (unsigned)(it & 1));
     cp_async_wait_all();

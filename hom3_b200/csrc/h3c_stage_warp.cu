@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(kBlock, H3C_WARP_MINB)
   const long long iend = instance_end(g, inst);
   const bool live = c < iend;
   const long long wend = w0 + 32 < iend ? w0 + 32 : iend;  // the warp's cells: [w0, wend)
+  if (MODE != 0 && live) prefetch_row_l2<NV>(out, g.ld, c);  // the in-place start state, read at the update
   const unsigned below = (1u << lane) - 1u;
   const long long ld = g.ld;
   const R gamma = (R)pc.gamma, gm1 = (R)pc.gm1;
