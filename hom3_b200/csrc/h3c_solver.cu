@@ -793,8 +793,6 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   if (!s || !grids || ninst < 1) return H3C_E_INVALID;
   Range r("h3c_set_grid");
   const int nd = s->nd, np = 2 * nd, nsubc = 1 << (nd - 1);
-  if (ninst > 1 && s->desc.physics == H3C_CNS)
-    return s->fail(H3C_E_INVALID, "h3c_set_grids: batches of CNS grids are not supported");
   std::vector<InstanceTables> T(ninst);
   for (int k = 0; k < ninst; ++k)
     if (int rc = prepare_instance(s, k, &grids[k], T[k])) return rc;

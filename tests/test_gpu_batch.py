@@ -117,3 +117,47 @@ def test_autotune_cns_times_the_tile_kernel_grids_and_the_per_cell_kernel():
     fg = o.first_ghost
     qa, qb = a.state(0)[:, :fg], b.state(0)[:, :fg]
     assert np.max(np.abs(qa - qb)) <= 1e-12 * np.max(np.abs(qb))
+
+
+@pytest.mark.parametrize("ti", [F.EULER_FORWARD, F.RUNGE_KUTTA_2])
+def test_cns_batch_matches_single_instances(ti):
+    """Batches of compressible Navier-Stokes grids (walls, slip walls,
+    isothermal walls with inflow/outflow; different sizes, so each keeps its
+    own dt) step in the per-cell CNS kernel exactly as each grid alone in the
+    same kernel."""
+    import cases
+    from oracle import h3o
+    from hom3_b200.solver import Condition
+    osolvers = [cases.cns_case(name, level=lvl, ti=ti)[1][0]
+                for name, lvl in (("walls", 4), ("slip", 5), ("isothermal", 4))]
+    info = osolvers[0].info()
+    props = {k: info[k] for k in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty", "ReInfty",
+                                  "Pr0", "Sutherland0", "time_end")}
+    tables, conds, states = [], [], []
+    for o in osolvers:
+        assert all(o.info()[k] == v for k, v in props.items())
+        t = dict(o.tables())
+        t["ncells"] = t["length"].shape[0]
+        tables.append(t)
+        conds.append([Condition(k, v) for k, v in o.info()["bcs"]])
+        states.append(o.state(0))
+    b = hb.Batch(2, F.CNS, F.FLUX_AUSM, ti, F.FP64, **props)
+    b.set_grids(tables, conds)
+    b.set_state(np.concatenate(states, axis=1), 0)
+    b.reset_time()
+    b.solve(5)
+    qb = b.state(0)
+    dtb, tb, sb = b.instances()
+    assert np.all(sb == 5)
+    assert len(set(np.round(dtb, 15))) > 1
+    for k, (t, q0) in enumerate(zip(tables, states)):
+        s = hb.Solver(2, F.CNS, F.FLUX_AUSM, ti, F.FP64, **props)
+        s.set_option(F.OPT_HALO_KERNEL, 0)  # the per-cell CNS kernel, as in the batch
+        s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"], conds[k],
+                   t["subface_cells"])
+        s.set_state(q0, 0)
+        s.reset_time()
+        s.solve(5)
+        fg = t["first_ghost"]
+        assert np.array_equal(b.instance_state(qb, k)[:, :fg], s.state(0)[:, :fg]), k
+        assert dtb[k] == s.dt() and tb[k] == s.time()
