@@ -128,8 +128,11 @@ __host__ __device__ inline double ord_to_dbl(long long o) {
 }
 constexpr long long kOrdMax = 0x7fefffffffffffffLL;  // bits of DBL_MAX
 
-__device__ __forceinline__ void block_min_atomic(long long v, long long* dst) {
-  __shared__ long long red[kBlock / 32];
+// Minimum of v over a block of at most TB threads (TB / 32 <= 32 warps),
+// folded into *dst by one atomicMin (NaN never wins).  Every thread calls it.
+template <int TB>
+__device__ __forceinline__ void block_min_atomic_tb(long long v, long long* dst) {
+  __shared__ long long red[TB / 32];
   for (int o = 16; o > 0; o >>= 1) {
     long long w = __shfl_down_sync(0xffffffffu, v, o);
     v = w < v ? w : v;
@@ -146,27 +149,7 @@ __device__ __forceinline__ void block_min_atomic(long long v, long long* dst) {
     if (lane == 0 && v < kOrdMax) atomicMin(dst, v);
   }
 }
-
-// block_min_atomic for a block of TB threads (TB / 32 <= 32 warps).
-template <int TB>
-__device__ __forceinline__ void block_min_atomic_tb(long long v, long long* dst) {
-  __shared__ long long red[TB / 32];
-  for (int o = 16; o > 0; o >>= 1) {
-    long long w = __shfl_down_sync(0xffffffffu, v, o);
-    v = w < v ? w : v;
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < TB / 32 ? red[lane] : kOrdMax;
-    for (int o = 16; o > 0; o >>= 1) {
-      long long w = __shfl_down_sync(0xffffffffu, v, o);
-      v = w < v ? w : v;
-    }
-    if (lane == 0 && v < kOrdMax) atomicMin(dst, v);
-  }
-}
+__device__ __forceinline__ void block_min_atomic(long long v, long long* dst) { block_min_atomic_tb<kBlock>(v, dst); }
 
 // The same minimum without a block barrier, for kernels that have none: each
 // warp folds its minimum into a shared slot; the last warp of the block to
