@@ -1070,10 +1070,15 @@ static int set_grids(h3c_solver s, int ninst, const h3c_grid* grids) {
   H3C_CUDA(s, cudaMemset(s->d_q[1], 0, sizeof(double) * s->nv * L));
   if (s->d_q[2]) H3C_CUDA(s, cudaMemset(s->d_q[2], 0, sizeof(double) * s->nv * L));
   if (s->d_slopes) H3C_CUDA(s, cudaMemset(s->d_slopes, 0, sizeof(double) * nd * s->nv * L));
+  // The uploads and clears above ran on the legacy default stream, which the
+  // solver's non-blocking stream does not wait for (a pageable cudaMemcpy may
+  // return before its DMA lands, a cudaMemset before it runs): finish them
+  // before the stream's kernels read the tables.
+  H3C_CUDA(s, cudaStreamSynchronize(cudaStreamLegacy));
   {
     unsigned long long* d_bad = nullptr;
     H3C_CUDA(s, cudaMalloc(&d_bad, sizeof(unsigned long long)));
-    cudaMemset(d_bad, 0, sizeof(unsigned long long));
+    H3C_CUDA(s, cudaMemsetAsync(d_bad, 0, sizeof(unsigned long long), s->stream));
     const long long nh = (s->halo_ok || s->cns_ok) && s->d_hids ? HH.ids.size() + CH.base.ids.size() : 0;
     const long long span = std::max({n_int, nsub, ng, nh, 1LL});
     const int hid_mask = s->halo_ok ? kHaloCellMask : -1;  // Euler entries carry a direction
@@ -1675,6 +1680,7 @@ int h3c_status(h3c_solver s, int* flags) {
       H3C_CUDA(s, cudaMemcpy(&s->d_sc[i].status, &zero, sizeof(int), cudaMemcpyHostToDevice));
     }
   }
+  if (f) H3C_CUDA(s, cudaStreamSynchronize(cudaStreamLegacy));  // cleared before the stream's next kernels
   *flags = f;
   return H3C_OK;
 }
@@ -1704,6 +1710,7 @@ int h3c_set_partner(h3c_solver s, h3c_solver partner, const int64_t* partner_cel
   }
   H3C_CUDA(s, cudaMemcpy(s->d_bcs, s->h_bcs.data(), sizeof(BcParam) * s->h_bcs.size(), cudaMemcpyHostToDevice));
   H3C_CUDA(s, cudaMemcpy(s->d_gpartner, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaStreamSynchronize(cudaStreamLegacy));  // the copies land before the stream's kernels read them
   s->partner = partner;
   s->partner_set = true;
   // coupled solvers run on one stream, so each sees the other's finished steps
@@ -1730,6 +1737,7 @@ int h3c_set_periodic(h3c_solver s, const int64_t* partner_cells) {
       return s->fail(H3C_E_INVALID, "h3c_set_periodic: periodic ghost %lld has no interior partner", i);
   }
   H3C_CUDA(s, cudaMemcpy(s->d_gpartner, h.data(), sizeof(int) * h.size(), cudaMemcpyHostToDevice));
+  H3C_CUDA(s, cudaStreamSynchronize(cudaStreamLegacy));  // the copy lands before the stream's kernels read it
   s->periodic_set = true;
   return H3C_OK;
 }
