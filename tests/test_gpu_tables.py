@@ -106,3 +106,25 @@ def test_condition_index_past_the_list_is_rejected():
     with pytest.raises(hb.H3cError, match="bc index"):
         s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], t["first_ghost"], conds[:-1],
                    t["subface_cells"])
+
+
+def test_set_grid_on_many_fresh_handles():
+    """Table uploads are ordered before the solver stream's kernels read them:
+    many handles created and given tables back to back (as a finite-difference
+    loop does) all accept the valid tables and step to the same state."""
+    o, _, t, conds = _case()
+    info = o.info()
+    props = {k: info[k] for k in ("cfl", "cfl_viscous", "gamma", "Rspecific", "T0", "rho0", "Minfty", "ReInfty",
+                                  "Pr0", "Sutherland0", "time_end")}
+    q0, fg, ref = o.state(0), t["first_ghost"], None
+    for _ in range(40):
+        s = hb.Solver(info["nd"], info["physics"], info["flux"], info["ti"], 0, **props)
+        s.set_grid(t["neighbors"], t["x_center"], t["length"], t["bc_idx"], fg, conds, t["subface_cells"])
+        s.set_state(q0, 0)
+        s.reset_time()
+        s.solve(1)
+        q = s.state(0)[:, :fg]
+        if ref is None:
+            ref = q
+        assert np.array_equal(q, ref)
+        del s
